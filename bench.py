@@ -1,0 +1,345 @@
+#!/usr/bin/env python3
+"""Benchmark: pseudo-transient Stokes T_eff on one B200 (or N replicas).
+
+Workload (one "step" = one PT iteration, advance_iteration!): the 3D
+gravity-driven ice slab at 511^3 cells -- extent 1 x 1 x 0.25, tilted 10 degrees
+(rho*g = (-sin a, 0, cos a)), Glen's law n=3, A=1 regularised at
+strain rate 1e-6 (ViscoplasticRegularisation(PowerLawRheology(1, 3), 5000)),
+free-slip bed, stress-free top, periodic x/y, zero initial fields; FP64 is the
+headline, FP32 is measured in the same run.  Inputs are synthetic (the
+reference publishes no dataset for this path).
+
+T_eff = A_eff / t_iter with A_eff the minimum field bytes of one iteration:
+P, tau(6), V(3) read and written, eta read, eta_next written, each at its exact
+staggered interior size.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun (N > 1) every rank runs an independent replica of the workload
+("replicas only": the single-GPU path has no data-path collective); the time is
+the max over ranks and ``value`` is the whole-job throughput.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+
+# DRAM bytes per cell of one fused-sweep launch, from the ncu capture summarised
+# in profiles/fused3d_slab_ncu.md (dram__bytes_read.sum + dram__bytes_write.sum
+# of a 255^3 launch divided by its cell count); None until captured.
+TRAFFIC_BYTES_PER_CELL = {"f64": None, "f32": None}
+
+
+def load_fastice():
+    name = "fastice_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    pkg = os.path.join(ROOT, "fastice.jl_b200")
+    spec = importlib.util.spec_from_file_location(name, os.path.join(pkg, "__init__.py"),
+                                                  submodule_search_locations=[pkg])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def a_eff_elements(n):
+    """Minimum field elements moved by one iteration (22 array passes)."""
+    nx, ny, nz = n
+    C = nx * ny * nz
+    txy, txz, tyz = (nx + 1) * (ny + 1) * nz, (nx + 1) * ny * (nz + 1), nx * (ny + 1) * (nz + 1)
+    vx, vy, vz = (nx + 1) * ny * nz, nx * (ny + 1) * nz, nx * ny * (nz + 1)
+    return 2 * (4 * C + txy + txz + tyz + vx + vy + vz) + 2 * C
+
+
+def slab_problem(fi, n, alpha_deg=10.0):
+    grid = fi.UniformGrid(origin=(0.0, 0.0, 0.0), extent=(1.0, 1.0, 0.25), dims=n)
+    a = math.radians(alpha_deg)
+    gravity = {"x": -math.sin(a), "y": 0.0, "z": math.cos(a)}
+    bcs = {"x": (fi.PBC(), fi.PBC()), "y": (fi.PBC(), fi.PBC()),
+           "z": (fi.SBC(0.0, 0.0, 0.0), fi.TBC(0.0, 0.0, 0.0))}
+    rheology = fi.glen_regularised(A=1.0, n=3, strain_rate_0=1e-6)
+    sp = fi.pt_params(grid, r=0.7, re_mech=8 * math.pi, vdtau_factor=1.1)
+    return grid, bcs, gravity, rheology, sp
+
+
+def make_model(fi, n, dtype, device, path="auto"):
+    grid, bcs, gravity, rheology, sp = slab_problem(fi, n)
+    m = fi.IsothermalFullStokesModel(arch=fi.Arch("cuda", device), grid=grid, boundary_conditions=bcs,
+                                     gravity=gravity, rheology=rheology, solver_params=sp, dtype=dtype, path=path)
+    # zero initial P, tau, V (allocation zero-fills); eta from the regularised law at tau = 0
+    m.set_field("eta", rheology.eta_reg)
+    m.set_field("eta_next", rheology.eta_reg)
+    m.apply_bcs()
+    return m
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in self.rows:
+            for nm, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def measured_peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def time_advance(fi, model, steps, torch):
+    """CUDA-event time of `steps` PT iterations on the model's stream (ms)."""
+    stream = torch.cuda.ExternalStream(model.stream_ptr)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    model.synchronize()
+    e0.record(stream)
+    model.advance(steps)
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def e2e_run(fi, n, dtype, device, steps, torch):
+    """End to end through the public API with pinned host buffers: upload the
+    state, run the iterations, read the residual norms and download the state."""
+    names = ("P", "txx", "tyy", "tzz", "txy", "txz", "tyz", "Vx", "Vy", "Vz", "eta")
+    m = make_model(fi, n, dtype, device)
+    npd = np.float64 if dtype == "f64" else np.float32
+    host = {}
+    for nm in names:
+        shape = m.field_shape(nm)
+        t = torch.empty(int(np.prod(shape)), dtype=torch.float64 if dtype == "f64" else torch.float32, pin_memory=True)
+        a = t.numpy().reshape(shape)
+        a[...] = 0.0 if nm != "eta" else 5000.0
+        host[nm] = (t, a)
+    h2d = sum(a.nbytes for _, a in host.values())
+    d2h = sum(a.nbytes for nm, (_, a) in host.items() if nm != "eta") + 8 * 12
+    m.advance(2)
+    m.synchronize()
+    t0 = time.perf_counter()
+    for nm, (_, a) in host.items():
+        m.set_field(nm, a)
+    m.set_field("eta_next", host["eta"][1])
+    m.apply_bcs()
+    m.advance(steps)
+    norms = m.residual_norms()
+    for nm, (_, a) in host.items():
+        if nm == "eta":
+            continue
+        a[...] = m.get_field(nm)
+    dt = time.perf_counter() - t0
+    m.close()
+    return dt, h2d, d2h, norms
+
+
+def cpu_baseline(n, seconds=12.0, warm=1):
+    """The CPU oracle (C restatement, OpenMP) on the same workload: whole
+    iterations at the full grid, as many as fit in `seconds` (at least one)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.build()
+    fi = load_fastice()
+    grid, bcs, gravity, rheology, sp = slab_problem(fi, n)
+    dt = sp["Δτ"]
+    taus = ("xx", "yy", "zz", "xy", "xz", "yz")
+    per, z = (O.BC_PERIODIC, (0, 0, 0)), ((O.BC_SLIP, (0, 0, 0)), (O.BC_TRACTION, (0, 0, 0)))
+    spec = O.Spec(nd=3, n=n, extent=grid.extent, origin=grid.origin, bcs=((per, per), (per, per), z),
+                  dt_P=dt["Pr"], dt_tau=tuple(dt["τ"][k] for k in taus), dt_V=tuple(dt["V"][k] for k in "xyz"),
+                  g_val=(gravity["x"], gravity["y"], gravity["z"]), rheo_inner=O.RHEO_POWER, rheo_A=1.0, rheo_n=3,
+                  rheo_has_reg=1, rheo_inv_eta_reg=1.0 / rheology.eta_reg)
+    m = O.OracleStokes(spec)
+    m.a["eta"][...] = rheology.eta_reg
+    m.a["eta_next"][...] = rheology.eta_reg
+    m.apply_initial_bcs()
+    for _ in range(warm):
+        m.advance(1)
+    its, t0 = 0, time.perf_counter()
+    while True:
+        m.advance(1)
+        its += 1
+        el = time.perf_counter() - t0
+        if el >= seconds:
+            break
+    cores = os.cpu_count()
+    try:
+        cores = int(os.environ.get("OMP_NUM_THREADS", cores))
+    except ValueError:
+        pass
+    return its, el, cores
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--n", type=int, default=511)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    n = (args.n, args.n, args.n)
+    ws, rank, local = dist_setup()
+    metric = "PT-Stokes T_eff GB/s (511^3, FP64)"
+    cfg = {"workload": f"3D tilted ice slab {n[0]}x{n[1]}x{n[2]} cells, Glen n=3 regularised, slip bed, free top, "
+                       "periodic x/y, one PT iteration per step",
+           "grid": list(n), "extent": [1.0, 1.0, 0.25], "alpha_deg": 10.0, "a_eff_arrays": 22,
+           "l2": "inputs (11.8 GB FP64) exceed L2 (126 MB): no flush needed", "parallelism": f"replicas x{ws}"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        its, el, cores = cpu_baseline(n, seconds=min(60.0, max(10.0, 0.5 * args.steps)), warm=min(args.warmup, 1))
+        v = a_eff_elements(n) * 8 * its / el / 1e9
+        line = {"metric": metric, "value": v, "unit": "GB/s", "n_gpus": args.gpus, "steps": its,
+                "warmup": min(args.warmup, 1), "ms_per_step": 1e3 * el / its, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+                "impl": "reference",
+                "cpu_baseline": {"value": v, "unit": "GB/s", "cores": cores, "kind": "port",
+                                 "sample": f"{its} whole PT iterations at {n[0]}^3 (C restatement of the reference "
+                                           "CPU path, OpenMP; the Julia reference cannot run: no Julia toolchain)"},
+                "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    pg = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    fi = load_fastice()
+    A = a_eff_elements(n)
+    res = {}
+    clocks = None
+    for dtype in ("f64", "f32"):
+        m = make_model(fi, n, dtype, local)
+        m.advance(args.warmup)
+        m.synchronize()
+        sampler = ClockSampler(local) if dtype == "f64" else None
+        if sampler:
+            sampler.start()
+            time.sleep(0.15)
+        if pg:
+            pg.barrier()
+        ms = time_advance(fi, m, args.steps, torch)
+        if pg:
+            pg.barrier()
+        if sampler:
+            clocks = sampler.stop()
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        if pg:
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms_max = float(t.item())
+        norms = m.residual_norms()
+        res[dtype] = {"ms_total": ms_max, "ms_per_step": ms_max / args.steps, "path": m.path,
+                      "finite": bool(norms[11] == 0.0)}
+        m.close()
+        torch.cuda.empty_cache()
+
+    esz = {"f64": 8, "f32": 4}
+    peak, peak_kind = measured_peak_hbm()
+    f64 = res["f64"]
+    value = ws * A * esz["f64"] * args.steps / (f64["ms_total"] / 1e3) / 1e9
+    achieved = A * esz["f64"] / (f64["ms_per_step"] / 1e3) / 1e9
+    tr = TRAFFIC_BYTES_PER_CELL["f64"]
+    line = {
+        "metric": metric, "value": value, "unit": "GB/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": f64["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic", "config": cfg, "kernel_path": f64["path"],
+        "gpu_launches": args.steps,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": peak_kind, "traffic": (tr * n[0] * n[1] * n[2]) if tr else None,
+                     "algorithmic_bytes": A * esz["f64"]},
+        "fp32": {"value": ws * A * 4 * args.steps / (res["f32"]["ms_total"] / 1e3) / 1e9, "unit": "GB/s",
+                 "ms_per_step": res["f32"]["ms_per_step"],
+                 "frac": (A * 4 / (res["f32"]["ms_per_step"] / 1e3) / 1e9) / peak},
+        "reference_convention_teff": 23 * 8 * n[0] * n[1] * n[2] / (f64["ms_per_step"] / 1e3) / 1e9,
+        "clocks": clocks,
+    }
+    if not args.no_e2e:
+        dt, h2d, d2h, _ = e2e_run(fi, n, "f64", local, args.steps, torch)
+        line["e2e"] = {"value": ws * A * 8 * args.steps / dt / 1e9, "unit": "GB/s",
+                       "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+                       "includes": "pinned host->device upload of the state, K iterations through the C ABI, "
+                                   "residual norms, device->host download of the state"}
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        its, el, cores = cpu_baseline(n, seconds=12.0)
+        line["cpu_baseline"] = {"value": A * 8 * its / el / 1e9, "unit": "GB/s", "cores": cores, "kind": "port",
+                                "sample": f"{its} whole PT iterations at {n[0]}^3 in FP64 (C restatement of the "
+                                          "reference CPU path, OpenMP)"}
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

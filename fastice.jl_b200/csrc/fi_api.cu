@@ -1,0 +1,733 @@
+// fi_api.cu -- C ABI of libfastice_b200: model lifecycle, field I/O, boundary
+// batches, the PT iteration driver and the solve loop.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <vector>
+
+#include "fi_internal.h"
+
+namespace fi {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+fi_status cuda_fail(cudaError_t e, const char *where) {
+    set_error(std::string(where) + ": " + cudaGetErrorString(e));
+    return FI_ERR_CUDA;
+}
+
+}  // namespace fi
+
+using namespace fi;
+
+#define FI_CHECK_CUDA(expr, where)                 \
+    do {                                           \
+        cudaError_t e_ = (expr);                   \
+        if (e_ != cudaSuccess) return cuda_fail(e_, where); \
+    } while (0)
+
+namespace {
+
+constexpr int kState = 10;  // P, txx, tyy, tzz, txy, txz, tyz, Vx, Vy, Vz
+
+// staggered location of each field (0 = Center, 1 = Vertex) per dim
+void field_loc(int field, int loc[3]) {
+    static const int L[FI_FIELD_COUNT][3] = {
+        {0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {1, 1, 0}, {1, 0, 1}, {0, 1, 1},  // P, tau
+        {1, 0, 0}, {0, 1, 0}, {0, 0, 1},                                            // V
+        {0, 0, 0}, {0, 0, 0},                                                       // eta, eta_next
+        {0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1},                                 // residuals
+        {1, 0, 0}, {0, 1, 0}, {0, 0, 1},                                            // gravity
+        {0, 0, 0}, {0, 0, 0},                                                       // eta_lin, A
+        {0, 0, 0}, {1, 1, 1}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 1, 0}, {1, 0, 1}, {0, 1, 1},  // na
+        {0, 0, 0}, {1, 1, 1}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 1, 0}, {1, 0, 1}, {0, 1, 1},  // ns
+    };
+    for (int d = 0; d < 3; d++) loc[d] = L[field][d];
+}
+
+float small_threshold_f32() {
+    // smallest float >= 1e-6: for float w, (w < t) <=> ((double)w < 1e-6)
+    float t = 1e-6f;
+    if ((double)t < 1e-6) t = std::nextafter(t, 1.0f);
+    return t;
+}
+
+}  // namespace
+
+struct fi_model {
+    fi_model_desc d{};
+    Geom g{};
+    KParams kp{};
+    size_t esz = 8;
+    size_t elems = 0;
+    void *base[FI_FIELD_COUNT] = {};
+    void *alt[kState] = {};
+    int parity = 0;           // 1: alt[] holds the current P..Vz
+    bool eta_swapped = false; // true: base[ETA_NEXT] holds the current eta
+    cudaStream_t stream = nullptr;
+    double *d_partials = nullptr;
+    double *d_out = nullptr;
+    double *h_out = nullptr;
+    int nblk = 0;
+    int path = FI_PATH_REFERENCE;
+    int fused_variant = 0;
+    bool ib = false;
+    long long iterations = 0;
+
+    bool is_f64() const { return d.dtype == FI_F64; }
+
+    void *cur(int field) const {
+        if (field < kState) return parity ? alt[field] : base[field];
+        if (field == FI_FIELD_ETA) return eta_swapped ? base[FI_FIELD_ETA_NEXT] : base[FI_FIELD_ETA];
+        if (field == FI_FIELD_ETA_NEXT) return eta_swapped ? base[FI_FIELD_ETA] : base[FI_FIELD_ETA_NEXT];
+        return base[field];
+    }
+    void *nxt(int field) const { return parity ? base[field] : alt[field]; }
+
+    template <typename T>
+    Ptrs<T> ptrs(bool next_state = false) const {
+        Ptrs<T> f{};
+        auto S = [&](int fld) { return (T *)(next_state ? nxt(fld) : cur(fld)); };
+        f.P = S(FI_FIELD_P);
+        f.txx = S(FI_FIELD_TXX);
+        f.tyy = S(FI_FIELD_TYY);
+        f.tzz = S(FI_FIELD_TZZ);
+        f.txy = S(FI_FIELD_TXY);
+        f.txz = S(FI_FIELD_TXZ);
+        f.tyz = S(FI_FIELD_TYZ);
+        f.Vx = S(FI_FIELD_VX);
+        f.Vy = S(FI_FIELD_VY);
+        f.Vz = S(FI_FIELD_VZ);
+        f.eta = (T *)cur(FI_FIELD_ETA);
+        f.eta_next = (T *)cur(FI_FIELD_ETA_NEXT);
+        f.rP = (T *)base[FI_FIELD_RP];
+        f.rVx = (T *)base[FI_FIELD_RVX];
+        f.rVy = (T *)base[FI_FIELD_RVY];
+        f.rVz = (T *)base[FI_FIELD_RVZ];
+        f.gx = (const T *)base[FI_FIELD_GX];
+        f.gy = (const T *)base[FI_FIELD_GY];
+        f.gz = (const T *)base[FI_FIELD_GZ];
+        f.eta_lin = (const T *)base[FI_FIELD_ETA_LIN];
+        f.A = (const T *)base[FI_FIELD_A];
+        for (int c = 0; c < 8; c++) {
+            f.wna[c] = (const T *)base[FI_FIELD_NA_CCC + c];
+            f.wns[c] = (const T *)base[FI_FIELD_NS_CCC + c];
+        }
+        return f;
+    }
+};
+
+namespace {
+
+fi_status validate(const fi_model_desc *d) {
+    if (!d) return set_error("null descriptor"), FI_ERR_ARG;
+    const fi_grid &gr = d->grid;
+    if (gr.nd != 2 && gr.nd != 3) return set_error("grid.nd must be 2 or 3"), FI_ERR_ARG;
+    for (int k = 0; k < gr.nd; k++) {
+        if (gr.n[k] < 3) return set_error("grid.n must be >= 3 in every dimension"), FI_ERR_ARG;
+        if (!(gr.extent[k] > 0.0)) return set_error("grid.extent must be positive"), FI_ERR_ARG;
+    }
+    if (d->dtype != FI_F64 && d->dtype != FI_F32) return set_error("dtype must be FI_F64 or FI_F32"), FI_ERR_ARG;
+    if (d->immersed && gr.nd != 3)
+        return set_error("the immersed-boundary model is 3D only (the reference 2D IB kernels are broken)"),
+               FI_ERR_UNSUPPORTED;
+    for (int k = 0; k < gr.nd; k++) {
+        bool p0 = d->bc[k][0].kind == FI_BC_PERIODIC, p1 = d->bc[k][1].kind == FI_BC_PERIODIC;
+        if (p0 != p1) return set_error("a periodic dimension must be periodic on both sides"), FI_ERR_ARG;
+        for (int s = 0; s < 2; s++)
+            if (d->bc[k][s].kind < 0 || d->bc[k][s].kind > FI_BC_PERIODIC)
+                return set_error("unknown boundary-condition kind"), FI_ERR_ARG;
+    }
+    const fi_rheology &r = d->rheology;
+    if (r.inner != FI_RHEO_LINEAR && r.inner != FI_RHEO_POWER) return set_error("unknown rheology"), FI_ERR_ARG;
+    if (r.has_reg && !(r.eta_reg > 0.0)) return set_error("eta_reg must be positive"), FI_ERR_ARG;
+    if (r.relax < FI_RELAX_NONE || r.relax > FI_RELAX_LOG10) return set_error("unknown relaxation"), FI_ERR_ARG;
+    if (d->path < FI_PATH_AUTO || d->path > FI_PATH_FUSED) return set_error("unknown path"), FI_ERR_ARG;
+    return FI_OK;
+}
+
+bool field_used(const fi_model *m, int f) {
+    const fi_model_desc &d = m->d;
+    bool three = d.grid.nd == 3;
+    switch (f) {
+        case FI_FIELD_TZZ: case FI_FIELD_TXZ: case FI_FIELD_TYZ: case FI_FIELD_VZ: case FI_FIELD_RVZ:
+            return three;
+        case FI_FIELD_GX: return d.gravity.kind[0] == FI_G_FIELD;
+        case FI_FIELD_GY: return d.gravity.kind[1] == FI_G_FIELD;
+        case FI_FIELD_GZ: return three && d.gravity.kind[2] == FI_G_FIELD;
+        case FI_FIELD_ETA_LIN: return d.rheology.inner == FI_RHEO_LINEAR && d.rheology.eta_is_field;
+        case FI_FIELD_A: return d.rheology.inner == FI_RHEO_POWER && d.rheology.A_is_field;
+        default:
+            if (f >= FI_FIELD_NA_CCC) return d.immersed != 0;
+            return true;
+    }
+}
+
+bool is_residual(int f) { return f >= FI_FIELD_RP && f <= FI_FIELD_RVZ; }
+
+fi_status ensure_residual_arrays(fi_model *m) {
+    for (int f = FI_FIELD_RP; f <= FI_FIELD_RVZ; f++) {
+        if (!field_used(m, f) || m->base[f]) continue;
+        void *p = nullptr;
+        cudaError_t e = cudaMalloc(&p, m->elems * m->esz);
+        if (e != cudaSuccess) return set_error("residual field allocation failed"), FI_ERR_OOM;
+        FI_CHECK_CUDA(cudaMemsetAsync(p, 0, m->elems * m->esz, m->stream), "memset");
+        m->base[f] = p;
+    }
+    return FI_OK;
+}
+
+size_t interior_count(const fi_model *m, int field) {
+    int loc[3];
+    field_loc(field, loc);
+    size_t c = 1;
+    for (int k = 0; k < m->d.grid.nd; k++) c *= (size_t)(m->d.grid.n[k] + loc[k]);
+    return c;
+}
+
+cudaMemcpy3DParms copy_params(const fi_model *m, int field, void *dev, void *host, bool to_dev) {
+    int loc[3];
+    field_loc(field, loc);
+    const int nd = m->d.grid.nd;
+    size_t nx = m->d.grid.n[0] + loc[0], ny = m->d.grid.n[1] + loc[1], nz = nd == 3 ? m->d.grid.n[2] + loc[2] : 1;
+    cudaMemcpy3DParms p{};
+    cudaPitchedPtr hp = make_cudaPitchedPtr(host, nx * m->esz, nx, ny);
+    cudaPitchedPtr dp = make_cudaPitchedPtr(dev, (size_t)m->g.pitch * m->esz, (size_t)m->g.pitch, (size_t)m->g.rows);
+    cudaPos dpos = make_cudaPos(m->esz, 1, nd == 3 ? 1 : 0);
+    if (to_dev) {
+        p.srcPtr = hp;
+        p.dstPtr = dp;
+        p.dstPos = dpos;
+        p.kind = cudaMemcpyHostToDevice;
+    } else {
+        p.srcPtr = dp;
+        p.srcPos = dpos;
+        p.dstPtr = hp;
+        p.kind = cudaMemcpyDeviceToHost;
+    }
+    p.extent = make_cudaExtent(nx * m->esz, ny, nz);
+    return p;
+}
+
+// ---- boundary-condition batches (boundary_conditions.jl) -------------------
+void add_op(BcBatch &b, void *f, int field, int side, int op, double v) {
+    BcOpDesc &o = b.ops[b.count++];
+    o.f = f;
+    field_loc(field, o.loc);
+    o.side = side;
+    o.op = op;
+    o.v = v;
+}
+
+// stress batch for dim d (boundary_conditions.jl:26-100, :117)
+BcBatch stress_batch(const fi_model *m, int d) {
+    BcBatch b{};
+    b.dim = d;
+    const int nd = m->d.grid.nd;
+    for (int s = 0; s < 2; s++) {
+        const fi_bc &bc = m->d.bc[d][s];
+        if (bc.kind == FI_BC_PERIODIC) {
+            if (s == 1) continue;
+            int fl3[] = {FI_FIELD_P, FI_FIELD_TXX, FI_FIELD_TYY, FI_FIELD_TZZ, FI_FIELD_TXY, FI_FIELD_TXZ, FI_FIELD_TYZ};
+            int fl2[] = {FI_FIELD_P, FI_FIELD_TXX, FI_FIELD_TYY, FI_FIELD_TXY};
+            if (nd == 3)
+                for (int f : fl3) add_op(b, m->cur(f), f, 0, BC_PERIODIC, 0);
+            else
+                for (int f : fl2) add_op(b, m->cur(f), f, 0, BC_PERIODIC, 0);
+            continue;
+        }
+        if (bc.kind == FI_BC_VELOCITY) continue;
+        const double *c = bc.c;
+        if (nd == 2) {
+            if (bc.kind == FI_BC_TRACTION) {
+                if (d == 0) {
+                    add_op(b, m->cur(FI_FIELD_P), FI_FIELD_P, s, BC_DIRICHLET, c[0]);
+                    add_op(b, m->cur(FI_FIELD_TXX), FI_FIELD_TXX, s, BC_DIRICHLET, c[0]);
+                    add_op(b, m->cur(FI_FIELD_TXY), FI_FIELD_TXY, s, BC_DIRICHLET, c[1]);
+                } else {
+                    add_op(b, m->cur(FI_FIELD_P), FI_FIELD_P, s, BC_DIRICHLET, c[1]);
+                    add_op(b, m->cur(FI_FIELD_TYY), FI_FIELD_TYY, s, BC_DIRICHLET, c[1]);
+                    add_op(b, m->cur(FI_FIELD_TXY), FI_FIELD_TXY, s, BC_DIRICHLET, c[0]);
+                }
+            } else {
+                add_op(b, m->cur(FI_FIELD_TXY), FI_FIELD_TXY, s, BC_DIRICHLET, c[1 - d]);
+            }
+            continue;
+        }
+        static const int tang[3][2] = {{1, 2}, {0, 2}, {0, 1}};
+        static const int shear[3][2] = {{FI_FIELD_TXY, FI_FIELD_TXZ}, {FI_FIELD_TXY, FI_FIELD_TYZ}, {FI_FIELD_TXZ, FI_FIELD_TYZ}};
+        static const int diag[3] = {FI_FIELD_TXX, FI_FIELD_TYY, FI_FIELD_TZZ};
+        if (bc.kind == FI_BC_TRACTION) {
+            add_op(b, m->cur(FI_FIELD_P), FI_FIELD_P, s, BC_DIRICHLET, c[d]);
+            add_op(b, m->cur(diag[d]), diag[d], s, BC_DIRICHLET, c[d]);
+        }
+        add_op(b, m->cur(shear[d][0]), shear[d][0], s, BC_DIRICHLET, c[tang[d][0]]);
+        add_op(b, m->cur(shear[d][1]), shear[d][1], s, BC_DIRICHLET, c[tang[d][1]]);
+    }
+    return b;
+}
+
+// velocity batch + eta_next Neumann for dim d (boundary_conditions.jl:104-115, Isothermal.jl:103-104)
+BcBatch velocity_batch(const fi_model *m, int d) {
+    BcBatch b{};
+    b.dim = d;
+    const int nd = m->d.grid.nd;
+    const int Vf[3] = {FI_FIELD_VX, FI_FIELD_VY, FI_FIELD_VZ};
+    for (int s = 0; s < 2; s++) {
+        const fi_bc &bc = m->d.bc[d][s];
+        if (bc.kind == FI_BC_PERIODIC) {
+            if (s == 1) continue;
+            for (int q = 0; q < nd; q++) add_op(b, m->cur(Vf[q]), Vf[q], 0, BC_PERIODIC, 0);
+            add_op(b, m->cur(FI_FIELD_ETA_NEXT), FI_FIELD_ETA_NEXT, 0, BC_PERIODIC, 0);
+            continue;
+        }
+        if (bc.kind == FI_BC_VELOCITY) {
+            for (int q = 0; q < nd; q++) add_op(b, m->cur(Vf[q]), Vf[q], s, BC_DIRICHLET, bc.c[q]);
+        } else if (bc.kind == FI_BC_SLIP) {
+            add_op(b, m->cur(Vf[d]), Vf[d], s, BC_DIRICHLET, bc.c[d]);
+        }
+        add_op(b, m->cur(FI_FIELD_ETA_NEXT), FI_FIELD_ETA_NEXT, s, BC_NEUMANN, 0);
+    }
+    return b;
+}
+
+BcBatch eta_batch(const fi_model *m, int d, int field) {
+    BcBatch b{};
+    b.dim = d;
+    for (int s = 0; s < 2; s++) {
+        const fi_bc &bc = m->d.bc[d][s];
+        if (bc.kind == FI_BC_PERIODIC) {
+            if (s == 0) add_op(b, m->cur(field), field, 0, BC_PERIODIC, 0);
+        } else {
+            add_op(b, m->cur(field), field, s, BC_NEUMANN, 0);
+        }
+    }
+    return b;
+}
+
+BcBatch residual_batch(const fi_model *m, int d) {
+    BcBatch b{};
+    b.dim = d;
+    const int Rf[3] = {FI_FIELD_RVX, FI_FIELD_RVY, FI_FIELD_RVZ};
+    for (int s = 0; s < 2; s++) {
+        int k = m->d.bc[d][s].kind;
+        if (k == FI_BC_TRACTION || k == FI_BC_PERIODIC) continue;
+        add_op(b, m->base[Rf[d]], Rf[d], s, BC_DIRICHLET, 0.0);
+    }
+    return b;
+}
+
+template <typename T>
+fi_status run_batch(fi_model *m, BcBatch (*mk)(const fi_model *, int)) {
+    for (int d = 0; d < m->d.grid.nd; d++) {
+        BcBatch b = mk(m, d);
+        FI_CHECK_CUDA(launch_bc_batch<T>(m->g, b, m->stream), "boundary batch");
+    }
+    return FI_OK;
+}
+
+template <typename T>
+fi_status run_eta_batch(fi_model *m, int field) {
+    for (int d = 0; d < m->d.grid.nd; d++) {
+        BcBatch b = eta_batch(m, d, field);
+        FI_CHECK_CUDA(launch_bc_batch<T>(m->g, b, m->stream), "eta boundary batch");
+    }
+    return FI_OK;
+}
+
+template <typename T>
+fi_status advance_t(fi_model *m, int niter) {
+    for (int it = 0; it < niter; it++) {
+        if (m->path == FI_PATH_FUSED) {
+            Ptrs<T> in = m->ptrs<T>(false);
+            Ptrs<T> out = m->ptrs<T>(true);
+            out.eta = in.eta;
+            out.eta_next = in.eta_next;
+            FI_CHECK_CUDA(launch_fused3d<T>(m->g, m->kp, in, out, m->ib, m->fused_variant, m->stream), "fused sweep");
+            m->parity ^= 1;
+        } else {
+            Ptrs<T> f = m->ptrs<T>();
+            FI_CHECK_CUDA(launch_update_sigma<T>(m->g, m->kp, f, m->ib, m->stream), "update_sigma");
+            fi_status st = run_batch<T>(m, stress_batch);
+            if (st != FI_OK) return st;
+            FI_CHECK_CUDA(launch_update_V<T>(m->g, m->kp, f, m->ib, m->stream), "update_V");
+            st = run_batch<T>(m, velocity_batch);
+            if (st != FI_OK) return st;
+        }
+        m->eta_swapped = !m->eta_swapped;
+        m->iterations++;
+    }
+    return FI_OK;
+}
+
+template <typename T>
+fi_status norms_t(fi_model *m, double *out) {
+    Ptrs<T> f = m->ptrs<T>();
+    FI_CHECK_CUDA(launch_residual_norms<T>(m->g, m->kp, f, m->ib, m->d_partials, m->nblk, m->d_out, m->stream),
+                  "residual norms");
+    FI_CHECK_CUDA(cudaMemcpyAsync(m->h_out, m->d_out, FI_NORMS_LEN * sizeof(double), cudaMemcpyDeviceToHost, m->stream),
+                  "norms copy");
+    FI_CHECK_CUDA(cudaStreamSynchronize(m->stream), "norms sync");
+    std::memcpy(out, m->h_out, FI_NORMS_LEN * sizeof(double));
+    return FI_OK;
+}
+
+template <typename T>
+fi_status apply_bcs_t(fi_model *m) {
+    fi_status st = run_batch<T>(m, stress_batch);
+    if (st == FI_OK) st = run_batch<T>(m, velocity_batch);
+    if (st == FI_OK) st = run_eta_batch<T>(m, FI_FIELD_ETA);
+    return st;
+}
+
+template <typename T>
+fi_status residuals_t(fi_model *m) {
+    fi_status st = ensure_residual_arrays(m);
+    if (st != FI_OK) return st;
+    Ptrs<T> f = m->ptrs<T>();
+    FI_CHECK_CUDA(launch_compute_residuals<T>(m->g, m->kp, f, m->ib, m->stream), "compute_residuals");
+    return run_batch<T>(m, residual_batch);
+}
+
+bool fused_ok(const fi_model *m) {
+    if (m->d.grid.nd != 3) return false;
+    return m->is_f64() ? fused3d_supported<double>(m->g, m->kp, m->ib) : fused3d_supported<float>(m->g, m->kp, m->ib);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *fi_last_error(void) { return g_last_error.c_str(); }
+int fi_abi_version(void) { return FI_ABI_VERSION; }
+
+fi_status fi_model_create(const fi_model_desc *desc, fi_model **out) {
+    if (!out) return set_error("null output handle"), FI_ERR_ARG;
+    *out = nullptr;
+    fi_status st = validate(desc);
+    if (st != FI_OK) return st;
+    int ndev = 0;
+    cudaError_t ce = cudaGetDeviceCount(&ndev);
+    if (ce != cudaSuccess || ndev == 0) return set_error("no CUDA device available"), FI_ERR_CUDA;
+    if (desc->device < 0 || desc->device >= ndev) return set_error("device ordinal out of range"), FI_ERR_ARG;
+    FI_CHECK_CUDA(cudaSetDevice(desc->device), "cudaSetDevice");
+
+    fi_model *m = new fi_model();
+    m->d = *desc;
+    m->esz = desc->dtype == FI_F64 ? 8 : 4;
+    m->ib = desc->immersed != 0;
+    const fi_grid &gr = desc->grid;
+    Geom &g = m->g;
+    g.nd = gr.nd;
+    for (int k = 0; k < 3; k++) g.n[k] = k < gr.nd ? gr.n[k] : 0;
+    g.pitch = ((long long)gr.n[0] + 3 + 31) / 32 * 32;
+    g.rows = gr.n[1] + 3;
+    g.sxy = g.pitch * g.rows;
+    g.planes = gr.nd == 3 ? gr.n[2] + 3 : 1;
+    m->elems = (size_t)g.sxy * (size_t)g.planes;
+
+    KParams &kp = m->kp;
+    for (int k = 0; k < 3; k++) kp.inv_dx[k] = k < gr.nd ? 1.0 / (gr.extent[k] / gr.n[k]) : 0.0;
+    kp.dt_P = desc->dtau.dt_P;
+    for (int k = 0; k < 6; k++) kp.dt_tau[k] = desc->dtau.dt_tau[k];
+    for (int k = 0; k < 3; k++) kp.dt_V[k] = desc->dtau.dt_V[k];
+    for (int k = 0; k < 3; k++) {
+        kp.g_kind[k] = desc->gravity.kind[k];
+        kp.g_val[k] = desc->gravity.value[k];
+    }
+    const fi_rheology &r = desc->rheology;
+    kp.rheo_inner = r.inner;
+    kp.rheo_eta_is_field = r.eta_is_field;
+    kp.rheo_A_is_field = r.A_is_field;
+    kp.rheo_n = r.n;
+    kp.rheo_has_reg = r.has_reg;
+    kp.rheo_relax = r.relax;
+    kp.rheo_eta = r.eta;
+    kp.rheo_A = r.A;
+    kp.rheo_inv_eta_reg = r.has_reg ? 1.0 / r.eta_reg : 0.0;  // Physics.jl:22 stores one(η_reg)/η_reg
+    kp.rheo_rate = r.rate;
+    for (int k = 0; k < 3; k++)
+        for (int s = 0; s < 2; s++) {
+            kp.bc_kind[k][s] = k < gr.nd ? desc->bc[k][s].kind : FI_BC_TRACTION;
+            for (int c = 0; c < 3; c++) kp.bc_val[k][s][c] = desc->bc[k][s].c[c];
+        }
+    kp.small = desc->dtype == FI_F64 ? 1e-6 : (double)small_threshold_f32();
+
+    auto fail = [&](fi_status s) {
+        fi_model_destroy(m);
+        return s;
+    };
+    if (cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return fail(cuda_fail(cudaGetLastError(), "stream create"));
+
+    // kernel path
+    int want = desc->path;
+    bool fok = fused_ok(m);
+    if (want == FI_PATH_FUSED && !fok) {
+        set_error("the fused sweep does not cover this problem (3D, FP32/FP64, no z-periodicity, no immersed boundary)");
+        return fail(FI_ERR_UNSUPPORTED);
+    }
+    m->path = (want == FI_PATH_REFERENCE || !fok) ? FI_PATH_REFERENCE : FI_PATH_FUSED;
+
+    const size_t bytes = m->elems * m->esz;
+    for (int f = 0; f < FI_FIELD_COUNT; f++) {
+        if (!field_used(m, f) || is_residual(f)) continue;
+        if (cudaMalloc(&m->base[f], bytes) != cudaSuccess) {
+            cudaGetLastError();
+            set_error("device allocation failed (" + std::to_string(bytes) + " bytes per field)");
+            return fail(FI_ERR_OOM);
+        }
+        if (cudaMemsetAsync(m->base[f], 0, bytes, m->stream) != cudaSuccess)
+            return fail(cuda_fail(cudaGetLastError(), "memset"));
+    }
+    if (m->path == FI_PATH_FUSED) {
+        for (int f = 0; f < kState; f++) {
+            if (!field_used(m, f)) continue;
+            if (cudaMalloc(&m->alt[f], bytes) != cudaSuccess) {
+                cudaGetLastError();
+                set_error("device allocation failed (second state buffer)");
+                return fail(FI_ERR_OOM);
+            }
+            if (cudaMemsetAsync(m->alt[f], 0, bytes, m->stream) != cudaSuccess)
+                return fail(cuda_fail(cudaGetLastError(), "memset"));
+        }
+    }
+    m->nblk = norm_blocks(g);
+    if (cudaMalloc(&m->d_partials, (size_t)m->nblk * kNormSlots * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&m->d_out, FI_NORMS_LEN * sizeof(double)) != cudaSuccess ||
+        cudaMallocHost(&m->h_out, FI_NORMS_LEN * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("norm scratch allocation failed");
+        return fail(FI_ERR_OOM);
+    }
+    if (cudaStreamSynchronize(m->stream) != cudaSuccess) return fail(cuda_fail(cudaGetLastError(), "create sync"));
+    *out = m;
+    return FI_OK;
+}
+
+fi_status fi_model_destroy(fi_model *m) {
+    if (!m) return FI_OK;
+    cudaSetDevice(m->d.device);
+    if (m->stream) cudaStreamSynchronize(m->stream);
+    for (int f = 0; f < FI_FIELD_COUNT; f++)
+        if (m->base[f]) cudaFree(m->base[f]);
+    for (int f = 0; f < kState; f++)
+        if (m->alt[f]) cudaFree(m->alt[f]);
+    if (m->d_partials) cudaFree(m->d_partials);
+    if (m->d_out) cudaFree(m->d_out);
+    if (m->h_out) cudaFreeHost(m->h_out);
+    if (m->stream) cudaStreamDestroy(m->stream);
+    delete m;
+    return FI_OK;
+}
+
+fi_status fi_model_field_size(const fi_model *m, int32_t field, size_t *count) {
+    if (!m || !count || field < 0 || field >= FI_FIELD_COUNT) return set_error("bad argument"), FI_ERR_ARG;
+    *count = interior_count(m, field);
+    return FI_OK;
+}
+
+fi_status fi_model_set_field(fi_model *m, int32_t field, const void *host, size_t nbytes) {
+    if (!m || !host || field < 0 || field >= FI_FIELD_COUNT) return set_error("bad argument"), FI_ERR_ARG;
+    if (!field_used(m, field)) return set_error("field not used by this model"), FI_ERR_ARG;
+    if (nbytes != interior_count(m, field) * m->esz) return set_error("byte count does not match the field's interior"), FI_ERR_ARG;
+    FI_CHECK_CUDA(cudaSetDevice(m->d.device), "cudaSetDevice");
+    if (is_residual(field)) {
+        fi_status st = ensure_residual_arrays(m);
+        if (st != FI_OK) return st;
+    }
+    cudaMemcpy3DParms p = copy_params(m, field, m->cur(field), const_cast<void *>(host), true);
+    FI_CHECK_CUDA(cudaMemcpy3DAsync(&p, m->stream), "set_field copy");
+    FI_CHECK_CUDA(cudaStreamSynchronize(m->stream), "set_field sync");
+    return FI_OK;
+}
+
+fi_status fi_model_get_field(fi_model *m, int32_t field, void *host, size_t nbytes) {
+    if (!m || !host || field < 0 || field >= FI_FIELD_COUNT) return set_error("bad argument"), FI_ERR_ARG;
+    if (!field_used(m, field)) return set_error("field not used by this model"), FI_ERR_ARG;
+    if (nbytes != interior_count(m, field) * m->esz) return set_error("byte count does not match the field's interior"), FI_ERR_ARG;
+    if (is_residual(field) && !m->base[field]) return set_error("residuals not computed yet"), FI_ERR_STATE;
+    FI_CHECK_CUDA(cudaSetDevice(m->d.device), "cudaSetDevice");
+    cudaMemcpy3DParms p = copy_params(m, field, m->cur(field), host, false);
+    FI_CHECK_CUDA(cudaMemcpy3DAsync(&p, m->stream), "get_field copy");
+    FI_CHECK_CUDA(cudaStreamSynchronize(m->stream), "get_field sync");
+    return FI_OK;
+}
+
+fi_status fi_model_apply_bcs(fi_model *m) {
+    if (!m) return set_error("null model"), FI_ERR_ARG;
+    FI_CHECK_CUDA(cudaSetDevice(m->d.device), "cudaSetDevice");
+    fi_status st = m->is_f64() ? apply_bcs_t<double>(m) : apply_bcs_t<float>(m);
+    if (st != FI_OK) return st;
+    FI_CHECK_CUDA(cudaStreamSynchronize(m->stream), "apply_bcs sync");
+    return FI_OK;
+}
+
+fi_status fi_model_advance(fi_model *m, int32_t niter) {
+    if (!m || niter < 0) return set_error("bad argument"), FI_ERR_ARG;
+    FI_CHECK_CUDA(cudaSetDevice(m->d.device), "cudaSetDevice");
+    return m->is_f64() ? advance_t<double>(m, niter) : advance_t<float>(m, niter);
+}
+
+fi_status fi_model_compute_residuals(fi_model *m) {
+    if (!m) return set_error("null model"), FI_ERR_ARG;
+    FI_CHECK_CUDA(cudaSetDevice(m->d.device), "cudaSetDevice");
+    return m->is_f64() ? residuals_t<double>(m) : residuals_t<float>(m);
+}
+
+fi_status fi_model_residual_norms(fi_model *m, double *out) {
+    if (!m || !out) return set_error("bad argument"), FI_ERR_ARG;
+    FI_CHECK_CUDA(cudaSetDevice(m->d.device), "cudaSetDevice");
+    return m->is_f64() ? norms_t<double>(m, out) : norms_t<float>(m, out);
+}
+
+fi_status fi_model_compute_tau(fi_model *m) {
+    if (!m) return set_error("null model"), FI_ERR_ARG;
+    if (m->ib) return set_error("compute_tau of the immersed-boundary model is broken in the reference"), FI_ERR_UNSUPPORTED;
+    FI_CHECK_CUDA(cudaSetDevice(m->d.device), "cudaSetDevice");
+    cudaError_t e = m->is_f64() ? launch_compute_tau<double>(m->g, m->kp, m->ptrs<double>(), m->stream)
+                                : launch_compute_tau<float>(m->g, m->kp, m->ptrs<float>(), m->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "compute_tau");
+    return FI_OK;
+}
+
+fi_status fi_model_device_ptr(fi_model *m, int32_t field, void **dptr) {
+    if (!m || !dptr || field < 0 || field >= FI_FIELD_COUNT) return set_error("bad argument"), FI_ERR_ARG;
+    if (is_residual(field)) {
+        fi_status st = ensure_residual_arrays(m);
+        if (st != FI_OK) return st;
+    }
+    *dptr = m->cur(field);
+    return FI_OK;
+}
+
+fi_status fi_model_layout(const fi_model *m, size_t *pitch, size_t *rows, size_t *planes) {
+    if (!m) return set_error("null model"), FI_ERR_ARG;
+    if (pitch) *pitch = (size_t)m->g.pitch;
+    if (rows) *rows = (size_t)m->g.rows;
+    if (planes) *planes = (size_t)m->g.planes;
+    return FI_OK;
+}
+
+fi_status fi_model_stream(const fi_model *m, void **stream) {
+    if (!m || !stream) return set_error("bad argument"), FI_ERR_ARG;
+    *stream = (void *)m->stream;
+    return FI_OK;
+}
+
+fi_status fi_model_synchronize(fi_model *m) {
+    if (!m) return set_error("null model"), FI_ERR_ARG;
+    FI_CHECK_CUDA(cudaStreamSynchronize(m->stream), "synchronize");
+    return FI_OK;
+}
+
+fi_status fi_model_path(const fi_model *m, int32_t *path) {
+    if (!m || !path) return set_error("bad argument"), FI_ERR_ARG;
+    *path = m->path;
+    return FI_OK;
+}
+
+fi_status fi_model_solve(fi_model *m, const fi_solve_opts *o, fi_solve_report *rep) {
+    if (!m || !o || !rep) return set_error("bad argument"), FI_ERR_ARG;
+    if (o->ncheck <= 0 || o->max_iter <= 0) return set_error("ncheck and max_iter must be positive"), FI_ERR_ARG;
+    if (o->mode != FI_SOLVE_PLAIN) return set_error("use fi_model_solve_mixed for the mixed-precision solve"), FI_ERR_ARG;
+    std::memset(rep, 0, sizeof(*rep));
+    auto t0 = std::chrono::steady_clock::now();
+    int it = 0;
+    fi_status st = FI_OK;
+    double norms[FI_NORMS_LEN];
+    while (it < o->max_iter) {
+        int n = o->ncheck;
+        if (it + n > o->max_iter) n = o->max_iter - it;
+        st = fi_model_advance(m, n);
+        if (st != FI_OK) return st;
+        it += n;
+        st = fi_model_residual_norms(m, norms);
+        if (st != FI_OK) return st;
+        double meas;
+        if (o->measure == FI_CONV_REL_SLAB) {
+            double rv = std::max(norms[1], std::max(norms[2], m->d.grid.nd == 3 ? norms[3] : 0.0));
+            double vmax = std::max(norms[8], std::max(norms[9], norms[10]));
+            double a = rv / (o->rho_g_inf > 0 ? o->rho_g_inf : 1.0);
+            double b = vmax > 0 ? norms[0] * o->length_z / vmax : norms[0];
+            meas = std::max(a, b);
+        } else {
+            meas = norms[0];
+            for (int q = 1; q < 4; q++) meas = std::max(meas, norms[q]);
+        }
+        rep->measure = meas;
+        std::memcpy(rep->norms, norms, sizeof(norms));
+        if (norms[11] != 0.0 || !std::isfinite(meas)) {
+            rep->iterations = it;
+            set_error("simulation failed: non-finite residual");
+            return FI_ERR_DIVERGED;
+        }
+        if (meas < o->tol) {
+            rep->converged = 1;
+            break;
+        }
+    }
+    rep->iterations = it;
+    rep->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return rep->converged ? FI_OK : FI_ERR_TIMEOUT;
+}
+
+fi_status fi_model_volfrac_from_levelset(fi_model *m, int32_t group, const double *psi_host) {
+    if (!m || !psi_host || (group != 0 && group != 1)) return set_error("bad argument"), FI_ERR_ARG;
+    if (!m->ib) return set_error("volume fractions need an immersed-boundary model"), FI_ERR_STATE;
+    FI_CHECK_CUDA(cudaSetDevice(m->d.device), "cudaSetDevice");
+    const Geom &g = m->g;
+    const size_t bytes = m->elems * sizeof(double);
+    void *dpsi = nullptr;
+    void *tmp[8] = {};
+    auto cleanup = [&]() {
+        if (dpsi) cudaFree(dpsi);
+        for (int c = 0; c < 8; c++)
+            if (tmp[c]) cudaFree(tmp[c]);
+    };
+    if (cudaMalloc(&dpsi, bytes) != cudaSuccess) return cleanup(), set_error("allocation failed"), FI_ERR_OOM;
+    cudaMemsetAsync(dpsi, 0, bytes, m->stream);
+    // dense halo storage (n0+3) x (n1+3) x (n2+3) -> pitched storage
+    cudaMemcpy3DParms cp{};
+    size_t nx = (size_t)g.n[0] + 3, ny = (size_t)g.n[1] + 3, nz = (size_t)g.planes;
+    cp.srcPtr = make_cudaPitchedPtr(const_cast<double *>(psi_host), nx * sizeof(double), nx, ny);
+    cp.dstPtr = make_cudaPitchedPtr(dpsi, (size_t)g.pitch * sizeof(double), (size_t)g.pitch, (size_t)g.rows);
+    cp.extent = make_cudaExtent(nx * sizeof(double), ny, nz);
+    cp.kind = cudaMemcpyHostToDevice;
+    if (cudaMemcpy3DAsync(&cp, m->stream) != cudaSuccess) return cleanup(), cuda_fail(cudaGetLastError(), "psi upload");
+    double *w[8];
+    const int base = group == 0 ? FI_FIELD_NA_CCC : FI_FIELD_NS_CCC;
+    for (int c = 0; c < 8; c++) {
+        if (m->is_f64()) {
+            w[c] = (double *)m->base[base + c];
+        } else {
+            if (cudaMalloc(&tmp[c], bytes) != cudaSuccess) return cleanup(), set_error("allocation failed"), FI_ERR_OOM;
+            cudaMemsetAsync(tmp[c], 0, bytes, m->stream);
+            w[c] = (double *)tmp[c];
+        }
+    }
+    double dx[3];
+    for (int k = 0; k < 3; k++) dx[k] = m->d.grid.extent[k] / m->d.grid.n[k];
+    cudaError_t e = launch_volfrac3d(g, dx, (const double *)dpsi, w, m->stream);
+    if (e != cudaSuccess) return cleanup(), cuda_fail(e, "volfrac kernel");
+    if (!m->is_f64()) {
+        for (int c = 0; c < 8; c++) {
+            e = launch_convert_f64_f32(w[c], (float *)m->base[base + c], (long long)m->elems, m->stream);
+            if (e != cudaSuccess) return cleanup(), cuda_fail(e, "convert");
+        }
+    }
+    e = cudaStreamSynchronize(m->stream);
+    cleanup();
+    if (e != cudaSuccess) return cuda_fail(e, "volfrac sync");
+    return FI_OK;
+}
+
+}  // extern "C"
+

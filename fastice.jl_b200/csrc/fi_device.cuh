@@ -1,0 +1,104 @@
+// fi_device.cuh -- device helpers shared by the reference-shaped and fused kernels.
+#pragma once
+
+#include "fi_internal.h"
+
+namespace fi {
+
+template <typename T>
+__device__ __forceinline__ T ipow_dev(T x, int m) {
+    // integer exponent as Julia evaluates x^n for an Int n: n == 2 -> x*x, n == 3 -> x*x*x
+    if (m == 2) return x * x;
+    if (m == 3) return x * x * x;
+    if (m == 1) return x;
+    if (m == 0) return T(1);
+    const int a = m < 0 ? -m : m;
+    T r = a == 2 ? x * x : (a == 3 ? x * x * x : (a == 1 ? x : T(pow(double(x), double(a)))));
+    return m < 0 ? T(1) / r : r;
+}
+
+// rheology(τII, I): src/Physics.jl:11 (linear), :18 (power law), :26
+// (viscoplastic regularisation), :46-47 (relaxation of the current viscosity)
+template <typename T>
+__device__ __forceinline__ T rheology_dev(const KParams &p, const T *eta_lin, const T *Afield, T eta_cur, long long I,
+                                          T tII) {
+    T inner;
+    if (p.rheo_inner == FI_RHEO_LINEAR) {
+        inner = p.rheo_eta_is_field ? eta_lin[I] : T(p.rheo_eta);
+    } else {
+        T A = p.rheo_A_is_field ? Afield[I] : T(p.rheo_A);
+        inner = T(0.5) / (A * ipow_dev(tII, p.rheo_n - 1));
+    }
+    if (p.rheo_has_reg) inner = T(1.0) / (T(1.0) / inner + T(p.rheo_inv_eta_reg));
+    if (p.rheo_relax != FI_RELAX_NONE) {
+        T a = T(1.0 - p.rheo_rate), b = T(p.rheo_rate);
+        if (p.rheo_relax == FI_RELAX_LIN) {
+            inner = eta_cur * a + inner * b;
+        } else if (p.rheo_relax == FI_RELAX_LOG) {
+            inner = T(exp(double(T(log(double(eta_cur))) * a + T(log(double(inner))) * b)));
+        } else {
+            inner = T(pow(10.0, double(T(log10(double(eta_cur))) * a + T(log10(double(inner))) * b)));
+        }
+    }
+    return inner;
+}
+
+template <typename T>
+__device__ __forceinline__ T gravity_dev(const KParams &p, const T *arr, int c, long long I) {
+    return p.g_kind[c] == FI_G_FIELD ? arr[I] : T(p.g_val[c]);
+}
+
+// sqrt with IEEE rounding in both precisions
+__device__ __forceinline__ double sqrt_dev(double x) { return sqrt(x); }
+__device__ __forceinline__ float sqrt_dev(float x) { return __fsqrt_rn(x); }
+__device__ __forceinline__ double div_dev(double a, double b) { return a / b; }
+__device__ __forceinline__ float div_dev(float a, float b) { return __fdiv_rn(a, b); }
+
+// immersed-boundary mask components: ccc vvv vcc cvc ccv vvc vcv cvv
+enum { W_CCC = 0, W_VVV, W_VCC, W_CVC, W_CCV, W_VVC, W_VCV, W_CVV };
+
+template <typename T>
+__device__ __forceinline__ bool small_dev(T w, T thr) {
+    return w < thr;
+}
+
+// isnullspace: src/Models/ImmersedBoundaryFullStokes/Isothermal/null_spaces.jl:13-37
+template <typename T>
+__device__ __forceinline__ bool nullspace_dev(const T *const w[8], int comp, long long I, long long sx, long long sxy,
+                                              T thr) {
+    switch (comp) {
+        case W_CCC:
+            return small_dev(w[W_VCC][I], thr) || small_dev(w[W_VCC][I + 1], thr) || small_dev(w[W_CVC][I], thr) ||
+                   small_dev(w[W_CVC][I + sx], thr) || small_dev(w[W_CCV][I], thr) || small_dev(w[W_CCV][I + sxy], thr);
+        case W_VCC:
+            return small_dev(w[W_CCC][I - 1], thr) || small_dev(w[W_CCC][I], thr) || small_dev(w[W_VVC][I], thr) ||
+                   small_dev(w[W_VVC][I + sx], thr) || small_dev(w[W_VCV][I], thr) || small_dev(w[W_VCV][I + sxy], thr);
+        case W_CVC:
+            return small_dev(w[W_VVC][I], thr) || small_dev(w[W_VVC][I + 1], thr) || small_dev(w[W_CCC][I - sx], thr) ||
+                   small_dev(w[W_CCC][I], thr) || small_dev(w[W_CVV][I], thr) || small_dev(w[W_CVV][I + sxy], thr);
+        case W_CCV:
+            return small_dev(w[W_VCV][I], thr) || small_dev(w[W_VCV][I + 1], thr) || small_dev(w[W_CVV][I], thr) ||
+                   small_dev(w[W_CVV][I + sx], thr) || small_dev(w[W_CCC][I - sxy], thr) || small_dev(w[W_CCC][I], thr);
+        case W_VVC:
+            return small_dev(w[W_CVC][I - 1], thr) || small_dev(w[W_CVC][I], thr) || small_dev(w[W_VCC][I - sx], thr) ||
+                   small_dev(w[W_VCC][I], thr);
+        case W_VCV:
+            return small_dev(w[W_CCV][I - 1], thr) || small_dev(w[W_CCV][I], thr) || small_dev(w[W_VCC][I - sxy], thr) ||
+                   small_dev(w[W_VCC][I], thr);
+        case W_CVV:
+            return small_dev(w[W_CCV][I - sx], thr) || small_dev(w[W_CCV][I], thr) || small_dev(w[W_CVC][I - sxy], thr) ||
+                   small_dev(w[W_CVC][I], thr);
+        default:
+            return false;
+    }
+}
+
+// isvalid(a, loc, I) && !isempty(b, loc, I)  (null_spaces.jl:41-43)
+template <typename T>
+__device__ __forceinline__ bool active_dev(const T *const a[8], const T *const b[8], int comp, long long I, long long sx,
+                                           long long sxy, T thr) {
+    bool valid = !(nullspace_dev(a, comp, I, sx, sxy, thr) || small_dev(a[comp][I], thr));
+    return valid && !small_dev(b[comp][I], thr);
+}
+
+}  // namespace fi

@@ -1,0 +1,112 @@
+// fi_internal.h -- internal types shared by the libfastice_b200 translation units.
+//
+// Storage: every field of a model lives in one uniform halo box per model:
+// (n0+3) x (n1+3) x (n2+3) logical elements (vertex count + one ghost layer on
+// each side, for every staggered location), x fastest, with the x row padded
+// to a multiple of 32 elements so that each row starts on a 128-byte (FP32) or
+// 256-byte (FP64) boundary.  Index (i,j,k) -> i + pitch*(j + rows*k); index 0
+// is the left ghost, 1..N_loc the interior (N_loc = n or n+1 per location).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+#include <string>
+
+#include "../../include/fastice_b200.h"
+
+namespace fi {
+
+constexpr int kMaxBcOps = 16;
+constexpr int kNormSlots = 12;  // per-block partial slots (FI_NORMS_LEN layout)
+
+// geometry as seen by device code
+struct Geom {
+    int nd;
+    int n[3];
+    long long pitch;  // elements per x row
+    long long rows;   // rows per plane (n1 + 3)
+    long long sxy;    // pitch * rows
+    long long planes; // n2 + 3 (1 in 2D)
+};
+
+// scalar parameters as seen by device code (doubles; kernels convert to T
+// exactly as the host would: (T)value)
+struct KParams {
+    double inv_dx[3];
+    double dt_P, dt_tau[6], dt_V[3];
+    int g_kind[3];
+    double g_val[3];
+    int rheo_inner, rheo_eta_is_field, rheo_A_is_field, rheo_n, rheo_has_reg, rheo_relax;
+    double rheo_eta, rheo_A, rheo_inv_eta_reg, rheo_rate;
+    int bc_kind[3][2];
+    double bc_val[3][2][3];
+    double small;  // immersed-boundary emptiness threshold (1e-6, or the FP32 value equivalent to it)
+};
+
+// device pointers of one model state (current buffers)
+template <typename T>
+struct Ptrs {
+    T *P, *txx, *tyy, *tzz, *txy, *txz, *tyz;
+    T *Vx, *Vy, *Vz;
+    T *eta, *eta_next;
+    T *rP, *rVx, *rVy, *rVz;
+    const T *gx, *gy, *gz;
+    const T *eta_lin, *A;
+    const T *wna[8];
+    const T *wns[8];
+};
+
+// one boundary-condition operation on a face (see kernel bc_dim_kernel)
+enum BcOp { BC_DIRICHLET = 0, BC_NEUMANN = 1, BC_PERIODIC = 2 };
+struct BcOpDesc {
+    void *f;
+    int loc[3];
+    int side;
+    int op;
+    double v;
+};
+struct BcBatch {
+    int count;
+    int dim;
+    BcOpDesc ops[kMaxBcOps];
+};
+
+void set_error(const std::string &msg);
+fi_status cuda_fail(cudaError_t e, const char *where);
+
+// ---- launchers implemented in fi_reference.cu ----
+template <typename T>
+cudaError_t launch_update_sigma(const Geom &g, const KParams &p, const Ptrs<T> &f, bool ib, cudaStream_t s);
+template <typename T>
+cudaError_t launch_update_V(const Geom &g, const KParams &p, const Ptrs<T> &f, bool ib, cudaStream_t s);
+template <typename T>
+cudaError_t launch_compute_residuals(const Geom &g, const KParams &p, const Ptrs<T> &f, bool ib, cudaStream_t s);
+template <typename T>
+cudaError_t launch_compute_tau(const Geom &g, const KParams &p, const Ptrs<T> &f, cudaStream_t s);
+template <typename T>
+cudaError_t launch_bc_batch(const Geom &g, const BcBatch &b, cudaStream_t s);
+template <typename T>
+cudaError_t launch_residual_norms(const Geom &g, const KParams &p, const Ptrs<T> &f, bool ib, double *partials,
+                                  int nblocks, double *out_dev, cudaStream_t s);
+int norm_blocks(const Geom &g);
+
+// ---- fused 3D sweep (fi_fused3d.cu) ----
+// P,tau,V read from `in`, written to `out`; eta read from in.eta, eta_next written.
+template <typename T>
+bool fused3d_supported(const Geom &g, const KParams &p, bool ib);
+template <typename T>
+cudaError_t launch_fused3d(const Geom &g, const KParams &p, const Ptrs<T> &in, const Ptrs<T> &out, bool ib,
+                           int variant, cudaStream_t s);
+int fused3d_num_variants();
+const char *fused3d_variant_name(int v);
+
+// ---- level sets (fi_levelsets.cu) ----
+cudaError_t launch_volfrac3d(const Geom &g, const double dx[3], const double *psi, double *const w[8], cudaStream_t s);
+cudaError_t launch_volfrac2d(const Geom &g, const double dx[2], const double *psi, double *const w[4], cudaStream_t s);
+cudaError_t launch_convert_f64_f32(const double *src, float *dst, long long n, cudaStream_t s);
+cudaError_t launch_levelset(const Geom &g3, const double o3[3], const double dx3[3], const int n2[2],
+                            const double o2[2], const double dx2[2], long long dem_pitch, const double *dem,
+                            const double *R, int has_R, double cutoff, int invert, double *psi, cudaStream_t s);
+
+}  // namespace fi

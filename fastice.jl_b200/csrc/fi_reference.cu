@@ -1,0 +1,608 @@
+// fi_reference.cu -- reference-shaped kernels: one thread per grid index over the
+// vertex-sized range 1..n+1 (the Chmy Launcher worksize), boundary-condition
+// batches applied dimension by dimension, and the fused residual-norm reduction.
+//
+// These kernels follow src/Models/FullStokes/Isothermal/kernels_{2d,3d}.jl and
+// src/Models/ImmersedBoundaryFullStokes/Isothermal/kernels_3d.jl operation by
+// operation (same grouping of sums and products), so a build without FMA
+// contraction reproduces the CPU oracle bit for bit.  They serve as the
+// FI_PATH_REFERENCE path and for the shapes the fused sweep does not cover.
+#include "fi_device.cuh"
+
+namespace fi {
+
+namespace {
+
+template <typename T>
+__device__ __forceinline__ T h(T x) { return T(0.5) * x; }
+
+struct Idx {
+    long long I;
+    int i, j, k;
+    bool ok;
+};
+
+__device__ __forceinline__ Idx vertex_index(const Geom &g) {
+    Idx r;
+    r.i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    r.j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    r.k = g.nd == 3 ? (int)blockIdx.z + 1 : 0;
+    r.ok = r.i <= g.n[0] + 1 && r.j <= g.n[1] + 1;
+    r.I = (long long)r.i + g.pitch * ((long long)r.j + g.rows * (long long)r.k);
+    return r;
+}
+
+dim3 vertex_grid(const Geom &g, dim3 blk) {
+    return dim3((g.n[0] + 1 + blk.x - 1) / blk.x, (g.n[1] + 1 + blk.y - 1) / blk.y, g.nd == 3 ? g.n[2] + 1 : 1);
+}
+
+// ---------------------------------------------------------------------------
+// update_σ!  (kernels_3d.jl:3-25, kernels_2d.jl:3-18; IB: IB kernels_3d.jl:3-44)
+// ---------------------------------------------------------------------------
+template <typename T, int ND, bool IB>
+__global__ void __launch_bounds__(256) update_sigma_kernel(Geom g, KParams p, Ptrs<T> f) {
+    Idx x = vertex_index(g);
+    if (!x.ok) return;
+    const long long I = x.I, sx = g.pitch, sxy = g.sxy;
+    const T idx = T(p.inv_dx[0]), idy = T(p.inv_dx[1]);
+    const T *Vx = f.Vx, *Vy = f.Vy, *eta = f.eta;
+    if (ND == 2) {
+        T exx = (Vx[I + 1] - Vx[I]) * idx;
+        T eyy = (Vy[I + sx] - Vy[I]) * idy;
+        T exy = T(0.5) * ((Vy[I] - Vy[I - 1]) * idx + (Vx[I] - Vx[I - sx]) * idy);
+        T divV = exx + eyy;
+        T etac = eta[I];
+        f.P[I] = f.P[I] - divV * etac * T(p.dt_P);
+        f.txx[I] = f.txx[I] - (f.txx[I] - T(2.0) * etac * (exx - divV / T(3.0))) * T(p.dt_tau[0]);
+        f.tyy[I] = f.tyy[I] - (f.tyy[I] - T(2.0) * etac * (eyy - divV / T(3.0))) * T(p.dt_tau[1]);
+        T exy_eta = h(h(eta[I - 1 - sx] + eta[I - sx]) + h(eta[I - 1] + eta[I]));
+        f.txy[I] = f.txy[I] - (f.txy[I] - T(2.0) * exy_eta * exy) * T(p.dt_tau[3]);
+        return;
+    }
+    const T idz = T(p.inv_dx[2]);
+    const T *Vz = f.Vz;
+    const T thr = T(p.small);
+    if (!IB) {
+        T exx = (Vx[I + 1] - Vx[I]) * idx;
+        T eyy = (Vy[I + sx] - Vy[I]) * idy;
+        T ezz = (Vz[I + sxy] - Vz[I]) * idz;
+        T exy = T(0.5) * ((Vy[I] - Vy[I - 1]) * idx + (Vx[I] - Vx[I - sx]) * idy);
+        T exz = T(0.5) * ((Vz[I] - Vz[I - 1]) * idx + (Vx[I] - Vx[I - sxy]) * idz);
+        T eyz = T(0.5) * ((Vz[I] - Vz[I - sx]) * idy + (Vy[I] - Vy[I - sxy]) * idz);
+        T divV = exx + eyy + ezz;
+        T etac = eta[I];
+        f.P[I] = f.P[I] - divV * etac * T(p.dt_P);
+        f.txx[I] = f.txx[I] - (f.txx[I] - T(2.0) * etac * (exx - divV / T(3.0))) * T(p.dt_tau[0]);
+        f.tyy[I] = f.tyy[I] - (f.tyy[I] - T(2.0) * etac * (eyy - divV / T(3.0))) * T(p.dt_tau[1]);
+        f.tzz[I] = f.tzz[I] - (f.tzz[I] - T(2.0) * etac * (ezz - divV / T(3.0))) * T(p.dt_tau[2]);
+        T e_xy = h(h(eta[I - 1 - sx] + eta[I - sx]) + h(eta[I - 1] + eta[I]));
+        T e_xz = h(h(eta[I - 1 - sxy] + eta[I - sxy]) + h(eta[I - 1] + eta[I]));
+        T e_yz = h(h(eta[I - sx - sxy] + eta[I - sxy]) + h(eta[I - sx] + eta[I]));
+        f.txy[I] = f.txy[I] - (f.txy[I] - T(2.0) * e_xy * exy) * T(p.dt_tau[3]);
+        f.txz[I] = f.txz[I] - (f.txz[I] - T(2.0) * e_xz * exz) * T(p.dt_tau[4]);
+        f.tyz[I] = f.tyz[I] - (f.tyz[I] - T(2.0) * e_yz * eyz) * T(p.dt_tau[5]);
+        return;
+    }
+    const T *const *na = f.wna;
+    const T *const *ns = f.wns;
+    if (active_dev(na, ns, W_CCC, I, sx, sxy, thr)) {
+        T exx = (ns[W_VCC][I + 1] * Vx[I + 1] - ns[W_VCC][I] * Vx[I]) * idx;
+        T eyy = (ns[W_CVC][I + sx] * Vy[I + sx] - ns[W_CVC][I] * Vy[I]) * idy;
+        T ezz = (ns[W_CCV][I + sxy] * Vz[I + sxy] - ns[W_CCV][I] * Vz[I]) * idz;
+        T divV = exx + eyy + ezz;
+        T etac = eta[I];
+        f.P[I] = f.P[I] - divV * etac * T(p.dt_P);
+        f.txx[I] = f.txx[I] - (f.txx[I] - T(2.0) * etac * (exx - divV / T(3.0))) * T(p.dt_tau[0]);
+        f.tyy[I] = f.tyy[I] - (f.tyy[I] - T(2.0) * etac * (eyy - divV / T(3.0))) * T(p.dt_tau[1]);
+        f.tzz[I] = f.tzz[I] - (f.tzz[I] - T(2.0) * etac * (ezz - divV / T(3.0))) * T(p.dt_tau[2]);
+    } else {
+        f.P[I] = T(0);
+        f.txx[I] = T(0);
+        f.tyy[I] = T(0);
+        f.tzz[I] = T(0);
+    }
+    if (active_dev(na, ns, W_VVC, I, sx, sxy, thr)) {
+        T exy = T(0.5) * ((ns[W_CVC][I] * Vy[I] - ns[W_CVC][I - 1] * Vy[I - 1]) * idx +
+                          (ns[W_VCC][I] * Vx[I] - ns[W_VCC][I - sx] * Vx[I - sx]) * idy);
+        T e_xy = h(h(eta[I - 1 - sx] + eta[I - sx]) + h(eta[I - 1] + eta[I]));
+        f.txy[I] = f.txy[I] - (f.txy[I] - T(2.0) * e_xy * exy) * T(p.dt_tau[3]);
+    } else {
+        f.txy[I] = T(0);
+    }
+    if (active_dev(na, ns, W_VCV, I, sx, sxy, thr)) {
+        T exz = T(0.5) * ((ns[W_CCV][I] * Vz[I] - ns[W_CCV][I - 1] * Vz[I - 1]) * idx +
+                          (ns[W_VCC][I] * Vx[I] - ns[W_VCC][I - sxy] * Vx[I - sxy]) * idz);
+        T e_xz = h(h(eta[I - 1 - sxy] + eta[I - sxy]) + h(eta[I - 1] + eta[I]));
+        f.txz[I] = f.txz[I] - (f.txz[I] - T(2.0) * e_xz * exz) * T(p.dt_tau[4]);
+    } else {
+        f.txz[I] = T(0);
+    }
+    if (active_dev(na, ns, W_CVV, I, sx, sxy, thr)) {
+        T eyz = T(0.5) * ((ns[W_CCV][I] * Vz[I] - ns[W_CCV][I - sx] * Vz[I - sx]) * idy +
+                          (ns[W_CVC][I] * Vy[I] - ns[W_CVC][I - sxy] * Vy[I - sxy]) * idz);
+        T e_yz = h(h(eta[I - sx - sxy] + eta[I - sxy]) + h(eta[I - sx] + eta[I]));
+        f.tyz[I] = f.tyz[I] - (f.tyz[I] - T(2.0) * e_yz * eyz) * T(p.dt_tau[5]);
+    } else {
+        f.tyz[I] = T(0);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// update_V!  (kernels_3d.jl:27-40, kernels_2d.jl:20-29; IB kernels_3d.jl:46-74)
+// ---------------------------------------------------------------------------
+template <typename T, int ND, bool IB>
+__global__ void __launch_bounds__(256) update_V_kernel(Geom g, KParams p, Ptrs<T> f) {
+    Idx x = vertex_index(g);
+    if (!x.ok) return;
+    const long long I = x.I, sx = g.pitch, sxy = g.sxy;
+    const T idx = T(p.inv_dx[0]), idy = T(p.inv_dx[1]);
+    const T *P = f.P, *txx = f.txx, *tyy = f.tyy, *txy = f.txy, *eta = f.eta;
+    if (ND == 2) {
+        T gx = gravity_dev(p, f.gx, 0, I), gy = gravity_dev(p, f.gy, 1, I);
+        T ex = h(eta[I - 1] + eta[I]);
+        T ey = h(eta[I - sx] + eta[I]);
+        f.Vx[I] = f.Vx[I] +
+                  div_dev(-(P[I] - P[I - 1]) * idx + (txx[I] - txx[I - 1]) * idx + (txy[I + sx] - txy[I]) * idy - gx, ex) *
+                      T(p.dt_V[0]);
+        f.Vy[I] = f.Vy[I] +
+                  div_dev(-(P[I] - P[I - sx]) * idy + (tyy[I] - tyy[I - sx]) * idy + (txy[I + 1] - txy[I]) * idx - gy, ey) *
+                      T(p.dt_V[1]);
+        T lxy = h(h(txy[I] + txy[I + 1]) + h(txy[I + sx] + txy[I + sx + 1]));
+        T tII = sqrt_dev(T(0.5) * (txx[I] * txx[I] + tyy[I] * tyy[I]) + lxy * lxy);
+        f.eta_next[I] = rheology_dev(p, f.eta_lin, f.A, eta[I], I, tII);
+        return;
+    }
+    const T idz = T(p.inv_dx[2]);
+    const T *tzz = f.tzz, *txz = f.txz, *tyz = f.tyz;
+    T gx = gravity_dev(p, f.gx, 0, I), gy = gravity_dev(p, f.gy, 1, I), gz = gravity_dev(p, f.gz, 2, I);
+    if (!IB) {
+        T ex = h(eta[I - 1] + eta[I]);
+        T ey = h(eta[I - sx] + eta[I]);
+        T ez = h(eta[I - sxy] + eta[I]);
+        f.Vx[I] = f.Vx[I] + div_dev(-(P[I] - P[I - 1]) * idx + (txx[I] - txx[I - 1]) * idx + (txy[I + sx] - txy[I]) * idy +
+                                        (txz[I + sxy] - txz[I]) * idz - gx,
+                                    ex) *
+                                T(p.dt_V[0]);
+        f.Vy[I] = f.Vy[I] + div_dev(-(P[I] - P[I - sx]) * idy + (tyy[I] - tyy[I - sx]) * idy + (txy[I + 1] - txy[I]) * idx +
+                                        (tyz[I + sxy] - tyz[I]) * idz - gy,
+                                    ey) *
+                                T(p.dt_V[1]);
+        f.Vz[I] = f.Vz[I] + div_dev(-(P[I] - P[I - sxy]) * idz + (tzz[I] - tzz[I - sxy]) * idz + (txz[I + 1] - txz[I]) * idx +
+                                        (tyz[I + sx] - tyz[I]) * idy - gz,
+                                    ez) *
+                                T(p.dt_V[2]);
+    } else {
+        const T *const *na = f.wna;
+        const T *const *ns = f.wns;
+        const T thr = T(p.small);
+        const T *wc = na[W_CCC], *wvvc = na[W_VVC], *wvcv = na[W_VCV], *wcvv = na[W_CVV];
+        if (active_dev(ns, na, W_VCC, I, sx, sxy, thr)) {
+            T ex = h(eta[I - 1] + eta[I]);
+            f.Vx[I] = f.Vx[I] + div_dev(div_dev(-(wc[I] * P[I] - wc[I - 1] * P[I - 1]) * idx +
+                                                    (wc[I] * txx[I] - wc[I - 1] * txx[I - 1]) * idx +
+                                                    (wvvc[I + sx] * txy[I + sx] - wvvc[I] * txy[I]) * idy +
+                                                    (wvcv[I + sxy] * txz[I + sxy] - wvcv[I] * txz[I]) * idz - gx,
+                                                ex),
+                                        ns[W_VCC][I]) *
+                                    T(p.dt_V[0]);
+        } else {
+            f.Vx[I] = T(0);
+        }
+        if (active_dev(ns, na, W_CVC, I, sx, sxy, thr)) {
+            T ey = h(eta[I - sx] + eta[I]);
+            f.Vy[I] = f.Vy[I] + div_dev(div_dev(-(wc[I] * P[I] - wc[I - sx] * P[I - sx]) * idy +
+                                                    (wc[I] * tyy[I] - wc[I - sx] * tyy[I - sx]) * idy +
+                                                    (wvvc[I + 1] * txy[I + 1] - wvvc[I] * txy[I]) * idx +
+                                                    (wcvv[I + sxy] * tyz[I + sxy] - wcvv[I] * tyz[I]) * idz - gy,
+                                                ey),
+                                        ns[W_CVC][I]) *
+                                    T(p.dt_V[1]);
+        } else {
+            f.Vy[I] = T(0);
+        }
+        if (active_dev(ns, na, W_CCV, I, sx, sxy, thr)) {
+            T ez = h(eta[I - sxy] + eta[I]);
+            f.Vz[I] = f.Vz[I] + div_dev(div_dev(-(wc[I] * P[I] - wc[I - sxy] * P[I - sxy]) * idz +
+                                                    (wc[I] * tzz[I] - wc[I - sxy] * tzz[I - sxy]) * idz +
+                                                    (wvcv[I + 1] * txz[I + 1] - wvcv[I] * txz[I]) * idx +
+                                                    (wcvv[I + sx] * tyz[I + sx] - wcvv[I] * tyz[I]) * idy - gz,
+                                                ez),
+                                        ns[W_CCV][I]) *
+                                    T(p.dt_V[2]);
+        } else {
+            f.Vz[I] = T(0);
+        }
+    }
+    T lxy = h(h(txy[I] + txy[I + 1]) + h(txy[I + sx] + txy[I + sx + 1]));
+    T lxz = h(h(txz[I] + txz[I + 1]) + h(txz[I + sxy] + txz[I + sxy + 1]));
+    T lyz = h(h(tyz[I] + tyz[I + sx]) + h(tyz[I + sxy] + tyz[I + sxy + sx]));
+    T s = T(0.5) * (txx[I] * txx[I] + tyy[I] * tyy[I] + tzz[I] * tzz[I]) + lxy * lxy + lxz * lxz + lyz * lyz;
+    T tII = sqrt_dev(s);
+    f.eta_next[I] = rheology_dev(p, f.eta_lin, f.A, eta[I], I, tII);
+}
+
+// ---------------------------------------------------------------------------
+// compute_residuals!  (kernels_3d.jl:66-75, kernels_2d.jl:46-54; IB :118-143)
+// ---------------------------------------------------------------------------
+template <typename T, int ND, bool IB>
+struct Resid {
+    T rP, rVx, rVy, rVz;
+};
+
+template <typename T, int ND, bool IB>
+__device__ __forceinline__ Resid<T, ND, IB> residual_at(const Geom &g, const KParams &p, const Ptrs<T> &f, long long I) {
+    Resid<T, ND, IB> r;
+    const long long sx = g.pitch, sxy = g.sxy;
+    const T idx = T(p.inv_dx[0]), idy = T(p.inv_dx[1]);
+    const T *P = f.P, *txx = f.txx, *tyy = f.tyy, *txy = f.txy, *Vx = f.Vx, *Vy = f.Vy;
+    if (ND == 2) {
+        T gx = gravity_dev(p, f.gx, 0, I), gy = gravity_dev(p, f.gy, 1, I);
+        r.rP = (Vx[I + 1] - Vx[I]) * idx + (Vy[I + sx] - Vy[I]) * idy;
+        r.rVx = -(P[I] - P[I - 1]) * idx + (txx[I] - txx[I - 1]) * idx + (txy[I + sx] - txy[I]) * idy - gx;
+        r.rVy = -(P[I] - P[I - sx]) * idy + (tyy[I] - tyy[I - sx]) * idy + (txy[I + 1] - txy[I]) * idx - gy;
+        r.rVz = T(0);
+        return r;
+    }
+    const T idz = T(p.inv_dx[2]);
+    const T *tzz = f.tzz, *txz = f.txz, *tyz = f.tyz, *Vz = f.Vz;
+    T gx = gravity_dev(p, f.gx, 0, I), gy = gravity_dev(p, f.gy, 1, I), gz = gravity_dev(p, f.gz, 2, I);
+    if (!IB) {
+        r.rP = (Vx[I + 1] - Vx[I]) * idx + (Vy[I + sx] - Vy[I]) * idy + (Vz[I + sxy] - Vz[I]) * idz;
+        r.rVx = -(P[I] - P[I - 1]) * idx + (txx[I] - txx[I - 1]) * idx + (txy[I + sx] - txy[I]) * idy +
+                (txz[I + sxy] - txz[I]) * idz - gx;
+        r.rVy = -(P[I] - P[I - sx]) * idy + (tyy[I] - tyy[I - sx]) * idy + (txy[I + 1] - txy[I]) * idx +
+                (tyz[I + sxy] - tyz[I]) * idz - gy;
+        r.rVz = -(P[I] - P[I - sxy]) * idz + (tzz[I] - tzz[I - sxy]) * idz + (txz[I + 1] - txz[I]) * idx +
+                (tyz[I + sx] - tyz[I]) * idy - gz;
+        return r;
+    }
+    const T *const *na = f.wna;
+    const T *const *ns = f.wns;
+    const T thr = T(p.small);
+    const T *wc = na[W_CCC], *wvvc = na[W_VVC], *wvcv = na[W_VCV], *wcvv = na[W_CVV];
+    r.rP = active_dev(na, ns, W_CCC, I, sx, sxy, thr)
+               ? (ns[W_VCC][I + 1] * Vx[I + 1] - ns[W_VCC][I] * Vx[I]) * idx +
+                     (ns[W_CVC][I + sx] * Vy[I + sx] - ns[W_CVC][I] * Vy[I]) * idy +
+                     (ns[W_CCV][I + sxy] * Vz[I + sxy] - ns[W_CCV][I] * Vz[I]) * idz
+               : T(0);
+    r.rVx = active_dev(ns, na, W_VCC, I, sx, sxy, thr)
+                ? -(wc[I] * P[I] - wc[I - 1] * P[I - 1]) * idx + (wc[I] * txx[I] - wc[I - 1] * txx[I - 1]) * idx +
+                      (wvvc[I + sx] * txy[I + sx] - wvvc[I] * txy[I]) * idy +
+                      (wvcv[I + sxy] * txz[I + sxy] - wvcv[I] * txz[I]) * idz - gx
+                : T(0);
+    r.rVy = active_dev(ns, na, W_CVC, I, sx, sxy, thr)
+                ? -(wc[I] * P[I] - wc[I - sx] * P[I - sx]) * idy + (wc[I] * tyy[I] - wc[I - sx] * tyy[I - sx]) * idy +
+                      (wvvc[I + 1] * txy[I + 1] - wvvc[I] * txy[I]) * idx +
+                      (wcvv[I + sxy] * tyz[I + sxy] - wcvv[I] * tyz[I]) * idz - gy
+                : T(0);
+    r.rVz = active_dev(ns, na, W_CCV, I, sx, sxy, thr)
+                ? -(wc[I] * P[I] - wc[I - sxy] * P[I - sxy]) * idz + (wc[I] * tzz[I] - wc[I - sxy] * tzz[I - sxy]) * idz +
+                      (wvcv[I + 1] * txz[I + 1] - wvcv[I] * txz[I]) * idx +
+                      (wcvv[I + sx] * tyz[I + sx] - wcvv[I] * tyz[I]) * idy - gz
+                : T(0);
+    return r;
+}
+
+template <typename T, int ND, bool IB>
+__global__ void __launch_bounds__(256) compute_residuals_kernel(Geom g, KParams p, Ptrs<T> f) {
+    Idx x = vertex_index(g);
+    if (!x.ok) return;
+    Resid<T, ND, IB> r = residual_at<T, ND, IB>(g, p, f, x.I);
+    f.rP[x.I] = r.rP;
+    f.rVx[x.I] = r.rVx;
+    f.rVy[x.I] = r.rVy;
+    if (ND == 3) f.rVz[x.I] = r.rVz;
+}
+
+// compute_τ!  (kernels_3d.jl:225-245, kernels_2d.jl:33-44)
+template <typename T, int ND>
+__global__ void __launch_bounds__(256) compute_tau_kernel(Geom g, KParams p, Ptrs<T> f) {
+    Idx x = vertex_index(g);
+    if (!x.ok) return;
+    const long long I = x.I, sx = g.pitch, sxy = g.sxy;
+    const T idx = T(p.inv_dx[0]), idy = T(p.inv_dx[1]);
+    const T *Vx = f.Vx, *Vy = f.Vy, *eta = f.eta;
+    if (ND == 2) {
+        T exx = (Vx[I + 1] - Vx[I]) * idx;
+        T eyy = (Vy[I + sx] - Vy[I]) * idy;
+        T exy = T(0.5) * ((Vy[I] - Vy[I - 1]) * idx + (Vx[I] - Vx[I - sx]) * idy);
+        T divV = exx + eyy;
+        f.txx[I] = T(2.0) * eta[I] * (exx - divV / T(3.0));
+        f.tyy[I] = T(2.0) * eta[I] * (eyy - divV / T(3.0));
+        T e_xy = h(h(eta[I - 1 - sx] + eta[I - sx]) + h(eta[I - 1] + eta[I]));
+        f.txy[I] = T(2.0) * e_xy * exy;
+        return;
+    }
+    const T idz = T(p.inv_dx[2]);
+    const T *Vz = f.Vz;
+    T exx = (Vx[I + 1] - Vx[I]) * idx;
+    T eyy = (Vy[I + sx] - Vy[I]) * idy;
+    T ezz = (Vz[I + sxy] - Vz[I]) * idz;
+    T exy = T(0.5) * ((Vy[I] - Vy[I - 1]) * idx + (Vx[I] - Vx[I - sx]) * idy);
+    T exz = T(0.5) * ((Vz[I] - Vz[I - 1]) * idx + (Vx[I] - Vx[I - sxy]) * idz);
+    T eyz = T(0.5) * ((Vz[I] - Vz[I - sx]) * idy + (Vy[I] - Vy[I - sxy]) * idz);
+    T divV = exx + eyy + ezz;
+    f.txx[I] = T(2.0) * eta[I] * (exx - divV / T(3.0));
+    f.tyy[I] = T(2.0) * eta[I] * (eyy - divV / T(3.0));
+    f.tzz[I] = T(2.0) * eta[I] * (ezz - divV / T(3.0));
+    T e_xy = h(h(eta[I - 1 - sx] + eta[I - sx]) + h(eta[I - 1] + eta[I]));
+    T e_xz = h(h(eta[I - 1 - sxy] + eta[I - sxy]) + h(eta[I - 1] + eta[I]));
+    T e_yz = h(h(eta[I - sx - sxy] + eta[I - sxy]) + h(eta[I - sx] + eta[I]));
+    f.txy[I] = T(2.0) * e_xy * exy;
+    f.txz[I] = T(2.0) * e_xz * exz;
+    f.tyz[I] = T(2.0) * e_yz * eyz;
+}
+
+// ---------------------------------------------------------------------------
+// Boundary-condition batch for one dimension: the face of dim d spans the full
+// storage range of the dims before d and the interior range of the dims after
+// d (per field location); left and right sides of every field in the batch.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void bc_dim_kernel(Geom g, BcBatch b) {
+    const int d = b.dim;
+    int e1 = -1, e2 = -1;
+    for (int e = 0; e < g.nd; e++) {
+        if (e == d) continue;
+        if (e1 < 0) e1 = e;
+        else e2 = e;
+    }
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = blockIdx.y * blockDim.y + threadIdx.y;
+    if (a > g.n[e1] + 2) return;
+    if (e2 >= 0 && c > g.n[e2] + 2) return;
+    if (e2 < 0 && c > 0) return;
+    const long long st[3] = {1, g.pitch, g.sxy};
+    for (int q = 0; q < b.count; q++) {
+        const BcOpDesc &op = b.ops[q];
+        // range check for the other dims
+        int pos[3] = {0, 0, 0};
+        pos[e1] = a;
+        if (e2 >= 0) pos[e2] = c;
+        bool ok = true;
+        for (int e = 0; e < g.nd; e++) {
+            if (e == d) continue;
+            if (e > d && (pos[e] < 1 || pos[e] > g.n[e] + op.loc[e])) ok = false;
+        }
+        if (!ok) continue;
+        T *f = (T *)op.f;
+        long long B = (long long)pos[0] + g.pitch * ((long long)pos[1] + g.rows * (long long)pos[2]);
+        const long long sd = st[d];
+        const int N = g.n[d];
+#define A(q_) f[B + (long long)(q_)*sd]
+        if (op.op == BC_DIRICHLET) {
+            T v = T(op.v);
+            T two_v = T(2.0) * v;
+            if (op.loc[d] == 0) {
+                if (op.side == 0) A(0) = two_v - A(1);
+                else A(N + 1) = two_v - A(N);
+            } else {
+                if (op.side == 0) A(1) = v;
+                else A(N + 1) = v;
+            }
+        } else if (op.op == BC_NEUMANN) {
+            if (op.loc[d] == 0) {
+                if (op.side == 0) A(0) = A(1);
+                else A(N + 1) = A(N);
+            } else {
+                if (op.side == 0) A(0) = A(2);
+                else A(N + 2) = A(N);
+            }
+        } else {
+            if (op.loc[d] == 0) {
+                A(0) = A(N);
+                A(N + 1) = A(1);
+            } else {
+                A(N + 1) = A(1);
+                A(0) = A(N);
+                A(N + 2) = A(2);
+            }
+        }
+#undef A
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Fused residual + norms: r is evaluated at every interior position of each
+// component (normal velocity residual = 0 on non-traction, non-periodic walls,
+// boundary_conditions.jl:120-128) and reduced to max|r|, sum r^2, max|V| per
+// block (warp shuffles, then shared memory); a second single-block pass adds
+// the per-block partials in a fixed order in FP64.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double warp_max(double v) {
+    for (int o = 16; o > 0; o >>= 1) {
+        double w = __shfl_xor_sync(0xffffffffu, v, o);
+        v = (w > v || w != w) ? w : v;  // NaN-propagating max
+    }
+    return v;
+}
+__device__ __forceinline__ double warp_sum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ double nmax(double a, double b) { return (b > a || b != b) ? b : a; }
+
+constexpr int kNormThreads = 256;
+
+template <typename T, int ND, bool IB>
+__global__ void __launch_bounds__(kNormThreads) residual_norms_kernel(Geom g, KParams p, Ptrs<T> f, double *partials) {
+    double mx[4] = {0, 0, 0, 0}, ss[4] = {0, 0, 0, 0}, vm[3] = {0, 0, 0};
+    const long long nx = g.n[0] + 1, ny = g.n[1] + 1, nz = ND == 3 ? g.n[2] + 1 : 1;
+    const long long total = nx * ny * nz;
+    bool wall0[3][2];
+    for (int d = 0; d < 3; d++)
+        for (int s = 0; s < 2; s++) {
+            int k = d < ND ? p.bc_kind[d][s] : FI_BC_TRACTION;
+            wall0[d][s] = !(k == FI_BC_TRACTION || k == FI_BC_PERIODIC);
+        }
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+        int i = int(t % nx) + 1;
+        long long r2 = t / nx;
+        int j = int(r2 % ny) + 1;
+        int k = ND == 3 ? int(r2 / ny) + 1 : 0;
+        long long I = (long long)i + g.pitch * ((long long)j + g.rows * (long long)k);
+        Resid<T, ND, IB> r = residual_at<T, ND, IB>(g, p, f, I);
+        bool cx = i <= g.n[0], cy = j <= g.n[1], cz = ND == 3 ? k <= g.n[2] : true;
+        // r_P at (C,C,C)
+        if (cx && cy && cz) {
+            double v = fabs(double(r.rP));
+            mx[0] = nmax(mx[0], v);
+            ss[0] += double(r.rP) * double(r.rP);
+        }
+        // r_Vx at (V,C,C)
+        if (cy && cz) {
+            double v = double(r.rVx);
+            if ((i == 1 && wall0[0][0]) || (i == g.n[0] + 1 && wall0[0][1])) v = 0.0;
+            mx[1] = nmax(mx[1], fabs(v));
+            ss[1] += v * v;
+            vm[0] = nmax(vm[0], fabs(double(f.Vx[I])));
+        }
+        if (cx && cz) {
+            double v = double(r.rVy);
+            if ((j == 1 && wall0[1][0]) || (j == g.n[1] + 1 && wall0[1][1])) v = 0.0;
+            mx[2] = nmax(mx[2], fabs(v));
+            ss[2] += v * v;
+            vm[1] = nmax(vm[1], fabs(double(f.Vy[I])));
+        }
+        if (ND == 3 && cx && cy) {
+            double v = double(r.rVz);
+            if ((k == 1 && wall0[2][0]) || (k == g.n[2] + 1 && wall0[2][1])) v = 0.0;
+            mx[3] = nmax(mx[3], fabs(v));
+            ss[3] += v * v;
+            vm[2] = nmax(vm[2], fabs(double(f.Vz[I])));
+        }
+    }
+    __shared__ double sh[kNormThreads / 32][11];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    double vals[11] = {mx[0], mx[1], mx[2], mx[3], ss[0], ss[1], ss[2], ss[3], vm[0], vm[1], vm[2]};
+#pragma unroll
+    for (int q = 0; q < 11; q++) {
+        double v = (q >= 4 && q < 8) ? warp_sum(vals[q]) : warp_max(vals[q]);
+        if (lane == 0) sh[wid][q] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 11) {
+        int q = threadIdx.x;
+        double acc = sh[0][q];
+        for (int w = 1; w < kNormThreads / 32; w++) acc = (q >= 4 && q < 8) ? acc + sh[w][q] : nmax(acc, sh[w][q]);
+        partials[(long long)blockIdx.x * kNormSlots + q] = acc;
+    }
+}
+
+__global__ void norms_finalize_kernel(const double *partials, int nblocks, double *out) {
+    // one warp per slot; fixed-order per-lane strided sums then a fixed shuffle tree
+    int q = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (q >= 11) return;
+    double acc = (q >= 4 && q < 8) ? 0.0 : 0.0;
+    for (int b = lane; b < nblocks; b += 32) {
+        double v = partials[(long long)b * kNormSlots + q];
+        acc = (q >= 4 && q < 8) ? acc + v : nmax(acc, v);
+    }
+    acc = (q >= 4 && q < 8) ? warp_sum(acc) : warp_max(acc);
+    if (lane == 0) {
+        if (q >= 4 && q < 8) acc = sqrt(acc);
+        out[q] = acc;
+    }
+    if (threadIdx.x == 0) out[11] = 0.0;
+}
+
+__global__ void norms_flag_kernel(double *out) {
+    bool bad = false;
+    for (int q = 0; q < 11; q++) bad |= !isfinite(out[q]);
+    out[11] = bad ? 1.0 : 0.0;
+}
+
+}  // namespace
+
+int norm_blocks(const Geom &g) {
+    long long total = (long long)(g.n[0] + 1) * (g.n[1] + 1) * (g.nd == 3 ? g.n[2] + 1 : 1);
+    long long b = (total + kNormThreads * 8 - 1) / (kNormThreads * 8);
+    if (b < 1) b = 1;
+    if (b > 148 * 8) b = 148 * 8;
+    return (int)b;
+}
+
+template <typename T>
+cudaError_t launch_update_sigma(const Geom &g, const KParams &p, const Ptrs<T> &f, bool ib, cudaStream_t s) {
+    dim3 blk(32, 8);
+    dim3 grd = vertex_grid(g, blk);
+    if (g.nd == 2) update_sigma_kernel<T, 2, false><<<grd, blk, 0, s>>>(g, p, f);
+    else if (ib) update_sigma_kernel<T, 3, true><<<grd, blk, 0, s>>>(g, p, f);
+    else update_sigma_kernel<T, 3, false><<<grd, blk, 0, s>>>(g, p, f);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_update_V(const Geom &g, const KParams &p, const Ptrs<T> &f, bool ib, cudaStream_t s) {
+    dim3 blk(32, 8);
+    dim3 grd = vertex_grid(g, blk);
+    if (g.nd == 2) update_V_kernel<T, 2, false><<<grd, blk, 0, s>>>(g, p, f);
+    else if (ib) update_V_kernel<T, 3, true><<<grd, blk, 0, s>>>(g, p, f);
+    else update_V_kernel<T, 3, false><<<grd, blk, 0, s>>>(g, p, f);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_compute_residuals(const Geom &g, const KParams &p, const Ptrs<T> &f, bool ib, cudaStream_t s) {
+    dim3 blk(32, 8);
+    dim3 grd = vertex_grid(g, blk);
+    if (g.nd == 2) compute_residuals_kernel<T, 2, false><<<grd, blk, 0, s>>>(g, p, f);
+    else if (ib) compute_residuals_kernel<T, 3, true><<<grd, blk, 0, s>>>(g, p, f);
+    else compute_residuals_kernel<T, 3, false><<<grd, blk, 0, s>>>(g, p, f);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_compute_tau(const Geom &g, const KParams &p, const Ptrs<T> &f, cudaStream_t s) {
+    dim3 blk(32, 8);
+    dim3 grd = vertex_grid(g, blk);
+    if (g.nd == 2) compute_tau_kernel<T, 2><<<grd, blk, 0, s>>>(g, p, f);
+    else compute_tau_kernel<T, 3><<<grd, blk, 0, s>>>(g, p, f);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_bc_batch(const Geom &g, const BcBatch &b, cudaStream_t s) {
+    if (b.count == 0) return cudaSuccess;
+    int e1 = -1, e2 = -1;
+    for (int e = 0; e < g.nd; e++) {
+        if (e == b.dim) continue;
+        if (e1 < 0) e1 = e;
+        else e2 = e;
+    }
+    int na = g.n[e1] + 3, nc = e2 >= 0 ? g.n[e2] + 3 : 1;
+    dim3 blk(32, 8);
+    dim3 grd((na + 31) / 32, (nc + 7) / 8);
+    bc_dim_kernel<T><<<grd, blk, 0, s>>>(g, b);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_residual_norms(const Geom &g, const KParams &p, const Ptrs<T> &f, bool ib, double *partials,
+                                  int nblocks, double *out_dev, cudaStream_t s) {
+    if (g.nd == 2) residual_norms_kernel<T, 2, false><<<nblocks, kNormThreads, 0, s>>>(g, p, f, partials);
+    else if (ib) residual_norms_kernel<T, 3, true><<<nblocks, kNormThreads, 0, s>>>(g, p, f, partials);
+    else residual_norms_kernel<T, 3, false><<<nblocks, kNormThreads, 0, s>>>(g, p, f, partials);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    norms_finalize_kernel<<<1, 11 * 32, 0, s>>>(partials, nblocks, out_dev);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    norms_flag_kernel<<<1, 1, 0, s>>>(out_dev);
+    return cudaGetLastError();
+}
+
+#define FI_INST(T)                                                                                                \
+    template cudaError_t launch_update_sigma<T>(const Geom &, const KParams &, const Ptrs<T> &, bool, cudaStream_t); \
+    template cudaError_t launch_update_V<T>(const Geom &, const KParams &, const Ptrs<T> &, bool, cudaStream_t);     \
+    template cudaError_t launch_compute_residuals<T>(const Geom &, const KParams &, const Ptrs<T> &, bool,          \
+                                                     cudaStream_t);                                               \
+    template cudaError_t launch_compute_tau<T>(const Geom &, const KParams &, const Ptrs<T> &, cudaStream_t);       \
+    template cudaError_t launch_bc_batch<T>(const Geom &, const BcBatch &, cudaStream_t);                          \
+    template cudaError_t launch_residual_norms<T>(const Geom &, const KParams &, const Ptrs<T> &, bool, double *,  \
+                                                  int, double *, cudaStream_t);
+FI_INST(double)
+FI_INST(float)
+#undef FI_INST
+
+}  // namespace fi

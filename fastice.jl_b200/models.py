@@ -1,0 +1,342 @@
+"""Host mirror of FastIce's Stokes models over the C ABI.
+
+``IsothermalFullStokesModel`` mirrors src/Models/FullStokes/Isothermal/Isothermal.jl:22-125
+and ``IsothermalImmersedBoundaryFullStokesModel`` mirrors
+src/Models/ImmersedBoundaryFullStokes/Isothermal/Isothermal.jl:22-136.  The
+library owns the device fields; the attribute tree ``model.stress.P``,
+``model.stress.τ.xx``, ``model.velocity.V.x``, ``model.viscosity.η``,
+``model.residual.r_P``, ``model.field_masks.na.ccc`` gives ``FieldRef`` handles
+whose ``interior()`` / ``set(...)`` copy to and from host numpy arrays (numpy
+order (z, y, x), i.e. x fastest as in Julia).
+
+``advance_iteration(model, t, Δt)`` and ``compute_residuals(model)`` are the
+reference's ``advance_iteration!`` / ``compute_residuals!``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from types import SimpleNamespace
+from typing import Optional
+
+import numpy as np
+
+from . import _lib as L
+from .grids import UniformGrid
+from .physics import (ArrayField, BoundaryCondition, FunctionField, Periodic, ValueField, rheology_desc)
+
+_DTYPES = {"f64": (L.FI_F64, np.float64), "f32": (L.FI_F32, np.float32)}
+_PATHS = {"auto": L.FI_PATH_AUTO, "reference": L.FI_PATH_REFERENCE, "fused": L.FI_PATH_FUSED}
+
+
+class Arch:
+    """``Arch(CUDABackend())``: one CUDA device."""
+
+    def __init__(self, backend: str = "cuda", device: int = 0):
+        if backend != "cuda":
+            raise ValueError("libfastice_b200 runs on CUDA devices only (no CPU backend)")
+        self.device = int(device)
+
+
+class FieldRef:
+    """Handle to one device field of a model."""
+
+    def __init__(self, model: "_StokesBase", name: str):
+        self.model = model
+        self.name = name
+
+    @property
+    def location(self):
+        return L.FIELD_LOC[self.name]
+
+    def shape(self):
+        g = self.model.grid
+        loc = self.location
+        return tuple(g.dims[d] + loc[d] for d in reversed(range(g.ndims)))
+
+    def interior(self) -> np.ndarray:
+        return self.model.get_field(self.name)
+
+    def set(self, value) -> None:
+        self.model.set_field(self.name, value)
+
+    def __array__(self, dtype=None):
+        a = self.interior()
+        return a if dtype is None else a.astype(dtype)
+
+    def __repr__(self):
+        return f"FieldRef({self.name}, shape={self.shape()})"
+
+
+def _ns(**kw):
+    return SimpleNamespace(**kw)
+
+
+def _bc_struct(bc) -> L.fi_bc:
+    s = L.fi_bc()
+    if not isinstance(bc, BoundaryCondition):
+        raise TypeError("boundary conditions must be BoundaryCondition objects")
+    s.kind = bc.kind.kind
+    for i, c in enumerate(bc.components[:3]):
+        s.c[i] = c
+    return s
+
+
+def _dtau(solver_params, nd):
+    sp = solver_params or {}
+    dt = sp.get("Δτ", sp.get("dtau"))
+    if dt is None:
+        raise ValueError("solver_params must contain Δτ = (Pr=..., τ=(xx=...,...), V=(x=...,...))")
+    p = L.fi_pt_params()
+    p.dt_P = float(dt["Pr"])
+    tau = dt.get("τ", dt.get("tau"))
+    V = dt["V"]
+    for i, k in enumerate(("xx", "yy", "zz", "xy", "xz", "yz")):
+        if k in tau:
+            p.dt_tau[i] = float(tau[k])
+    for i, k in enumerate(("x", "y", "z")[:nd]):
+        p.dt_V[i] = float(V[k])
+    return p
+
+
+class _StokesBase:
+    immersed = False
+
+    def __init__(self, *, grid: UniformGrid, boundary_conditions, gravity, rheology, solver_params, arch=None,
+                 dtype: str = "f64", path: str = "auto", outer_width=None, level_sets=None, library: str = "fast"):
+        self.lib = L.load(library)
+        self.grid = grid
+        self.arch = arch or Arch()
+        self.dtype = dtype
+        self.np_dtype = _DTYPES[dtype][1]
+        self.boundary_conditions = boundary_conditions
+        self.gravity = gravity
+        self.rheology = rheology
+        self.solver_params = solver_params
+        self.level_sets = level_sets
+        self.outer_width = outer_width  # accepted for signature parity; the fused sweep has no inner/outer split
+        nd = grid.ndims
+        d = L.fi_model_desc()
+        d.grid.nd = nd
+        for k in range(nd):
+            d.grid.n[k] = grid.dims[k]
+            d.grid.origin[k] = grid.origin[k]
+            d.grid.extent[k] = grid.extent[k]
+        names = ("x", "y", "z")[:nd]
+        for k, nm in enumerate(names):
+            left, right = boundary_conditions[nm]
+            d.bc[k][0] = _bc_struct(left)
+            d.bc[k][1] = _bc_struct(right)
+        field_inputs = {}
+        for k, nm in enumerate(names):
+            g = gravity.get(nm, 0.0) if isinstance(gravity, dict) else getattr(gravity, nm)
+            if isinstance(g, (int, float)):
+                d.gravity.kind[k], d.gravity.value[k] = L.FI_G_VALUE, float(g)
+            elif isinstance(g, ValueField):
+                d.gravity.kind[k], d.gravity.value[k] = L.FI_G_VALUE, g.value
+            else:
+                d.gravity.kind[k] = L.FI_G_FIELD
+                field_inputs["g" + nm] = g
+        d.rheology, rfields = rheology_desc(rheology)
+        field_inputs.update(rfields)
+        d.dtau = _dtau(solver_params, nd)
+        d.dtype = _DTYPES[dtype][0]
+        d.immersed = 1 if self.immersed else 0
+        d.path = _PATHS[path]
+        d.device = self.arch.device
+        self._desc = d
+        h = C.c_void_p()
+        L.check(self.lib, self.lib.fi_model_create(C.byref(d), C.byref(h)))
+        self._h = h
+        for name, src in field_inputs.items():
+            self._upload_input(name, src)
+        self._build_tree()
+
+    # -- lifecycle ---------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.fi_model_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- field access --------------------------------------------------------
+    def _build_tree(self):
+        f = lambda n: FieldRef(self, n)
+        nd = self.grid.ndims
+        if nd == 3:
+            tau = _ns(xx=f("txx"), yy=f("tyy"), zz=f("tzz"), xy=f("txy"), xz=f("txz"), yz=f("tyz"))
+            V = _ns(x=f("Vx"), y=f("Vy"), z=f("Vz"))
+            rV = _ns(x=f("rVx"), y=f("rVy"), z=f("rVz"))
+        else:
+            tau = _ns(xx=f("txx"), yy=f("tyy"), xy=f("txy"))
+            V = _ns(x=f("Vx"), y=f("Vy"))
+            rV = _ns(x=f("rVx"), y=f("rVy"))
+        self.stress = _ns(P=f("P"), Pr=f("P"), τ=tau, tau=tau)
+        self.velocity = _ns(V=V)
+        self.viscosity = _ns(η=f("eta"), η_next=f("eta_next"), eta=f("eta"), eta_next=f("eta_next"))
+        self.residual = _ns(r_V=rV, r_P=f("rP"), r_Pr=f("rP"))
+        if self.immersed:
+            comps = ("ccc", "vvv", "vcc", "cvc", "ccv", "vvc", "vcv", "cvv")
+            self.field_masks = _ns(na=_ns(**{c: f("na_" + c) for c in comps}),
+                                   ns=_ns(**{c: f("ns_" + c) for c in comps}))
+
+    def field_shape(self, name):
+        loc = L.FIELD_LOC[name]
+        return tuple(self.grid.dims[d] + loc[d] for d in reversed(range(self.grid.ndims)))
+
+    def set_field(self, name: str, value) -> None:
+        shape = self.field_shape(name)
+        if np.isscalar(value):
+            arr = np.full(shape, value, dtype=self.np_dtype)
+        else:
+            arr = np.ascontiguousarray(np.asarray(value, dtype=self.np_dtype))
+            if arr.shape != shape:
+                arr = np.ascontiguousarray(np.broadcast_to(arr, shape))
+        L.check(self.lib, self.lib.fi_model_set_field(self._h, L.FIELD_ID[name], arr.ctypes.data, arr.nbytes))
+
+    def get_field(self, name: str) -> np.ndarray:
+        arr = np.empty(self.field_shape(name), dtype=self.np_dtype)
+        L.check(self.lib, self.lib.fi_model_get_field(self._h, L.FIELD_ID[name], arr.ctypes.data, arr.nbytes))
+        return arr
+
+    def _upload_input(self, name, src):
+        if isinstance(src, FunctionField):
+            full = src.sample(halo=True)
+            sl = tuple(slice(1, s + 1) for s in self.field_shape(name))
+            self.set_field(name, full[sl])
+        elif isinstance(src, ArrayField):
+            self.set_field(name, src.values)
+        elif isinstance(src, np.ndarray):
+            self.set_field(name, src)
+        else:
+            raise TypeError(f"cannot use {type(src).__name__} as the input field {name}")
+
+    # -- reference operations ---------------------------------------------------
+    def apply_bcs(self):
+        L.check(self.lib, self.lib.fi_model_apply_bcs(self._h))
+
+    def advance(self, niter: int = 1):
+        L.check(self.lib, self.lib.fi_model_advance(self._h, int(niter)))
+
+    def compute_residuals(self):
+        L.check(self.lib, self.lib.fi_model_compute_residuals(self._h))
+
+    def residual_norms(self) -> np.ndarray:
+        out = (C.c_double * L.FI_NORMS_LEN)()
+        L.check(self.lib, self.lib.fi_model_residual_norms(self._h, out))
+        return np.array(out[:], dtype=np.float64)
+
+    def compute_tau(self):
+        L.check(self.lib, self.lib.fi_model_compute_tau(self._h))
+
+    def synchronize(self):
+        L.check(self.lib, self.lib.fi_model_synchronize(self._h))
+
+    @property
+    def path(self) -> str:
+        v = C.c_int32()
+        L.check(self.lib, self.lib.fi_model_path(self._h, C.byref(v)))
+        return {L.FI_PATH_REFERENCE: "reference", L.FI_PATH_FUSED: "fused"}[v.value]
+
+    @property
+    def stream_ptr(self) -> int:
+        s = C.c_void_p()
+        L.check(self.lib, self.lib.fi_model_stream(self._h, C.byref(s)))
+        return s.value or 0
+
+    def device_ptr(self, name: str) -> int:
+        p = C.c_void_p()
+        L.check(self.lib, self.lib.fi_model_device_ptr(self._h, L.FIELD_ID[name], C.byref(p)))
+        return p.value or 0
+
+    def layout(self):
+        a, b, c = C.c_size_t(), C.c_size_t(), C.c_size_t()
+        L.check(self.lib, self.lib.fi_model_layout(self._h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
+    def solve(self, *, max_iter: int, ncheck: int, tol: float, measure: str = "abs_inf", rho_g_inf: float = 1.0,
+              length_z: float = 1.0):
+        """Driver loop with a convergence check every ``ncheck`` iterations
+        (tm_stokes_chmy.jl:283-305); returns a dict report."""
+        o = L.fi_solve_opts()
+        o.max_iter, o.ncheck, o.tol = int(max_iter), int(ncheck), float(tol)
+        o.measure = {"abs_inf": L.FI_CONV_ABS_INF, "rel_slab": L.FI_CONV_REL_SLAB}[measure]
+        o.rho_g_inf, o.length_z = float(rho_g_inf), float(length_z)
+        o.mode = L.FI_SOLVE_PLAIN
+        r = L.fi_solve_report()
+        st = self.lib.fi_model_solve(self._h, C.byref(o), C.byref(r))
+        if st not in (L.FI_OK, L.FI_ERR_TIMEOUT):
+            L.check(self.lib, st)
+        return {"iterations": r.iterations, "measure": r.measure, "norms": list(r.norms), "seconds": r.seconds,
+                "converged": bool(r.converged)}
+
+
+class IsothermalFullStokesModel(_StokesBase):
+    """``IsothermalFullStokesModel(; arch, grid, boundary_conditions, gravity,
+    rheology, solver_params, outer_width)`` (FullStokes/Isothermal/Isothermal.jl:60-89)."""
+
+    immersed = False
+
+
+class IsothermalImmersedBoundaryFullStokesModel(_StokesBase):
+    """``IsothermalImmersedBoundaryFullStokesModel(; ..., level_sets)``
+    (ImmersedBoundaryFullStokes/Isothermal/Isothermal.jl:63-98).  The volume
+    fractions ``field_masks.na`` / ``field_masks.ns`` are filled with
+    :func:`omega_from_psi` or set directly."""
+
+    immersed = True
+
+    def omega_from_psi(self, group: str, psi_halo: np.ndarray) -> None:
+        """ω_from_ψ!(arch, launch, model.field_masks.<group>, ψ, grid) on the device."""
+        psi = np.ascontiguousarray(psi_halo, dtype=np.float64)
+        n = self.grid.dims
+        if psi.shape != (n[2] + 3, n[1] + 3, n[0] + 3):
+            raise ValueError("psi must be a vertex field in halo storage (n+3 per dim)")
+        L.check(self.lib, self.lib.fi_model_volfrac_from_levelset(self._h, {"na": 0, "ns": 1}[group], psi.ctypes.data))
+
+
+# -- free functions with the reference names ----------------------------------------
+def advance_iteration(model: _StokesBase, t: float = 0.0, dt: float = 1.0) -> None:
+    """``advance_iteration!(model, t, Δt)`` (t and Δt are unused, as in the reference)."""
+    model.advance(1)
+
+
+def compute_residuals(model: _StokesBase) -> None:
+    """``compute_residuals!(model)``: fills ``model.residual``."""
+    model.compute_residuals()
+
+
+def set_(field: FieldRef, value) -> None:
+    """``set!(field, value)``."""
+    field.set(value)
+
+
+def interior(field: FieldRef) -> np.ndarray:
+    """``Array(interior(field))``."""
+    return field.interior()
+
+
+def pt_params(grid: UniformGrid, r: float = 0.7, re_mech: float = 8 * math.pi, vdtau_factor: float = 1.1,
+              use_center_spacing: bool = True) -> dict:
+    """Pseudo-transient steps as the drivers compute them
+    (stokes_manufactured_solution_free_slip_2D.jl:67-77; tm_stokes_chmy.jl:48-54 uses
+    re_mech=2π and factor 1.5): returns solver_params with Δτ."""
+    nd = grid.ndims
+    ltau = min(grid.extent) / re_mech
+    vdtau = min(grid.spacing()) / math.sqrt(nd * vdtau_factor)
+    theta = ltau * (r + 4 / 3) / vdtau
+    dt_r = 1.0 / (theta + 1.0)
+    nudt = vdtau * ltau
+    taus = ("xx", "yy", "zz", "xy", "xz", "yz") if nd == 3 else ("xx", "yy", "xy")
+    return {"Δτ": {"Pr": r / theta, "τ": {k: dt_r for k in taus}, "V": {k: nudt for k in ("x", "y", "z")[:nd]}}}

@@ -1,0 +1,248 @@
+/*
+ * fastice_b200.h -- C ABI of libfastice_b200, a B200 (sm_100a) implementation of
+ * the FastIce.jl pseudo-transient (PT) Stokes iteration.
+ *
+ * The ABI is shaped for a Julia `ccall` shim that keeps FastIce's API: plain C
+ * types, opaque handles and host pointers; no CUDA, torch or C++ types cross
+ * it.  Each entry point names the reference (PTsolvers/FastIce.jl v0.3.3)
+ * function it replaces.  All functions return an fi_status; fi_last_error()
+ * gives the message of the last failure on the calling thread.
+ *
+ * Data layout.  A model owns its device fields.  Host arrays passed to
+ * fi_model_set_field / fi_model_get_field hold a field's interior in Julia
+ * column-major order (x fastest), sized by the field's staggered location:
+ * n per Center dimension and n+1 per Vertex dimension -- exactly
+ * `Array(interior(field))` on the Julia side.
+ *
+ * Threading.  One CUDA stream per model.  fi_model_advance is asynchronous;
+ * functions returning host data synchronise the model's stream.  A model may be
+ * used by one thread at a time; distinct models are independent.
+ */
+#ifndef FASTICE_B200_H
+#define FASTICE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FI_ABI_VERSION 1
+
+/* ---- status codes (Julia exceptions in the reference, e.g. the
+ *      error("simulation failed") of scripts_future_API/tm_stokes_chmy.jl:104-106) */
+typedef enum {
+    FI_OK = 0,
+    FI_ERR_ARG = 1,         /* invalid argument or descriptor */
+    FI_ERR_OOM = 2,         /* device or host allocation failed, or over budget */
+    FI_ERR_DIVERGED = 3,    /* non-finite residual */
+    FI_ERR_TIMEOUT = 4,     /* iteration budget or bounded wait exhausted */
+    FI_ERR_CUDA = 5,        /* CUDA runtime error */
+    FI_ERR_UNSUPPORTED = 6, /* valid request this build does not implement */
+    FI_ERR_STATE = 7        /* call not valid in the object's current state */
+} fi_status;
+
+typedef enum { FI_F64 = 0, FI_F32 = 1 } fi_dtype;
+
+/* ---- boundary conditions: BoundaryCondition{Slip|Traction|Velocity}(components...)
+ *      src/Models/FullStokes/Isothermal/boundary_conditions.jl:1-13.  PERIODIC is
+ *      an extension (both sides of a dim must be PERIODIC). */
+typedef enum { FI_BC_SLIP = 0, FI_BC_TRACTION = 1, FI_BC_VELOCITY = 2, FI_BC_PERIODIC = 3 } fi_bc_kind;
+
+typedef struct {
+    int32_t kind;   /* fi_bc_kind */
+    double c[3];    /* components (x, y, z) */
+} fi_bc;
+
+/* ---- grid: Chmy UniformGrid(arch; origin, extent, dims) */
+typedef struct {
+    int32_t nd;        /* 2 or 3 */
+    int32_t n[3];      /* cells per dimension */
+    double origin[3];
+    double extent[3];
+} fi_grid;
+
+/* ---- rheology: src/Physics.jl.  inner law, optionally wrapped by
+ *      ViscoplasticRegularisation (:20-26) and then by Relaxation (:28-47, the
+ *      relaxed field being the model's current viscosity). */
+typedef enum { FI_RHEO_LINEAR = 0, FI_RHEO_POWER = 1 } fi_rheo_inner;
+typedef enum { FI_RELAX_NONE = 0, FI_RELAX_LIN = 1, FI_RELAX_LOG = 2, FI_RELAX_LOG10 = 3 } fi_relax;
+
+typedef struct {
+    int32_t inner;         /* fi_rheo_inner */
+    int32_t eta_is_field;  /* LinearViscousRheology(field): values via FI_FIELD_ETA_LIN */
+    double eta;            /* LinearViscousRheology(constant) */
+    int32_t A_is_field;    /* PowerLawRheology(A field): values via FI_FIELD_A */
+    double A;              /* PowerLawRheology A (constant) */
+    int32_t n;             /* PowerLawRheology exponent (integer) */
+    int32_t has_reg;       /* wrap in ViscoplasticRegularisation(., eta_reg) */
+    double eta_reg;
+    int32_t relax;         /* fi_relax */
+    double rate;
+} fi_rheology;
+
+/* ---- gravity (rho*g) per component: ZeroField/ValueField (value) or a field
+ *      sampled at the velocity component's location (FunctionField), set with
+ *      FI_FIELD_GX/GY/GZ. */
+typedef enum { FI_G_VALUE = 0, FI_G_FIELD = 1 } fi_gravity_kind;
+
+typedef struct {
+    int32_t kind[3];
+    double value[3];
+} fi_gravity;
+
+/* ---- PT pseudo-time steps: solver_params.Δτ = (Pr, τ = (xx, yy, zz, xy, xz, yz),
+ *      V = (x, y, z)), scripts_future_API/stokes_manufactured_solution_free_slip_2D.jl:67-77 */
+typedef struct {
+    double dt_P;
+    double dt_tau[6];
+    double dt_V[3];
+} fi_pt_params;
+
+/* kernel-path selection (fi_model_desc.path) */
+typedef enum {
+    FI_PATH_AUTO = 0,      /* fused single-pass sweep where supported, else reference-shaped */
+    FI_PATH_REFERENCE = 1, /* reference-shaped: update_sigma, BC batch, update_V, BC batch */
+    FI_PATH_FUSED = 2      /* fused sweep; FI_ERR_UNSUPPORTED if the problem is not covered */
+} fi_path;
+
+/* ---- model: IsothermalFullStokesModel(; arch, grid, boundary_conditions,
+ *      gravity, rheology, solver_params) (FullStokes/Isothermal/Isothermal.jl:60-89)
+ *      and IsothermalImmersedBoundaryFullStokesModel(; ..., level_sets)
+ *      (ImmersedBoundaryFullStokes/Isothermal/Isothermal.jl:63-98). */
+typedef struct {
+    fi_grid grid;
+    fi_bc bc[3][2];          /* [dim][side]: boundary_conditions = (x=(l,r), y=..., z=...) */
+    fi_gravity gravity;
+    fi_rheology rheology;
+    fi_pt_params dtau;
+    int32_t dtype;           /* fi_dtype */
+    int32_t immersed;        /* 1: immersed-boundary model (3D only), masks via FI_FIELD_NA_* / NS_* */
+    int32_t path;            /* fi_path */
+    int32_t device;          /* CUDA device ordinal */
+} fi_model_desc;
+
+typedef struct fi_model fi_model;
+
+/* field identifiers (model.stress.P, model.stress.τ.xx, ..., model.velocity.V.x,
+ * model.viscosity.η, model.residual.r_P, model.field_masks.na.ccc, ...) */
+typedef enum {
+    FI_FIELD_P = 0, FI_FIELD_TXX, FI_FIELD_TYY, FI_FIELD_TZZ, FI_FIELD_TXY, FI_FIELD_TXZ, FI_FIELD_TYZ,
+    FI_FIELD_VX, FI_FIELD_VY, FI_FIELD_VZ,
+    FI_FIELD_ETA, FI_FIELD_ETA_NEXT,
+    FI_FIELD_RP, FI_FIELD_RVX, FI_FIELD_RVY, FI_FIELD_RVZ,
+    FI_FIELD_GX, FI_FIELD_GY, FI_FIELD_GZ,
+    FI_FIELD_ETA_LIN, FI_FIELD_A,
+    FI_FIELD_NA_CCC, FI_FIELD_NA_VVV, FI_FIELD_NA_VCC, FI_FIELD_NA_CVC,
+    FI_FIELD_NA_CCV, FI_FIELD_NA_VVC, FI_FIELD_NA_VCV, FI_FIELD_NA_CVV,
+    FI_FIELD_NS_CCC, FI_FIELD_NS_VVV, FI_FIELD_NS_VCC, FI_FIELD_NS_CVC,
+    FI_FIELD_NS_CCV, FI_FIELD_NS_VVC, FI_FIELD_NS_VCV, FI_FIELD_NS_CVV,
+    FI_FIELD_COUNT
+} fi_field;
+
+/* length of the fi_model_residual_norms output: [0..3] inf-norms of r_P, r_Vx,
+ * r_Vy, r_Vz; [4..7] L2 norms of the same; [8..10] max |Vx|, |Vy|, |Vz|;
+ * [11] 1.0 if any value was non-finite. */
+#define FI_NORMS_LEN 12
+
+const char *fi_last_error(void);
+int fi_abi_version(void);
+
+/* IsothermalFullStokesModel(...) / IsothermalImmersedBoundaryFullStokesModel(...):
+ * allocates every field on the device, zero-filled. */
+fi_status fi_model_create(const fi_model_desc *desc, fi_model **out);
+fi_status fi_model_destroy(fi_model *m);
+
+/* set!(field, array) / Array(interior(field)): interior values, x fastest, in the
+ * model's dtype; nbytes must equal the field's interior size times sizeof(dtype). */
+fi_status fi_model_set_field(fi_model *m, int32_t field, const void *host, size_t nbytes);
+fi_status fi_model_get_field(fi_model *m, int32_t field, void *host, size_t nbytes);
+/* interior element count of a field (n or n+1 per dim by location) */
+fi_status fi_model_field_size(const fi_model *m, int32_t field, size_t *count);
+
+/* Ghost fill that drivers do after set!: stress and velocity BC batches and
+ * Neumann on η / η_next (tm_stokes_chmy.jl:273-281). */
+fi_status fi_model_apply_bcs(fi_model *m);
+
+/* advance_iteration!(model, t, Δt) repeated niter times
+ * (FullStokes/Isothermal/Isothermal.jl:91-112; IB: Isothermal.jl:100-122).
+ * Asynchronous on the model's stream. */
+fi_status fi_model_advance(fi_model *m, int32_t niter);
+
+/* compute_residuals!(model) (Isothermal.jl:114-125): writes r_P and r_V fields. */
+fi_status fi_model_compute_residuals(fi_model *m);
+
+/* compute_residuals!(model) followed by norm(r, Inf) / norm(r, 2) of every
+ * component (tm_stokes_chmy.jl:286-290), fused: no residual field is written.
+ * Synchronises; out has FI_NORMS_LEN doubles. */
+fi_status fi_model_residual_norms(fi_model *m, double *out);
+
+/* compute_τ! helper (kernels_3d.jl:225-245, kernels_2d.jl:33-44): τ = 2η dev(ε̇). */
+fi_status fi_model_compute_tau(fi_model *m);
+
+/* Driver loop (tm_stokes_chmy.jl:283-305): advance, every ncheck iterations take
+ * the residual norms, stop when the convergence measure drops below tol or after
+ * max_iter iterations.  FI_ERR_DIVERGED on a non-finite residual. */
+typedef enum { FI_CONV_ABS_INF = 0, FI_CONV_REL_SLAB = 1 } fi_conv_measure;
+typedef enum { FI_SOLVE_PLAIN = 0, FI_SOLVE_MIXED = 1 } fi_solve_mode;
+
+typedef struct {
+    int32_t max_iter;
+    int32_t ncheck;
+    double tol;
+    int32_t measure;        /* fi_conv_measure */
+    double rho_g_inf;       /* FI_CONV_REL_SLAB: ||ρg||∞ */
+    double length_z;        /* FI_CONV_REL_SLAB: L_z */
+    int32_t mode;           /* fi_solve_mode: MIXED = FP32 sweeps in FP64 defect correction */
+    int32_t inner_iter;     /* MIXED: FP32 sweeps per correction */
+    double inner_reduction; /* MIXED: stop a correction once its residual dropped by this factor */
+} fi_solve_opts;
+
+typedef struct {
+    int32_t iterations;     /* PT sweeps (all precisions) */
+    int32_t outer;          /* defect-correction steps (MIXED) */
+    double measure;         /* final convergence measure */
+    double norms[FI_NORMS_LEN];
+    double seconds;         /* wall time of the solve */
+    int32_t converged;
+} fi_solve_report;
+
+fi_status fi_model_solve(fi_model *m, const fi_solve_opts *opts, fi_solve_report *rep);
+
+/* swap-free view of the model state for callers that manage device memory:
+ * device pointer of a field's storage (uniform halo box, see fi_model_layout). */
+fi_status fi_model_device_ptr(fi_model *m, int32_t field, void **dptr);
+/* storage box: pitch (elements per x row, >= n0+3), rows per plane (n1+3),
+ * planes (n2+3, 1 in 2D); index (i,j,k) -> i + pitch*(j + rows*k), 0 = ghost. */
+fi_status fi_model_layout(const fi_model *m, size_t *pitch, size_t *rows, size_t *planes);
+/* cudaStream_t of the model, as void* */
+fi_status fi_model_stream(const fi_model *m, void **stream);
+fi_status fi_model_synchronize(fi_model *m);
+/* which kernel path the model runs (fi_path, never AUTO) */
+fi_status fi_model_path(const fi_model *m, int32_t *path);
+
+/* ---- level sets and volume fractions (setup path) --------------------------- */
+
+/* ω_from_ψ!(arch, launch, ω, ψ, grid) (LevelSets/volume_fractions_kernels.jl:228-237):
+ * psi is the level set at grid vertices in halo storage of a model's grid
+ * ((n0+3) x (n1+3) x (n2+3), x fastest, ghosts filled); writes the model's
+ * mask group (0 = na, 1 = ns), all 8 components (4 in 2D is not supported). */
+fi_status fi_model_volfrac_from_levelset(fi_model *m, int32_t group, const double *psi_host);
+
+/* compute_levelset_from_dem!(arch, launch, Ψ, dem, dem_grid2D, grid, R)
+ * (LevelSets/compute_levelsets.jl:113-117) followed by invert_levelset! when
+ * invert != 0 (:124-127).  dem: vertex values of the 2D DEM grid in halo storage
+ * ((m0+3) x (m1+3), x fastest, valid up to index m+2); R: row-major 3x3 or NULL
+ * (identity).  psi_host receives the 3D vertex level set in halo storage. */
+fi_status fi_levelset_from_dem(const fi_grid *grid3, const fi_grid *dem_grid2, const double *dem_host,
+                               const double *R, int32_t invert, double *psi_host, int32_t device);
+
+/* Standalone ω_from_ψ! on host arrays (3D: 8 outputs ccc vvv vcc cvc ccv vvc
+ * vcv cvv; 2D: 4 outputs cc vv vc cv), halo storage, FP64. */
+fi_status fi_volfrac(const fi_grid *grid, const double *psi_host, double **w_host, int32_t device);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FASTICE_B200_H */
