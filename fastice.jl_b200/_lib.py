@@ -115,6 +115,10 @@ SIGNATURES = [
     ("fi_levelset_from_dem", C.c_int, [C.POINTER(fi_grid), C.POINTER(fi_grid), C.c_void_p, C.c_void_p, C.c_int32,
                                        C.c_void_p, C.c_int32]),
     ("fi_volfrac", C.c_int, [C.POINTER(fi_grid), C.c_void_p, C.POINTER(C.c_void_p), C.c_int32]),
+    ("fi_fused_variant_count", C.c_int, []),
+    ("fi_fused_variant_name", C.c_char_p, [C.c_int32]),
+    ("fi_model_set_variant", C.c_int, [C.c_void_p, C.c_int32]),
+    ("fi_model_autotune", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
 ]
 
 _libs = {}

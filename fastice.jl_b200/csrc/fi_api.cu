@@ -59,6 +59,22 @@ float small_threshold_f32() {
     return t;
 }
 
+// field buffers: the field pointer sits kXOff elements past the allocation
+cudaError_t field_alloc(void **field_ptr, size_t elems, size_t esz) {
+    void *raw = nullptr;
+    cudaError_t e = cudaMalloc(&raw, (elems + 64) * esz);
+    if (e != cudaSuccess) {
+        *field_ptr = nullptr;
+        return e;
+    }
+    *field_ptr = (char *)raw + kXOff * esz;
+    return cudaSuccess;
+}
+void *field_raw(void *field_ptr, size_t esz) { return field_ptr ? (char *)field_ptr - kXOff * esz : nullptr; }
+void field_free(void *field_ptr, size_t esz) {
+    if (field_ptr) cudaFree(field_raw(field_ptr, esz));
+}
+
 }  // namespace
 
 struct fi_model {
@@ -78,8 +94,14 @@ struct fi_model {
     int nblk = 0;
     int path = FI_PATH_REFERENCE;
     int fused_variant = 0;
+    int maps_ty = -1;  // tile height the tensor maps were encoded for
     bool ib = false;
     long long iterations = 0;
+    int *d_err = nullptr;  // device error word written by bounded waits
+    // TMA maps (128 bytes each) of every buffer the fused sweep reads
+    alignas(64) unsigned char map_base[kState][128];
+    alignas(64) unsigned char map_alt[kState][128];
+    alignas(64) unsigned char map_eta[2][128];  // base[ETA], base[ETA_NEXT]
 
     bool is_f64() const { return d.dtype == FI_F64; }
 
@@ -176,9 +198,9 @@ fi_status ensure_residual_arrays(fi_model *m) {
     for (int f = FI_FIELD_RP; f <= FI_FIELD_RVZ; f++) {
         if (!field_used(m, f) || m->base[f]) continue;
         void *p = nullptr;
-        cudaError_t e = cudaMalloc(&p, m->elems * m->esz);
+        cudaError_t e = field_alloc(&p, m->elems, m->esz);
         if (e != cudaSuccess) return set_error("residual field allocation failed"), FI_ERR_OOM;
-        FI_CHECK_CUDA(cudaMemsetAsync(p, 0, m->elems * m->esz, m->stream), "memset");
+        FI_CHECK_CUDA(cudaMemsetAsync(field_raw(p, m->esz), 0, (m->elems + 64) * m->esz, m->stream), "memset");
         m->base[f] = p;
     }
     return FI_OK;
@@ -199,8 +221,9 @@ cudaMemcpy3DParms copy_params(const fi_model *m, int field, void *dev, void *hos
     size_t nx = m->d.grid.n[0] + loc[0], ny = m->d.grid.n[1] + loc[1], nz = nd == 3 ? m->d.grid.n[2] + loc[2] : 1;
     cudaMemcpy3DParms p{};
     cudaPitchedPtr hp = make_cudaPitchedPtr(host, nx * m->esz, nx, ny);
-    cudaPitchedPtr dp = make_cudaPitchedPtr(dev, (size_t)m->g.pitch * m->esz, (size_t)m->g.pitch, (size_t)m->g.rows);
-    cudaPos dpos = make_cudaPos(m->esz, 1, nd == 3 ? 1 : 0);
+    cudaPitchedPtr dp =
+        make_cudaPitchedPtr(field_raw(dev, m->esz), (size_t)m->g.pitch * m->esz, (size_t)m->g.pitch, (size_t)m->g.rows);
+    cudaPos dpos = make_cudaPos((size_t)(kXOff + 1) * m->esz, 1, nd == 3 ? 1 : 0);
     if (to_dev) {
         p.srcPtr = hp;
         p.dstPtr = dp;
@@ -350,7 +373,11 @@ fi_status advance_t(fi_model *m, int niter) {
             Ptrs<T> out = m->ptrs<T>(true);
             out.eta = in.eta;
             out.eta_next = in.eta_next;
-            FI_CHECK_CUDA(launch_fused3d<T>(m->g, m->kp, in, out, m->ib, m->fused_variant, m->stream), "fused sweep");
+            alignas(64) unsigned char maps[11][128];
+            for (int f = 0; f < kState; f++) std::memcpy(maps[f], m->parity ? m->map_alt[f] : m->map_base[f], 128);
+            std::memcpy(maps[10], m->map_eta[m->eta_swapped ? 1 : 0], 128);
+            FI_CHECK_CUDA(launch_fused3d<T>(m->g, m->kp, in, out, maps, m->fused_variant, m->d_err, m->stream),
+                          "fused sweep");
             m->parity ^= 1;
         } else {
             Ptrs<T> f = m->ptrs<T>();
@@ -367,6 +394,34 @@ fi_status advance_t(fi_model *m, int niter) {
     return FI_OK;
 }
 
+fi_status check_err_word(fi_model *m) {
+    int h = 0;
+    FI_CHECK_CUDA(cudaMemcpy(&h, m->d_err, sizeof(int), cudaMemcpyDeviceToHost), "error word");
+    if (h != 0) {
+        cudaMemset(m->d_err, 0, sizeof(int));
+        set_error("a bounded wait in the fused sweep expired; results of that launch are invalid");
+        return (fi_status)h;
+    }
+    return FI_OK;
+}
+
+// (re)encode the tensor maps of every buffer the fused sweep reads, for the
+// current variant's tile height
+fi_status encode_maps(fi_model *m) {
+    int ty = fused3d_variant_ty(m->fused_variant);
+    if (ty == m->maps_ty) return FI_OK;
+    for (int f = 0; f < kState; f++) {
+        if (!fused3d_encode_map(field_raw(m->base[f], m->esz), m->g, (int)m->esz, ty, m->map_base[f]) ||
+            !fused3d_encode_map(field_raw(m->alt[f], m->esz), m->g, (int)m->esz, ty, m->map_alt[f]))
+            return set_error("cuTensorMapEncodeTiled failed"), FI_ERR_CUDA;
+    }
+    if (!fused3d_encode_map(field_raw(m->base[FI_FIELD_ETA], m->esz), m->g, (int)m->esz, ty, m->map_eta[0]) ||
+        !fused3d_encode_map(field_raw(m->base[FI_FIELD_ETA_NEXT], m->esz), m->g, (int)m->esz, ty, m->map_eta[1]))
+        return set_error("cuTensorMapEncodeTiled failed"), FI_ERR_CUDA;
+    m->maps_ty = ty;
+    return FI_OK;
+}
+
 template <typename T>
 fi_status norms_t(fi_model *m, double *out) {
     Ptrs<T> f = m->ptrs<T>();
@@ -376,7 +431,7 @@ fi_status norms_t(fi_model *m, double *out) {
                   "norms copy");
     FI_CHECK_CUDA(cudaStreamSynchronize(m->stream), "norms sync");
     std::memcpy(out, m->h_out, FI_NORMS_LEN * sizeof(double));
-    return FI_OK;
+    return check_err_word(m);
 }
 
 template <typename T>
@@ -427,7 +482,7 @@ fi_status fi_model_create(const fi_model_desc *desc, fi_model **out) {
     Geom &g = m->g;
     g.nd = gr.nd;
     for (int k = 0; k < 3; k++) g.n[k] = k < gr.nd ? gr.n[k] : 0;
-    g.pitch = ((long long)gr.n[0] + 3 + 31) / 32 * 32;
+    g.pitch = ((long long)gr.n[0] + 3 + kXOff + 31) / 32 * 32;
     g.rows = gr.n[1] + 3;
     g.sxy = g.pitch * g.rows;
     g.planes = gr.nd == 3 ? gr.n[2] + 3 : 1;
@@ -479,25 +534,31 @@ fi_status fi_model_create(const fi_model_desc *desc, fi_model **out) {
     const size_t bytes = m->elems * m->esz;
     for (int f = 0; f < FI_FIELD_COUNT; f++) {
         if (!field_used(m, f) || is_residual(f)) continue;
-        if (cudaMalloc(&m->base[f], bytes) != cudaSuccess) {
+        if (field_alloc(&m->base[f], m->elems, m->esz) != cudaSuccess) {
             cudaGetLastError();
             set_error("device allocation failed (" + std::to_string(bytes) + " bytes per field)");
             return fail(FI_ERR_OOM);
         }
-        if (cudaMemsetAsync(m->base[f], 0, bytes, m->stream) != cudaSuccess)
+        if (cudaMemsetAsync(field_raw(m->base[f], m->esz), 0, bytes + 64 * m->esz, m->stream) != cudaSuccess)
             return fail(cuda_fail(cudaGetLastError(), "memset"));
     }
     if (m->path == FI_PATH_FUSED) {
         for (int f = 0; f < kState; f++) {
             if (!field_used(m, f)) continue;
-            if (cudaMalloc(&m->alt[f], bytes) != cudaSuccess) {
+            if (field_alloc(&m->alt[f], m->elems, m->esz) != cudaSuccess) {
                 cudaGetLastError();
                 set_error("device allocation failed (second state buffer)");
                 return fail(FI_ERR_OOM);
             }
-            if (cudaMemsetAsync(m->alt[f], 0, bytes, m->stream) != cudaSuccess)
+            if (cudaMemsetAsync(field_raw(m->alt[f], m->esz), 0, bytes + 64 * m->esz, m->stream) != cudaSuccess)
                 return fail(cuda_fail(cudaGetLastError(), "memset"));
         }
+    }
+    if (cudaMalloc(&m->d_err, sizeof(int)) != cudaSuccess) return fail(cuda_fail(cudaGetLastError(), "error word"));
+    cudaMemsetAsync(m->d_err, 0, sizeof(int), m->stream);
+    if (m->path == FI_PATH_FUSED) {
+        fi_status es = encode_maps(m);
+        if (es != FI_OK) return fail(es);
     }
     m->nblk = norm_blocks(g);
     if (cudaMalloc(&m->d_partials, (size_t)m->nblk * kNormSlots * sizeof(double)) != cudaSuccess ||
@@ -516,10 +577,9 @@ fi_status fi_model_destroy(fi_model *m) {
     if (!m) return FI_OK;
     cudaSetDevice(m->d.device);
     if (m->stream) cudaStreamSynchronize(m->stream);
-    for (int f = 0; f < FI_FIELD_COUNT; f++)
-        if (m->base[f]) cudaFree(m->base[f]);
-    for (int f = 0; f < kState; f++)
-        if (m->alt[f]) cudaFree(m->alt[f]);
+    for (int f = 0; f < FI_FIELD_COUNT; f++) field_free(m->base[f], m->esz);
+    for (int f = 0; f < kState; f++) field_free(m->alt[f], m->esz);
+    if (m->d_err) cudaFree(m->d_err);
     if (m->d_partials) cudaFree(m->d_partials);
     if (m->d_out) cudaFree(m->d_out);
     if (m->h_out) cudaFreeHost(m->h_out);
@@ -625,7 +685,7 @@ fi_status fi_model_stream(const fi_model *m, void **stream) {
 fi_status fi_model_synchronize(fi_model *m) {
     if (!m) return set_error("null model"), FI_ERR_ARG;
     FI_CHECK_CUDA(cudaStreamSynchronize(m->stream), "synchronize");
-    return FI_OK;
+    return check_err_word(m);
 }
 
 fi_status fi_model_path(const fi_model *m, int32_t *path) {
@@ -688,17 +748,19 @@ fi_status fi_model_volfrac_from_levelset(fi_model *m, int32_t group, const doubl
     void *dpsi = nullptr;
     void *tmp[8] = {};
     auto cleanup = [&]() {
-        if (dpsi) cudaFree(dpsi);
-        for (int c = 0; c < 8; c++)
-            if (tmp[c]) cudaFree(tmp[c]);
+        field_free(dpsi, sizeof(double));
+        for (int c = 0; c < 8; c++) field_free(tmp[c], sizeof(double));
     };
-    if (cudaMalloc(&dpsi, bytes) != cudaSuccess) return cleanup(), set_error("allocation failed"), FI_ERR_OOM;
-    cudaMemsetAsync(dpsi, 0, bytes, m->stream);
+    if (field_alloc(&dpsi, m->elems, sizeof(double)) != cudaSuccess)
+        return cleanup(), set_error("allocation failed"), FI_ERR_OOM;
+    cudaMemsetAsync(field_raw(dpsi, sizeof(double)), 0, bytes + 64 * sizeof(double), m->stream);
     // dense halo storage (n0+3) x (n1+3) x (n2+3) -> pitched storage
     cudaMemcpy3DParms cp{};
     size_t nx = (size_t)g.n[0] + 3, ny = (size_t)g.n[1] + 3, nz = (size_t)g.planes;
     cp.srcPtr = make_cudaPitchedPtr(const_cast<double *>(psi_host), nx * sizeof(double), nx, ny);
-    cp.dstPtr = make_cudaPitchedPtr(dpsi, (size_t)g.pitch * sizeof(double), (size_t)g.pitch, (size_t)g.rows);
+    cp.dstPtr = make_cudaPitchedPtr(field_raw(dpsi, sizeof(double)), (size_t)g.pitch * sizeof(double), (size_t)g.pitch,
+                                    (size_t)g.rows);
+    cp.dstPos = make_cudaPos((size_t)kXOff * sizeof(double), 0, 0);
     cp.extent = make_cudaExtent(nx * sizeof(double), ny, nz);
     cp.kind = cudaMemcpyHostToDevice;
     if (cudaMemcpy3DAsync(&cp, m->stream) != cudaSuccess) return cleanup(), cuda_fail(cudaGetLastError(), "psi upload");
@@ -708,8 +770,9 @@ fi_status fi_model_volfrac_from_levelset(fi_model *m, int32_t group, const doubl
         if (m->is_f64()) {
             w[c] = (double *)m->base[base + c];
         } else {
-            if (cudaMalloc(&tmp[c], bytes) != cudaSuccess) return cleanup(), set_error("allocation failed"), FI_ERR_OOM;
-            cudaMemsetAsync(tmp[c], 0, bytes, m->stream);
+            if (field_alloc(&tmp[c], m->elems, sizeof(double)) != cudaSuccess)
+                return cleanup(), set_error("allocation failed"), FI_ERR_OOM;
+            cudaMemsetAsync(field_raw(tmp[c], sizeof(double)), 0, bytes + 64 * sizeof(double), m->stream);
             w[c] = (double *)tmp[c];
         }
     }
@@ -729,5 +792,56 @@ fi_status fi_model_volfrac_from_levelset(fi_model *m, int32_t group, const doubl
     return FI_OK;
 }
 
-}  // extern "C"
+int fi_fused_variant_count(void) { return fused3d_num_variants(); }
+const char *fi_fused_variant_name(int32_t variant) { return fused3d_variant_name(variant); }
 
+fi_status fi_model_set_variant(fi_model *m, int32_t variant) {
+    if (!m || variant < 0 || variant >= fused3d_num_variants()) return set_error("bad argument"), FI_ERR_ARG;
+    if (m->path != FI_PATH_FUSED) return set_error("the model does not run the fused sweep"), FI_ERR_STATE;
+    FI_CHECK_CUDA(cudaSetDevice(m->d.device), "cudaSetDevice");
+    FI_CHECK_CUDA(cudaStreamSynchronize(m->stream), "sync");
+    m->fused_variant = variant;
+    return encode_maps(m);
+}
+
+fi_status fi_model_autotune(fi_model *m, int32_t iters, int32_t *best, double *ms) {
+    if (!m || iters <= 0) return set_error("bad argument"), FI_ERR_ARG;
+    if (m->path != FI_PATH_FUSED) return set_error("the model does not run the fused sweep"), FI_ERR_STATE;
+    FI_CHECK_CUDA(cudaSetDevice(m->d.device), "cudaSetDevice");
+    cudaEvent_t e0, e1;
+    FI_CHECK_CUDA(cudaEventCreate(&e0), "event");
+    FI_CHECK_CUDA(cudaEventCreate(&e1), "event");
+    int nv = fused3d_num_variants(), bestv = m->fused_variant;
+    double bestms = 1e300;
+    fi_status st = FI_OK;
+    for (int v = 0; v < nv && st == FI_OK; v++) {
+        st = fi_model_set_variant(m, v);
+        if (st != FI_OK) break;
+        st = fi_model_advance(m, 1);  // warm-up of this launch shape
+        if (st != FI_OK) break;
+        cudaEventRecord(e0, m->stream);
+        st = fi_model_advance(m, iters);
+        cudaEventRecord(e1, m->stream);
+        if (st != FI_OK) break;
+        if (cudaEventSynchronize(e1) != cudaSuccess) {
+            st = cuda_fail(cudaGetLastError(), "autotune sync");
+            break;
+        }
+        float t = 0.f;
+        cudaEventElapsedTime(&t, e0, e1);
+        double per = (double)t / iters;
+        if (ms) ms[v] = per;
+        if (per < bestms) {
+            bestms = per;
+            bestv = v;
+        }
+        st = check_err_word(m);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != FI_OK) return st;
+    if (best) *best = bestv;
+    return fi_model_set_variant(m, bestv);
+}
+
+}  // extern "C"

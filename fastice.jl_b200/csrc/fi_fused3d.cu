@@ -1,32 +1,45 @@
 // fi_fused3d.cu -- fused single-pass 3D PT iteration (update_σ! + stress BCs +
-// update_V! + velocity/η_next BCs in one kernel).
+// update_V! + velocity/η_next BCs in one kernel), TMA-staged.
 //
 // Reference semantics: src/Models/FullStokes/Isothermal/Isothermal.jl:91-112
 // with kernels_3d.jl:3-40 and boundary_conditions.jl.  The two reference
 // kernels touch the state twice per iteration (33 array passes); this sweep
-// touches it once (22 passes: P, τ(6), V(3) read + written, η read, η_next
-// written) by keeping the new stresses on chip.
+// reads P, τ(6), V(3), η once and writes P, τ(6), V(3), η_next once (22 passes).
 //
-// Work decomposition.  A CTA owns a TX x TY column of grid positions (x, y) and a
-// block of z planes [kb, ke).  It marches up in z: at step t it computes the new
-// stresses of plane t+1 on its column widened by one position on every side
-// (the ring is recomputed redundantly by neighbouring CTAs so that no grid-wide
-// synchronisation is needed), applies the stress boundary conditions to that
-// plane in shared memory, then updates V and η_next of plane t from the stress
-// planes t-1, t, t+1 held in shared-memory plane rings.
+// Work decomposition.  A CTA owns a 32 x TY column of grid positions (x, y) and a
+// block of z planes.  It marches up in z.  For every plane s the tensor-memory
+// accelerator copies an (x, y) box covering the column plus a one-position ring
+// of all eleven input fields (old P, τ, V, η; V.z one plane higher) into
+// shared-memory plane rings, one plane ahead of the compute, signalled by an
+// mbarrier.  The new stresses of plane s are computed in place over the column
+// (all seven components) and over the ring (only the components the velocity
+// update reads there), the stress boundary conditions are applied to the plane
+// in shared memory, and V / η_next of plane s-1 are updated from the stress
+// planes s-2, s-1, s.  Neighbouring CTAs recompute each other's ring: no
+// grid-wide synchronisation is needed.
 //
 // Double buffering.  Stresses and velocities are read from `in` and written to
-// `out` (distinct buffers), so a CTA never sees a value another CTA already
-// updated; the pointwise in-place updates of the reference are equivalent.
+// `out` (distinct buffers), so the pointwise in-place updates of the reference
+// are reproduced exactly.  With a no-FMA build the sweep matches the CPU oracle
+// bit for bit.
 //
 // Boundary conditions.  Stress BCs are applied per plane in the order x-faces,
 // y-faces, z-faces (a face of dim d spans all positions in the dims before d and
-// the field's interior in the dims after d), exactly as the CPU oracle does.
-// Velocity Dirichlet values are written at the boundary nodes; ghost values
-// (Velocity BC ghosts 2c - v, η_next Neumann copies, periodic images) are
-// written by the thread that computes the interior value they derive from.
-// Periodic dims (x, y) need no stress fix-up: the ring is computed from the
-// wrapped ghosts of the previous iteration.
+// the field's interior in the dims after d), as the CPU oracle does.  Velocity
+// Dirichlet values are written at the boundary nodes; ghost values (Velocity BC
+// ghosts 2c - v, η_next Neumann copies, periodic images) are written by the
+// thread that computes the interior value they derive from.  Periodic x / y need
+// no stress fix-up: ghost-ring stresses follow from the wrapped ghosts of the
+// previous iteration.
+//
+// Waits.  Every mbarrier wait is bounded (about one second of SM clock); on
+// expiry the CTA records FI_ERR_TIMEOUT in the model's error word, waits once
+// more (bounded) for its own copies in flight, and returns.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <cstdio>
+
 #include "fi_device.cuh"
 
 namespace fi {
@@ -34,204 +47,336 @@ namespace fi {
 namespace {
 
 constexpr int TX = 32;
+constexpr long long kWaitCycles = 1ll << 31;
 
 struct Variant {
     int ty;
     int zb;
 };
-constexpr Variant kVariants[] = {{8, 32}, {8, 64}, {8, 128}, {4, 64}, {16, 32}, {8, 16}};
+constexpr Variant kVariants[] = {{8, 32}, {8, 64}, {8, 128}, {4, 64}, {8, 16}};
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
-// shared-memory plane rings: field base plane and ring length
-enum { SL_P = 0, SL_ZZ = 3, SL_XX = 6, SL_YY = 8, SL_XY = 10, SL_XZ = 12, SL_YZ = 14, SL_COUNT = 16 };
-
+// TMA box width (elements) and position of the column's first x inside the box:
+// the box starts XB positions left of the column so that its global x coordinate
+// times the element size is a multiple of 16 bytes.
 template <typename T>
-struct BcSide {
-    int kind;
-    T c[3];
+struct BoxX;
+template <>
+struct BoxX<double> {
+    static constexpr int BX = 36, XB = 2;
+};
+template <>
+struct BoxX<float> {
+    static constexpr int BX = 40, XB = 4;
+};
+
+// shared-memory plane slots: ring base and length per field
+enum {
+    S_P = 0, R_P = 4,
+    S_ZZ = 4, R_ZZ = 4,
+    S_XX = 8, R_XX = 3,
+    S_YY = 11, R_YY = 3,
+    S_XY = 14, R_XY = 3,
+    S_XZ = 17, R_XZ = 3,
+    S_YZ = 20, R_YZ = 3,
+    S_VX = 23, R_VX = 3,
+    S_VY = 26, R_VY = 3,
+    S_VZ = 29, R_VZ = 4,
+    S_ET = 33, R_ET = 4,
+    S_COUNT = 37
+};
+constexpr int kBars = 3;
+
+template <typename T, int TY>
+struct Layout {
+    static constexpr int BX = BoxX<T>::BX;
+    static constexpr int XB = BoxX<T>::XB;
+    static constexpr int RY = TY + 2;
+    static constexpr int PLANE = BX * RY;  // elements in one box
+    static constexpr int PLANE_BYTES = PLANE * (int)sizeof(T);
+    static constexpr int SLOT = ((PLANE_BYTES + 127) / 128) * 128 / (int)sizeof(T);  // 128-byte aligned slots
+    static constexpr int NT = TX * TY;
+    static constexpr size_t SMEM = (size_t)S_COUNT * SLOT * sizeof(T) + 128;
+};
+
+// ---- PTX helpers (sm_90+ mbarrier / bulk tensor copy; no multicast) -------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// bounded wait; false on expiry
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity)) {
+        if (clock64() - t0 > kWaitCycles) return false;
+    }
+    return true;
+}
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
+            smem_u32(dst)),
+        "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// the eleven input maps of one sweep, in field order P, txx, tyy, tzz, txy, txz, tyz, Vx, Vy, Vz, eta
+struct InMaps {
+    CUtensorMap m[11];
 };
 
 template <typename T, int TY>
 struct Ctx {
-    static constexpr int RX = TX + 2;
-    static constexpr int RY = TY + 2;
-    static constexpr int RXY = RX * RY;
-    static constexpr int NT = TX * TY;
-
+    using Lay = Layout<T, TY>;
     T *sm;
     int i0, j0, kb, ke;
     int n0, n1, n2;
     long long sx, sxy;
     bool perx, pery;
-    BcSide<T> bc[3][2];
+    bool bnd_x, bnd_y;  // column touches an x / y boundary (needs fix-ups or ghost writes)
 
-    __device__ __forceinline__ int slot(int base, int len, int s) const { return (base + s % len) * RXY; }
-    __device__ __forceinline__ int rpos(int i, int j) const { return (j - j0 + 1) * RX + (i - i0 + 1); }
-    __device__ __forceinline__ T &P(int s, int i, int j) const { return sm[slot(SL_P, 3, s) + rpos(i, j)]; }
-    __device__ __forceinline__ T &Tzz(int s, int i, int j) const { return sm[slot(SL_ZZ, 3, s) + rpos(i, j)]; }
-    __device__ __forceinline__ T &Txx(int s, int i, int j) const { return sm[slot(SL_XX, 2, s) + rpos(i, j)]; }
-    __device__ __forceinline__ T &Tyy(int s, int i, int j) const { return sm[slot(SL_YY, 2, s) + rpos(i, j)]; }
-    __device__ __forceinline__ T &Txy(int s, int i, int j) const { return sm[slot(SL_XY, 2, s) + rpos(i, j)]; }
-    __device__ __forceinline__ T &Txz(int s, int i, int j) const { return sm[slot(SL_XZ, 2, s) + rpos(i, j)]; }
-    __device__ __forceinline__ T &Tyz(int s, int i, int j) const { return sm[slot(SL_YZ, 2, s) + rpos(i, j)]; }
+    __device__ __forceinline__ int at(int i, int j) const { return (j - j0 + 1) * Lay::BX + (i - i0 + Lay::XB); }
+    __device__ __forceinline__ T *slot(int base, int len, int p) const { return sm + (base + p % len) * Lay::SLOT; }
+    __device__ __forceinline__ T &P(int p, int i, int j) const { return slot(S_P, R_P, p)[at(i, j)]; }
+    __device__ __forceinline__ T &Tzz(int p, int i, int j) const { return slot(S_ZZ, R_ZZ, p)[at(i, j)]; }
+    __device__ __forceinline__ T &Txx(int p, int i, int j) const { return slot(S_XX, R_XX, p)[at(i, j)]; }
+    __device__ __forceinline__ T &Tyy(int p, int i, int j) const { return slot(S_YY, R_YY, p)[at(i, j)]; }
+    __device__ __forceinline__ T &Txy(int p, int i, int j) const { return slot(S_XY, R_XY, p)[at(i, j)]; }
+    __device__ __forceinline__ T &Txz(int p, int i, int j) const { return slot(S_XZ, R_XZ, p)[at(i, j)]; }
+    __device__ __forceinline__ T &Tyz(int p, int i, int j) const { return slot(S_YZ, R_YZ, p)[at(i, j)]; }
+    __device__ __forceinline__ T Vx(int p, int i, int j) const { return slot(S_VX, R_VX, p)[at(i, j)]; }
+    __device__ __forceinline__ T Vy(int p, int i, int j) const { return slot(S_VY, R_VY, p)[at(i, j)]; }
+    __device__ __forceinline__ T Vz(int p, int i, int j) const { return slot(S_VZ, R_VZ, p)[at(i, j)]; }
+    __device__ __forceinline__ T Eta(int p, int i, int j) const { return slot(S_ET, R_ET, p)[at(i, j)]; }
     __device__ __forceinline__ long long gidx(int i, int j, int k) const {
         return (long long)i + sx * (long long)j + sxy * (long long)k;
     }
-    // owner of an x (y) position: tile range, plus the ghosts beyond the domain
     __device__ __forceinline__ bool own_x(int i) const {
         if (i >= 1 && i <= n0 + 1) return i >= i0 && i < i0 + TX;
         if (i == 0) return i0 == 1;
-        return i == n0 + 2 && n0 + 1 < i0 + TX && n0 + 1 >= i0;
+        return i == n0 + 2 && n0 + 1 < i0 + TX;
     }
     __device__ __forceinline__ bool own_y(int j) const {
         if (j >= 1 && j <= n1 + 1) return j >= j0 && j < j0 + TY;
         if (j == 0) return j0 == 1;
-        return j == n1 + 2 && n1 + 1 < j0 + TY && n1 + 1 >= j0;
+        return j == n1 + 2 && n1 + 1 < j0 + TY;
     }
 };
 
 template <typename T>
 __device__ __forceinline__ T h(T x) { return T(0.5) * x; }
 
-template <typename T>
-__device__ __forceinline__ T ld(const T *p) { return __ldg(p); }
-
-// ---------------------------------------------------------------------------
-// new stresses of plane s on the widened column, BC fix-ups, owned writes
-// ---------------------------------------------------------------------------
+// issue the TMA copies of input group p (planes: σ_old(p), Vx(p), Vy(p), Vz(p+1), η(p))
 template <typename T, int TY>
-__device__ void sigma_plane(const Ctx<T, TY> &c, const KParams &p, const Ptrs<T> &in, const Ptrs<T> &out, int s) {
-    using C = Ctx<T, TY>;
-    const int tid = threadIdx.x;
+__device__ __forceinline__ void issue_group(const Ctx<T, TY> &c, const InMaps &mp, int p, bool full, uint64_t *bar) {
+    using Lay = Layout<T, TY>;
+    const int x = (int)kXOff + c.i0 - Lay::XB, y = c.j0 - 1;
+    const uint32_t bytes = (full ? 11u : 4u) * (uint32_t)Lay::PLANE_BYTES;
+    mbar_expect_tx(bar, bytes);
+    if (full) {
+        tma_load_3d(c.slot(S_P, R_P, p), &mp.m[0], x, y, p, bar);
+        tma_load_3d(c.slot(S_XX, R_XX, p), &mp.m[1], x, y, p, bar);
+        tma_load_3d(c.slot(S_YY, R_YY, p), &mp.m[2], x, y, p, bar);
+        tma_load_3d(c.slot(S_ZZ, R_ZZ, p), &mp.m[3], x, y, p, bar);
+        tma_load_3d(c.slot(S_XY, R_XY, p), &mp.m[4], x, y, p, bar);
+        tma_load_3d(c.slot(S_XZ, R_XZ, p), &mp.m[5], x, y, p, bar);
+        tma_load_3d(c.slot(S_YZ, R_YZ, p), &mp.m[6], x, y, p, bar);
+    }
+    tma_load_3d(c.slot(S_VX, R_VX, p), &mp.m[7], x, y, p, bar);
+    tma_load_3d(c.slot(S_VY, R_VY, p), &mp.m[8], x, y, p, bar);
+    tma_load_3d(c.slot(S_VZ, R_VZ, p + 1), &mp.m[9], x, y, p + 1, bar);
+    tma_load_3d(c.slot(S_ET, R_ET, p), &mp.m[10], x, y, p, bar);
+}
+
+// raw stress update of plane s at (i, j): which components is a compile-time mask
+enum { F_P = 1, F_XX = 2, F_YY = 4, F_ZZ = 8, F_XY = 16, F_XZ = 32, F_YZ = 64, F_ALL = 127 };
+
+template <typename T, int TY>
+__device__ __forceinline__ void sigma_point(const Ctx<T, TY> &c, const KParams &p, int s, int i, int j, int mask,
+                                            bool write_now, const Ptrs<T> &out) {
+    if (i > c.n0 + 2 || j > c.n1 + 2) return;
     const T idx = T(p.inv_dx[0]), idy = T(p.inv_dx[1]), idz = T(p.inv_dx[2]);
-    const long long sx = c.sx, sxy = c.sxy;
     const bool cz = s >= 1 && s <= c.n2, vz = s >= 1 && s <= c.n2 + 1;
-    for (int r = tid; r < C::RXY; r += C::NT) {
-        const int i = c.i0 - 1 + r % C::RX, j = c.j0 - 1 + r / C::RX;
-        T vP = T(0), vxx = T(0), vyy = T(0), vzz = T(0), vxy = T(0), vxz = T(0), vyz = T(0);
-        if (i <= c.n0 + 2 && j <= c.n1 + 2) {
-            const bool cx = (i >= 1 && i <= c.n0) || (c.perx && (i == 0 || i == c.n0 + 1));
-            const bool vx = i >= 1 && i <= c.n0 + 1;
-            const bool cy = (j >= 1 && j <= c.n1) || (c.pery && (j == 0 || j == c.n1 + 1));
-            const bool vy = j >= 1 && j <= c.n1 + 1;
-            const long long I = c.gidx(i, j, s);
-            const T *Vx = in.Vx, *Vy = in.Vy, *Vz = in.Vz, *eta = in.eta;
-            if (cx && cy && cz) {
-                T exx = (ld(Vx + I + 1) - ld(Vx + I)) * idx;
-                T eyy = (ld(Vy + I + sx) - ld(Vy + I)) * idy;
-                T ezz = (ld(Vz + I + sxy) - ld(Vz + I)) * idz;
-                T divV = exx + eyy + ezz;
-                T etac = ld(eta + I);
-                T P0 = ld(in.P + I), xx0 = ld(in.txx + I), yy0 = ld(in.tyy + I), zz0 = ld(in.tzz + I);
-                vP = P0 - divV * etac * T(p.dt_P);
-                vxx = xx0 - (xx0 - T(2.0) * etac * (exx - divV / T(3.0))) * T(p.dt_tau[0]);
-                vyy = yy0 - (yy0 - T(2.0) * etac * (eyy - divV / T(3.0))) * T(p.dt_tau[1]);
-                vzz = zz0 - (zz0 - T(2.0) * etac * (ezz - divV / T(3.0))) * T(p.dt_tau[2]);
-            }
-            if (vx && vy && cz) {
-                T exy = T(0.5) * ((ld(Vy + I) - ld(Vy + I - 1)) * idx + (ld(Vx + I) - ld(Vx + I - sx)) * idy);
-                T e_xy = h(h(ld(eta + I - 1 - sx) + ld(eta + I - sx)) + h(ld(eta + I - 1) + ld(eta + I)));
-                T xy0 = ld(in.txy + I);
-                vxy = xy0 - (xy0 - T(2.0) * e_xy * exy) * T(p.dt_tau[3]);
-            }
-            if (vx && cy && vz) {
-                T exz = T(0.5) * ((ld(Vz + I) - ld(Vz + I - 1)) * idx + (ld(Vx + I) - ld(Vx + I - sxy)) * idz);
-                T e_xz = h(h(ld(eta + I - 1 - sxy) + ld(eta + I - sxy)) + h(ld(eta + I - 1) + ld(eta + I)));
-                T xz0 = ld(in.txz + I);
-                vxz = xz0 - (xz0 - T(2.0) * e_xz * exz) * T(p.dt_tau[4]);
-            }
-            if (cx && vy && vz) {
-                T eyz = T(0.5) * ((ld(Vz + I) - ld(Vz + I - sx)) * idy + (ld(Vy + I) - ld(Vy + I - sxy)) * idz);
-                T e_yz = h(h(ld(eta + I - sx - sxy) + ld(eta + I - sxy)) + h(ld(eta + I - sx) + ld(eta + I)));
-                T yz0 = ld(in.tyz + I);
-                vyz = yz0 - (yz0 - T(2.0) * e_yz * eyz) * T(p.dt_tau[5]);
-            }
+    const bool cx = (i >= 1 && i <= c.n0) || (c.perx && (i == 0 || i == c.n0 + 1));
+    const bool vx = i >= 1 && i <= c.n0 + 1;
+    const bool cy = (j >= 1 && j <= c.n1) || (c.pery && (j == 0 || j == c.n1 + 1));
+    const bool vy = j >= 1 && j <= c.n1 + 1;
+    const int a = c.at(i, j);
+    if ((mask & (F_P | F_XX | F_YY | F_ZZ)) && cx && cy && cz) {
+        const T *vxs = c.slot(S_VX, R_VX, s), *vys = c.slot(S_VY, R_VY, s);
+        T exx = (vxs[a + 1] - vxs[a]) * idx;
+        T eyy = (vys[a + Ctx<T, TY>::Lay::BX] - vys[a]) * idy;
+        T ezz = (c.slot(S_VZ, R_VZ, s + 1)[a] - c.slot(S_VZ, R_VZ, s)[a]) * idz;
+        T divV = exx + eyy + ezz;
+        T etac = c.slot(S_ET, R_ET, s)[a];
+        if (mask & F_P) {
+            T &v = c.slot(S_P, R_P, s)[a];
+            v = v - divV * etac * T(p.dt_P);
         }
-        const int rp = r;
-        c.sm[c.slot(SL_P, 3, s) + rp] = vP;
-        c.sm[c.slot(SL_ZZ, 3, s) + rp] = vzz;
-        c.sm[c.slot(SL_XX, 2, s) + rp] = vxx;
-        c.sm[c.slot(SL_YY, 2, s) + rp] = vyy;
-        c.sm[c.slot(SL_XY, 2, s) + rp] = vxy;
-        c.sm[c.slot(SL_XZ, 2, s) + rp] = vxz;
-        c.sm[c.slot(SL_YZ, 2, s) + rp] = vyz;
+        if (mask & F_XX) {
+            T &v = c.slot(S_XX, R_XX, s)[a];
+            v = v - (v - T(2.0) * etac * (exx - divV / T(3.0))) * T(p.dt_tau[0]);
+        }
+        if (mask & F_YY) {
+            T &v = c.slot(S_YY, R_YY, s)[a];
+            v = v - (v - T(2.0) * etac * (eyy - divV / T(3.0))) * T(p.dt_tau[1]);
+        }
+        if (mask & F_ZZ) {
+            T &v = c.slot(S_ZZ, R_ZZ, s)[a];
+            v = v - (v - T(2.0) * etac * (ezz - divV / T(3.0))) * T(p.dt_tau[2]);
+        }
+    }
+    constexpr int BX = Ctx<T, TY>::Lay::BX;
+    if ((mask & F_XY) && vx && vy && cz) {
+        const T *vxs = c.slot(S_VX, R_VX, s), *vys = c.slot(S_VY, R_VY, s), *et = c.slot(S_ET, R_ET, s);
+        T exy = T(0.5) * ((vys[a] - vys[a - 1]) * idx + (vxs[a] - vxs[a - BX]) * idy);
+        T e_xy = h(h(et[a - 1 - BX] + et[a - BX]) + h(et[a - 1] + et[a]));
+        T &v = c.slot(S_XY, R_XY, s)[a];
+        v = v - (v - T(2.0) * e_xy * exy) * T(p.dt_tau[3]);
+    }
+    if ((mask & F_XZ) && vx && cy && vz) {
+        const T *vzs = c.slot(S_VZ, R_VZ, s), *et = c.slot(S_ET, R_ET, s), *etm = c.slot(S_ET, R_ET, s - 1);
+        T exz = T(0.5) * ((vzs[a] - vzs[a - 1]) * idx + (c.slot(S_VX, R_VX, s)[a] - c.slot(S_VX, R_VX, s - 1)[a]) * idz);
+        T e_xz = h(h(etm[a - 1] + etm[a]) + h(et[a - 1] + et[a]));
+        T &v = c.slot(S_XZ, R_XZ, s)[a];
+        v = v - (v - T(2.0) * e_xz * exz) * T(p.dt_tau[4]);
+    }
+    if ((mask & F_YZ) && cx && vy && vz) {
+        const T *vzs = c.slot(S_VZ, R_VZ, s), *et = c.slot(S_ET, R_ET, s), *etm = c.slot(S_ET, R_ET, s - 1);
+        T eyz = T(0.5) * ((vzs[a] - vzs[a - BX]) * idy + (c.slot(S_VY, R_VY, s)[a] - c.slot(S_VY, R_VY, s - 1)[a]) * idz);
+        T e_yz = h(h(etm[a - BX] + etm[a]) + h(et[a - BX] + et[a]));
+        T &v = c.slot(S_YZ, R_YZ, s)[a];
+        v = v - (v - T(2.0) * e_yz * eyz) * T(p.dt_tau[5]);
+    }
+    if (write_now) {
+        const long long I = c.gidx(i, j, s);
+        out.P[I] = c.slot(S_P, R_P, s)[a];
+        out.txx[I] = c.slot(S_XX, R_XX, s)[a];
+        out.tyy[I] = c.slot(S_YY, R_YY, s)[a];
+        out.tzz[I] = c.slot(S_ZZ, R_ZZ, s)[a];
+        out.txy[I] = c.slot(S_XY, R_XY, s)[a];
+        out.txz[I] = c.slot(S_XZ, R_XZ, s)[a];
+        out.tyz[I] = c.slot(S_YZ, R_YZ, s)[a];
+    }
+}
+
+// stress boundary fix-ups of one face side on plane s at region point (i, j)
+template <typename T, int TY>
+__device__ __forceinline__ void fix_x(const Ctx<T, TY> &c, const KParams &p, int s, int i, int j, int side) {
+    const int kind = p.bc_kind[0][side];
+    if (kind != FI_BC_TRACTION && kind != FI_BC_SLIP) return;
+    const bool cz = s >= 1 && s <= c.n2, vz = s >= 1 && s <= c.n2 + 1;
+    const int ghost = side == 0 ? 0 : c.n0 + 1, adj = side == 0 ? 1 : c.n0, node = side == 0 ? 1 : c.n0 + 1;
+    if (kind == FI_BC_TRACTION && i == ghost && j >= 1 && j <= c.n1 && cz && adj >= c.i0 - 1 && adj <= c.i0 + TX) {
+        T tv = T(2.0) * T(p.bc_val[0][side][0]);
+        c.P(s, i, j) = tv - c.P(s, adj, j);
+        c.Txx(s, i, j) = tv - c.Txx(s, adj, j);
+    }
+    if (i == node) {
+        if (j >= 1 && j <= c.n1 + 1 && cz) c.Txy(s, i, j) = T(p.bc_val[0][side][1]);
+        if (j >= 1 && j <= c.n1 && vz) c.Txz(s, i, j) = T(p.bc_val[0][side][2]);
+    }
+}
+template <typename T, int TY>
+__device__ __forceinline__ void fix_y(const Ctx<T, TY> &c, const KParams &p, int s, int i, int j, int side) {
+    const int kind = p.bc_kind[1][side];
+    if (kind != FI_BC_TRACTION && kind != FI_BC_SLIP) return;
+    const bool cz = s >= 1 && s <= c.n2, vz = s >= 1 && s <= c.n2 + 1;
+    const int ghost = side == 0 ? 0 : c.n1 + 1, adj = side == 0 ? 1 : c.n1, node = side == 0 ? 1 : c.n1 + 1;
+    if (kind == FI_BC_TRACTION && j == ghost && cz && adj >= c.j0 - 1 && adj <= c.j0 + TY) {
+        T tv = T(2.0) * T(p.bc_val[1][side][1]);
+        c.P(s, i, j) = tv - c.P(s, i, adj);
+        c.Tyy(s, i, j) = tv - c.Tyy(s, i, adj);
+    }
+    if (j == node) {
+        if (cz) c.Txy(s, i, j) = T(p.bc_val[1][side][0]);
+        if (vz) c.Tyz(s, i, j) = T(p.bc_val[1][side][2]);
+    }
+}
+
+template <typename T, int TY>
+__device__ void sigma_plane(const Ctx<T, TY> &c, const KParams &p, const Ptrs<T> &out, int s) {
+    using Lay = Layout<T, TY>;
+    const int tid = threadIdx.x;
+    const bool zb_plane = s == 1 || s == c.n2 + 1;
+    const bool late = c.bnd_x || c.bnd_y || zb_plane;
+    const bool own_s = s >= c.kb && s < c.ke;
+    // pass 1: the column, all components
+    sigma_point<T, TY>(c, p, s, c.i0 + (tid % TX), c.j0 + (tid / TX), F_ALL, own_s && !late, out);
+    // pass 2: the ring, only the components read there
+    constexpr int NR = 2 * TY + 2 * TX + 1;
+    if (tid < NR) {
+        int i, j, mask;
+        if (tid < TY) { i = c.i0 - 1; j = c.j0 + tid; mask = F_P | F_XX; }
+        else if (tid < 2 * TY) { i = c.i0 + TX; j = c.j0 + tid - TY; mask = F_XY | F_XZ; }
+        else if (tid < 2 * TY + TX) { i = c.i0 + tid - 2 * TY; j = c.j0 - 1; mask = F_P | F_YY; }
+        else if (tid < 2 * TY + 2 * TX) { i = c.i0 + tid - 2 * TY - TX; j = c.j0 + TY; mask = F_XY | F_YZ; }
+        else { i = c.i0 + TX; j = c.j0 + TY; mask = F_XY; }
+        sigma_point<T, TY>(c, p, s, i, j, mask, false, out);
     }
     __syncthreads();
-
-    // ---- x faces (boundary_conditions.jl:51-58, 78-84): j, s in the field's interior
-    const bool touch_x = (c.i0 == 1 || c.i0 + TX >= c.n0 + 1) && !c.perx;
-    if (touch_x) {
-        for (int r = tid; r < C::RXY; r += C::NT) {
-            const int i = c.i0 - 1 + r % C::RX, j = c.j0 - 1 + r / C::RX;
-            for (int side = 0; side < 2; side++) {
-                const BcSide<T> &b = c.bc[0][side];
-                if (b.kind != FI_BC_TRACTION && b.kind != FI_BC_SLIP) continue;
-                const int ghost = side == 0 ? 0 : c.n0 + 1, adj = side == 0 ? 1 : c.n0, node = side == 0 ? 1 : c.n0 + 1;
-                if (b.kind == FI_BC_TRACTION && i == ghost && j >= 1 && j <= c.n1 && cz && adj >= c.i0 - 1 &&
-                    adj <= c.i0 + TX) {
-                    T tv = T(2.0) * b.c[0];
-                    c.P(s, i, j) = tv - c.P(s, adj, j);
-                    c.Txx(s, i, j) = tv - c.Txx(s, adj, j);
-                }
-                if (i == node) {
-                    if (j >= 1 && j <= c.n1 + 1 && cz) c.Txy(s, i, j) = b.c[1];
-                    if (j >= 1 && j <= c.n1 && vz) c.Txz(s, i, j) = b.c[2];
-                }
-            }
+    if (!late) return;
+    constexpr int NREG = (TX + 2) * (TY + 2);
+    if (c.bnd_x && !c.perx) {
+        for (int r = tid; r < NREG; r += Lay::NT) {
+            const int i = c.i0 - 1 + r % (TX + 2), j = c.j0 - 1 + r / (TX + 2);
+            fix_x<T, TY>(c, p, s, i, j, 0);
+            fix_x<T, TY>(c, p, s, i, j, 1);
         }
         __syncthreads();
     }
-    // ---- y faces (boundary_conditions.jl:60-67, 86-92): all x, s in the field's interior
-    const bool touch_y = (c.j0 == 1 || c.j0 + TY >= c.n1 + 1) && !c.pery;
-    if (touch_y) {
-        for (int r = tid; r < C::RXY; r += C::NT) {
-            const int i = c.i0 - 1 + r % C::RX, j = c.j0 - 1 + r / C::RX;
-            for (int side = 0; side < 2; side++) {
-                const BcSide<T> &b = c.bc[1][side];
-                if (b.kind != FI_BC_TRACTION && b.kind != FI_BC_SLIP) continue;
-                const int ghost = side == 0 ? 0 : c.n1 + 1, adj = side == 0 ? 1 : c.n1, node = side == 0 ? 1 : c.n1 + 1;
-                if (b.kind == FI_BC_TRACTION && j == ghost && cz && adj >= c.j0 - 1 && adj <= c.j0 + TY) {
-                    T tv = T(2.0) * b.c[1];
-                    c.P(s, i, j) = tv - c.P(s, i, adj);
-                    c.Tyy(s, i, j) = tv - c.Tyy(s, i, adj);
-                }
-                if (j == node) {
-                    if (cz) c.Txy(s, i, j) = b.c[0];
-                    if (vz) c.Tyz(s, i, j) = b.c[2];
-                }
-            }
+    if (c.bnd_y && !c.pery) {
+        for (int r = tid; r < NREG; r += Lay::NT) {
+            const int i = c.i0 - 1 + r % (TX + 2), j = c.j0 - 1 + r / (TX + 2);
+            fix_y<T, TY>(c, p, s, i, j, 0);
+            fix_y<T, TY>(c, p, s, i, j, 1);
         }
         __syncthreads();
     }
-    // ---- z faces (boundary_conditions.jl:69-76, 94-100): all x and y
-    if (s == 1 || s == c.n2 + 1) {
+    if (zb_plane) {
         const int side = s == 1 ? 0 : 1;
-        const BcSide<T> &b = c.bc[2][side];
-        if (b.kind == FI_BC_TRACTION || b.kind == FI_BC_SLIP) {
-            for (int r = tid; r < C::RXY; r += C::NT) {
-                const int i = c.i0 - 1 + r % C::RX, j = c.j0 - 1 + r / C::RX;
-                if (b.kind == FI_BC_TRACTION) {
-                    T tv = T(2.0) * b.c[2];
-                    if (side == 0) {  // ghost plane 0 from plane 1
+        const int kind = p.bc_kind[2][side];
+        if (kind == FI_BC_TRACTION || kind == FI_BC_SLIP) {
+            const T c0 = T(p.bc_val[2][side][0]), c1 = T(p.bc_val[2][side][1]), tv = T(2.0) * T(p.bc_val[2][side][2]);
+            for (int r = tid; r < NREG; r += Lay::NT) {
+                const int i = c.i0 - 1 + r % (TX + 2), j = c.j0 - 1 + r / (TX + 2);
+                if (kind == FI_BC_TRACTION) {
+                    if (side == 0) {
                         c.P(0, i, j) = tv - c.P(1, i, j);
                         c.Tzz(0, i, j) = tv - c.Tzz(1, i, j);
-                    } else {  // ghost plane n2+1 from plane n2
+                    } else {
                         c.P(s, i, j) = tv - c.P(s - 1, i, j);
                         c.Tzz(s, i, j) = tv - c.Tzz(s - 1, i, j);
                     }
                 }
-                c.Txz(s, i, j) = b.c[0];
-                c.Tyz(s, i, j) = b.c[1];
+                c.Txz(s, i, j) = c0;
+                c.Tyz(s, i, j) = c1;
             }
             __syncthreads();
         }
     }
-    // ---- owned writes (the next iteration reads these, ghosts included)
-    const bool own_s = s >= c.kb && s < c.ke;
-    const bool own_0 = s == 1 && c.kb == 1;
+    const bool own_0 = s == 1 && c.kb == 1 && p.bc_kind[2][0] == FI_BC_TRACTION;
     if (own_s || own_0) {
-        for (int r = tid; r < C::RXY; r += C::NT) {
-            const int i = c.i0 - 1 + r % C::RX, j = c.j0 - 1 + r / C::RX;
+        for (int r = tid; r < NREG; r += Lay::NT) {
+            const int i = c.i0 - 1 + r % (TX + 2), j = c.j0 - 1 + r / (TX + 2);
             if (i > c.n0 + 2 || j > c.n1 + 2 || !c.own_x(i) || !c.own_y(j)) continue;
             if (own_s) {
                 const long long I = c.gidx(i, j, s);
@@ -250,168 +395,193 @@ __device__ void sigma_plane(const Ctx<T, TY> &c, const KParams &p, const Ptrs<T>
             }
         }
     }
+    // the V update of the same step reads the fixed-up plane
+    __syncthreads();
 }
 
-// images of a value written at an interior position: per dim up to three
-// (position, mode) entries; mode 0 = copy, 1 = Dirichlet ghost 2c - v
+// ---- ghost / image writes: per dim a fixed three-entry list (own, low, high) ----
 template <typename T>
-struct DimImg {
-    int n;
+struct Img {
     int pos[3];
-    int mode[3];
+    bool ok[3];
+    bool dir[3];  // Dirichlet ghost 2c - v (else copy)
     T c[3];
-    __device__ __forceinline__ void add(int ps, int md, T cv) {
-        pos[n] = ps;
-        mode[n] = md;
-        c[n] = cv;
-        n++;
-    }
 };
 
-// dim image list for a Center-located value at index q (1..N) along a dim.
-// vel_comp >= 0: Velocity-BC Dirichlet ghosts of that component; -1: Neumann (η)
 template <typename T>
-__device__ __forceinline__ DimImg<T> img_center(int q, int N, bool periodic, const BcSide<T> *bc, int vel_comp) {
-    DimImg<T> d;
-    d.n = 0;
-    d.add(q, 0, T(0));
+__device__ __forceinline__ Img<T> img_own(int q) {
+    Img<T> d;
+    d.pos[0] = q; d.ok[0] = true; d.dir[0] = false; d.c[0] = T(0);
+    d.pos[1] = 0; d.ok[1] = false; d.dir[1] = false; d.c[1] = T(0);
+    d.pos[2] = 0; d.ok[2] = false; d.dir[2] = false; d.c[2] = T(0);
+    return d;
+}
+// Center-located value at index q (1..N) along a dim with BC kinds kl/kr.
+// comp >= 0: Velocity-BC ghosts of that velocity component; comp < 0: Neumann (η_next)
+template <typename T>
+__device__ __forceinline__ Img<T> img_center(int q, int N, bool periodic, int kl, int kr, T cl, T cr, bool neumann) {
+    Img<T> d = img_own<T>(q);
     if (periodic) {
-        if (q == 1) d.add(N + 1, 0, T(0));
-        if (q == N) d.add(0, 0, T(0));
+        if (q == N) { d.pos[1] = 0; d.ok[1] = true; }
+        if (q == 1) { d.pos[2] = N + 1; d.ok[2] = true; }
         return d;
     }
-    if (bc) {
-        if (vel_comp < 0) {
-            if (q == 1) d.add(0, 0, T(0));
-            if (q == N) d.add(N + 1, 0, T(0));
-        } else {
-            if (q == 1 && bc[0].kind == FI_BC_VELOCITY) d.add(0, 1, bc[0].c[vel_comp]);
-            if (q == N && bc[1].kind == FI_BC_VELOCITY) d.add(N + 1, 1, bc[1].c[vel_comp]);
-        }
+    if (neumann) {
+        if (q == 1) { d.pos[1] = 0; d.ok[1] = true; }
+        if (q == N) { d.pos[2] = N + 1; d.ok[2] = true; }
+    } else {
+        if (q == 1 && kl == FI_BC_VELOCITY) { d.pos[1] = 0; d.ok[1] = true; d.dir[1] = true; d.c[1] = cl; }
+        if (q == N && kr == FI_BC_VELOCITY) { d.pos[2] = N + 1; d.ok[2] = true; d.dir[2] = true; d.c[2] = cr; }
     }
     return d;
 }
-
-// dim image list for a Vertex-located value at index q (1..N+1)
 template <typename T>
-__device__ __forceinline__ DimImg<T> img_vertex(int q, int N, bool periodic) {
-    DimImg<T> d;
-    d.n = 0;
-    d.add(q, 0, T(0));
+__device__ __forceinline__ Img<T> img_vertex(int q, int N, bool periodic) {
+    Img<T> d = img_own<T>(q);
     if (periodic) {
-        if (q == 1) d.add(N + 1, 0, T(0));
-        if (q == 2) d.add(N + 2, 0, T(0));
-        if (q == N) d.add(0, 0, T(0));
+        if (q == N) { d.pos[1] = 0; d.ok[1] = true; }
+        if (q == 1) { d.pos[2] = N + 1; d.ok[2] = true; }
+        if (q == 2) { d.pos[2] = N + 2; d.ok[2] = true; }
     }
     return d;
 }
 
 template <typename T, int TY>
-__device__ __forceinline__ void write_with_images(const Ctx<T, TY> &c, T *f, T v, const DimImg<T> &ix,
-                                                  const DimImg<T> &iy, const DimImg<T> &iz) {
-    for (int a = 0; a < ix.n; a++) {
-        T va = ix.mode[a] ? T(2.0) * ix.c[a] - v : v;
-        for (int b = 0; b < iy.n; b++) {
-            T vb = iy.mode[b] ? T(2.0) * iy.c[b] - va : va;
-            for (int e = 0; e < iz.n; e++) {
-                T ve = iz.mode[e] ? T(2.0) * iz.c[e] - vb : vb;
+__device__ __forceinline__ void write_images(const Ctx<T, TY> &c, T *f, T v, const Img<T> &ix, const Img<T> &iy,
+                                             const Img<T> &iz) {
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        if (!ix.ok[a]) continue;
+        T va = ix.dir[a] ? T(2.0) * ix.c[a] - v : v;
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+            if (!iy.ok[b]) continue;
+            T vb = iy.dir[b] ? T(2.0) * iy.c[b] - va : va;
+#pragma unroll
+            for (int e = 0; e < 3; e++) {
+                if (!iz.ok[e]) continue;
+                T ve = iz.dir[e] ? T(2.0) * iz.c[e] - vb : vb;
                 f[c.gidx(ix.pos[a], iy.pos[b], iz.pos[e])] = ve;
             }
         }
     }
 }
 
-// ---------------------------------------------------------------------------
-// new V and η_next of plane t on the CTA's own column
-// ---------------------------------------------------------------------------
+// ---- velocity / η_next update of plane t on the column ----------------------------
+template <typename T, int TY>
+__device__ __forceinline__ T vx_raw(const Ctx<T, TY> &c, const KParams &p, const Ptrs<T> &in, int t, int i, int j,
+                                    long long I) {
+    const T idx = T(p.inv_dx[0]), idy = T(p.inv_dx[1]), idz = T(p.inv_dx[2]);
+    T gx = gravity_dev(p, in.gx, 0, I);
+    T ex = h(c.Eta(t, i - 1, j) + c.Eta(t, i, j));
+    return c.Vx(t, i, j) + div_dev(-(c.P(t, i, j) - c.P(t, i - 1, j)) * idx + (c.Txx(t, i, j) - c.Txx(t, i - 1, j)) * idx +
+                                       (c.Txy(t, i, j + 1) - c.Txy(t, i, j)) * idy +
+                                       (c.Txz(t + 1, i, j) - c.Txz(t, i, j)) * idz - gx,
+                                   ex) *
+                               T(p.dt_V[0]);
+}
+template <typename T, int TY>
+__device__ __forceinline__ T vy_raw(const Ctx<T, TY> &c, const KParams &p, const Ptrs<T> &in, int t, int i, int j,
+                                    long long I) {
+    const T idx = T(p.inv_dx[0]), idy = T(p.inv_dx[1]), idz = T(p.inv_dx[2]);
+    T gy = gravity_dev(p, in.gy, 1, I);
+    T ey = h(c.Eta(t, i, j - 1) + c.Eta(t, i, j));
+    return c.Vy(t, i, j) + div_dev(-(c.P(t, i, j) - c.P(t, i, j - 1)) * idy + (c.Tyy(t, i, j) - c.Tyy(t, i, j - 1)) * idy +
+                                       (c.Txy(t, i + 1, j) - c.Txy(t, i, j)) * idx +
+                                       (c.Tyz(t + 1, i, j) - c.Tyz(t, i, j)) * idz - gy,
+                                   ey) *
+                               T(p.dt_V[1]);
+}
+template <typename T, int TY>
+__device__ __forceinline__ T vz_raw(const Ctx<T, TY> &c, const KParams &p, const Ptrs<T> &in, int t, int i, int j,
+                                    long long I) {
+    const T idx = T(p.inv_dx[0]), idy = T(p.inv_dx[1]), idz = T(p.inv_dx[2]);
+    T gz = gravity_dev(p, in.gz, 2, I);
+    T ez = h(c.Eta(t - 1, i, j) + c.Eta(t, i, j));
+    return c.Vz(t, i, j) + div_dev(-(c.P(t, i, j) - c.P(t - 1, i, j)) * idz + (c.Tzz(t, i, j) - c.Tzz(t - 1, i, j)) * idz +
+                                       (c.Txz(t, i + 1, j) - c.Txz(t, i, j)) * idx +
+                                       (c.Tyz(t, i, j + 1) - c.Tyz(t, i, j)) * idy - gz,
+                                   ez) *
+                               T(p.dt_V[2]);
+}
+template <typename T, int TY>
+__device__ __forceinline__ T eta_raw(const Ctx<T, TY> &c, const KParams &p, const Ptrs<T> &in, int t, int i, int j,
+                                     long long I) {
+    T xx = c.Txx(t, i, j), yy = c.Tyy(t, i, j), zz = c.Tzz(t, i, j);
+    T lxy = h(h(c.Txy(t, i, j) + c.Txy(t, i + 1, j)) + h(c.Txy(t, i, j + 1) + c.Txy(t, i + 1, j + 1)));
+    T lxz = h(h(c.Txz(t, i, j) + c.Txz(t, i + 1, j)) + h(c.Txz(t + 1, i, j) + c.Txz(t + 1, i + 1, j)));
+    T lyz = h(h(c.Tyz(t, i, j) + c.Tyz(t, i, j + 1)) + h(c.Tyz(t + 1, i, j) + c.Tyz(t + 1, i, j + 1)));
+    T s2 = T(0.5) * (xx * xx + yy * yy + zz * zz) + lxy * lxy + lxz * lxz + lyz * lyz;
+    T tII = sqrt_dev(s2);
+    return rheology_dev(p, in.eta_lin, in.A, c.Eta(t, i, j), I, tII);
+}
+
 template <typename T, int TY>
 __device__ void v_plane(const Ctx<T, TY> &c, const KParams &p, const Ptrs<T> &in, const Ptrs<T> &out, int t) {
     const int i = c.i0 + (threadIdx.x % TX), j = c.j0 + (threadIdx.x / TX);
-    if (i > c.n0 + 1 || j > c.n1 + 1) return;
-    const T idx = T(p.inv_dx[0]), idy = T(p.inv_dx[1]), idz = T(p.inv_dx[2]);
-    const long long I = c.gidx(i, j, t);
-    const long long sx = c.sx, sxy = c.sxy;
-    const T *eta = in.eta;
     const int n0 = c.n0, n1 = c.n1, n2 = c.n2;
-    const BcSide<T> *bx = c.bc[0], *by = c.bc[1], *bz = c.bc[2];
-    auto node_fixed = [](const BcSide<T> &b) { return b.kind == FI_BC_SLIP || b.kind == FI_BC_VELOCITY; };
-
+    if (i > n0 + 1 || j > n1 + 1) return;
+    const long long I = c.gidx(i, j, t);
+    const bool near = i <= 2 || i >= n0 || j <= 2 || j >= n1 || t <= 1 || t >= n2;
+    if (!near) {
+        out.Vx[I] = vx_raw(c, p, in, t, i, j, I);
+        out.Vy[I] = vy_raw(c, p, in, t, i, j, I);
+        out.Vz[I] = vz_raw(c, p, in, t, i, j, I);
+        out.eta_next[I] = eta_raw(c, p, in, t, i, j, I);
+        return;
+    }
+    auto node_fixed = [](int kind) { return kind == FI_BC_SLIP || kind == FI_BC_VELOCITY; };
+    const int xl = p.bc_kind[0][0], xr = p.bc_kind[0][1], yl = p.bc_kind[1][0], yr = p.bc_kind[1][1];
+    const int zl = p.bc_kind[2][0], zr = p.bc_kind[2][1];
     // ---- V.x at (V, C, C)
     if (j <= n1 && t >= 1 && t <= n2 && !(c.perx && i == n0 + 1)) {
         T v;
-        if (!c.perx && i == 1 && node_fixed(bx[0])) v = bx[0].c[0];
-        else if (!c.perx && i == n0 + 1 && node_fixed(bx[1])) v = bx[1].c[0];
-        else {
-            T gx = gravity_dev(p, in.gx, 0, I);
-            T ex = h(ld(eta + I - 1) + ld(eta + I));
-            v = ld(in.Vx + I) + div_dev(-(c.P(t, i, j) - c.P(t, i - 1, j)) * idx + (c.Txx(t, i, j) - c.Txx(t, i - 1, j)) * idx +
-                                            (c.Txy(t, i, j + 1) - c.Txy(t, i, j)) * idy +
-                                            (c.Txz(t + 1, i, j) - c.Txz(t, i, j)) * idz - gx,
-                                        ex) *
-                                    T(p.dt_V[0]);
-        }
-        write_with_images(c, out.Vx, v, img_vertex<T>(i, n0, c.perx),
-                          img_center<T>(j, n1, c.pery, c.pery ? nullptr : by, 0),
-                          img_center<T>(t, n2, false, bz, 0));
+        if (!c.perx && i == 1 && node_fixed(xl)) v = T(p.bc_val[0][0][0]);
+        else if (!c.perx && i == n0 + 1 && node_fixed(xr)) v = T(p.bc_val[0][1][0]);
+        else v = vx_raw(c, p, in, t, i, j, I);
+        write_images(c, out.Vx, v, img_vertex<T>(i, n0, c.perx),
+                     img_center<T>(j, n1, c.pery, yl, yr, T(p.bc_val[1][0][0]), T(p.bc_val[1][1][0]), false),
+                     img_center<T>(t, n2, false, zl, zr, T(p.bc_val[2][0][0]), T(p.bc_val[2][1][0]), false));
     }
     // ---- V.y at (C, V, C)
     if (i <= n0 && t >= 1 && t <= n2 && !(c.pery && j == n1 + 1)) {
         T v;
-        if (!c.pery && j == 1 && node_fixed(by[0])) v = by[0].c[1];
-        else if (!c.pery && j == n1 + 1 && node_fixed(by[1])) v = by[1].c[1];
-        else {
-            T gy = gravity_dev(p, in.gy, 1, I);
-            T ey = h(ld(eta + I - sx) + ld(eta + I));
-            v = ld(in.Vy + I) + div_dev(-(c.P(t, i, j) - c.P(t, i, j - 1)) * idy + (c.Tyy(t, i, j) - c.Tyy(t, i, j - 1)) * idy +
-                                            (c.Txy(t, i + 1, j) - c.Txy(t, i, j)) * idx +
-                                            (c.Tyz(t + 1, i, j) - c.Tyz(t, i, j)) * idz - gy,
-                                        ey) *
-                                    T(p.dt_V[1]);
-        }
-        write_with_images(c, out.Vy, v, img_center<T>(i, n0, c.perx, c.perx ? nullptr : bx, 1),
-                          img_vertex<T>(j, n1, c.pery), img_center<T>(t, n2, false, bz, 1));
+        if (!c.pery && j == 1 && node_fixed(yl)) v = T(p.bc_val[1][0][1]);
+        else if (!c.pery && j == n1 + 1 && node_fixed(yr)) v = T(p.bc_val[1][1][1]);
+        else v = vy_raw(c, p, in, t, i, j, I);
+        write_images(c, out.Vy, v,
+                     img_center<T>(i, n0, c.perx, xl, xr, T(p.bc_val[0][0][1]), T(p.bc_val[0][1][1]), false),
+                     img_vertex<T>(j, n1, c.pery),
+                     img_center<T>(t, n2, false, zl, zr, T(p.bc_val[2][0][1]), T(p.bc_val[2][1][1]), false));
     }
     // ---- V.z at (C, C, V)
     if (i <= n0 && j <= n1 && t >= 1 && t <= n2 + 1) {
         T v;
-        if (t == 1 && node_fixed(bz[0])) v = bz[0].c[2];
-        else if (t == n2 + 1 && node_fixed(bz[1])) v = bz[1].c[2];
-        else {
-            T gz = gravity_dev(p, in.gz, 2, I);
-            T ez = h(ld(eta + I - sxy) + ld(eta + I));
-            v = ld(in.Vz + I) + div_dev(-(c.P(t, i, j) - c.P(t - 1, i, j)) * idz + (c.Tzz(t, i, j) - c.Tzz(t - 1, i, j)) * idz +
-                                            (c.Txz(t, i + 1, j) - c.Txz(t, i, j)) * idx +
-                                            (c.Tyz(t, i, j + 1) - c.Tyz(t, i, j)) * idy - gz,
-                                        ez) *
-                                    T(p.dt_V[2]);
-        }
-        DimImg<T> iz;
-        iz.n = 0;
-        iz.add(t, 0, T(0));
-        write_with_images(c, out.Vz, v, img_center<T>(i, n0, c.perx, c.perx ? nullptr : bx, 2),
-                          img_center<T>(j, n1, c.pery, c.pery ? nullptr : by, 2), iz);
+        if (t == 1 && node_fixed(zl)) v = T(p.bc_val[2][0][2]);
+        else if (t == n2 + 1 && node_fixed(zr)) v = T(p.bc_val[2][1][2]);
+        else v = vz_raw(c, p, in, t, i, j, I);
+        write_images(c, out.Vz, v,
+                     img_center<T>(i, n0, c.perx, xl, xr, T(p.bc_val[0][0][2]), T(p.bc_val[0][1][2]), false),
+                     img_center<T>(j, n1, c.pery, yl, yr, T(p.bc_val[1][0][2]), T(p.bc_val[1][1][2]), false),
+                     img_own<T>(t));
     }
-    // ---- τII and η_next at (C, C, C)
+    // ---- η_next at (C, C, C), Neumann / periodic ghosts
     if (i <= n0 && j <= n1 && t >= 1 && t <= n2) {
-        T xx = c.Txx(t, i, j), yy = c.Tyy(t, i, j), zz = c.Tzz(t, i, j);
-        T lxy = h(h(c.Txy(t, i, j) + c.Txy(t, i + 1, j)) + h(c.Txy(t, i, j + 1) + c.Txy(t, i + 1, j + 1)));
-        T lxz = h(h(c.Txz(t, i, j) + c.Txz(t, i + 1, j)) + h(c.Txz(t + 1, i, j) + c.Txz(t + 1, i + 1, j)));
-        T lyz = h(h(c.Tyz(t, i, j) + c.Tyz(t, i, j + 1)) + h(c.Tyz(t + 1, i, j) + c.Tyz(t + 1, i, j + 1)));
-        T s2 = T(0.5) * (xx * xx + yy * yy + zz * zz) + lxy * lxy + lxz * lxz + lyz * lyz;
-        T tII = sqrt_dev(s2);
-        T en = rheology_dev(p, in.eta_lin, in.A, ld(eta + I), I, tII);
-        write_with_images(c, out.eta_next, en, img_center<T>(i, n0, c.perx, c.perx ? nullptr : bx, -1),
-                          img_center<T>(j, n1, c.pery, c.pery ? nullptr : by, -1), img_center<T>(t, n2, false, bz, -1));
+        T en = eta_raw(c, p, in, t, i, j, I);
+        write_images(c, out.eta_next, en, img_center<T>(i, n0, c.perx, xl, xr, T(0), T(0), true),
+                     img_center<T>(j, n1, c.pery, yl, yr, T(0), T(0), true),
+                     img_center<T>(t, n2, false, zl, zr, T(0), T(0), true));
     }
 }
 
 template <typename T, int TY>
-__global__ void __launch_bounds__(TX *TY, (TY <= 8 ? 2 : 1)) fused3d_kernel(Geom g, KParams p, Ptrs<T> in, Ptrs<T> out,
-                                                                             int zb) {
-    using C = Ctx<T, TY>;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    C c;
+__global__ void __launch_bounds__(TX *TY, (sizeof(T) == 8 ? 2 : 3))
+    fused3d_kernel(Geom g, KParams p, Ptrs<T> in, Ptrs<T> out, const __grid_constant__ InMaps maps, int zb, int *err) {
+    using Lay = Layout<T, TY>;
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    Ctx<T, TY> c;
     c.sm = reinterpret_cast<T *>(smem_raw);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + (size_t)S_COUNT * Lay::SLOT * sizeof(T));
     c.i0 = 1 + blockIdx.x * TX;
     c.j0 = 1 + blockIdx.y * TY;
     c.kb = 1 + blockIdx.z * zb;
@@ -423,38 +593,75 @@ __global__ void __launch_bounds__(TX *TY, (TY <= 8 ? 2 : 1)) fused3d_kernel(Geom
     c.sxy = g.sxy;
     c.perx = p.bc_kind[0][0] == FI_BC_PERIODIC;
     c.pery = p.bc_kind[1][0] == FI_BC_PERIODIC;
-    for (int d = 0; d < 3; d++)
-        for (int s = 0; s < 2; s++) {
-            c.bc[d][s].kind = p.bc_kind[d][s];
-            for (int q = 0; q < 3; q++) c.bc[d][s].c[q] = T(p.bc_val[d][s][q]);
-        }
-    for (int r = threadIdx.x; r < SL_COUNT * C::RXY; r += C::NT) c.sm[r] = T(0);
+    c.bnd_x = c.i0 == 1 || c.i0 + TX >= c.n0 + 1;
+    c.bnd_y = c.j0 == 1 || c.j0 + TY >= c.n1 + 1;
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        for (int b = 0; b < kBars; b++) mbar_init(&bars[b], 1);
+        mbar_fence_init();
+    }
     __syncthreads();
-
-    if (c.kb - 1 >= 1) sigma_plane<T, TY>(c, p, in, out, c.kb - 1);
-    sigma_plane<T, TY>(c, p, in, out, c.kb);
-    for (int t = c.kb; t < c.ke; t++) {
-        if (t + 1 <= c.n2 + 1) sigma_plane<T, TY>(c, p, in, out, t + 1);
-        __syncthreads();
-        v_plane<T, TY>(c, p, in, out, t);
+    const int f = max(c.kb - 1, 1), last = min(c.ke, c.n2 + 1);
+    uint32_t phase = 0;  // bit b: parity of the next completion of bars[b]
+    if (tid == 0) {
+        issue_group<T, TY>(c, maps, f - 1, false, &bars[(f - 1) % kBars]);
+        issue_group<T, TY>(c, maps, f, true, &bars[f % kBars]);
+    }
+    auto wait_group = [&](int pl) -> bool {
+        const int b = pl % kBars;
+        bool ok = mbar_wait(&bars[b], (phase >> b) & 1u);
+        phase ^= 1u << b;
+        return ok;
+    };
+    bool ok = wait_group(f - 1);
+    for (int s = f; s <= last && ok; s++) {
+        if (tid == 0 && s + 1 <= last) {
+            fence_proxy_async();
+            issue_group<T, TY>(c, maps, s + 1, true, &bars[(s + 1) % kBars]);
+        }
+        ok = wait_group(s);
+        if (!ok) break;
+        sigma_plane<T, TY>(c, p, out, s);
+        if (s - 1 >= c.kb && s - 1 < c.ke) v_plane<T, TY>(c, p, in, out, s - 1);
         __syncthreads();
     }
+    if (ok) {
+        if (c.ke - 1 == last && last == c.n2 + 1) v_plane<T, TY>(c, p, in, out, last);
+        return;
+    }
+    // bounded wait expired: record it and drain this CTA's own copies (bounded) before leaving
+    atomicExch(err, (int)FI_ERR_TIMEOUT);
+    for (int b = 0; b < kBars; b++) mbar_wait(&bars[b], (phase >> b) & 1u);
 }
 
 template <typename T, int TY>
-cudaError_t launch_variant(const Geom &g, const KParams &p, const Ptrs<T> &in, const Ptrs<T> &out, int zb,
-                           cudaStream_t s) {
-    using C = Ctx<T, TY>;
-    size_t shmem = (size_t)SL_COUNT * C::RXY * sizeof(T);
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(fused3d_kernel<T, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem);
+cudaError_t launch_variant(const Geom &g, const KParams &p, const Ptrs<T> &in, const Ptrs<T> &out, const InMaps &maps,
+                           int zb, int *err, cudaStream_t s) {
+    using Lay = Layout<T, TY>;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    static bool attr_set[64] = {};
+    if (dev < 64 && !attr_set[dev]) {
+        cudaError_t e =
+            cudaFuncSetAttribute(fused3d_kernel<T, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lay::SMEM);
         if (e != cudaSuccess) return e;
-        attr_set = true;
+        attr_set[dev] = true;
     }
     dim3 grd((g.n[0] + 1 + TX - 1) / TX, (g.n[1] + 1 + TY - 1) / TY, (g.n[2] + 1 + zb - 1) / zb);
-    fused3d_kernel<T, TY><<<grd, C::NT, shmem, s>>>(g, p, in, out, zb);
+    fused3d_kernel<T, TY><<<grd, Lay::NT, Lay::SMEM, s>>>(g, p, in, out, maps, zb, err);
     return cudaGetLastError();
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 get_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        cudaDriverEntryPointQueryResult q;
+        void *ptr = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)ptr;
+    }
+    return fn;
 }
 
 }  // namespace
@@ -466,31 +673,48 @@ const char *fused3d_variant_name(int v) {
     snprintf(buf[v], sizeof(buf[v]), "tile32x%d_zb%d", kVariants[v].ty, kVariants[v].zb);
     return buf[v];
 }
+int fused3d_variant_ty(int v) { return kVariants[(v < 0 || v >= kNumVariants) ? 0 : v].ty; }
 
 template <typename T>
 bool fused3d_supported(const Geom &g, const KParams &p, bool ib) {
     if (g.nd != 3 || ib) return false;
     if (p.bc_kind[2][0] == FI_BC_PERIODIC) return false;
-    return true;
+    return g.pitch >= kXOff + g.n[0] + 3;
+}
+
+// one 3D tensor map over a field allocation (raw base, aligned), box = one plane of
+// the widened column for tile height ty
+bool fused3d_encode_map(void *raw_base, const Geom &g, int esz, int ty, void *map_out) {
+    PFN_cuTensorMapEncodeTiled_v12000 enc = get_encoder();
+    if (!enc) return false;
+    const int bx = esz == 8 ? BoxX<double>::BX : BoxX<float>::BX;
+    cuuint64_t dims[3] = {(cuuint64_t)g.pitch, (cuuint64_t)g.rows, (cuuint64_t)g.planes};
+    cuuint64_t strides[2] = {(cuuint64_t)(g.pitch * esz), (cuuint64_t)(g.sxy * esz)};
+    cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)(ty + 2), 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = enc((CUtensorMap *)map_out, esz == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                     3, raw_base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
 }
 
 template <typename T>
-cudaError_t launch_fused3d(const Geom &g, const KParams &p, const Ptrs<T> &in, const Ptrs<T> &out, bool ib, int variant,
-                           cudaStream_t s) {
+cudaError_t launch_fused3d(const Geom &g, const KParams &p, const Ptrs<T> &in, const Ptrs<T> &out, const void *maps11,
+                           int variant, int *err, cudaStream_t s) {
     if (variant < 0 || variant >= kNumVariants) variant = 0;
     const Variant v = kVariants[variant];
+    const InMaps &mp = *reinterpret_cast<const InMaps *>(maps11);
     switch (v.ty) {
-        case 4: return launch_variant<T, 4>(g, p, in, out, v.zb, s);
-        case 16: return launch_variant<T, 16>(g, p, in, out, v.zb, s);
-        default: return launch_variant<T, 8>(g, p, in, out, v.zb, s);
+        case 4: return launch_variant<T, 4>(g, p, in, out, mp, v.zb, err, s);
+        default: return launch_variant<T, 8>(g, p, in, out, mp, v.zb, err, s);
     }
 }
 
 template bool fused3d_supported<double>(const Geom &, const KParams &, bool);
 template bool fused3d_supported<float>(const Geom &, const KParams &, bool);
 template cudaError_t launch_fused3d<double>(const Geom &, const KParams &, const Ptrs<double> &, const Ptrs<double> &,
-                                            bool, int, cudaStream_t);
+                                            const void *, int, int *, cudaStream_t);
 template cudaError_t launch_fused3d<float>(const Geom &, const KParams &, const Ptrs<float> &, const Ptrs<float> &,
-                                           bool, int, cudaStream_t);
+                                           const void *, int, int *, cudaStream_t);
 
 }  // namespace fi

@@ -2,9 +2,11 @@
 //
 // Storage: every field of a model lives in one uniform halo box per model:
 // (n0+3) x (n1+3) x (n2+3) logical elements (vertex count + one ghost layer on
-// each side, for every staggered location), x fastest, with the x row padded
-// to a multiple of 32 elements so that each row starts on a 128-byte (FP32) or
-// 256-byte (FP64) boundary.  Index (i,j,k) -> i + pitch*(j + rows*k); index 0
+// each side, for every staggered location), x fastest.  Index (i,j,k) maps to
+// field[i + pitch*(j + rows*k)] where the field pointer sits kXOff elements past
+// its allocation, and pitch is a multiple of 32: interior index 1 of every row
+// starts on a 256-byte (FP64) / 128-byte (FP32) boundary, so a warp storing 32
+// consecutive positions of a column tile writes whole 32-byte sectors.  Index 0
 // is the left ghost, 1..N_loc the interior (N_loc = n or n+1 per location).
 #pragma once
 
@@ -18,6 +20,7 @@
 namespace fi {
 
 constexpr int kMaxBcOps = 16;
+constexpr long long kXOff = 31;  // field pointer offset (elements) inside its allocation
 constexpr int kNormSlots = 12;  // per-block partial slots (FI_NORMS_LEN layout)
 
 // geometry as seen by device code
@@ -95,10 +98,14 @@ int norm_blocks(const Geom &g);
 // P,tau,V read from `in`, written to `out`; eta read from in.eta, eta_next written.
 template <typename T>
 bool fused3d_supported(const Geom &g, const KParams &p, bool ib);
+// maps11: the eleven input tensor maps (P, txx, tyy, tzz, txy, txz, tyz, Vx, Vy, Vz, eta),
+// 128 bytes each, encoded with fused3d_encode_map for the variant's tile height
 template <typename T>
-cudaError_t launch_fused3d(const Geom &g, const KParams &p, const Ptrs<T> &in, const Ptrs<T> &out, bool ib,
-                           int variant, cudaStream_t s);
+cudaError_t launch_fused3d(const Geom &g, const KParams &p, const Ptrs<T> &in, const Ptrs<T> &out, const void *maps11,
+                           int variant, int *err, cudaStream_t s);
+bool fused3d_encode_map(void *raw_base, const Geom &g, int esz, int ty, void *map_out);
 int fused3d_num_variants();
+int fused3d_variant_ty(int v);
 const char *fused3d_variant_name(int v);
 
 // ---- level sets (fi_levelsets.cu) ----

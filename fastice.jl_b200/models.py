@@ -249,6 +249,19 @@ class _StokesBase:
         L.check(self.lib, self.lib.fi_model_path(self._h, C.byref(v)))
         return {L.FI_PATH_REFERENCE: "reference", L.FI_PATH_FUSED: "fused"}[v.value]
 
+    def set_variant(self, variant: int) -> None:
+        L.check(self.lib, self.lib.fi_model_set_variant(self._h, int(variant)))
+
+    def autotune(self, iters: int = 3):
+        """Time every fused-sweep variant (advancing the model) and keep the fastest;
+        returns (best index, {variant name: ms per iteration})."""
+        nv = self.lib.fi_fused_variant_count()
+        ms = (C.c_double * nv)()
+        best = C.c_int32()
+        L.check(self.lib, self.lib.fi_model_autotune(self._h, int(iters), C.byref(best), ms))
+        names = [self.lib.fi_fused_variant_name(v).decode() for v in range(nv)]
+        return best.value, dict(zip(names, ms[:]))
+
     @property
     def stream_ptr(self) -> int:
         s = C.c_void_p()

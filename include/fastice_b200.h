@@ -222,6 +222,18 @@ fi_status fi_model_synchronize(fi_model *m);
 /* which kernel path the model runs (fi_path, never AUTO) */
 fi_status fi_model_path(const fi_model *m, int32_t *path);
 
+/* Tile shape and z-block depth of the fused sweep.  fi_model_autotune times
+ * every variant for `iters` iterations on the model itself (so the model
+ * advances by n_variants * iters PT iterations, like warm-up iterations), keeps
+ * the fastest and writes its index and the per-variant milliseconds per
+ * iteration to best / ms (ms may be NULL; it needs fi_fused_variant_count()
+ * slots).  No counterpart in the reference (its launch shape is fixed by Chmy's
+ * Launcher). */
+int fi_fused_variant_count(void);
+const char *fi_fused_variant_name(int32_t variant);
+fi_status fi_model_set_variant(fi_model *m, int32_t variant);
+fi_status fi_model_autotune(fi_model *m, int32_t iters, int32_t *best, double *ms);
+
 /* ---- level sets and volume fractions (setup path) --------------------------- */
 
 /* ω_from_ψ!(arch, launch, ω, ψ, grid) (LevelSets/volume_fractions_kernels.jl:228-237):

@@ -1,0 +1,168 @@
+"""Pins of the CPU oracle and the host grid mirror (no GPU).
+
+The reference's only tests touching the discretisation are the Chmy grid
+geometry checks of test/test_chmy_grids.jl; their expected values are restated
+here and checked against the host UniformGrid and the oracle's coordinate
+convention.  The operators are further anchored by the O(h^2) convergence of
+the manufactured solution of scripts_future_API/stokes_manufactured_solution_free_slip_2D.jl,
+and the cut-cell volumes by closed-form known answers.
+"""
+import math
+
+import numpy as np
+import pytest
+
+
+# ---- test/test_chmy_grids.jl:17-160 (origin=(-1,-2), extent=(2,4), dims=(5,20)) -------
+@pytest.fixture
+def chmy_grid(fi):
+    return fi.UniformGrid(origin=(-1, -2), extent=(2, 4), dims=(5, 20))
+
+
+def test_flip(fi):
+    assert fi.flip(fi.Center()) == fi.Vertex()
+    assert fi.flip(fi.Vertex()) == fi.Center()
+
+
+def test_sizes(fi, chmy_grid):
+    g, C, V = chmy_grid, fi.Center(), fi.Vertex()
+    assert g.size(C) == (5, 20)
+    assert g.size(V) == (6, 21)
+    assert g.size((C, V)) == (5, 21)
+    assert g.size((V, C)) == (6, 20)
+    assert g.size(C) == g.size((C, C)) and g.size(V) == g.size((V, V))
+
+
+def test_bounds_extent_origin(fi, chmy_grid):
+    g, C, V = chmy_grid, fi.Center(), fi.Vertex()
+    assert np.allclose(g.bounds(V, 0), (-1.0, 1.0)) and np.allclose(g.bounds(V, 1), (-2.0, 2.0))
+    assert np.allclose(g.bounds(C, 0), (-0.8, 0.8)) and np.allclose(g.bounds(C, 1), (-1.9, 1.9))
+    assert math.isclose(g.grid_extent(V, 0), 2.0) and math.isclose(g.grid_extent(V, 1), 4.0)
+    assert math.isclose(g.grid_extent(C, 0), 1.6) and math.isclose(g.grid_extent(C, 1), 3.8)
+    assert math.isclose(g.grid_origin(V, 0), -1) and math.isclose(g.grid_origin(C, 0), -0.8)
+    assert math.isclose(g.grid_origin(C, 1), -1.9)
+
+
+def test_spacing_and_inverse(fi, chmy_grid):
+    g = chmy_grid
+    assert np.allclose(g.spacing(), (0.4, 0.2))
+    assert np.allclose(g.inv_spacing(), (2.5, 5.0))
+
+
+def test_coords(fi, chmy_grid):
+    g, C, V = chmy_grid, fi.Center(), fi.Vertex()
+    assert math.isclose(g.coord(V, 0, 1), -1.0) and math.isclose(g.coord(V, 1, 1), -2.0)
+    assert math.isclose(g.coord(V, 0, 6), 1.0) and math.isclose(g.coord(V, 1, 21), 2.0)
+    assert math.isclose(g.coord(C, 0, 1), -0.8) and math.isclose(g.coord(C, 1, 1), -1.9)
+    assert math.isclose(g.coord(C, 0, 5), 0.8) and math.isclose(g.coord(C, 1, 20), 1.9)
+    xs = g.coords(V, 0, halo=True)  # storage index 0 is the ghost left of vertex 1
+    assert math.isclose(xs[1], -1.0) and math.isclose(xs[0], -1.4)
+
+
+# ---- manufactured solution (config 1 on the unit square) ---------------------------------
+def _mms2d_oracle(orc, n, max_iter_factor=60):
+    ext, org = (1.0, 1.0), (0.0, 0.0)
+    dx = ext[0] / n
+    r, re = 0.7, 8 * math.pi
+    lt = min(ext) / re
+    vdt = dx / math.sqrt(2 * 1.1)
+    th = lt * (r + 4 / 3) / vdt
+    dtr, nud = 1.0 / (th + 1.0), vdt * lt
+    slip = (orc.BC_SLIP, (0, 0, 0))
+    spec = orc.Spec(nd=2, n=(n, n), extent=ext, origin=org, bcs=((slip, slip), (slip, slip)), dt_P=r / th,
+                    dt_tau=(dtr, dtr, 0, dtr, 0, 0), dt_V=(nud, nud, 0))
+    sh = spec.storage_shape()
+    iy, ix = np.meshgrid(np.arange(sh[0]), np.arange(sh[1]), indexing="ij")
+    xv, xc = org[0] + (ix - 1) * dx, org[0] + (ix - 0.5) * dx
+    yv, yc = org[1] + (iy - 1) * dx, org[1] + (iy - 0.5) * dx
+    gx = -2 * math.pi ** 2 * np.sin(math.pi * xv) * np.cos(math.pi * yc)
+    gy = 2 * math.pi ** 2 * np.cos(math.pi * xc) * np.sin(math.pi * yv)
+    m = orc.OracleStokes(spec, gravity_arrays={"gx": gx, "gy": gy})
+    m.a["eta"][:] = 1.0
+    m.a["eta_next"][:] = 1.0
+    m.apply_initial_bcs()
+    it = 0
+    while it < max_iter_factor * n:
+        m.advance(n)
+        it += n
+        nr = m.residual_norms()
+        if max(nr[:3]) < 1e-8:
+            break
+    ex = (np.sin(math.pi * xv) * np.cos(math.pi * yc))[1:n + 1, 1:n + 2]
+    ey = (-np.cos(math.pi * xc) * np.sin(math.pi * yv))[1:n + 2, 1:n + 1]
+    Vx, Vy = m.interior("Vx"), m.interior("Vy")
+    err = math.sqrt((np.sum((Vx - ex) ** 2) + np.sum((Vy - ey) ** 2)) / (np.sum(ex ** 2) + np.sum(ey ** 2)))
+    return err, it, max(nr[:3])
+
+
+def test_oracle_mms2d_second_order(orc):
+    errs = []
+    for n in (16, 32, 64):
+        err, it, res = _mms2d_oracle(orc, n)
+        assert res < 1e-8, (n, it, res)
+        errs.append(err)
+    orders = [math.log2(errs[i] / errs[i + 1]) for i in range(len(errs) - 1)]
+    assert all(1.9 < o < 2.1 for o in orders), orders
+
+
+# ---- cut-cell volumes (volume_fractions.jl) -------------------------------------------------
+def test_vol_box_full_and_empty(orc):
+    d = (0.3, 0.2, 0.5)
+    assert orc.vol_box3([-1.0] * 8, d) == pytest.approx(0.03, rel=1e-14)
+    assert orc.vol_box3([1.0] * 8, d) == 0.0
+    assert orc.vol_box2([-1.0] * 4, (0.3, 0.2)) == pytest.approx(0.06, rel=1e-14)
+    assert orc.vol_box2([1.0] * 4, (0.3, 0.2)) == 0.0
+
+
+@pytest.mark.parametrize("h", [0.1, 0.37, 0.5, 0.83])
+def test_vol_box_planar_cut(orc, h):
+    # psi = z - h*dz: the fraction below the plane is exactly h
+    d = (0.3, 0.2, 0.5)
+    psi = [((m >> 2) & 1) * d[2] - h * d[2] for m in range(8)]
+    assert orc.vol_box3(psi, d) / (d[0] * d[1] * d[2]) == pytest.approx(h, rel=1e-12)
+    psi2 = [((m >> 1) & 1) * 0.2 - h * 0.2 for m in range(4)]
+    assert orc.vol_box2(psi2, (0.3, 0.2)) / 0.06 == pytest.approx(h, rel=1e-12)
+
+
+def test_vol_box_oblique_plane(orc):
+    # plane x + y + z = s through a unit cube: exact volume of the corner region
+    d = (1.0, 1.0, 1.0)
+    for s in (0.4, 0.9, 1.5, 2.2):
+        psi = [(m & 1) + ((m >> 1) & 1) + ((m >> 2) & 1) - s for m in range(8)]
+        v = orc.vol_box3(psi, d)
+
+        def corner(t):
+            return max(t, 0.0) ** 3 / 6.0
+        exact = corner(s) - 3 * corner(s - 1) + 3 * corner(s - 2) - corner(s - 3)
+        assert v == pytest.approx(exact, rel=1e-12, abs=1e-15)
+
+
+def test_volfrac3d_planar_field(orc):
+    n, dx = (6, 5, 8), (0.2, 0.25, 0.125)
+    sh = (n[2] + 3, n[1] + 3, n[0] + 3)
+    k = np.arange(sh[0])[:, None, None]
+    z = (k - 1) * dx[2]
+    h = 0.43
+    psi = np.broadcast_to(z - h, sh).astype(np.float64).copy()
+    w = orc.volfrac3d(n, dx, psi)
+    # cell-centred fraction of the cell spanning z in [(k-1)dz, k dz]
+    for kk in range(1, n[2] + 1):
+        lo, hi = (kk - 1) * dx[2], kk * dx[2]
+        exact = min(max((h - lo) / dx[2], 0.0), 1.0)
+        assert np.allclose(w["ccc"][kk, 1:n[1] + 1, 1:n[0] + 1], exact, rtol=1e-12, atol=1e-14)
+
+
+def test_levelset_flat_dem(orc):
+    # a flat DEM at height h: the signed distance is z - h inside the window
+    n3, o3, dx3 = (6, 6, 6), (0.0, 0.0, 0.0), (1 / 6, 1 / 6, 1 / 6)
+    n2, o2, dx2 = (12, 12), (-0.5, -0.5), (2 / 12, 2 / 12)
+    h = 0.41
+    dem = np.full((n2[1] + 3, n2[0] + 3), h)
+    psi = orc.levelset_from_dem(n3, o3, dx3, n2, o2, dx2, dem)
+    k = np.arange(n3[2] + 3)
+    z = o3[2] + (k - 1) * dx3[2]
+    inner = psi[1:n3[2] + 2, 1:n3[1] + 2, 1:n3[0] + 2]
+    expect = np.broadcast_to((z[1:n3[2] + 2] - h)[:, None, None], inner.shape)
+    assert np.allclose(inner, expect, atol=1e-13)
+    inv = orc.invert_levelset(n3, psi.copy())
+    assert np.allclose(inv[1:-1, 1:-1, 1:-1], -psi[1:-1, 1:-1, 1:-1])
