@@ -54,6 +54,26 @@ __device__ __forceinline__ float sqrt_dev(float x) { return __fsqrt_rn(x); }
 __device__ __forceinline__ double div_dev(double a, double b) { return a / b; }
 __device__ __forceinline__ float div_dev(float a, float b) { return __fdiv_rn(a, b); }
 
+// η_next from τII² = s2 (rheology(τII) with τII = sqrt(s2)).  Production builds
+// evaluate Glen's law with the integer exponent n = 3 as 0.5/(A s2) and its
+// viscoplastic regularisation as 1/(2 A s2 + 1/η_reg): the same function without
+// the square root and with one division instead of three (a few ulp from the
+// reference's rounding sequence).  Builds with FI_EXACT_ORDER keep the
+// reference's operation order (sqrt, then the divisions of Physics.jl:18, :26)
+// for bit-level comparison with the CPU oracle.
+template <typename T>
+__device__ __forceinline__ T rheology_s2(const KParams &p, T A_const, T inv_reg, const T *eta_lin, const T *Afield,
+                                         T eta_cur, long long I, T s2) {
+#ifndef FI_EXACT_ORDER
+    if (p.rheo_inner == FI_RHEO_POWER && p.rheo_n == 3 && p.rheo_relax == FI_RELAX_NONE) {
+        T A = p.rheo_A_is_field ? Afield[I] : A_const;
+        T As2 = A * s2;
+        return p.rheo_has_reg ? div_dev(T(1.0), T(2.0) * As2 + inv_reg) : div_dev(T(0.5), As2);
+    }
+#endif
+    return rheology_dev(p, eta_lin, Afield, eta_cur, I, sqrt_dev(s2));
+}
+
 // immersed-boundary mask components: ccc vvv vcc cvc ccv vvc vcv cvv
 enum { W_CCC = 0, W_VVV, W_VCC, W_CVC, W_CCV, W_VVC, W_VCV, W_CVV };
 

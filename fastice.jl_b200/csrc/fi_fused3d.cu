@@ -39,6 +39,7 @@
 #include <cudaTypedefs.h>
 
 #include <cstdio>
+#include <cstdlib>
 
 #include "fi_device.cuh"
 
@@ -53,7 +54,7 @@ struct Variant {
     int ty;
     int zb;
 };
-constexpr Variant kVariants[] = {{8, 32}, {8, 64}, {8, 128}, {4, 64}, {8, 16}};
+constexpr Variant kVariants[] = {{8, 32}, {8, 64}, {8, 128}, {4, 64}, {16, 32}, {16, 64}, {16, 128}};
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
 // TMA box width (elements) and position of the column's first x inside the box:
@@ -210,10 +211,10 @@ __device__ __forceinline__ void issue_group(const Ctx<T, TY> &c, const InMaps &m
 enum { F_P = 1, F_XX = 2, F_YY = 4, F_ZZ = 8, F_XY = 16, F_XZ = 32, F_YZ = 64, F_ALL = 127 };
 
 template <typename T, int TY>
-__device__ __forceinline__ void sigma_point(const Ctx<T, TY> &c, const KParams &p, int s, int i, int j, int mask,
+__device__ __forceinline__ void sigma_point(const Ctx<T, TY> &c, const KParams &p, const TConst<T> &q, int s, int i, int j, int mask,
                                             bool write_now, const Ptrs<T> &out) {
     if (i > c.n0 + 2 || j > c.n1 + 2) return;
-    const T idx = T(p.inv_dx[0]), idy = T(p.inv_dx[1]), idz = T(p.inv_dx[2]);
+    const T idx = q.inv_dx[0], idy = q.inv_dx[1], idz = q.inv_dx[2];
     const bool cz = s >= 1 && s <= c.n2, vz = s >= 1 && s <= c.n2 + 1;
     const bool cx = (i >= 1 && i <= c.n0) || (c.perx && (i == 0 || i == c.n0 + 1));
     const bool vx = i >= 1 && i <= c.n0 + 1;
@@ -229,19 +230,19 @@ __device__ __forceinline__ void sigma_point(const Ctx<T, TY> &c, const KParams &
         T etac = c.slot(S_ET, R_ET, s)[a];
         if (mask & F_P) {
             T &v = c.slot(S_P, R_P, s)[a];
-            v = v - divV * etac * T(p.dt_P);
+            v = v - divV * etac * q.dt_P;
         }
         if (mask & F_XX) {
             T &v = c.slot(S_XX, R_XX, s)[a];
-            v = v - (v - T(2.0) * etac * (exx - divV / T(3.0))) * T(p.dt_tau[0]);
+            v = v - (v - T(2.0) * etac * (exx - divV / T(3.0))) * q.dt_tau[0];
         }
         if (mask & F_YY) {
             T &v = c.slot(S_YY, R_YY, s)[a];
-            v = v - (v - T(2.0) * etac * (eyy - divV / T(3.0))) * T(p.dt_tau[1]);
+            v = v - (v - T(2.0) * etac * (eyy - divV / T(3.0))) * q.dt_tau[1];
         }
         if (mask & F_ZZ) {
             T &v = c.slot(S_ZZ, R_ZZ, s)[a];
-            v = v - (v - T(2.0) * etac * (ezz - divV / T(3.0))) * T(p.dt_tau[2]);
+            v = v - (v - T(2.0) * etac * (ezz - divV / T(3.0))) * q.dt_tau[2];
         }
     }
     constexpr int BX = Ctx<T, TY>::Lay::BX;
@@ -250,21 +251,21 @@ __device__ __forceinline__ void sigma_point(const Ctx<T, TY> &c, const KParams &
         T exy = T(0.5) * ((vys[a] - vys[a - 1]) * idx + (vxs[a] - vxs[a - BX]) * idy);
         T e_xy = h(h(et[a - 1 - BX] + et[a - BX]) + h(et[a - 1] + et[a]));
         T &v = c.slot(S_XY, R_XY, s)[a];
-        v = v - (v - T(2.0) * e_xy * exy) * T(p.dt_tau[3]);
+        v = v - (v - T(2.0) * e_xy * exy) * q.dt_tau[3];
     }
     if ((mask & F_XZ) && vx && cy && vz) {
         const T *vzs = c.slot(S_VZ, R_VZ, s), *et = c.slot(S_ET, R_ET, s), *etm = c.slot(S_ET, R_ET, s - 1);
         T exz = T(0.5) * ((vzs[a] - vzs[a - 1]) * idx + (c.slot(S_VX, R_VX, s)[a] - c.slot(S_VX, R_VX, s - 1)[a]) * idz);
         T e_xz = h(h(etm[a - 1] + etm[a]) + h(et[a - 1] + et[a]));
         T &v = c.slot(S_XZ, R_XZ, s)[a];
-        v = v - (v - T(2.0) * e_xz * exz) * T(p.dt_tau[4]);
+        v = v - (v - T(2.0) * e_xz * exz) * q.dt_tau[4];
     }
     if ((mask & F_YZ) && cx && vy && vz) {
         const T *vzs = c.slot(S_VZ, R_VZ, s), *et = c.slot(S_ET, R_ET, s), *etm = c.slot(S_ET, R_ET, s - 1);
         T eyz = T(0.5) * ((vzs[a] - vzs[a - BX]) * idy + (c.slot(S_VY, R_VY, s)[a] - c.slot(S_VY, R_VY, s - 1)[a]) * idz);
         T e_yz = h(h(etm[a - BX] + etm[a]) + h(et[a - BX] + et[a]));
         T &v = c.slot(S_YZ, R_YZ, s)[a];
-        v = v - (v - T(2.0) * e_yz * eyz) * T(p.dt_tau[5]);
+        v = v - (v - T(2.0) * e_yz * eyz) * q.dt_tau[5];
     }
     if (write_now) {
         const long long I = c.gidx(i, j, s);
@@ -280,47 +281,47 @@ __device__ __forceinline__ void sigma_point(const Ctx<T, TY> &c, const KParams &
 
 // stress boundary fix-ups of one face side on plane s at region point (i, j)
 template <typename T, int TY>
-__device__ __forceinline__ void fix_x(const Ctx<T, TY> &c, const KParams &p, int s, int i, int j, int side) {
+__device__ __forceinline__ void fix_x(const Ctx<T, TY> &c, const KParams &p, const TConst<T> &q, int s, int i, int j, int side) {
     const int kind = p.bc_kind[0][side];
     if (kind != FI_BC_TRACTION && kind != FI_BC_SLIP) return;
     const bool cz = s >= 1 && s <= c.n2, vz = s >= 1 && s <= c.n2 + 1;
     const int ghost = side == 0 ? 0 : c.n0 + 1, adj = side == 0 ? 1 : c.n0, node = side == 0 ? 1 : c.n0 + 1;
     if (kind == FI_BC_TRACTION && i == ghost && j >= 1 && j <= c.n1 && cz && adj >= c.i0 - 1 && adj <= c.i0 + TX) {
-        T tv = T(2.0) * T(p.bc_val[0][side][0]);
+        T tv = T(2.0) * q.bc_val[0][side][0];
         c.P(s, i, j) = tv - c.P(s, adj, j);
         c.Txx(s, i, j) = tv - c.Txx(s, adj, j);
     }
     if (i == node) {
-        if (j >= 1 && j <= c.n1 + 1 && cz) c.Txy(s, i, j) = T(p.bc_val[0][side][1]);
-        if (j >= 1 && j <= c.n1 && vz) c.Txz(s, i, j) = T(p.bc_val[0][side][2]);
+        if (j >= 1 && j <= c.n1 + 1 && cz) c.Txy(s, i, j) = q.bc_val[0][side][1];
+        if (j >= 1 && j <= c.n1 && vz) c.Txz(s, i, j) = q.bc_val[0][side][2];
     }
 }
 template <typename T, int TY>
-__device__ __forceinline__ void fix_y(const Ctx<T, TY> &c, const KParams &p, int s, int i, int j, int side) {
+__device__ __forceinline__ void fix_y(const Ctx<T, TY> &c, const KParams &p, const TConst<T> &q, int s, int i, int j, int side) {
     const int kind = p.bc_kind[1][side];
     if (kind != FI_BC_TRACTION && kind != FI_BC_SLIP) return;
     const bool cz = s >= 1 && s <= c.n2, vz = s >= 1 && s <= c.n2 + 1;
     const int ghost = side == 0 ? 0 : c.n1 + 1, adj = side == 0 ? 1 : c.n1, node = side == 0 ? 1 : c.n1 + 1;
     if (kind == FI_BC_TRACTION && j == ghost && cz && adj >= c.j0 - 1 && adj <= c.j0 + TY) {
-        T tv = T(2.0) * T(p.bc_val[1][side][1]);
+        T tv = T(2.0) * q.bc_val[1][side][1];
         c.P(s, i, j) = tv - c.P(s, i, adj);
         c.Tyy(s, i, j) = tv - c.Tyy(s, i, adj);
     }
     if (j == node) {
-        if (cz) c.Txy(s, i, j) = T(p.bc_val[1][side][0]);
-        if (vz) c.Tyz(s, i, j) = T(p.bc_val[1][side][2]);
+        if (cz) c.Txy(s, i, j) = q.bc_val[1][side][0];
+        if (vz) c.Tyz(s, i, j) = q.bc_val[1][side][2];
     }
 }
 
 template <typename T, int TY>
-__device__ void sigma_plane(const Ctx<T, TY> &c, const KParams &p, const Ptrs<T> &out, int s) {
+__device__ __forceinline__ void sigma_plane(const Ctx<T, TY> &c, const KParams &p, const TConst<T> &q, const Ptrs<T> &out, int s) {
     using Lay = Layout<T, TY>;
     const int tid = threadIdx.x;
     const bool zb_plane = s == 1 || s == c.n2 + 1;
     const bool late = c.bnd_x || c.bnd_y || zb_plane;
     const bool own_s = s >= c.kb && s < c.ke;
     // pass 1: the column, all components
-    sigma_point<T, TY>(c, p, s, c.i0 + (tid % TX), c.j0 + (tid / TX), F_ALL, own_s && !late, out);
+    sigma_point<T, TY>(c, p, q, s, c.i0 + (tid % TX), c.j0 + (tid / TX), F_ALL, own_s && !late, out);
     // pass 2: the ring, only the components read there
     constexpr int NR = 2 * TY + 2 * TX + 1;
     if (tid < NR) {
@@ -330,7 +331,7 @@ __device__ void sigma_plane(const Ctx<T, TY> &c, const KParams &p, const Ptrs<T>
         else if (tid < 2 * TY + TX) { i = c.i0 + tid - 2 * TY; j = c.j0 - 1; mask = F_P | F_YY; }
         else if (tid < 2 * TY + 2 * TX) { i = c.i0 + tid - 2 * TY - TX; j = c.j0 + TY; mask = F_XY | F_YZ; }
         else { i = c.i0 + TX; j = c.j0 + TY; mask = F_XY; }
-        sigma_point<T, TY>(c, p, s, i, j, mask, false, out);
+        sigma_point<T, TY>(c, p, q, s, i, j, mask, false, out);
     }
     __syncthreads();
     if (!late) return;
@@ -338,16 +339,16 @@ __device__ void sigma_plane(const Ctx<T, TY> &c, const KParams &p, const Ptrs<T>
     if (c.bnd_x && !c.perx) {
         for (int r = tid; r < NREG; r += Lay::NT) {
             const int i = c.i0 - 1 + r % (TX + 2), j = c.j0 - 1 + r / (TX + 2);
-            fix_x<T, TY>(c, p, s, i, j, 0);
-            fix_x<T, TY>(c, p, s, i, j, 1);
+            fix_x<T, TY>(c, p, q, s, i, j, 0);
+            fix_x<T, TY>(c, p, q, s, i, j, 1);
         }
         __syncthreads();
     }
     if (c.bnd_y && !c.pery) {
         for (int r = tid; r < NREG; r += Lay::NT) {
             const int i = c.i0 - 1 + r % (TX + 2), j = c.j0 - 1 + r / (TX + 2);
-            fix_y<T, TY>(c, p, s, i, j, 0);
-            fix_y<T, TY>(c, p, s, i, j, 1);
+            fix_y<T, TY>(c, p, q, s, i, j, 0);
+            fix_y<T, TY>(c, p, q, s, i, j, 1);
         }
         __syncthreads();
     }
@@ -355,7 +356,7 @@ __device__ void sigma_plane(const Ctx<T, TY> &c, const KParams &p, const Ptrs<T>
         const int side = s == 1 ? 0 : 1;
         const int kind = p.bc_kind[2][side];
         if (kind == FI_BC_TRACTION || kind == FI_BC_SLIP) {
-            const T c0 = T(p.bc_val[2][side][0]), c1 = T(p.bc_val[2][side][1]), tv = T(2.0) * T(p.bc_val[2][side][2]);
+            const T c0 = q.bc_val[2][side][0], c1 = q.bc_val[2][side][1], tv = T(2.0) * q.bc_val[2][side][2];
             for (int r = tid; r < NREG; r += Lay::NT) {
                 const int i = c.i0 - 1 + r % (TX + 2), j = c.j0 - 1 + r / (TX + 2);
                 if (kind == FI_BC_TRACTION) {
@@ -469,65 +470,64 @@ __device__ __forceinline__ void write_images(const Ctx<T, TY> &c, T *f, T v, con
 
 // ---- velocity / η_next update of plane t on the column ----------------------------
 template <typename T, int TY>
-__device__ __forceinline__ T vx_raw(const Ctx<T, TY> &c, const KParams &p, const Ptrs<T> &in, int t, int i, int j,
+__device__ __forceinline__ T vx_raw(const Ctx<T, TY> &c, const KParams &p, const TConst<T> &q, const Ptrs<T> &in, int t, int i, int j,
                                     long long I) {
-    const T idx = T(p.inv_dx[0]), idy = T(p.inv_dx[1]), idz = T(p.inv_dx[2]);
-    T gx = gravity_dev(p, in.gx, 0, I);
+    const T idx = q.inv_dx[0], idy = q.inv_dx[1], idz = q.inv_dx[2];
+    T gx = (p.g_kind[0] == FI_G_FIELD ? in.gx[I] : q.g_val[0]);
     T ex = h(c.Eta(t, i - 1, j) + c.Eta(t, i, j));
     return c.Vx(t, i, j) + div_dev(-(c.P(t, i, j) - c.P(t, i - 1, j)) * idx + (c.Txx(t, i, j) - c.Txx(t, i - 1, j)) * idx +
                                        (c.Txy(t, i, j + 1) - c.Txy(t, i, j)) * idy +
                                        (c.Txz(t + 1, i, j) - c.Txz(t, i, j)) * idz - gx,
                                    ex) *
-                               T(p.dt_V[0]);
+                               q.dt_V[0];
 }
 template <typename T, int TY>
-__device__ __forceinline__ T vy_raw(const Ctx<T, TY> &c, const KParams &p, const Ptrs<T> &in, int t, int i, int j,
+__device__ __forceinline__ T vy_raw(const Ctx<T, TY> &c, const KParams &p, const TConst<T> &q, const Ptrs<T> &in, int t, int i, int j,
                                     long long I) {
-    const T idx = T(p.inv_dx[0]), idy = T(p.inv_dx[1]), idz = T(p.inv_dx[2]);
-    T gy = gravity_dev(p, in.gy, 1, I);
+    const T idx = q.inv_dx[0], idy = q.inv_dx[1], idz = q.inv_dx[2];
+    T gy = (p.g_kind[1] == FI_G_FIELD ? in.gy[I] : q.g_val[1]);
     T ey = h(c.Eta(t, i, j - 1) + c.Eta(t, i, j));
     return c.Vy(t, i, j) + div_dev(-(c.P(t, i, j) - c.P(t, i, j - 1)) * idy + (c.Tyy(t, i, j) - c.Tyy(t, i, j - 1)) * idy +
                                        (c.Txy(t, i + 1, j) - c.Txy(t, i, j)) * idx +
                                        (c.Tyz(t + 1, i, j) - c.Tyz(t, i, j)) * idz - gy,
                                    ey) *
-                               T(p.dt_V[1]);
+                               q.dt_V[1];
 }
 template <typename T, int TY>
-__device__ __forceinline__ T vz_raw(const Ctx<T, TY> &c, const KParams &p, const Ptrs<T> &in, int t, int i, int j,
+__device__ __forceinline__ T vz_raw(const Ctx<T, TY> &c, const KParams &p, const TConst<T> &q, const Ptrs<T> &in, int t, int i, int j,
                                     long long I) {
-    const T idx = T(p.inv_dx[0]), idy = T(p.inv_dx[1]), idz = T(p.inv_dx[2]);
-    T gz = gravity_dev(p, in.gz, 2, I);
+    const T idx = q.inv_dx[0], idy = q.inv_dx[1], idz = q.inv_dx[2];
+    T gz = (p.g_kind[2] == FI_G_FIELD ? in.gz[I] : q.g_val[2]);
     T ez = h(c.Eta(t - 1, i, j) + c.Eta(t, i, j));
     return c.Vz(t, i, j) + div_dev(-(c.P(t, i, j) - c.P(t - 1, i, j)) * idz + (c.Tzz(t, i, j) - c.Tzz(t - 1, i, j)) * idz +
                                        (c.Txz(t, i + 1, j) - c.Txz(t, i, j)) * idx +
                                        (c.Tyz(t, i, j + 1) - c.Tyz(t, i, j)) * idy - gz,
                                    ez) *
-                               T(p.dt_V[2]);
+                               q.dt_V[2];
 }
 template <typename T, int TY>
-__device__ __forceinline__ T eta_raw(const Ctx<T, TY> &c, const KParams &p, const Ptrs<T> &in, int t, int i, int j,
+__device__ __forceinline__ T eta_raw(const Ctx<T, TY> &c, const KParams &p, const TConst<T> &q, const Ptrs<T> &in, int t, int i, int j,
                                      long long I) {
     T xx = c.Txx(t, i, j), yy = c.Tyy(t, i, j), zz = c.Tzz(t, i, j);
     T lxy = h(h(c.Txy(t, i, j) + c.Txy(t, i + 1, j)) + h(c.Txy(t, i, j + 1) + c.Txy(t, i + 1, j + 1)));
     T lxz = h(h(c.Txz(t, i, j) + c.Txz(t, i + 1, j)) + h(c.Txz(t + 1, i, j) + c.Txz(t + 1, i + 1, j)));
     T lyz = h(h(c.Tyz(t, i, j) + c.Tyz(t, i, j + 1)) + h(c.Tyz(t + 1, i, j) + c.Tyz(t + 1, i, j + 1)));
     T s2 = T(0.5) * (xx * xx + yy * yy + zz * zz) + lxy * lxy + lxz * lxz + lyz * lyz;
-    T tII = sqrt_dev(s2);
-    return rheology_dev(p, in.eta_lin, in.A, c.Eta(t, i, j), I, tII);
+    return rheology_s2(p, q.rheo_A, q.rheo_inv_eta_reg, in.eta_lin, in.A, c.Eta(t, i, j), I, s2);
 }
 
 template <typename T, int TY>
-__device__ void v_plane(const Ctx<T, TY> &c, const KParams &p, const Ptrs<T> &in, const Ptrs<T> &out, int t) {
+__device__ __forceinline__ void v_plane(const Ctx<T, TY> &c, const KParams &p, const TConst<T> &q, const Ptrs<T> &in, const Ptrs<T> &out, int t) {
     const int i = c.i0 + (threadIdx.x % TX), j = c.j0 + (threadIdx.x / TX);
     const int n0 = c.n0, n1 = c.n1, n2 = c.n2;
     if (i > n0 + 1 || j > n1 + 1) return;
     const long long I = c.gidx(i, j, t);
     const bool near = i <= 2 || i >= n0 || j <= 2 || j >= n1 || t <= 1 || t >= n2;
     if (!near) {
-        out.Vx[I] = vx_raw(c, p, in, t, i, j, I);
-        out.Vy[I] = vy_raw(c, p, in, t, i, j, I);
-        out.Vz[I] = vz_raw(c, p, in, t, i, j, I);
-        out.eta_next[I] = eta_raw(c, p, in, t, i, j, I);
+        out.Vx[I] = vx_raw(c, p, q, in, t, i, j, I);
+        out.Vy[I] = vy_raw(c, p, q, in, t, i, j, I);
+        out.Vz[I] = vz_raw(c, p, q, in, t, i, j, I);
+        out.eta_next[I] = eta_raw(c, p, q, in, t, i, j, I);
         return;
     }
     auto node_fixed = [](int kind) { return kind == FI_BC_SLIP || kind == FI_BC_VELOCITY; };
@@ -536,38 +536,38 @@ __device__ void v_plane(const Ctx<T, TY> &c, const KParams &p, const Ptrs<T> &in
     // ---- V.x at (V, C, C)
     if (j <= n1 && t >= 1 && t <= n2 && !(c.perx && i == n0 + 1)) {
         T v;
-        if (!c.perx && i == 1 && node_fixed(xl)) v = T(p.bc_val[0][0][0]);
-        else if (!c.perx && i == n0 + 1 && node_fixed(xr)) v = T(p.bc_val[0][1][0]);
-        else v = vx_raw(c, p, in, t, i, j, I);
+        if (!c.perx && i == 1 && node_fixed(xl)) v = q.bc_val[0][0][0];
+        else if (!c.perx && i == n0 + 1 && node_fixed(xr)) v = q.bc_val[0][1][0];
+        else v = vx_raw(c, p, q, in, t, i, j, I);
         write_images(c, out.Vx, v, img_vertex<T>(i, n0, c.perx),
-                     img_center<T>(j, n1, c.pery, yl, yr, T(p.bc_val[1][0][0]), T(p.bc_val[1][1][0]), false),
-                     img_center<T>(t, n2, false, zl, zr, T(p.bc_val[2][0][0]), T(p.bc_val[2][1][0]), false));
+                     img_center<T>(j, n1, c.pery, yl, yr, q.bc_val[1][0][0], q.bc_val[1][1][0], false),
+                     img_center<T>(t, n2, false, zl, zr, q.bc_val[2][0][0], q.bc_val[2][1][0], false));
     }
     // ---- V.y at (C, V, C)
     if (i <= n0 && t >= 1 && t <= n2 && !(c.pery && j == n1 + 1)) {
         T v;
-        if (!c.pery && j == 1 && node_fixed(yl)) v = T(p.bc_val[1][0][1]);
-        else if (!c.pery && j == n1 + 1 && node_fixed(yr)) v = T(p.bc_val[1][1][1]);
-        else v = vy_raw(c, p, in, t, i, j, I);
+        if (!c.pery && j == 1 && node_fixed(yl)) v = q.bc_val[1][0][1];
+        else if (!c.pery && j == n1 + 1 && node_fixed(yr)) v = q.bc_val[1][1][1];
+        else v = vy_raw(c, p, q, in, t, i, j, I);
         write_images(c, out.Vy, v,
-                     img_center<T>(i, n0, c.perx, xl, xr, T(p.bc_val[0][0][1]), T(p.bc_val[0][1][1]), false),
+                     img_center<T>(i, n0, c.perx, xl, xr, q.bc_val[0][0][1], q.bc_val[0][1][1], false),
                      img_vertex<T>(j, n1, c.pery),
-                     img_center<T>(t, n2, false, zl, zr, T(p.bc_val[2][0][1]), T(p.bc_val[2][1][1]), false));
+                     img_center<T>(t, n2, false, zl, zr, q.bc_val[2][0][1], q.bc_val[2][1][1], false));
     }
     // ---- V.z at (C, C, V)
     if (i <= n0 && j <= n1 && t >= 1 && t <= n2 + 1) {
         T v;
-        if (t == 1 && node_fixed(zl)) v = T(p.bc_val[2][0][2]);
-        else if (t == n2 + 1 && node_fixed(zr)) v = T(p.bc_val[2][1][2]);
-        else v = vz_raw(c, p, in, t, i, j, I);
+        if (t == 1 && node_fixed(zl)) v = q.bc_val[2][0][2];
+        else if (t == n2 + 1 && node_fixed(zr)) v = q.bc_val[2][1][2];
+        else v = vz_raw(c, p, q, in, t, i, j, I);
         write_images(c, out.Vz, v,
-                     img_center<T>(i, n0, c.perx, xl, xr, T(p.bc_val[0][0][2]), T(p.bc_val[0][1][2]), false),
-                     img_center<T>(j, n1, c.pery, yl, yr, T(p.bc_val[1][0][2]), T(p.bc_val[1][1][2]), false),
+                     img_center<T>(i, n0, c.perx, xl, xr, q.bc_val[0][0][2], q.bc_val[0][1][2], false),
+                     img_center<T>(j, n1, c.pery, yl, yr, q.bc_val[1][0][2], q.bc_val[1][1][2], false),
                      img_own<T>(t));
     }
     // ---- η_next at (C, C, C), Neumann / periodic ghosts
     if (i <= n0 && j <= n1 && t >= 1 && t <= n2) {
-        T en = eta_raw(c, p, in, t, i, j, I);
+        T en = eta_raw(c, p, q, in, t, i, j, I);
         write_images(c, out.eta_next, en, img_center<T>(i, n0, c.perx, xl, xr, T(0), T(0), true),
                      img_center<T>(j, n1, c.pery, yl, yr, T(0), T(0), true),
                      img_center<T>(t, n2, false, zl, zr, T(0), T(0), true));
@@ -575,8 +575,9 @@ __device__ void v_plane(const Ctx<T, TY> &c, const KParams &p, const Ptrs<T> &in
 }
 
 template <typename T, int TY>
-__global__ void __launch_bounds__(TX *TY, (sizeof(T) == 8 ? 2 : 3))
-    fused3d_kernel(Geom g, KParams p, Ptrs<T> in, Ptrs<T> out, const __grid_constant__ InMaps maps, int zb, int *err) {
+__global__ void __launch_bounds__(TX *TY, (TY >= 16 ? (sizeof(T) == 8 ? 1 : 2) : (sizeof(T) == 8 ? 2 : 3)))
+    fused3d_kernel(Geom g, KParams p, TConst<T> q, Ptrs<T> in, Ptrs<T> out, const __grid_constant__ InMaps maps, int zb,
+                   int *err) {
     using Lay = Layout<T, TY>;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     Ctx<T, TY> c;
@@ -621,12 +622,12 @@ __global__ void __launch_bounds__(TX *TY, (sizeof(T) == 8 ? 2 : 3))
         }
         ok = wait_group(s);
         if (!ok) break;
-        sigma_plane<T, TY>(c, p, out, s);
-        if (s - 1 >= c.kb && s - 1 < c.ke) v_plane<T, TY>(c, p, in, out, s - 1);
+        sigma_plane<T, TY>(c, p, q, out, s);
+        if (s - 1 >= c.kb && s - 1 < c.ke) v_plane<T, TY>(c, p, q, in, out, s - 1);
         __syncthreads();
     }
     if (ok) {
-        if (c.ke - 1 == last && last == c.n2 + 1) v_plane<T, TY>(c, p, in, out, last);
+        if (c.ke - 1 == last && last == c.n2 + 1) v_plane<T, TY>(c, p, q, in, out, last);
         return;
     }
     // bounded wait expired: record it and drain this CTA's own copies (bounded) before leaving
@@ -648,7 +649,7 @@ cudaError_t launch_variant(const Geom &g, const KParams &p, const Ptrs<T> &in, c
         attr_set[dev] = true;
     }
     dim3 grd((g.n[0] + 1 + TX - 1) / TX, (g.n[1] + 1 + TY - 1) / TY, (g.n[2] + 1 + zb - 1) / zb);
-    fused3d_kernel<T, TY><<<grd, Lay::NT, Lay::SMEM, s>>>(g, p, in, out, maps, zb, err);
+    fused3d_kernel<T, TY><<<grd, Lay::NT, Lay::SMEM, s>>>(g, p, make_tconst<T>(p), in, out, maps, zb, err);
     return cudaGetLastError();
 }
 
@@ -692,9 +693,17 @@ bool fused3d_encode_map(void *raw_base, const Geom &g, int esz, int ty, void *ma
     cuuint64_t strides[2] = {(cuuint64_t)(g.pitch * esz), (cuuint64_t)(g.sxy * esz)};
     cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)(ty + 2), 1};
     cuuint32_t estr[3] = {1, 1, 1};
+    // L2 promotion of the box rows (rows are 160 / 288 bytes); FI_TMA_L2_PROMOTION=0/64/128/256 overrides
+    CUtensorMapL2promotion promo = CU_TENSOR_MAP_L2_PROMOTION_L2_256B;
+    if (const char *e = getenv("FI_TMA_L2_PROMOTION")) {
+        int v = atoi(e);
+        promo = v == 0 ? CU_TENSOR_MAP_L2_PROMOTION_NONE
+                       : v == 64 ? CU_TENSOR_MAP_L2_PROMOTION_L2_64B
+                                 : v == 128 ? CU_TENSOR_MAP_L2_PROMOTION_L2_128B : CU_TENSOR_MAP_L2_PROMOTION_L2_256B;
+    }
     CUresult r = enc((CUtensorMap *)map_out, esz == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
                      3, raw_base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                     promo, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS;
 }
 
@@ -706,6 +715,7 @@ cudaError_t launch_fused3d(const Geom &g, const KParams &p, const Ptrs<T> &in, c
     const InMaps &mp = *reinterpret_cast<const InMaps *>(maps11);
     switch (v.ty) {
         case 4: return launch_variant<T, 4>(g, p, in, out, mp, v.zb, err, s);
+        case 16: return launch_variant<T, 16>(g, p, in, out, mp, v.zb, err, s);
         default: return launch_variant<T, 8>(g, p, in, out, mp, v.zb, err, s);
     }
 }

@@ -47,6 +47,30 @@ struct KParams {
     double small;  // immersed-boundary emptiness threshold (1e-6, or the FP32 value equivalent to it)
 };
 
+// the scalar parameters converted once to the compute type T (the conversion
+// (T)value the reference-shaped kernels perform at each use)
+template <typename T>
+struct TConst {
+    T inv_dx[3], dt_P, dt_tau[6], dt_V[3], g_val[3], bc_val[3][2][3];
+    T rheo_A, rheo_inv_eta_reg;
+};
+template <typename T>
+inline TConst<T> make_tconst(const KParams &p) {
+    TConst<T> q{};
+    for (int d = 0; d < 3; d++) {
+        q.inv_dx[d] = T(p.inv_dx[d]);
+        q.dt_V[d] = T(p.dt_V[d]);
+        q.g_val[d] = T(p.g_val[d]);
+        for (int s = 0; s < 2; s++)
+            for (int c = 0; c < 3; c++) q.bc_val[d][s][c] = T(p.bc_val[d][s][c]);
+    }
+    q.dt_P = T(p.dt_P);
+    for (int k = 0; k < 6; k++) q.dt_tau[k] = T(p.dt_tau[k]);
+    q.rheo_A = T(p.rheo_A);
+    q.rheo_inv_eta_reg = T(p.rheo_inv_eta_reg);
+    return q;
+}
+
 // device pointers of one model state (current buffers)
 template <typename T>
 struct Ptrs {

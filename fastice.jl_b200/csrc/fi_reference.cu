@@ -148,8 +148,8 @@ __global__ void __launch_bounds__(256) update_V_kernel(Geom g, KParams p, Ptrs<T
                   div_dev(-(P[I] - P[I - sx]) * idy + (tyy[I] - tyy[I - sx]) * idy + (txy[I + 1] - txy[I]) * idx - gy, ey) *
                       T(p.dt_V[1]);
         T lxy = h(h(txy[I] + txy[I + 1]) + h(txy[I + sx] + txy[I + sx + 1]));
-        T tII = sqrt_dev(T(0.5) * (txx[I] * txx[I] + tyy[I] * tyy[I]) + lxy * lxy);
-        f.eta_next[I] = rheology_dev(p, f.eta_lin, f.A, eta[I], I, tII);
+        T s2 = T(0.5) * (txx[I] * txx[I] + tyy[I] * tyy[I]) + lxy * lxy;
+        f.eta_next[I] = rheology_s2(p, T(p.rheo_A), T(p.rheo_inv_eta_reg), f.eta_lin, f.A, eta[I], I, s2);
         return;
     }
     const T idz = T(p.inv_dx[2]);
@@ -217,8 +217,7 @@ __global__ void __launch_bounds__(256) update_V_kernel(Geom g, KParams p, Ptrs<T
     T lxz = h(h(txz[I] + txz[I + 1]) + h(txz[I + sxy] + txz[I + sxy + 1]));
     T lyz = h(h(tyz[I] + tyz[I + sx]) + h(tyz[I + sxy] + tyz[I + sxy + sx]));
     T s = T(0.5) * (txx[I] * txx[I] + tyy[I] * tyy[I] + tzz[I] * tzz[I]) + lxy * lxy + lxz * lxz + lyz * lyz;
-    T tII = sqrt_dev(s);
-    f.eta_next[I] = rheology_dev(p, f.eta_lin, f.A, eta[I], I, tII);
+    f.eta_next[I] = rheology_s2(p, T(p.rheo_A), T(p.rheo_inv_eta_reg), f.eta_lin, f.A, eta[I], I, s);
 }
 
 // ---------------------------------------------------------------------------

@@ -121,6 +121,22 @@ def test_3d_relaxation_log_scales(scale):
     assert max(err.values()) <= 1e-10, err
 
 
+@pytest.mark.parametrize("variant", range(7))
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_every_fused_variant_bitwise(variant, dtype):
+    # each launch shape the autotuner may pick: tiles and z-blocks cut across the grid
+    p = Pair((70, 37, 150), BC3["mixed_values"], path="fused", library="strict", dtype=dtype, seed=13)
+    nv = p.model.lib.fi_fused_variant_count()
+    if variant >= nv:
+        p.close()
+        pytest.skip("no such variant")
+    p.model.set_variant(variant)
+    p.advance(3)
+    bad = p.bitwise_equal()
+    p.close()
+    assert not bad, bad
+
+
 def test_fused_equals_reference_path():
     a = Pair((40, 17, 70), BC3["noslip_bed_free_top"], path="fused", seed=8, rheo={"kind": "glen"})
     b = Pair((40, 17, 70), BC3["noslip_bed_free_top"], path="reference", seed=8, rheo={"kind": "glen"})
