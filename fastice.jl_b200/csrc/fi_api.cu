@@ -52,13 +52,6 @@ void field_loc(int field, int loc[3]) {
     for (int d = 0; d < 3; d++) loc[d] = L[field][d];
 }
 
-float small_threshold_f32() {
-    // smallest float >= 1e-6: for float w, (w < t) <=> ((double)w < 1e-6)
-    float t = 1e-6f;
-    if ((double)t < 1e-6) t = std::nextafter(t, 1.0f);
-    return t;
-}
-
 // field buffers: the field pointer sits kXOff elements past the allocation
 cudaError_t field_alloc(void **field_ptr, size_t elems, size_t esz) {
     void *raw = nullptr;

@@ -12,6 +12,7 @@
 
 #include <cuda_runtime.h>
 #include <cstddef>
+#include <cmath>
 #include <cstdint>
 #include <string>
 
@@ -98,6 +99,14 @@ struct BcBatch {
     int dim;
     BcOpDesc ops[kMaxBcOps];
 };
+
+// smallest float >= 1e-6: for a float w, (w < t) <=> ((double)w < 1e-6), the
+// comparison the reference makes after promoting Float32 masks to Float64
+inline float small_threshold_f32() {
+    float t = 1e-6f;
+    if ((double)t < 1e-6) t = std::nextafter(t, 1.0f);
+    return t;
+}
 
 void set_error(const std::string &msg);
 fi_status cuda_fail(cudaError_t e, const char *where);

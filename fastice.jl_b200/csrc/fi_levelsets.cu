@@ -458,7 +458,7 @@ fi_status fi_levelset_from_dem(const fi_grid *grid3, const fi_grid *dem_grid2, c
         dx2[q] = dem_grid2->extent[q] / dem_grid2->n[q];
         n2[q] = dem_grid2->n[q];
     }
-    double cutoff = 4.0 * mx;  // compute_levelsets.jl:114
+    double cutoff = 4.0 * mx;  // compute_levelsets.jl:22
     cudaError_t e = launch_levelset(g, o3, dx3, n2, o2, dx2, dem_grid2->n[0] + 3, (const double *)ddem.p, R, R != nullptr,
                                     cutoff, invert, (double *)dpsi.p, 0);
     if (e != cudaSuccess) return cuda_fail(e, "levelset kernel");

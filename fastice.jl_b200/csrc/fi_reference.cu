@@ -293,7 +293,7 @@ __global__ void __launch_bounds__(256) compute_residuals_kernel(Geom g, KParams 
     if (ND == 3) f.rVz[x.I] = r.rVz;
 }
 
-// compute_τ!  (kernels_3d.jl:225-245, kernels_2d.jl:33-44)
+// compute_τ!  (kernels_3d.jl:44-64, kernels_2d.jl:33-44)
 template <typename T, int ND>
 __global__ void __launch_bounds__(256) compute_tau_kernel(Geom g, KParams p, Ptrs<T> f) {
     Idx x = vertex_index(g);

@@ -2,9 +2,9 @@
 
 ``compute_levelset_from_dem(grid, dem_grid2d, dem)`` mirrors
 ``compute_levelset_from_dem!(arch, launch, Ψ, dem, dem_grid2D, grid, R)``
-(compute_levelsets.jl:113-117), ``invert`` applies ``invert_levelset!``
-(:124-127), and ``omega_from_psi`` mirrors ``ω_from_ψ!``
-(volume_fractions_kernels.jl:228-237).  Arrays use the uniform halo box
+(compute_levelsets.jl:21-25), ``invert`` applies ``invert_levelset!``
+(:32-35), and ``omega_from_psi`` mirrors ``ω_from_ψ!``
+(volume_fractions_kernels.jl:101-110).  Arrays use the uniform halo box
 (n+3 per dim), numpy order (z, y, x).
 """
 from __future__ import annotations

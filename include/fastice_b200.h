@@ -178,7 +178,7 @@ fi_status fi_model_compute_residuals(fi_model *m);
  * Synchronises; out has FI_NORMS_LEN doubles. */
 fi_status fi_model_residual_norms(fi_model *m, double *out);
 
-/* compute_τ! helper (kernels_3d.jl:225-245, kernels_2d.jl:33-44): τ = 2η dev(ε̇). */
+/* compute_τ! helper (kernels_3d.jl:44-64, kernels_2d.jl:33-44): τ = 2η dev(ε̇). */
 fi_status fi_model_compute_tau(fi_model *m);
 
 /* Driver loop (tm_stokes_chmy.jl:283-305): advance, every ncheck iterations take
@@ -236,15 +236,15 @@ fi_status fi_model_autotune(fi_model *m, int32_t iters, int32_t *best, double *m
 
 /* ---- level sets and volume fractions (setup path) --------------------------- */
 
-/* ω_from_ψ!(arch, launch, ω, ψ, grid) (LevelSets/volume_fractions_kernels.jl:228-237):
+/* ω_from_ψ!(arch, launch, ω, ψ, grid) (LevelSets/volume_fractions_kernels.jl:101-110):
  * psi is the level set at grid vertices in halo storage of a model's grid
  * ((n0+3) x (n1+3) x (n2+3), x fastest, ghosts filled); writes the model's
  * mask group (0 = na, 1 = ns), all 8 components (4 in 2D is not supported). */
 fi_status fi_model_volfrac_from_levelset(fi_model *m, int32_t group, const double *psi_host);
 
 /* compute_levelset_from_dem!(arch, launch, Ψ, dem, dem_grid2D, grid, R)
- * (LevelSets/compute_levelsets.jl:113-117) followed by invert_levelset! when
- * invert != 0 (:124-127).  dem: vertex values of the 2D DEM grid in halo storage
+ * (LevelSets/compute_levelsets.jl:21-25) followed by invert_levelset! when
+ * invert != 0 (:32-35).  dem: vertex values of the 2D DEM grid in halo storage
  * ((m0+3) x (m1+3), x fastest, valid up to index m+2); R: row-major 3x3 or NULL
  * (identity).  psi_host receives the 3D vertex level set in halo storage. */
 fi_status fi_levelset_from_dem(const fi_grid *grid3, const fi_grid *dem_grid2, const double *dem_host,

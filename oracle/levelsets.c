@@ -354,7 +354,7 @@ void fo_neumann_vertex3(const int n3[3], double *psi) {
         }
 }
 
-/* compute_levelsets.jl:10-14, 124-127 */
+/* compute_levelsets.jl:10-14, 32-35 */
 void fo_invert_levelset(const int n3[3], double *psi) {
     size_t sx = (size_t)n3[0] + 3, sy = (size_t)n3[1] + 3, sxy = sx * sy;
     for (int k = 1; k <= n3[2] + 1; k++)

@@ -313,7 +313,7 @@ def volfrac2d(n, dx, psi):
 
 
 def levelset_from_dem(n3, o3, dx3, n2, o2, dx2, dem, R=None, cutoff=None):
-    """compute_levelset_from_dem! (compute_levelsets.jl:113-117): returns psi (halo storage)."""
+    """compute_levelset_from_dem! (compute_levelsets.jl:21-25): returns psi (halo storage)."""
     dem = np.ascontiguousarray(dem, dtype=np.float64)
     assert dem.shape == (n2[1] + 3, n2[0] + 3)
     psi = np.zeros((n3[2] + 3, n3[1] + 3, n3[0] + 3), np.float64)

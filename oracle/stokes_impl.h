@@ -494,7 +494,7 @@ void F(fo_residual_norms)(const fo_params *p, fo_fields *fl, double *out) {
     F(norms_from_arrays)(p, fl, out);
 }
 
-/* compute_tau!: kernels_3d.jl:225-245, kernels_2d.jl:33-44 */
+/* compute_tau!: kernels_3d.jl:44-64, kernels_2d.jl:33-44 */
 void F(fo_compute_tau)(const fo_params *p, fo_fields *fl) {
     F(geom) g = F(mkgeom)(p);
     REAL *txx = (REAL *)fl->txx, *tyy = (REAL *)fl->tyy, *txy = (REAL *)fl->txy;
@@ -575,11 +575,11 @@ static int F(nullspace)(const REAL *const w[8], int comp, size_t I, size_t sx, s
     case W_CCV:
         return SMALL(w[W_VCV][I]) || SMALL(w[W_VCV][I + 1]) || SMALL(w[W_CVV][I]) || SMALL(w[W_CVV][I + sx]) ||
                SMALL(w[W_CCC][I - sxy]) || SMALL(w[W_CCC][I]);
-    case W_VVC: /* :24-26, dims x and y only */
+    case W_VVC: /* :24-27, dims x and y only */
         return SMALL(w[W_CVC][I - 1]) || SMALL(w[W_CVC][I]) || SMALL(w[W_VCC][I - sx]) || SMALL(w[W_VCC][I]);
-    case W_VCV: /* :28-31, dims x and z */
+    case W_VCV: /* :29-32, dims x and z */
         return SMALL(w[W_CCV][I - 1]) || SMALL(w[W_CCV][I]) || SMALL(w[W_VCC][I - sxy]) || SMALL(w[W_VCC][I]);
-    case W_CVV: /* :33-36, dims y and z */
+    case W_CVV: /* :34-37, dims y and z */
         return SMALL(w[W_CCV][I - sx]) || SMALL(w[W_CCV][I]) || SMALL(w[W_CVC][I - sxy]) || SMALL(w[W_CVC][I]);
     default:
         return 0;
