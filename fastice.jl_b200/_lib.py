@@ -83,6 +83,11 @@ class fi_solve_report(C.Structure):
                 ("norms", C.c_double * FI_NORMS_LEN), ("seconds", C.c_double), ("converged", C.c_int32)]
 
 
+class fi_state_view(C.Structure):
+    _fields_ = [(k, C.c_void_p) for k in ("P", "txx", "tyy", "tzz", "txy", "txz", "tyz", "Vx", "Vy", "Vz")] + [
+        ("g", C.c_void_p * 3), ("na", C.c_void_p * 8), ("ns", C.c_void_p * 8), ("pitch", C.c_size_t)]
+
+
 class FastIceError(RuntimeError):
     """Raised for a non-FI_OK status; ``status`` holds the fi_status code."""
 
@@ -119,6 +124,8 @@ SIGNATURES = [
     ("fi_fused_variant_name", C.c_char_p, [C.c_int32]),
     ("fi_model_set_variant", C.c_int, [C.c_void_p, C.c_int32]),
     ("fi_model_autotune", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
+    ("fi_residual_norms_noalloc", C.c_int, [C.POINTER(fi_model_desc), C.POINTER(fi_state_view), C.c_void_p,
+                                            C.c_void_p]),
 ]
 
 _libs = {}

@@ -234,6 +234,37 @@ const char *fi_fused_variant_name(int32_t variant);
 fi_status fi_model_set_variant(fi_model *m, int32_t variant);
 fi_status fi_model_autotune(fi_model *m, int32_t iters, int32_t *best, double *ms);
 
+/* Device-side view of a model state for callers that own the field memory:
+ * device pointers to index (0,0,0) of each field's uniform halo box (x fastest,
+ * index (i,j,k) at ptr[i + pitch*(j + (n1+3)*k)], ghosts included), in the
+ * model's dtype.  fi_model_device_ptr / fi_model_layout give a model's own view. */
+typedef struct {
+    const void *P, *txx, *tyy, *tzz, *txy, *txz, *tyz;
+    const void *Vx, *Vy, *Vz;
+    const void *g[3];   /* gravity fields where gravity.kind[c] == FI_G_FIELD, else NULL */
+    const void *na[8];  /* immersed-boundary masks (immersed models only), else NULL */
+    const void *ns[8];
+    size_t pitch;       /* elements per x row, >= n0 + 3 */
+} fi_state_view;
+
+/* Residual norms that allocate nothing.  No counterpart in the reference: it is
+ * fi_model_residual_norms for callers that cannot allocate device memory -- a
+ * host program whose device memory belongs to another runtime's allocator, code
+ * running while a stream is captured into a CUDA graph, services that forbid
+ * allocation after start-up.  It computes the same FI_NORMS_LEN values for the
+ * state in `state` (problem described by `desc`; desc->path and device are
+ * ignored, the current device is used) into the caller's device buffer out_dev,
+ * asynchronously on `stream` (a cudaStream_t, NULL for the default stream).
+ * Per-block partial sums live in a static device array of 32768 slots (3 MiB,
+ * held by every device that loads the library until the process exits); a grid
+ * with more than 32768 * 4096 vertex-range indices ((n0+1)(n1+1)(n2+1), i.e.
+ * more than 511^3 cells) is rejected with FI_ERR_ARG.  The first call on a
+ * device looks up that array's device address (cudaGetSymbolAddress); make that
+ * first call before any stream capture.  All calls on a device share the array:
+ * calls that overlap on the GPU race and must be serialised by the caller. */
+fi_status fi_residual_norms_noalloc(const fi_model_desc *desc, const fi_state_view *state, double *out_dev,
+                                    void *stream);
+
 /* ---- level sets and volume fractions (setup path) --------------------------- */
 
 /* ω_from_ψ!(arch, launch, ω, ψ, grid) (LevelSets/volume_fractions_kernels.jl:101-110):
