@@ -36,10 +36,11 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 
-# DRAM bytes per cell of one fused-sweep launch, from the ncu capture summarised
-# in profiles/fused3d_slab_ncu.md (dram__bytes_read.sum + dram__bytes_write.sum
-# of a 255^3 launch divided by its cell count); None until captured.
-TRAFFIC_BYTES_PER_CELL = {"f64": None, "f32": None}
+# DRAM bytes per cell of one fused-sweep launch: dram__bytes_read.sum +
+# dram__bytes_write.sum of one ncu-captured 255^3 launch (32x8 tiles, z-blocks of
+# 64, summarised in profiles/fused3d_slab255_ncu_full.md) divided by its cell
+# count; traffic grows with the cell count, so it scales to 511^3.
+TRAFFIC_BYTES_PER_CELL = {"f64": 231.7, "f32": None}
 
 
 def load_fastice():
@@ -156,7 +157,7 @@ def time_advance(fi, model, steps, torch):
     return e0.elapsed_time(e1)
 
 
-def e2e_run(fi, n, dtype, device, steps, torch):
+def e2e_run(fi, n, dtype, device, steps, torch, variant=None):
     """End to end through the public API with pinned host buffers: upload the
     state, run the iterations, read the residual norms and download the state."""
     names = ("P", "txx", "tyy", "tzz", "txy", "txz", "tyz", "Vx", "Vy", "Vz", "eta")
@@ -169,8 +170,10 @@ def e2e_run(fi, n, dtype, device, steps, torch):
         a = t.numpy().reshape(shape)
         a[...] = 0.0 if nm != "eta" else 5000.0
         host[nm] = (t, a)
-    h2d = sum(a.nbytes for _, a in host.values())
+    h2d = sum(a.nbytes for _, a in host.values()) + host["eta"][1].nbytes
     d2h = sum(a.nbytes for nm, (_, a) in host.items() if nm != "eta") + 8 * 12
+    if variant is not None:
+        m.set_variant(variant)
     m.advance(2)
     m.synchronize()
     t0 = time.perf_counter()
@@ -181,9 +184,8 @@ def e2e_run(fi, n, dtype, device, steps, torch):
     m.advance(steps)
     norms = m.residual_norms()
     for nm, (_, a) in host.items():
-        if nm == "eta":
-            continue
-        a[...] = m.get_field(nm)
+        if nm != "eta":
+            m.get_field(nm, out=a)
     dt = time.perf_counter() - t0
     m.close()
     return dt, h2d, d2h, norms
@@ -241,6 +243,9 @@ def main():
     ap.add_argument("--n", type=int, default=511)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape (profiling runs)")
+    ap.add_argument("--variant", type=int, default=None, help="fused launch shape index (implies --no-autotune)")
+    ap.add_argument("--dtypes", default="f64,f32", help="precisions to time, FP64 first")
     args = ap.parse_args()
     n = (args.n, args.n, args.n)
     ws, rank, local = dist_setup()
@@ -278,8 +283,16 @@ def main():
     A = a_eff_elements(n)
     res = {}
     clocks = None
-    for dtype in ("f64", "f32"):
+    for dtype in [d for d in args.dtypes.split(",") if d in ("f64", "f32")]:
         m = make_model(fi, n, dtype, local)
+        tuned = None
+        if args.variant is not None and m.path == "fused":
+            m.set_variant(args.variant)
+        elif m.path == "fused" and not args.no_autotune:
+            # the autotuner times every launch shape on the model itself (3 iterations each);
+            # those iterations are part of the warm-up
+            best, per = m.autotune(iters=3)
+            tuned = {"variant": best, "ms_per_iter": per}
         m.advance(args.warmup)
         m.synchronize()
         sampler = ClockSampler(local) if dtype == "f64" else None
@@ -299,7 +312,7 @@ def main():
         ms_max = float(t.item())
         norms = m.residual_norms()
         res[dtype] = {"ms_total": ms_max, "ms_per_step": ms_max / args.steps, "path": m.path,
-                      "finite": bool(norms[11] == 0.0)}
+                      "finite": bool(norms[11] == 0.0), "tuned": tuned}
         m.close()
         torch.cuda.empty_cache()
 
@@ -313,18 +326,22 @@ def main():
         "metric": metric, "value": value, "unit": "GB/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": f64["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic", "config": cfg, "kernel_path": f64["path"],
+        "launch_shape": {dt: (None if res[dt]["tuned"] is None else
+                              list(res[dt]["tuned"]["ms_per_iter"])[res[dt]["tuned"]["variant"]]) for dt in res},
         "gpu_launches": args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_kind, "traffic": (tr * n[0] * n[1] * n[2]) if tr else None,
                      "algorithmic_bytes": A * esz["f64"]},
-        "fp32": {"value": ws * A * 4 * args.steps / (res["f32"]["ms_total"] / 1e3) / 1e9, "unit": "GB/s",
-                 "ms_per_step": res["f32"]["ms_per_step"],
-                 "frac": (A * 4 / (res["f32"]["ms_per_step"] / 1e3) / 1e9) / peak},
         "reference_convention_teff": 23 * 8 * n[0] * n[1] * n[2] / (f64["ms_per_step"] / 1e3) / 1e9,
         "clocks": clocks,
     }
+    if "f32" in res:
+        line["fp32"] = {"value": ws * A * 4 * args.steps / (res["f32"]["ms_total"] / 1e3) / 1e9, "unit": "GB/s",
+                        "ms_per_step": res["f32"]["ms_per_step"],
+                        "frac": (A * 4 / (res["f32"]["ms_per_step"] / 1e3) / 1e9) / peak}
     if not args.no_e2e:
-        dt, h2d, d2h, _ = e2e_run(fi, n, "f64", local, args.steps, torch)
+        v64 = res["f64"]["tuned"]["variant"] if res["f64"]["tuned"] else None
+        dt, h2d, d2h, _ = e2e_run(fi, n, "f64", local, args.steps, torch, variant=v64)
         line["e2e"] = {"value": ws * A * 8 * args.steps / dt / 1e9, "unit": "GB/s",
                        "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                        "includes": "pinned host->device upload of the state, K iterations through the C ABI, "

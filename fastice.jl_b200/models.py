@@ -205,8 +205,12 @@ class _StokesBase:
                 arr = np.ascontiguousarray(np.broadcast_to(arr, shape))
         L.check(self.lib, self.lib.fi_model_set_field(self._h, L.FIELD_ID[name], arr.ctypes.data, arr.nbytes))
 
-    def get_field(self, name: str) -> np.ndarray:
-        arr = np.empty(self.field_shape(name), dtype=self.np_dtype)
+    def get_field(self, name: str, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """Interior of a field as a host array; ``out`` (contiguous, right shape and
+        dtype, e.g. a pinned buffer) is filled in place when given."""
+        arr = np.empty(self.field_shape(name), dtype=self.np_dtype) if out is None else out
+        if arr.shape != self.field_shape(name) or arr.dtype != self.np_dtype or not arr.flags.c_contiguous:
+            raise ValueError("out must be a contiguous array of the field's interior shape and the model's dtype")
         L.check(self.lib, self.lib.fi_model_get_field(self._h, L.FIELD_ID[name], arr.ctypes.data, arr.nbytes))
         return arr
 

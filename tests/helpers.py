@@ -65,7 +65,7 @@ class Pair:
     """Library model + oracle model for the same problem and initial state."""
 
     def __init__(self, n, bcs, rheo=None, gravity=(0.3, -0.2, 1.0), dtype="f64", path="auto", seed=0,
-                 extent=None, origin=None, library="fast", random_state=True, immersed_masks=None):
+                 extent=None, origin=None, library="fast", random_state=True, immersed_psi=None):
         fi = load_fastice()
         O = load_oracle()
         nd = len(n)
@@ -77,7 +77,7 @@ class Pair:
         sp = fi.pt_params(grid)
         dt = sp["Δτ"]
         g = {nm: float(gravity[d]) for d, nm in enumerate(("x", "y", "z")[:nd])}
-        cls = fi.IsothermalImmersedBoundaryFullStokesModel if immersed_masks is not None else fi.IsothermalFullStokesModel
+        cls = fi.IsothermalImmersedBoundaryFullStokesModel if immersed_psi is not None else fi.IsothermalFullStokesModel
         self.model = cls(grid=grid, boundary_conditions=make_bcs(fi, bcs, nd), gravity=g,
                          rheology=rheology_objects(fi, rheo), solver_params=sp, dtype=dtype, path=path,
                          library=library)
@@ -88,18 +88,17 @@ class Pair:
                            dt_V=tuple(dt["V"].get(k, 0.0) for k in ("x", "y", "z")),
                            g_val=tuple(float(v) for v in gravity), dtype=dtype, **oracle_rheo_kwargs(O, rheo))
         masks = None
-        if immersed_masks is not None:
-            masks = immersed_masks
+        if immersed_psi is not None:
+            # ω_from_ψ! on both sides: the model computes its masks on the device, the
+            # oracle with its own volume-fraction restatement
+            dxs = tuple(extent[d] / n[d] for d in range(nd))
+            masks = {grp: O.volfrac3d(n, dxs, immersed_psi[grp]) for grp in ("na", "ns")}
+            for grp in ("na", "ns"):
+                self.model.omega_from_psi(grp, immersed_psi[grp])
         self.oracle = O.OracleStokes(self.spec, masks=masks)
         self.state = STATE_3D if nd == 3 else STATE_2D
         npd = np.float64 if dtype == "f64" else np.float32
         rng = np.random.default_rng(seed)
-        if immersed_masks is not None:
-            for grp in ("na", "ns"):
-                for c in ("ccc", "vvv", "vcc", "cvc", "ccv", "vvc", "vcv", "cvv"):
-                    full = np.asarray(immersed_masks[grp][c], dtype=npd)
-                    sl = tuple(slice(1, s + 1) for s in self.model.field_shape(f"{grp}_{c}"))
-                    self.model.set_field(f"{grp}_{c}", full[sl])
         for name in self.state:
             shape = self.model.field_shape(name)
             if name == "eta":
