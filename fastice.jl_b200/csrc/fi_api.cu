@@ -5,6 +5,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <limits>
 #include <string>
@@ -91,6 +92,8 @@ struct fi_model {
     bool ib = false;
     long long iterations = 0;
     int *d_err = nullptr;  // device error word written by bounded waits
+    void *fP = nullptr;    // pressure forcing (defect-correction shadow models only)
+    fi_model *shadow = nullptr;  // FP32 model of the mixed-precision solve (created on first use)
     // TMA maps (128 bytes each) of every buffer the fused sweep reads
     alignas(64) unsigned char map_base[kState][128];
     alignas(64) unsigned char map_alt[kState][128];
@@ -131,6 +134,7 @@ struct fi_model {
         f.gz = (const T *)base[FI_FIELD_GZ];
         f.eta_lin = (const T *)base[FI_FIELD_ETA_LIN];
         f.A = (const T *)base[FI_FIELD_A];
+        f.fP = (const T *)fP;
         for (int c = 0; c < 8; c++) {
             f.wna[c] = (const T *)base[FI_FIELD_NA_CCC + c];
             f.wns[c] = (const T *)base[FI_FIELD_NS_CCC + c];
@@ -381,7 +385,7 @@ fi_status advance_t(fi_model *m, int niter) {
             st = run_batch<T>(m, velocity_batch);
             if (st != FI_OK) return st;
         }
-        m->eta_swapped = !m->eta_swapped;
+        if (!m->kp.freeze_eta) m->eta_swapped = !m->eta_swapped;
         m->iterations++;
     }
     return FI_OK;
@@ -573,6 +577,8 @@ fi_status fi_model_destroy(fi_model *m) {
     for (int f = 0; f < FI_FIELD_COUNT; f++) field_free(m->base[f], m->esz);
     for (int f = 0; f < kState; f++) field_free(m->alt[f], m->esz);
     if (m->d_err) cudaFree(m->d_err);
+    field_free(m->fP, m->esz);
+    if (m->shadow) fi_model_destroy(m->shadow);
     if (m->d_partials) cudaFree(m->d_partials);
     if (m->d_out) cudaFree(m->d_out);
     if (m->h_out) cudaFreeHost(m->h_out);
@@ -687,12 +693,268 @@ fi_status fi_model_path(const fi_model *m, int32_t *path) {
     return FI_OK;
 }
 
+}  // extern "C"
+
+// convergence measure of a norm vector (fi_conv_measure)
+static double measure_of(const fi_model *m, const fi_solve_opts *o, const double *norms) {
+    if (o->measure == FI_CONV_REL_SLAB) {
+        double rv = std::max(norms[1], std::max(norms[2], m->d.grid.nd == 3 ? norms[3] : 0.0));
+        double vmax = std::max(norms[8], std::max(norms[9], norms[10]));
+        double a = rv / (o->rho_g_inf > 0 ? o->rho_g_inf : 1.0);
+        double b = vmax > 0 ? norms[0] * o->length_z / vmax : norms[0];
+        return std::max(a, b);
+    }
+    double meas = norms[0];
+    for (int q = 1; q < 4; q++) meas = std::max(meas, norms[q]);
+    return meas;
+}
+
+// ---- mixed precision: FP32 PT sweeps inside an FP64 defect correction -------------
+// The FP32 shadow holds the same grid, boundary kinds and rheology; its gravity
+// fields carry -r_V and its pressure forcing r_P during corrections.
+static fi_status make_shadow(fi_model *m) {
+    if (m->shadow) return FI_OK;
+    fi_model_desc d = m->d;
+    d.dtype = FI_F32;
+    for (int c = 0; c < d.grid.nd; c++) d.gravity.kind[c] = FI_G_FIELD;
+    fi_model *s = nullptr;
+    fi_status st = fi_model_create(&d, &s);
+    if (st != FI_OK) return st;
+    if (field_alloc(&s->fP, s->elems, s->esz) != cudaSuccess) {
+        fi_model_destroy(s);
+        return set_error("forcing allocation failed"), FI_ERR_OOM;
+    }
+    cudaMemsetAsync(field_raw(s->fP, s->esz), 0, (s->elems + 64) * s->esz, s->stream);
+    for (int f : {(int)FI_FIELD_ETA_LIN, (int)FI_FIELD_A})
+        if (field_used(m, f)) {
+            cudaError_t e = launch_convert<double, float>((const double *)m->base[f], (float *)s->base[f],
+                                                          (long long)m->elems, 1.0, s->stream);
+            if (e != cudaSuccess) {
+                fi_model_destroy(s);
+                return cuda_fail(e, "shadow inputs");
+            }
+        }
+    if (s->path == FI_PATH_FUSED && fused3d_num_variants() > 4) {
+        s->fused_variant = 4;  // 32x16 tiles: the FP32 shape the autotuner prefers on the slab
+        fi_status es = encode_maps(s);
+        if (es != FI_OK) {
+            fi_model_destroy(s);
+            return es;
+        }
+    }
+    if (cudaStreamSynchronize(s->stream) != cudaSuccess) {
+        fi_model_destroy(s);
+        return cuda_fail(cudaGetLastError(), "shadow sync");
+    }
+    m->shadow = s;
+    return FI_OK;
+}
+
+template <typename S, typename D>
+static fi_status convert_field(void *dst, const void *src, long long n, double scale, cudaStream_t st) {
+    cudaError_t e = launch_convert<S, D>((const S *)src, (D *)dst, n, scale, st);
+    return e == cudaSuccess ? FI_OK : cuda_fail(e, "convert");
+}
+
+// Rounding floor of an FP32 residual evaluation on the shadow: a difference of two
+// values of magnitude S over a spacing dx carries an error of about eps32 * S / dx,
+// so r_V bottoms out near eps32 * max|P, τ| / dx and r_P near eps32 * max|V| / dx.
+// kFloorMargin (measured: the floors of the 3D manufactured solution sit 10-20x
+// above the bare estimate at 127^3-255^3) keeps the stop comfortably above them.
+constexpr double kFloorMargin = 48.0;
+constexpr double kEps32 = 1.1920928955078125e-07;
+
+static fi_status fp32_floors(fi_model *s, const double *nn, double *fl_P, double *fl_V) {
+    const float *fs[7];
+    int cnt = 0;
+    for (int f = FI_FIELD_P; f <= FI_FIELD_TYZ; f++)
+        if (field_used(s, f)) fs[cnt++] = (const float *)s->cur(f);
+    unsigned *d = reinterpret_cast<unsigned *>(s->d_out);
+    FI_CHECK_CUDA(launch_absmax_f32(fs, cnt, (long long)s->elems, d, s->stream), "abs max");
+    unsigned bits = 0;
+    FI_CHECK_CUDA(cudaMemcpyAsync(&bits, d, sizeof(bits), cudaMemcpyDeviceToHost, s->stream), "abs max copy");
+    FI_CHECK_CUDA(cudaStreamSynchronize(s->stream), "abs max sync");
+    float smax;
+    std::memcpy(&smax, &bits, sizeof(smax));
+    double idx = 0.0;
+    for (int c = 0; c < s->d.grid.nd; c++) idx = std::max(idx, s->kp.inv_dx[c]);
+    const double vmax = std::max(nn[8], std::max(nn[9], nn[10]));
+    *fl_V = kFloorMargin * kEps32 * (double)smax * idx;
+    *fl_P = kFloorMargin * kEps32 * vmax * idx;
+    return FI_OK;
+}
+
+static fi_status solve_mixed(fi_model *m, const fi_solve_opts *o, fi_solve_report *rep) {
+    if (!m->is_f64()) return set_error("the mixed-precision solve refines an FP64 model"), FI_ERR_ARG;
+    if (m->ib) return set_error("the mixed-precision solve does not cover the immersed-boundary model"), FI_ERR_UNSUPPORTED;
+    FI_CHECK_CUDA(cudaSetDevice(m->d.device), "cudaSetDevice");
+    fi_status st = make_shadow(m);
+    if (st != FI_OK) return st;
+    fi_model *s = m->shadow;
+    const long long n = (long long)m->elems;
+    const int nd = m->d.grid.nd;
+    const double inner_red = o->inner_reduction > 0 ? o->inner_reduction : 1e-5;
+    const int inner_max = o->inner_iter > 0 ? o->inner_iter : 50 * o->ncheck;
+    // a stage that has not halved its best residual over this many sweeps has stalled
+    int window = 0;
+    for (int c = 0; c < nd; c++) window = std::max(window, 2 * (m->d.grid.n[c] + 1));
+    window = std::max(window, 2 * o->ncheck);
+    const KParams kbase = s->kp;
+    KParams ka = kbase;  // phase A: the full problem in FP32
+    for (int c = 0; c < 3; c++) {
+        ka.g_kind[c] = m->kp.g_kind[c];
+        ka.g_val[c] = m->kp.g_val[c];
+    }
+    KParams kc = kbase;  // corrections: homogeneous boundary values, frozen η, forcing r
+    for (int d = 0; d < 3; d++)
+        for (int sd = 0; sd < 2; sd++)
+            for (int c = 0; c < 3; c++) kc.bc_val[d][sd][c] = 0.0;
+    kc.freeze_eta = 1;
+    kc.p_forcing = 1;
+    const int gf[3] = {FI_FIELD_GX, FI_FIELD_GY, FI_FIELD_GZ};
+    const int rf[3] = {FI_FIELD_RVX, FI_FIELD_RVY, FI_FIELD_RVZ};
+    auto t0 = std::chrono::steady_clock::now();
+    double norms[FI_NORMS_LEN];
+    int sweeps = 0;
+    const bool trace = std::getenv("FI_SOLVE_TRACE") != nullptr;  // per-check progress on stderr
+
+    // FP32 sweeps on the shadow, a check every ncheck, until (a) the FP64 tolerance
+    // in the solve's measure (phase A only), (b) the four residual inf-norms drop to
+    // target, (c) they reach the FP32 rounding floor, (d) the best of them has not
+    // halved for `window` sweeps, or (e) max_sweeps
+    auto stage = [&](bool phase_a, double target, int max_sweeps, const char *what) -> fi_status {
+        double best = 1e300;
+        int since = 0, done = 0;
+        double nn[FI_NORMS_LEN];
+        while (done < max_sweeps && sweeps < o->max_iter) {
+            int k = std::min(o->ncheck, o->max_iter - sweeps);
+            fi_status e = fi_model_advance(s, k);
+            if (e != FI_OK) return e;
+            sweeps += k;
+            done += k;
+            if ((e = fi_model_residual_norms(s, nn)) != FI_OK) return e;
+            const double rv = std::max(nn[1], std::max(nn[2], nn[3]));
+            const double r = std::max(nn[0], rv);
+            if (nn[11] != 0.0 || !std::isfinite(r)) {
+                rep->iterations = sweeps;
+                return set_error(std::string("simulation failed: non-finite residual in the ") + what), FI_ERR_DIVERGED;
+            }
+            double fl_P = 0, fl_V = 0;
+            if ((e = fp32_floors(s, nn, &fl_P, &fl_V)) != FI_OK) return e;
+            if (trace)
+                std::fprintf(stderr, "[fi mixed] %s sweeps=%d r=%.3e target=%.3e floors P %.2e V %.2e\n", what, sweeps,
+                             r, target, fl_P, fl_V);
+            if (phase_a && measure_of(s, o, nn) < o->tol) break;
+            if (r <= target) break;
+            if (nn[0] <= fl_P && rv <= fl_V) break;
+            if (r < 0.5 * best) {
+                best = r;
+                since = 0;
+            } else if ((since += k) >= window) {
+                break;
+            }
+        }
+        return FI_OK;
+    };
+
+    // ---- phase A: FP32 PT on the full problem down to the FP32 floor
+    for (int f = 0; f < kState; f++)
+        if (field_used(m, f) && (st = convert_field<double, float>(s->cur(f), m->cur(f), n, 1.0, m->stream)) != FI_OK)
+            return st;
+    for (int f : {(int)FI_FIELD_ETA, (int)FI_FIELD_ETA_NEXT})
+        if ((st = convert_field<double, float>(s->cur(f), m->cur(f), n, 1.0, m->stream)) != FI_OK) return st;
+    for (int c = 0; c < nd; c++)
+        if (m->kp.g_kind[c] == FI_G_FIELD &&
+            (st = convert_field<double, float>(s->base[gf[c]], m->base[gf[c]], n, 1.0, m->stream)) != FI_OK)
+            return st;
+    FI_CHECK_CUDA(cudaStreamSynchronize(m->stream), "mixed sync");
+    s->kp = ka;
+    if ((st = stage(true, 0.0, o->max_iter, "fp32 phase")) != FI_OK) return st;
+    for (int f = 0; f < kState; f++)
+        if (field_used(m, f) && (st = convert_field<float, double>(m->cur(f), s->cur(f), n, 1.0, s->stream)) != FI_OK)
+            return st;
+    for (int f : {(int)FI_FIELD_ETA, (int)FI_FIELD_ETA_NEXT})
+        if ((st = convert_field<float, double>(m->cur(f), s->cur(f), n, 1.0, s->stream)) != FI_OK) return st;
+    FI_CHECK_CUDA(cudaStreamSynchronize(s->stream), "mixed sync");
+
+    // ---- phase B: FP64 defect correction with FP32 correction sweeps
+    int outer = 0;
+    double best_outer = 1e300;
+    while (true) {
+        // viscosity from the current stresses (Picard step), then τ = 2η dev(ε̇(V)), BCs
+        Ptrs<double> f = m->ptrs<double>();
+        FI_CHECK_CUDA(launch_eta_from_tau<double>(m->g, m->kp, f, m->stream), "eta refresh");
+        m->eta_swapped = !m->eta_swapped;
+        if ((st = run_eta_batch<double>(m, FI_FIELD_ETA)) != FI_OK) return st;
+        FI_CHECK_CUDA(launch_compute_tau<double>(m->g, m->kp, m->ptrs<double>(), m->stream), "projection");
+        if ((st = run_batch<double>(m, stress_batch)) != FI_OK) return st;
+        // FP64 residual fields and norms
+        if ((st = residuals_t<double>(m)) != FI_OK) return st;
+        if ((st = norms_t<double>(m, norms)) != FI_OK) return st;
+        double meas = measure_of(m, o, norms);
+        if (trace) std::fprintf(stderr, "[fi mixed] outer=%d sweeps=%d fp64 measure=%.3e\n", outer, sweeps, meas);
+        rep->measure = meas;
+        std::memcpy(rep->norms, norms, sizeof(norms));
+        if (norms[11] != 0.0 || !std::isfinite(meas) || meas > 100.0 * best_outer) {
+            rep->iterations = sweeps;
+            rep->outer = outer;
+            return set_error("simulation failed: the defect correction diverged"), FI_ERR_DIVERGED;
+        }
+        best_outer = std::min(best_outer, meas);
+        if (meas < o->tol) {
+            rep->converged = 1;
+            break;
+        }
+        if (sweeps >= o->max_iter) break;
+        // the correction problem on the shadow: frozen η, forcing r_P and -r_V, zero state
+        if ((st = convert_field<double, float>(s->cur(FI_FIELD_ETA), m->cur(FI_FIELD_ETA), n, 1.0, m->stream)) != FI_OK)
+            return st;
+        if ((st = convert_field<double, float>(s->fP, m->base[FI_FIELD_RP], n, 1.0, m->stream)) != FI_OK) return st;
+        for (int c = 0; c < nd; c++)
+            if ((st = convert_field<double, float>(s->base[gf[c]], m->base[rf[c]], n, -1.0, m->stream)) != FI_OK)
+                return st;
+        for (int fl = 0; fl < kState; fl++) {
+            if (!field_used(s, fl)) continue;
+            FI_CHECK_CUDA(cudaMemsetAsync(field_raw(s->base[fl], s->esz), 0, (s->elems + 64) * s->esz, m->stream), "zero");
+            if (s->alt[fl])
+                FI_CHECK_CUDA(cudaMemsetAsync(field_raw(s->alt[fl], s->esz), 0, (s->elems + 64) * s->esz, m->stream),
+                              "zero");
+        }
+        FI_CHECK_CUDA(cudaStreamSynchronize(m->stream), "mixed sync");
+        s->kp = kc;
+        // target: inner_reduction of r0, but no further than a third of the tolerance
+        // (scaled from the solve's measure to the residual inf-norms)
+        const double r0 = std::max(std::max(norms[0], norms[1]), std::max(norms[2], norms[3]));
+        const double target = std::max(inner_red * r0, meas > 0 ? o->tol / 3.0 * r0 / meas : 0.0);
+        if ((st = stage(false, target, inner_max, "correction")) != FI_OK) {
+            rep->outer = outer;
+            return st;
+        }
+        // x += δ in FP64
+        for (int fl = 0; fl < kState; fl++)
+            if (field_used(m, fl)) {
+                cudaError_t e = launch_accumulate<double, float>((double *)m->cur(fl), (const float *)s->cur(fl), n,
+                                                                 m->stream);
+                if (e != cudaSuccess) return cuda_fail(e, "accumulate");
+            }
+        outer++;
+    }
+    rep->iterations = sweeps;
+    rep->outer = outer;
+    rep->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return rep->converged ? FI_OK : FI_ERR_TIMEOUT;
+}
+
+extern "C" {
+
 fi_status fi_model_solve(fi_model *m, const fi_solve_opts *o, fi_solve_report *rep) {
     if (!m || !o || !rep) return set_error("bad argument"), FI_ERR_ARG;
     if (o->ncheck <= 0 || o->max_iter <= 0) return set_error("ncheck and max_iter must be positive"), FI_ERR_ARG;
-    if (o->mode != FI_SOLVE_PLAIN) return set_error("use fi_model_solve_mixed for the mixed-precision solve"), FI_ERR_ARG;
+    if (o->mode != FI_SOLVE_PLAIN && o->mode != FI_SOLVE_MIXED) return set_error("unknown solve mode"), FI_ERR_ARG;
     std::memset(rep, 0, sizeof(*rep));
+    if (o->mode == FI_SOLVE_MIXED) return solve_mixed(m, o, rep);
     auto t0 = std::chrono::steady_clock::now();
+    const bool trace = std::getenv("FI_SOLVE_TRACE") != nullptr;
     int it = 0;
     fi_status st = FI_OK;
     double norms[FI_NORMS_LEN];
@@ -704,17 +966,8 @@ fi_status fi_model_solve(fi_model *m, const fi_solve_opts *o, fi_solve_report *r
         it += n;
         st = fi_model_residual_norms(m, norms);
         if (st != FI_OK) return st;
-        double meas;
-        if (o->measure == FI_CONV_REL_SLAB) {
-            double rv = std::max(norms[1], std::max(norms[2], m->d.grid.nd == 3 ? norms[3] : 0.0));
-            double vmax = std::max(norms[8], std::max(norms[9], norms[10]));
-            double a = rv / (o->rho_g_inf > 0 ? o->rho_g_inf : 1.0);
-            double b = vmax > 0 ? norms[0] * o->length_z / vmax : norms[0];
-            meas = std::max(a, b);
-        } else {
-            meas = norms[0];
-            for (int q = 1; q < 4; q++) meas = std::max(meas, norms[q]);
-        }
+        double meas = measure_of(m, o, norms);
+        if (trace) std::fprintf(stderr, "[fi solve] sweeps=%d measure=%.3e\n", it, meas);
         rep->measure = meas;
         std::memcpy(rep->norms, norms, sizeof(norms));
         if (norms[11] != 0.0 || !std::isfinite(meas)) {

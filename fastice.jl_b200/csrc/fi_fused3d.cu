@@ -230,7 +230,7 @@ __device__ __forceinline__ void sigma_point(const Ctx<T, TY> &c, const KParams &
         T etac = c.slot(S_ET, R_ET, s)[a];
         if (mask & F_P) {
             T &v = c.slot(S_P, R_P, s)[a];
-            v = v - divV * etac * q.dt_P;
+            v = v - (p.p_forcing ? divV + __ldg(out.fP + c.gidx(i, j, s)) : divV) * etac * q.dt_P;
         }
         if (mask & F_XX) {
             T &v = c.slot(S_XX, R_XX, s)[a];
@@ -527,7 +527,7 @@ __device__ __forceinline__ void v_plane(const Ctx<T, TY> &c, const KParams &p, c
         out.Vx[I] = vx_raw(c, p, q, in, t, i, j, I);
         out.Vy[I] = vy_raw(c, p, q, in, t, i, j, I);
         out.Vz[I] = vz_raw(c, p, q, in, t, i, j, I);
-        out.eta_next[I] = eta_raw(c, p, q, in, t, i, j, I);
+        if (!p.freeze_eta) out.eta_next[I] = eta_raw(c, p, q, in, t, i, j, I);
         return;
     }
     auto node_fixed = [](int kind) { return kind == FI_BC_SLIP || kind == FI_BC_VELOCITY; };
@@ -566,7 +566,7 @@ __device__ __forceinline__ void v_plane(const Ctx<T, TY> &c, const KParams &p, c
                      img_own<T>(t));
     }
     // ---- η_next at (C, C, C), Neumann / periodic ghosts
-    if (i <= n0 && j <= n1 && t >= 1 && t <= n2) {
+    if (!p.freeze_eta && i <= n0 && j <= n1 && t >= 1 && t <= n2) {
         T en = eta_raw(c, p, q, in, t, i, j, I);
         write_images(c, out.eta_next, en, img_center<T>(i, n0, c.perx, xl, xr, T(0), T(0), true),
                      img_center<T>(j, n1, c.pery, yl, yr, T(0), T(0), true),

@@ -46,6 +46,8 @@ struct KParams {
     int bc_kind[3][2];
     double bc_val[3][2][3];
     double small;  // immersed-boundary emptiness threshold (1e-6, or the FP32 value equivalent to it)
+    int freeze_eta;  // 1: η is held fixed (no η_next is computed or written)
+    int p_forcing;   // 1: the pressure update and r_P carry the forcing field fP (defect correction)
 };
 
 // the scalar parameters converted once to the compute type T (the conversion
@@ -81,6 +83,7 @@ struct Ptrs {
     T *rP, *rVx, *rVy, *rVz;
     const T *gx, *gy, *gz;
     const T *eta_lin, *A;
+    const T *fP;  // pressure forcing of the defect-correction problem (p_forcing)
     const T *wna[8];
     const T *wns[8];
 };
@@ -140,6 +143,16 @@ bool fused3d_encode_map(void *raw_base, const Geom &g, int esz, int ty, void *ma
 int fused3d_num_variants();
 int fused3d_variant_ty(int v);
 const char *fused3d_variant_name(int v);
+
+// ---- mixed-precision solve helpers (fi_mixed.cu) ----
+template <typename S, typename D>
+cudaError_t launch_convert(const S *src, D *dst, long long n, double scale, cudaStream_t s);
+template <typename D, typename S>
+cudaError_t launch_accumulate(D *x, const S *d, long long n, cudaStream_t s);
+template <typename T>
+cudaError_t launch_eta_from_tau(const Geom &g, const KParams &p, const Ptrs<T> &f, cudaStream_t s);
+// max |value| over up to 8 FP32 arrays of n elements each, as float bits in *out_bits
+cudaError_t launch_absmax_f32(const float *const *fields, int count, long long n, unsigned *out_bits, cudaStream_t s);
 
 // ---- level sets (fi_levelsets.cu) ----
 cudaError_t launch_volfrac3d(const Geom &g, const double dx[3], const double *psi, double *const w[8], cudaStream_t s);

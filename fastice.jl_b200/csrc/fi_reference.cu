@@ -52,7 +52,7 @@ __global__ void __launch_bounds__(256) update_sigma_kernel(Geom g, KParams p, Pt
         T exy = T(0.5) * ((Vy[I] - Vy[I - 1]) * idx + (Vx[I] - Vx[I - sx]) * idy);
         T divV = exx + eyy;
         T etac = eta[I];
-        f.P[I] = f.P[I] - divV * etac * T(p.dt_P);
+        f.P[I] = f.P[I] - (p.p_forcing ? divV + f.fP[I] : divV) * etac * T(p.dt_P);
         f.txx[I] = f.txx[I] - (f.txx[I] - T(2.0) * etac * (exx - divV / T(3.0))) * T(p.dt_tau[0]);
         f.tyy[I] = f.tyy[I] - (f.tyy[I] - T(2.0) * etac * (eyy - divV / T(3.0))) * T(p.dt_tau[1]);
         T exy_eta = h(h(eta[I - 1 - sx] + eta[I - sx]) + h(eta[I - 1] + eta[I]));
@@ -71,7 +71,7 @@ __global__ void __launch_bounds__(256) update_sigma_kernel(Geom g, KParams p, Pt
         T eyz = T(0.5) * ((Vz[I] - Vz[I - sx]) * idy + (Vy[I] - Vy[I - sxy]) * idz);
         T divV = exx + eyy + ezz;
         T etac = eta[I];
-        f.P[I] = f.P[I] - divV * etac * T(p.dt_P);
+        f.P[I] = f.P[I] - (p.p_forcing ? divV + f.fP[I] : divV) * etac * T(p.dt_P);
         f.txx[I] = f.txx[I] - (f.txx[I] - T(2.0) * etac * (exx - divV / T(3.0))) * T(p.dt_tau[0]);
         f.tyy[I] = f.tyy[I] - (f.tyy[I] - T(2.0) * etac * (eyy - divV / T(3.0))) * T(p.dt_tau[1]);
         f.tzz[I] = f.tzz[I] - (f.tzz[I] - T(2.0) * etac * (ezz - divV / T(3.0))) * T(p.dt_tau[2]);
@@ -91,7 +91,7 @@ __global__ void __launch_bounds__(256) update_sigma_kernel(Geom g, KParams p, Pt
         T ezz = (ns[W_CCV][I + sxy] * Vz[I + sxy] - ns[W_CCV][I] * Vz[I]) * idz;
         T divV = exx + eyy + ezz;
         T etac = eta[I];
-        f.P[I] = f.P[I] - divV * etac * T(p.dt_P);
+        f.P[I] = f.P[I] - (p.p_forcing ? divV + f.fP[I] : divV) * etac * T(p.dt_P);
         f.txx[I] = f.txx[I] - (f.txx[I] - T(2.0) * etac * (exx - divV / T(3.0))) * T(p.dt_tau[0]);
         f.tyy[I] = f.tyy[I] - (f.tyy[I] - T(2.0) * etac * (eyy - divV / T(3.0))) * T(p.dt_tau[1]);
         f.tzz[I] = f.tzz[I] - (f.tzz[I] - T(2.0) * etac * (ezz - divV / T(3.0))) * T(p.dt_tau[2]);
@@ -149,7 +149,8 @@ __global__ void __launch_bounds__(256) update_V_kernel(Geom g, KParams p, Ptrs<T
                       T(p.dt_V[1]);
         T lxy = h(h(txy[I] + txy[I + 1]) + h(txy[I + sx] + txy[I + sx + 1]));
         T s2 = T(0.5) * (txx[I] * txx[I] + tyy[I] * tyy[I]) + lxy * lxy;
-        f.eta_next[I] = rheology_s2(p, T(p.rheo_A), T(p.rheo_inv_eta_reg), f.eta_lin, f.A, eta[I], I, s2);
+        if (!p.freeze_eta)
+            f.eta_next[I] = rheology_s2(p, T(p.rheo_A), T(p.rheo_inv_eta_reg), f.eta_lin, f.A, eta[I], I, s2);
         return;
     }
     const T idz = T(p.inv_dx[2]);
@@ -217,7 +218,7 @@ __global__ void __launch_bounds__(256) update_V_kernel(Geom g, KParams p, Ptrs<T
     T lxz = h(h(txz[I] + txz[I + 1]) + h(txz[I + sxy] + txz[I + sxy + 1]));
     T lyz = h(h(tyz[I] + tyz[I + sx]) + h(tyz[I + sxy] + tyz[I + sxy + sx]));
     T s = T(0.5) * (txx[I] * txx[I] + tyy[I] * tyy[I] + tzz[I] * tzz[I]) + lxy * lxy + lxz * lxz + lyz * lyz;
-    f.eta_next[I] = rheology_s2(p, T(p.rheo_A), T(p.rheo_inv_eta_reg), f.eta_lin, f.A, eta[I], I, s);
+    if (!p.freeze_eta) f.eta_next[I] = rheology_s2(p, T(p.rheo_A), T(p.rheo_inv_eta_reg), f.eta_lin, f.A, eta[I], I, s);
 }
 
 // ---------------------------------------------------------------------------
@@ -287,6 +288,7 @@ __global__ void __launch_bounds__(256) compute_residuals_kernel(Geom g, KParams 
     Idx x = vertex_index(g);
     if (!x.ok) return;
     Resid<T, ND, IB> r = residual_at<T, ND, IB>(g, p, f, x.I);
+    if (p.p_forcing) r.rP = r.rP + f.fP[x.I];
     f.rP[x.I] = r.rP;
     f.rVx[x.I] = r.rVx;
     f.rVy[x.I] = r.rVy;
@@ -441,6 +443,7 @@ __global__ void __launch_bounds__(kNormThreads) residual_norms_kernel(Geom g, KP
         int k = ND == 3 ? int(r2 / ny) + 1 : 0;
         long long I = (long long)i + g.pitch * ((long long)j + g.rows * (long long)k);
         Resid<T, ND, IB> r = residual_at<T, ND, IB>(g, p, f, I);
+        if (p.p_forcing) r.rP = r.rP + f.fP[I];
         bool cx = i <= g.n[0], cy = j <= g.n[1], cz = ND == 3 ? k <= g.n[2] : true;
         // r_P at (C,C,C)
         if (cx && cy && cz) {

@@ -283,20 +283,22 @@ class _StokesBase:
         return a.value, b.value, c.value
 
     def solve(self, *, max_iter: int, ncheck: int, tol: float, measure: str = "abs_inf", rho_g_inf: float = 1.0,
-              length_z: float = 1.0):
+              length_z: float = 1.0, mode: str = "plain", inner_iter: int = 0, inner_reduction: float = 0.0):
         """Driver loop with a convergence check every ``ncheck`` iterations
-        (tm_stokes_chmy.jl:283-305); returns a dict report."""
+        (tm_stokes_chmy.jl:283-305); returns a dict report.  ``mode="mixed"``
+        (FP64 models): FP32 PT sweeps inside an FP64 defect correction."""
         o = L.fi_solve_opts()
         o.max_iter, o.ncheck, o.tol = int(max_iter), int(ncheck), float(tol)
         o.measure = {"abs_inf": L.FI_CONV_ABS_INF, "rel_slab": L.FI_CONV_REL_SLAB}[measure]
         o.rho_g_inf, o.length_z = float(rho_g_inf), float(length_z)
-        o.mode = L.FI_SOLVE_PLAIN
+        o.mode = {"plain": L.FI_SOLVE_PLAIN, "mixed": L.FI_SOLVE_MIXED}[mode]
+        o.inner_iter, o.inner_reduction = int(inner_iter), float(inner_reduction)
         r = L.fi_solve_report()
         st = self.lib.fi_model_solve(self._h, C.byref(o), C.byref(r))
         if st not in (L.FI_OK, L.FI_ERR_TIMEOUT):
             L.check(self.lib, st)
-        return {"iterations": r.iterations, "measure": r.measure, "norms": list(r.norms), "seconds": r.seconds,
-                "converged": bool(r.converged)}
+        return {"iterations": r.iterations, "outer": r.outer, "measure": r.measure, "norms": list(r.norms),
+                "seconds": r.seconds, "converged": bool(r.converged)}
 
 
 class IsothermalFullStokesModel(_StokesBase):

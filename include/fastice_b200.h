@@ -195,8 +195,9 @@ typedef struct {
     double rho_g_inf;       /* FI_CONV_REL_SLAB: ||ρg||∞ */
     double length_z;        /* FI_CONV_REL_SLAB: L_z */
     int32_t mode;           /* fi_solve_mode: MIXED = FP32 sweeps in FP64 defect correction */
-    int32_t inner_iter;     /* MIXED: FP32 sweeps per correction */
-    double inner_reduction; /* MIXED: stop a correction once its residual dropped by this factor */
+    int32_t inner_iter;     /* MIXED: most FP32 sweeps per correction (0: 50 * ncheck) */
+    double inner_reduction; /* MIXED: stop a correction once its residual dropped by this
+                               factor (0: 1e-5) or stopped halving over two checks */
 } fi_solve_opts;
 
 typedef struct {

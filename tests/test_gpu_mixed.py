@@ -1,0 +1,55 @@
+"""Mixed-precision refinement (FP32 PT sweeps inside an FP64 defect correction)
+reaches the FP64 tolerance and agrees with the plain FP64 solve, on the 3D
+manufactured solution of stokes_manufactured_solution_free_slip_3D.jl."""
+import math
+
+import numpy as np
+import pytest
+
+from conftest import load_fastice
+from helpers import mms3d_error, mms3d_model
+
+pytestmark = pytest.mark.gpu
+
+
+def test_mixed_reaches_fp64_tolerance_and_matches_plain():
+    fi = load_fastice()
+    n = 24
+    kw = dict(max_iter=200 * n, ncheck=n, tol=1e-8)
+    grid, plain = mms3d_model(fi, n)
+    rp = plain.solve(**kw)
+    _, mixed = mms3d_model(fi, n)
+    rm = mixed.solve(mode="mixed", **kw)
+    assert rp["converged"] and rm["converged"], (rp, rm)
+    assert rm["measure"] < 1e-8 and rm["outer"] >= 1
+    for name in ("Vx", "Vy", "Vz", "txx", "txy"):
+        a, b = mixed.get_field(name), plain.get_field(name)
+        rel = np.max(np.abs(a - b)) / np.max(np.abs(b))
+        assert rel < 1e-7, (name, rel)
+    # the exact pressure is zero and the free-slip box fixes it only up to a
+    # constant: compare the mean-free parts on the deviatoric stress scale
+    a, b = mixed.get_field("P"), plain.get_field("P")
+    scale = np.max(np.abs(plain.get_field("txx")))
+    assert np.max(np.abs((a - a.mean()) - (b - b.mean()))) < 1e-7 * scale
+    # both carry the same discretisation error against the manufactured solution
+    ep, em = mms3d_error(fi, grid, plain), mms3d_error(fi, grid, mixed)
+    assert abs(ep - em) < 1e-6 * ep and ep < 1e-2
+    plain.close()
+    mixed.close()
+
+
+def test_fp32_alone_stalls_above_fp64_tolerance():
+    fi = load_fastice()
+    n = 24
+    _, m = mms3d_model(fi, n, dtype="f32")
+    r = m.solve(max_iter=100 * n, ncheck=n, tol=1e-8)
+    assert not r["converged"] and r["measure"] > 1e-7
+    m.close()
+
+
+def test_mixed_rejects_fp32_model():
+    fi = load_fastice()
+    _, m = mms3d_model(fi, 12, dtype="f32")
+    with pytest.raises(fi.FastIceError):
+        m.solve(mode="mixed", max_iter=100, ncheck=10, tol=1e-8)
+    m.close()
