@@ -8,14 +8,14 @@ from . import _lib
 from ._lib import FastIceError
 from .grids import Center, UniformGrid, Vertex, flip
 from .levelsets import compute_levelset_from_dem, omega_from_psi
-from .models import (Arch, FieldRef, IsothermalFullStokesModel, IsothermalImmersedBoundaryFullStokesModel,
+from .models import (Arch, BatchedStokes2D, FieldRef, IsothermalFullStokesModel, IsothermalImmersedBoundaryFullStokesModel,
                      advance_iteration, compute_residuals, interior, pt_params, set_)
 from .physics import (ArrayField, BoundaryCondition, ConstantField, FunctionField, LinearViscousRheology, OneField,
                       PBC, Periodic, PowerLawRheology, Relaxation, SBC, Slip, TBC, Traction, VBC, ValueField, Velocity,
                       ViscoplasticRegularisation, ZeroField, glen_regularised)
 
 __all__ = [
-    "FastIceError", "Center", "Vertex", "UniformGrid", "flip", "compute_levelset_from_dem", "omega_from_psi", "Arch",
+    "FastIceError", "BatchedStokes2D", "Center", "Vertex", "UniformGrid", "flip", "compute_levelset_from_dem", "omega_from_psi", "Arch",
     "FieldRef", "IsothermalFullStokesModel", "IsothermalImmersedBoundaryFullStokesModel", "advance_iteration",
     "compute_residuals", "interior", "pt_params", "set_", "ArrayField", "BoundaryCondition", "ConstantField",
     "FunctionField", "LinearViscousRheology", "OneField", "PBC", "Periodic", "PowerLawRheology", "Relaxation", "SBC",

@@ -88,6 +88,18 @@ class fi_state_view(C.Structure):
         ("g", C.c_void_p * 3), ("na", C.c_void_p * 8), ("ns", C.c_void_p * 8), ("pitch", C.c_size_t)]
 
 
+class fi_batch_opts(C.Structure):
+    _fields_ = [("max_iter", C.c_int32), ("ncheck", C.c_int32), ("tol", C.c_double), ("use_graph", C.c_int32),
+                ("window", C.c_int32)]
+
+
+class fi_batch_item(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("status", C.c_int32), ("measure", C.c_double)]
+
+
+FI_ITEM_STATUS = {0: "active", 1: "converged", 2: "stalled", 3: "diverged", 4: "max_iter"}
+
+
 class FastIceError(RuntimeError):
     """Raised for a non-FI_OK status; ``status`` holds the fi_status code."""
 
@@ -126,6 +138,21 @@ SIGNATURES = [
     ("fi_model_autotune", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
     ("fi_residual_norms_noalloc", C.c_int, [C.POINTER(fi_model_desc), C.POINTER(fi_state_view), C.c_void_p,
                                             C.c_void_p]),
+    ("fi_batch_create", C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_void_p)]),
+    ("fi_batch_destroy", C.c_int, [C.c_void_p]),
+    ("fi_batch_add", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("fi_batch_remove", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("fi_batch_size", C.c_int32, [C.c_void_p]),
+    ("fi_batch_step", C.c_int, [C.c_void_p, C.POINTER(fi_batch_opts), C.c_int32, C.POINTER(fi_batch_item),
+                                C.POINTER(C.c_int32)]),
+    ("fi_batch_advance", C.c_int, [C.c_void_p, C.c_int32]),
+    ("fi_batch_solve", C.c_int, [C.c_void_p, C.POINTER(fi_batch_opts), C.POINTER(fi_batch_item),
+                                 C.POINTER(C.c_double)]),
+    ("fi_batch_measure", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    ("fi_batch_variant_count", C.c_int, []),
+    ("fi_batch_variant_name", C.c_char_p, [C.c_int32]),
+    ("fi_batch_set_variant", C.c_int, [C.c_void_p, C.c_int32]),
+    ("fi_batch_autotune", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
 ]
 
 _libs = {}

@@ -11,7 +11,7 @@
 #include <string>
 #include <vector>
 
-#include "fi_internal.h"
+#include "fi_model.h"
 
 namespace fi {
 
@@ -35,8 +35,6 @@ using namespace fi;
     } while (0)
 
 namespace {
-
-constexpr int kState = 10;  // P, txx, tyy, tzz, txy, txz, tyz, Vx, Vy, Vz
 
 // staggered location of each field (0 = Center, 1 = Vertex) per dim
 void field_loc(int field, int loc[3]) {
@@ -70,78 +68,6 @@ void field_free(void *field_ptr, size_t esz) {
 }
 
 }  // namespace
-
-struct fi_model {
-    fi_model_desc d{};
-    Geom g{};
-    KParams kp{};
-    size_t esz = 8;
-    size_t elems = 0;
-    void *base[FI_FIELD_COUNT] = {};
-    void *alt[kState] = {};
-    int parity = 0;           // 1: alt[] holds the current P..Vz
-    bool eta_swapped = false; // true: base[ETA_NEXT] holds the current eta
-    cudaStream_t stream = nullptr;
-    double *d_partials = nullptr;
-    double *d_out = nullptr;
-    double *h_out = nullptr;
-    int nblk = 0;
-    int path = FI_PATH_REFERENCE;
-    int fused_variant = 0;
-    int maps_ty = -1;  // tile height the tensor maps were encoded for
-    bool ib = false;
-    long long iterations = 0;
-    int *d_err = nullptr;  // device error word written by bounded waits
-    void *fP = nullptr;    // pressure forcing (defect-correction shadow models only)
-    fi_model *shadow = nullptr;  // FP32 model of the mixed-precision solve (created on first use)
-    // TMA maps (128 bytes each) of every buffer the fused sweep reads
-    alignas(64) unsigned char map_base[kState][128];
-    alignas(64) unsigned char map_alt[kState][128];
-    alignas(64) unsigned char map_eta[2][128];  // base[ETA], base[ETA_NEXT]
-
-    bool is_f64() const { return d.dtype == FI_F64; }
-
-    void *cur(int field) const {
-        if (field < kState) return parity ? alt[field] : base[field];
-        if (field == FI_FIELD_ETA) return eta_swapped ? base[FI_FIELD_ETA_NEXT] : base[FI_FIELD_ETA];
-        if (field == FI_FIELD_ETA_NEXT) return eta_swapped ? base[FI_FIELD_ETA] : base[FI_FIELD_ETA_NEXT];
-        return base[field];
-    }
-    void *nxt(int field) const { return parity ? base[field] : alt[field]; }
-
-    template <typename T>
-    Ptrs<T> ptrs(bool next_state = false) const {
-        Ptrs<T> f{};
-        auto S = [&](int fld) { return (T *)(next_state ? nxt(fld) : cur(fld)); };
-        f.P = S(FI_FIELD_P);
-        f.txx = S(FI_FIELD_TXX);
-        f.tyy = S(FI_FIELD_TYY);
-        f.tzz = S(FI_FIELD_TZZ);
-        f.txy = S(FI_FIELD_TXY);
-        f.txz = S(FI_FIELD_TXZ);
-        f.tyz = S(FI_FIELD_TYZ);
-        f.Vx = S(FI_FIELD_VX);
-        f.Vy = S(FI_FIELD_VY);
-        f.Vz = S(FI_FIELD_VZ);
-        f.eta = (T *)cur(FI_FIELD_ETA);
-        f.eta_next = (T *)cur(FI_FIELD_ETA_NEXT);
-        f.rP = (T *)base[FI_FIELD_RP];
-        f.rVx = (T *)base[FI_FIELD_RVX];
-        f.rVy = (T *)base[FI_FIELD_RVY];
-        f.rVz = (T *)base[FI_FIELD_RVZ];
-        f.gx = (const T *)base[FI_FIELD_GX];
-        f.gy = (const T *)base[FI_FIELD_GY];
-        f.gz = (const T *)base[FI_FIELD_GZ];
-        f.eta_lin = (const T *)base[FI_FIELD_ETA_LIN];
-        f.A = (const T *)base[FI_FIELD_A];
-        f.fP = (const T *)fP;
-        for (int c = 0; c < 8; c++) {
-            f.wna[c] = (const T *)base[FI_FIELD_NA_CCC + c];
-            f.wns[c] = (const T *)base[FI_FIELD_NS_CCC + c];
-        }
-        return f;
-    }
-};
 
 namespace {
 
@@ -454,6 +380,26 @@ bool fused_ok(const fi_model *m) {
 }
 
 }  // namespace
+
+// Second state buffer of every state field, for drivers that double-buffer a
+// model whose own path updates in place (the batched 2D sweep); a new buffer
+// starts as a copy of the current state, ghosts included.
+fi_status model_ensure_second_state(fi_model *m) {
+    for (int f = 0; f < kState; f++) {
+        if (!field_used(m, f) || m->alt[f]) continue;
+        if (field_alloc(&m->alt[f], m->elems, m->esz) != cudaSuccess) {
+            cudaGetLastError();
+            set_error("device allocation failed (second state buffer)");
+            return FI_ERR_OOM;
+        }
+        void *dst = field_raw(m->parity ? m->base[f] : m->alt[f], m->esz);
+        const void *src = field_raw(m->parity ? m->alt[f] : m->base[f], m->esz);
+        FI_CHECK_CUDA(cudaMemcpyAsync(dst, src, (m->elems + 64) * m->esz, cudaMemcpyDeviceToDevice, m->stream),
+                      "second state buffer");
+    }
+    FI_CHECK_CUDA(cudaStreamSynchronize(m->stream), "second state buffer");
+    return FI_OK;
+}
 
 extern "C" {
 

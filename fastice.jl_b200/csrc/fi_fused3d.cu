@@ -543,27 +543,35 @@ __device__ __forceinline__ void v_plane(const Ctx<T, TY> &c, const KParams &p, c
                      img_center<T>(j, n1, c.pery, yl, yr, q.bc_val[1][0][0], q.bc_val[1][1][0], false),
                      img_center<T>(t, n2, false, zl, zr, q.bc_val[2][0][0], q.bc_val[2][1][0], false));
     }
+    // A value on a fixed node of its own dim d is written there last by the
+    // reference's dim-d node assignment, which spans the ghosts of the dims before
+    // d: its images along those dims are copies, not mirrors (as_copies).
+    auto as_copies = [](Img<T> d) {
+        d.dir[1] = false;
+        d.dir[2] = false;
+        return d;
+    };
     // ---- V.y at (C, V, C)
     if (i <= n0 && t >= 1 && t <= n2 && !(c.pery && j == n1 + 1)) {
         T v;
+        const bool y_node = !c.pery && ((j == 1 && node_fixed(yl)) || (j == n1 + 1 && node_fixed(yr)));
         if (!c.pery && j == 1 && node_fixed(yl)) v = q.bc_val[1][0][1];
         else if (!c.pery && j == n1 + 1 && node_fixed(yr)) v = q.bc_val[1][1][1];
         else v = vy_raw(c, p, q, in, t, i, j, I);
-        write_images(c, out.Vy, v,
-                     img_center<T>(i, n0, c.perx, xl, xr, q.bc_val[0][0][1], q.bc_val[0][1][1], false),
-                     img_vertex<T>(j, n1, c.pery),
+        Img<T> ix = img_center<T>(i, n0, c.perx, xl, xr, q.bc_val[0][0][1], q.bc_val[0][1][1], false);
+        write_images(c, out.Vy, v, y_node ? as_copies(ix) : ix, img_vertex<T>(j, n1, c.pery),
                      img_center<T>(t, n2, false, zl, zr, q.bc_val[2][0][1], q.bc_val[2][1][1], false));
     }
     // ---- V.z at (C, C, V)
     if (i <= n0 && j <= n1 && t >= 1 && t <= n2 + 1) {
         T v;
+        const bool z_node = (t == 1 && node_fixed(zl)) || (t == n2 + 1 && node_fixed(zr));
         if (t == 1 && node_fixed(zl)) v = q.bc_val[2][0][2];
         else if (t == n2 + 1 && node_fixed(zr)) v = q.bc_val[2][1][2];
         else v = vz_raw(c, p, q, in, t, i, j, I);
-        write_images(c, out.Vz, v,
-                     img_center<T>(i, n0, c.perx, xl, xr, q.bc_val[0][0][2], q.bc_val[0][1][2], false),
-                     img_center<T>(j, n1, c.pery, yl, yr, q.bc_val[1][0][2], q.bc_val[1][1][2], false),
-                     img_own<T>(t));
+        Img<T> ix = img_center<T>(i, n0, c.perx, xl, xr, q.bc_val[0][0][2], q.bc_val[0][1][2], false);
+        Img<T> iy = img_center<T>(j, n1, c.pery, yl, yr, q.bc_val[1][0][2], q.bc_val[1][1][2], false);
+        write_images(c, out.Vz, v, z_node ? as_copies(ix) : ix, z_node ? as_copies(iy) : iy, img_own<T>(t));
     }
     // ---- η_next at (C, C, C), Neumann / periodic ghosts
     if (!p.freeze_eta && i <= n0 && j <= n1 && t >= 1 && t <= n2) {

@@ -1,0 +1,91 @@
+// fi_model.h -- the model object behind the opaque fi_model handle, shared by
+// the translation units that drive a model's device state (fi_api.cu,
+// fi_batch.cu).
+#pragma once
+
+#include "fi_internal.h"
+
+namespace fi {
+constexpr int kState = 10;  // P, txx, tyy, tzz, txy, txz, tyz, Vx, Vy, Vz
+}  // namespace fi
+
+struct fi_model {
+    using Geom = fi::Geom;
+    using KParams = fi::KParams;
+    template <typename T>
+    using Ptrs = fi::Ptrs<T>;
+    static constexpr int kState = fi::kState;
+
+    fi_model_desc d{};
+    Geom g{};
+    KParams kp{};
+    size_t esz = 8;
+    size_t elems = 0;
+    void *base[FI_FIELD_COUNT] = {};
+    void *alt[kState] = {};
+    int parity = 0;           // 1: alt[] holds the current P..Vz
+    bool eta_swapped = false; // true: base[ETA_NEXT] holds the current eta
+    cudaStream_t stream = nullptr;
+    double *d_partials = nullptr;
+    double *d_out = nullptr;
+    double *h_out = nullptr;
+    int nblk = 0;
+    int path = FI_PATH_REFERENCE;
+    int fused_variant = 0;
+    int maps_ty = -1;  // tile height the tensor maps were encoded for
+    bool ib = false;
+    long long iterations = 0;
+    int *d_err = nullptr;  // device error word written by bounded waits
+    void *fP = nullptr;    // pressure forcing (defect-correction shadow models only)
+    fi_model *shadow = nullptr;  // FP32 model of the mixed-precision solve (created on first use)
+    // TMA maps (128 bytes each) of every buffer the fused sweep reads
+    alignas(64) unsigned char map_base[kState][128];
+    alignas(64) unsigned char map_alt[kState][128];
+    alignas(64) unsigned char map_eta[2][128];  // base[ETA], base[ETA_NEXT]
+
+    bool is_f64() const { return d.dtype == FI_F64; }
+
+    void *cur(int field) const {
+        if (field < kState) return parity ? alt[field] : base[field];
+        if (field == FI_FIELD_ETA) return eta_swapped ? base[FI_FIELD_ETA_NEXT] : base[FI_FIELD_ETA];
+        if (field == FI_FIELD_ETA_NEXT) return eta_swapped ? base[FI_FIELD_ETA] : base[FI_FIELD_ETA_NEXT];
+        return base[field];
+    }
+    void *nxt(int field) const { return parity ? base[field] : alt[field]; }
+
+    template <typename T>
+    Ptrs<T> ptrs(bool next_state = false) const {
+        Ptrs<T> f{};
+        auto S = [&](int fld) { return (T *)(next_state ? nxt(fld) : cur(fld)); };
+        f.P = S(FI_FIELD_P);
+        f.txx = S(FI_FIELD_TXX);
+        f.tyy = S(FI_FIELD_TYY);
+        f.tzz = S(FI_FIELD_TZZ);
+        f.txy = S(FI_FIELD_TXY);
+        f.txz = S(FI_FIELD_TXZ);
+        f.tyz = S(FI_FIELD_TYZ);
+        f.Vx = S(FI_FIELD_VX);
+        f.Vy = S(FI_FIELD_VY);
+        f.Vz = S(FI_FIELD_VZ);
+        f.eta = (T *)cur(FI_FIELD_ETA);
+        f.eta_next = (T *)cur(FI_FIELD_ETA_NEXT);
+        f.rP = (T *)base[FI_FIELD_RP];
+        f.rVx = (T *)base[FI_FIELD_RVX];
+        f.rVy = (T *)base[FI_FIELD_RVY];
+        f.rVz = (T *)base[FI_FIELD_RVZ];
+        f.gx = (const T *)base[FI_FIELD_GX];
+        f.gy = (const T *)base[FI_FIELD_GY];
+        f.gz = (const T *)base[FI_FIELD_GZ];
+        f.eta_lin = (const T *)base[FI_FIELD_ETA_LIN];
+        f.A = (const T *)base[FI_FIELD_A];
+        f.fP = (const T *)fP;
+        for (int c = 0; c < 8; c++) {
+            f.wna[c] = (const T *)base[FI_FIELD_NA_CCC + c];
+            f.wns[c] = (const T *)base[FI_FIELD_NS_CCC + c];
+        }
+        return f;
+    }
+};
+
+// allocates the second buffer of every state field a model lacks (fi_api.cu)
+fi_status model_ensure_second_state(fi_model *m);

@@ -326,6 +326,112 @@ class IsothermalImmersedBoundaryFullStokesModel(_StokesBase):
 
 
 # -- free functions with the reference names ----------------------------------------
+class BatchedStokes2D:
+    """Many independent 2D models solved together (fi_batch_* in the C ABI).
+
+    One persistent launch per PT iteration covers the tiles of every instance
+    still iterating; checks, retirement and work-list compaction run on the
+    device, and the check-to-check step replays as a CUDA graph.  Each member
+    follows advance_iteration! of its own model (linear rheology, viscosity held
+    at the member's current η).  The members stay usable as models: their state
+    and iteration counts are updated in place.
+    """
+
+    def __init__(self, models):
+        models = list(models)
+        if not models:
+            raise ValueError("empty batch")
+        self.lib = models[0].lib
+        if any(m.lib is not self.lib for m in models):
+            raise ValueError("all members must come from one library build")
+        self.models = models
+        arr = (C.c_void_p * len(models))(*[m._h for m in models])
+        h = C.c_void_p()
+        L.check(self.lib, self.lib.fi_batch_create(arr, len(models), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.fi_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def add(self, model) -> None:
+        """Admit a member between steps; its solve starts at the next step."""
+        if model.lib is not self.lib:
+            raise ValueError("all members must come from one library build")
+        L.check(self.lib, self.lib.fi_batch_add(self._h, model._h))
+        self.models.append(model)
+
+    def remove(self, model) -> None:
+        L.check(self.lib, self.lib.fi_batch_remove(self._h, model._h))
+        self.models.remove(model)
+
+    def __len__(self) -> int:
+        return int(self.lib.fi_batch_size(self._h))
+
+    def advance(self, niter: int = 1) -> None:
+        L.check(self.lib, self.lib.fi_batch_advance(self._h, int(niter)))
+
+    @staticmethod
+    def _opts(max_iter, ncheck, tol, use_graph, window):
+        o = L.fi_batch_opts()
+        o.max_iter, o.ncheck, o.tol = int(max_iter), int(ncheck), float(tol)
+        o.use_graph, o.window = 1 if use_graph else 0, int(window)
+        return o
+
+    def _items(self, items):
+        return [{"iterations": it.iterations, "status": L.FI_ITEM_STATUS[it.status], "measure": it.measure}
+                for it in items]
+
+    def step(self, *, max_iter: int, ncheck: int, tol: float, rounds: int = 1, use_graph: bool = True,
+             window: int = 0):
+        """Up to ``rounds`` check-to-check steps of the members still iterating (no
+        restart).  Returns (items, n_active)."""
+        o = self._opts(max_iter, ncheck, tol, use_graph, window)
+        items = (L.fi_batch_item * max(len(self.models), 1))()
+        na = C.c_int32()
+        L.check(self.lib, self.lib.fi_batch_step(self._h, C.byref(o), int(rounds), items, C.byref(na)))
+        return self._items(items[:len(self.models)]), na.value
+
+    def measures(self) -> np.ndarray:
+        out = np.zeros(len(self.models))
+        L.check(self.lib, self.lib.fi_batch_measure(self._h, out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
+    def set_variant(self, variant: int) -> None:
+        L.check(self.lib, self.lib.fi_batch_set_variant(self._h, int(variant)))
+
+    def autotune(self, iters: int = 10):
+        nv = self.lib.fi_batch_variant_count()
+        ms = (C.c_double * nv)()
+        best = C.c_int32()
+        L.check(self.lib, self.lib.fi_batch_autotune(self._h, int(iters), C.byref(best), ms))
+        names = [self.lib.fi_batch_variant_name(v).decode() for v in range(nv)]
+        return best.value, dict(zip(names, list(ms)))
+
+    def solve(self, *, max_iter: int, ncheck: int, tol: float, use_graph: bool = True, window: int = 0):
+        """Iterate every member until it converges (measure < tol), stalls, fails or
+        reaches max_iter.  Returns (items, seconds); items[k] is a dict with
+        iterations, status and measure of member k."""
+        o = self._opts(max_iter, ncheck, tol, use_graph, window)
+        items = (L.fi_batch_item * len(self.models))()
+        sec = C.c_double()
+        L.check(self.lib, self.lib.fi_batch_solve(self._h, C.byref(o), items, C.byref(sec)))
+        return self._items(items), sec.value
+
+
 def advance_iteration(model: _StokesBase, t: float = 0.0, dt: float = 1.0) -> None:
     """``advance_iteration!(model, t, Δt)`` (t and Δt are unused, as in the reference)."""
     model.advance(1)

@@ -1,0 +1,130 @@
+"""Seeded problem set-ups of the benchmark workloads, in the pattern of the
+reference's driver scripts (scripts_future_API/*.jl): each builds a model
+through the public API and returns it with a description of what was drawn.
+
+* ``inclusion_model`` -- 2D pure shear of a matrix with circular inclusions of
+  contrasting viscosity between free-slip walls (the wall-velocity pattern of
+  scripts_future_API/tm_stokes_wip.jl:41-52: normal velocity -ε̇·x on the x walls,
+  +ε̇·y on the y walls, zero shear stress).
+* ``bed_model`` -- 3D gravity-driven ice over a seeded bed of Gaussian bumps
+  (the DEM -> level set -> volume fraction set-up of
+  scripts_future_API/test_volume_fractions.jl:93-100, with the bed level set
+  restated analytically as height above the bed).
+
+Random draws use numpy's PCG64 generator seeded per instance.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .grids import UniformGrid
+from .models import IsothermalFullStokesModel, pt_params
+from .physics import ArrayField, LinearViscousRheology, SBC
+
+INCLUSION_N_RANGE = (63, 511)
+
+
+def inclusion_params(seed: int, n=None, n_range=INCLUSION_N_RANGE, sigma: float = 3.0, max_contrast: float = 1e4):
+    """Draw one inclusion instance: cells per side (independent in x and y),
+    1-16 circles of radius U(0.02, 0.15) centred U([0,1]^2), inclusion viscosity
+    exp(N(0, sigma)) clipped to [1/max_contrast, max_contrast] (background 1)."""
+    rng = np.random.default_rng(seed)
+    if n is None:
+        n = (int(rng.integers(n_range[0], n_range[1] + 1)), int(rng.integers(n_range[0], n_range[1] + 1)))
+    k = int(rng.integers(1, 17))
+    circles = []
+    lim = math.log(max_contrast)
+    for _ in range(k):
+        r = float(rng.uniform(0.02, 0.15))
+        cx, cy = (float(v) for v in rng.uniform(0.0, 1.0, 2))
+        eta = float(math.exp(min(max(rng.normal(0.0, sigma), -lim), lim)))
+        circles.append((cx, cy, r, eta))
+    return {"n": tuple(n), "circles": circles}
+
+
+def inclusion_viscosity(n, circles) -> np.ndarray:
+    """Cell-centre viscosity (numpy order (y, x)) on [0,1]^2: 1 in the matrix, the
+    circle's value inside a circle (later circles over earlier ones)."""
+    xc = (np.arange(n[0]) + 0.5) / n[0]
+    yc = (np.arange(n[1]) + 0.5) / n[1]
+    Y, X = np.meshgrid(yc, xc, indexing="ij")
+    eta = np.ones((n[1], n[0]))
+    for cx, cy, r, e in circles:
+        eta[(X - cx) ** 2 + (Y - cy) ** 2 <= r * r] = e
+    return eta
+
+
+def smooth_log(eta: np.ndarray, passes: int) -> np.ndarray:
+    """``passes`` five-point averages of log η (edge-replicated borders): spreads a
+    viscosity jump over a few cells, as PT codes do before iterating sharp
+    inclusions."""
+    lg = np.log(eta)
+    for _ in range(passes):
+        p = np.pad(lg, 1, mode="edge")
+        lg = 0.2 * (p[1:-1, 1:-1] + p[:-2, 1:-1] + p[2:, 1:-1] + p[1:-1, :-2] + p[1:-1, 2:])
+    return np.exp(lg)
+
+
+def stiffness_ratio(eta: np.ndarray) -> float:
+    """Largest ratio, over the velocity points, of the viscosities entering a
+    velocity update's stencil (the two cells, and the four-cell vertex averages
+    the shear stresses use) to the face average the update divides by.  The PT
+    velocity step of kernels_2d.jl:20-29 scales with the inverse face average, so
+    the step has to shrink by this ratio for the update to stay stable."""
+    p = np.pad(eta, 1, mode="edge")
+    exy = 0.25 * (p[:-1, :-1] + p[:-1, 1:] + p[1:, :-1] + p[1:, 1:])
+    fx = 0.5 * (p[1:-1, :-1] + p[1:-1, 1:])
+    mx = np.maximum(np.maximum(exy[:-1, :], exy[1:, :]), np.maximum(p[1:-1, :-1], p[1:-1, 1:]))
+    fy = 0.5 * (p[:-1, 1:-1] + p[1:, 1:-1])
+    my = np.maximum(np.maximum(exy[:, :-1], exy[:, 1:]), np.maximum(p[:-1, 1:-1], p[1:, 1:-1]))
+    return float(max((mx / fx).max(), (my / fy).max(), 1.0))
+
+
+def inclusion_model(seed: int, n=None, dtype: str = "f32", library: str = "fast", path: str = "auto",
+                    strain_rate: float = 1.0, smooth: int = 4, vdtau_factor=None, **draw):
+    """Build the pure-shear inclusion model of ``seed``: returns (model, params).
+    The viscosity (smoothed by ``smooth`` log-space passes) is the linear
+    rheology's field; η is set to it (with its Neumann ghosts), as drivers do
+    before iterating.  The PT steps are the drivers' (pt_params) with the
+    velocity-step factor raised by the field's stiffness ratio unless
+    ``vdtau_factor`` is given."""
+    prm = inclusion_params(seed, n=n, **draw)
+    n = prm["n"]
+    grid = UniformGrid(origin=(0.0, 0.0), extent=(1.0, 1.0), dims=n)
+    e = float(strain_rate)
+    bcs = {"x": (SBC(-e * 0.0, 0.0), SBC(-e * 1.0, 0.0)), "y": (SBC(0.0, e * 0.0), SBC(0.0, e * 1.0))}
+    eta = smooth_log(inclusion_viscosity(n, prm["circles"]), smooth)
+    ratio = stiffness_ratio(eta)
+    factor = vdtau_factor if vdtau_factor is not None else 1.1 * ratio
+    prm.update(smooth=smooth, stiffness_ratio=ratio, vdtau_factor=factor)
+    m = IsothermalFullStokesModel(grid=grid, boundary_conditions=bcs, gravity={"x": 0.0, "y": 0.0},
+                                  rheology=LinearViscousRheology(ArrayField(eta)),
+                                  solver_params=pt_params(grid, vdtau_factor=factor),
+                                  dtype=dtype, library=library, path=path)
+    m.set_field("eta", eta)
+    m.set_field("eta_next", eta)
+    m.apply_bcs()
+    return m, prm
+
+
+def bed_params(seed: int, n: int, bumps: int = 64):
+    """Seeded bed of ``bumps`` Gaussian bumps a·exp(-|x-c|^2/w^2), a~U(0,0.2),
+    w~U(0.05,0.2), c~U([0,1]^2), and the surface z = 0.6 + 0.05 sin(2πx)."""
+    rng = np.random.default_rng(seed)
+    a = rng.uniform(0.0, 0.2, bumps)
+    w = rng.uniform(0.05, 0.2, bumps)
+    c = rng.uniform(0.0, 1.0, (bumps, 2))
+    return {"n": n, "a": a, "w": w, "c": c}
+
+
+def bed_height(prm, x, y):
+    h = np.zeros(np.broadcast(x, y).shape)
+    for a, w, (cx, cy) in zip(prm["a"], prm["w"], prm["c"]):
+        h = h + a * np.exp(-((x - cx) ** 2 + (y - cy) ** 2) / (w * w))
+    return h
+
+
+__all__ = ["inclusion_params", "inclusion_viscosity", "inclusion_model", "smooth_log", "stiffness_ratio",
+           "bed_params", "bed_height", "INCLUSION_N_RANGE"]

@@ -266,6 +266,79 @@ typedef struct {
 fi_status fi_residual_norms_noalloc(const fi_model_desc *desc, const fi_state_view *state, double *out_dev,
                                     void *stream);
 
+/* ---- batched 2D solves -------------------------------------------------------
+ * Many independent 2D models advanced together: one persistent launch per PT
+ * iteration strides over a device-side work list of the tiles of the instances
+ * still iterating; every ncheck iterations an FP64 check, per-instance
+ * retirement and work-list compaction run on the device, and the check-to-check
+ * step replays as one CUDA graph.  No counterpart in the reference, which runs one
+ * model per driver loop (scripts_future_API/tm_stokes_chmy.jl:283-305); each
+ * instance follows advance_iteration! of its own model.
+ *
+ * Members: 2D IsothermalFullStokesModel handles of one dtype and device, linear
+ * rheology without regularisation or relaxation, no periodic sides.  The batch
+ * holds each member's viscosity fixed at its current η (linear rheology: the
+ * rheology's viscosity with Neumann ghosts, as after the reference's first η
+ * swap).  The models must outlive the batch; batch calls synchronise the
+ * members' streams first, and each member's state and iteration count are
+ * updated in place.
+ *
+ * Measure of an instance (FP64 arithmetic on the stored state): the cell-scaled
+ * relative residual max(||r_V||∞ h / max|P, τ|, ||r_P||∞ h / max|V|), h the
+ * smallest grid spacing, over the points the residual boundary batch leaves free. */
+typedef struct fi_batch fi_batch;
+
+typedef enum {
+    FI_ITEM_ACTIVE = 0,    /* still iterating (never reported by fi_batch_solve) */
+    FI_ITEM_CONVERGED = 1, /* measure < tol */
+    FI_ITEM_STALLED = 2,   /* the measure did not halve for `window` iterations */
+    FI_ITEM_DIVERGED = 3,  /* non-finite residual or state */
+    FI_ITEM_MAXITER = 4    /* max_iter iterations */
+} fi_batch_item_status;
+
+typedef struct {
+    int32_t max_iter;   /* per instance */
+    int32_t ncheck;     /* iterations between checks (even) */
+    double tol;         /* on the measure above */
+    int32_t use_graph;  /* 1: replay the check-to-check step as a CUDA graph */
+    int32_t window;     /* stall window in iterations (0: never stall) */
+} fi_batch_opts;
+
+typedef struct {
+    int32_t iterations;
+    int32_t status;     /* fi_batch_item_status */
+    double measure;     /* at the last check */
+} fi_batch_item;
+
+/* count >= 1: the first member fixes the batch's dtype and device */
+fi_status fi_batch_create(fi_model *const *models, int32_t count, fi_batch **out);
+fi_status fi_batch_destroy(fi_batch *b);
+/* membership between steps (continuous batching): a new member starts its own
+ * solve (iteration count 0) at the next step; removing a member leaves its state
+ * as the batch last wrote it */
+fi_status fi_batch_add(fi_batch *b, fi_model *m);
+fi_status fi_batch_remove(fi_batch *b, fi_model *m);
+int32_t fi_batch_size(const fi_batch *b);
+/* niter PT iterations of every member (no checks) */
+fi_status fi_batch_advance(fi_batch *b, int32_t niter);
+/* restart every member's solve and iterate until all retire; items has one entry
+ * per member, in order;
+ * seconds (may be NULL) receives the wall time */
+fi_status fi_batch_solve(fi_batch *b, const fi_batch_opts *opts, fi_batch_item *items, double *seconds);
+/* at most max_rounds check-to-check steps of the members still iterating, without
+ * resetting anyone's solve; items (may be NULL) gets every member's state, in
+ * membership order; nactive (may be NULL) the members still iterating */
+fi_status fi_batch_step(fi_batch *b, const fi_batch_opts *opts, int32_t max_rounds, fi_batch_item *items,
+                        int32_t *nactive);
+/* current measure of every member (count doubles) */
+fi_status fi_batch_measure(fi_batch *b, double *out);
+/* tile shapes of the batched sweep; autotune times each for `iters` iterations on
+ * the batch itself (the members advance by (2 + iters) * count_of_variants) */
+int fi_batch_variant_count(void);
+const char *fi_batch_variant_name(int32_t variant);
+fi_status fi_batch_set_variant(fi_batch *b, int32_t variant);
+fi_status fi_batch_autotune(fi_batch *b, int32_t iters, int32_t *best, double *ms);
+
 /* ---- level sets and volume fractions (setup path) --------------------------- */
 
 /* ω_from_ψ!(arch, launch, ω, ψ, grid) (LevelSets/volume_fractions_kernels.jl:101-110):

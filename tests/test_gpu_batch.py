@@ -1,0 +1,206 @@
+"""Batched 2D solves (fi_batch_*): each member against the CPU oracle bit for bit
+(no-FMA build), results alone and in the mix, graph replay against direct
+launches, continuous batching (members admitted between steps), and the
+convergence of the pure-shear inclusion workload."""
+import numpy as np
+import pytest
+
+from conftest import load_fastice, load_oracle
+from helpers import KIND, make_bcs
+
+pytestmark = pytest.mark.gpu
+
+STATE = ("P", "txx", "tyy", "txy", "Vx", "Vy")
+
+CASES = [
+    ((37, 29), ((("slip", (0.0, 0.0)), ("slip", (-1.0, 0.0))), (("slip", (0.0, 0.0)), ("slip", (0.0, 1.0))))),
+    ((64, 41), ((("velocity", (0.2, -0.1)), ("traction", (0.05, 0.0))),
+                (("slip", (0.0, 0.0)), ("velocity", (0.0, 0.0))))),
+    ((20, 70), ((("traction", (0.0, 0.0)), ("traction", (0.1, -0.05))),
+                (("traction", (0.0, 0.1)), ("slip", (0.0, 0.0))))),
+    ((45, 33), ((("velocity", (0.1, 0.2)), ("velocity", (-0.3, 0.05))),
+                (("velocity", (0.2, -0.4)), ("velocity", (0.15, 0.3))))),
+]
+
+
+def _pair(fi, O, n, bcs, dtype, library, seed):
+    """A 2D model with a viscosity field and its oracle twin, same random state."""
+    rng = np.random.default_rng(seed)
+    grid = fi.UniformGrid(origin=(0.0, -0.2), extent=(1.0, 0.8 + 0.1 * seed), dims=n)
+    eta = np.exp(rng.normal(0.0, 1.0, (n[1], n[0])))
+    g = (0.3, -0.7)
+    m = fi.IsothermalFullStokesModel(grid=grid, boundary_conditions=make_bcs(fi, bcs, 2),
+                                     gravity={"x": g[0], "y": g[1]},
+                                     rheology=fi.LinearViscousRheology(fi.ArrayField(eta)),
+                                     solver_params=fi.pt_params(grid), dtype=dtype, library=library)
+    dt = fi.pt_params(grid)["Δτ"]
+    spec_bcs = tuple(tuple((KIND[k], tuple(c) + (0.0,) * (3 - len(c))) for k, c in bcs[d]) for d in range(2))
+    spec = O.Spec(nd=2, n=n, extent=grid.extent, origin=grid.origin, bcs=spec_bcs, dt_P=dt["Pr"],
+                  dt_tau=(dt["τ"]["xx"], dt["τ"]["yy"], 0.0, dt["τ"]["xy"], 0.0, 0.0),
+                  dt_V=(dt["V"]["x"], dt["V"]["y"], 0.0), g_val=(g[0], g[1], 0.0), dtype=dtype)
+    eta_halo = np.zeros((n[1] + 3, n[0] + 3))
+    eta_halo[1:n[1] + 1, 1:n[0] + 1] = eta
+    o = O.OracleStokes(spec, eta_lin=eta_halo)
+    npd = np.float64 if dtype == "f64" else np.float32
+    for name in STATE:
+        vals = (0.1 * rng.standard_normal(m.field_shape(name))).astype(npd)
+        m.set_field(name, vals)
+        o.set_interior(name, vals)
+    for name in ("eta", "eta_next"):
+        m.set_field(name, eta.astype(npd))
+        o.set_interior(name, eta.astype(npd))
+    m.apply_bcs()
+    o.apply_initial_bcs()
+    return m, o
+
+
+def _bits(a):
+    return a.view(np.uint64 if a.dtype == np.float64 else np.uint32)
+
+
+@pytest.mark.parametrize("dtype", ["f32", "f64"])
+@pytest.mark.parametrize("variant", [0, 1, 2])
+def test_batch_members_bitwise_vs_oracle(dtype, variant):
+    fi, O = load_fastice(), load_oracle()
+    pairs = [_pair(fi, O, n, bcs, dtype, "strict", seed) for seed, (n, bcs) in enumerate(CASES)]
+    batch = fi.BatchedStokes2D([m for m, _ in pairs])
+    batch.set_variant(variant)
+    batch.advance(7)
+    bad = []
+    for k, (m, o) in enumerate(pairs):
+        o.advance(7)
+        for name in STATE:
+            a, b = m.get_field(name), o.interior(name)
+            if not np.array_equal(_bits(a), _bits(b)):
+                bad.append((k, name, int(np.sum(a != b))))
+    batch.close()
+    for m, _ in pairs:
+        m.close()
+    assert not bad, bad
+
+
+def _inclusions(fi, seeds, n_range=(40, 96), library="fast", dtype="f32", max_contrast=100.0):
+    # moderate contrasts keep the reference PT scheme's iteration counts small here
+    from fastice_b200 import scenarios
+    return [scenarios.inclusion_model(s, n_range=n_range, library=library, dtype=dtype,
+                                      max_contrast=max_contrast)[0] for s in seeds]
+
+
+# FP32 storage: the cell-scaled residual of these sizes bottoms out near 1e-5
+SOLVE = dict(max_iter=60000, ncheck=200, tol=1e-4, window=20000)
+
+
+def test_alone_and_in_the_mix_agree_bitwise():
+    fi = load_fastice()
+    mix = _inclusions(fi, range(5))
+    batch = fi.BatchedStokes2D(mix)
+    items, _ = batch.solve(**SOLVE)
+    batch.close()
+    assert all(it["status"] == "converged" for it in items), items
+    alone_model = _inclusions(fi, [3])[0]
+    alone = fi.BatchedStokes2D([alone_model])
+    items1, _ = alone.solve(**SOLVE)
+    alone.close()
+    assert items1[0]["iterations"] == items[3]["iterations"]
+    assert items1[0]["measure"] == items[3]["measure"]
+    for name in STATE:
+        assert np.array_equal(_bits(alone_model.get_field(name)), _bits(mix[3].get_field(name))), name
+    for m in mix + [alone_model]:
+        m.close()
+
+
+def test_graph_replay_matches_direct_launches():
+    fi = load_fastice()
+    a = _inclusions(fi, [7, 8])
+    b = _inclusions(fi, [7, 8])
+    ba, bb = fi.BatchedStokes2D(a), fi.BatchedStokes2D(b)
+    ia, _ = ba.solve(use_graph=True, **SOLVE)
+    ib, _ = bb.solve(use_graph=False, **SOLVE)
+    ba.close()
+    bb.close()
+    assert ia == ib
+    for ma, mb in zip(a, b):
+        for name in STATE:
+            assert np.array_equal(_bits(ma.get_field(name)), _bits(mb.get_field(name))), name
+        ma.close()
+        mb.close()
+
+
+def test_continuous_batching_admits_members_between_steps():
+    fi = load_fastice()
+    first = _inclusions(fi, [11, 12])
+    late = _inclusions(fi, [13])[0]
+    batch = fi.BatchedStokes2D(first)
+    kw = dict(max_iter=SOLVE["max_iter"], ncheck=SOLVE["ncheck"], tol=SOLVE["tol"], window=SOLVE["window"])
+    items, active = batch.step(rounds=3, **kw)
+    assert all(it["iterations"] == 600 or it["status"] == "converged" for it in items), items
+    batch.add(late)
+    while active:
+        items, active = batch.step(rounds=5, **kw)
+    assert len(batch) == 3 and all(it["status"] == "converged" for it in items), items
+    batch.remove(first[0])
+    assert len(batch) == 2
+    batch.close()
+    # the member admitted late matches its own solve alone
+    solo = _inclusions(fi, [13])[0]
+    sb = fi.BatchedStokes2D([solo])
+    s_items, _ = sb.solve(**SOLVE)
+    sb.close()
+    assert s_items[0]["iterations"] == items[2]["iterations"]
+    for name in STATE:
+        assert np.array_equal(_bits(solo.get_field(name)), _bits(late.get_field(name))), name
+    for m in first + [late, solo]:
+        m.close()
+
+
+@pytest.mark.parametrize("dtype,tol", [("f32", 1e-4), ("f64", 1e-6)])
+def test_inclusion_solves_reach_tolerance_and_measure_agrees(dtype, tol):
+    fi = load_fastice()
+    ms = _inclusions(fi, range(20, 26), dtype=dtype)
+    batch = fi.BatchedStokes2D(ms)
+    best, times = batch.autotune(iters=4)
+    assert set(times) == {"tile32x8", "tile32x4", "tile32x16"} and all(t > 0 for t in times.values())
+    items, sec = batch.solve(max_iter=80000, ncheck=200, tol=tol, window=30000)
+    meas = batch.measures()
+    batch.close()
+    assert all(it["status"] == "converged" and it["measure"] < tol for it in items), items
+    np.testing.assert_array_equal(meas, [it["measure"] for it in items])
+    # the velocity field follows the imposed pure shear on the walls
+    for m in ms:
+        vx = m.get_field("Vx")
+        assert np.allclose(vx[:, -1], -1.0) and np.allclose(vx[:, 0], 0.0)
+        m.close()
+
+
+def test_batch_rejects_unsupported_members():
+    fi = load_fastice()
+    g3 = fi.UniformGrid(origin=(0, 0, 0), extent=(1, 1, 1), dims=(8, 8, 8))
+    s3 = fi.SBC(0.0, 0.0, 0.0)
+    m3 = fi.IsothermalFullStokesModel(grid=g3, boundary_conditions={"x": (s3, s3), "y": (s3, s3), "z": (s3, s3)},
+                                      gravity={"x": 0.0, "y": 0.0, "z": 1.0}, rheology=fi.LinearViscousRheology(1.0),
+                                      solver_params=fi.pt_params(g3), dtype="f32")
+    with pytest.raises(fi.FastIceError):
+        fi.BatchedStokes2D([m3])
+    g2 = fi.UniformGrid(origin=(0, 0), extent=(1, 1), dims=(16, 16))
+    s2 = fi.SBC(0.0, 0.0)
+    glen = fi.IsothermalFullStokesModel(grid=g2, boundary_conditions={"x": (s2, s2), "y": (s2, s2)},
+                                        gravity={"x": 0.0, "y": 1.0}, rheology=fi.PowerLawRheology(1.0, 3),
+                                        solver_params=fi.pt_params(g2), dtype="f32")
+    with pytest.raises(fi.FastIceError):
+        fi.BatchedStokes2D([glen])
+    a = fi.IsothermalFullStokesModel(grid=g2, boundary_conditions={"x": (s2, s2), "y": (s2, s2)},
+                                     gravity={"x": 0.0, "y": 1.0}, rheology=fi.LinearViscousRheology(1.0),
+                                     solver_params=fi.pt_params(g2), dtype="f32")
+    b64 = fi.IsothermalFullStokesModel(grid=g2, boundary_conditions={"x": (s2, s2), "y": (s2, s2)},
+                                       gravity={"x": 0.0, "y": 1.0}, rheology=fi.LinearViscousRheology(1.0),
+                                       solver_params=fi.pt_params(g2), dtype="f64")
+    with pytest.raises(fi.FastIceError):
+        fi.BatchedStokes2D([a, b64])
+    with pytest.raises(fi.FastIceError):
+        fi.BatchedStokes2D([a, a])
+    batch = fi.BatchedStokes2D([a])
+    with pytest.raises(fi.FastIceError):
+        batch.solve(max_iter=10, ncheck=3, tol=1e-6)  # odd ncheck
+    batch.close()
+    for m in (m3, glen, a, b64):
+        m.close()

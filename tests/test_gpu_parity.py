@@ -27,6 +27,11 @@ BC3 = {
                      (("velocity", (0.2, -0.1, 0.0)), ("slip", (0.05, -0.05, 0.0)))),
     "shear_walls": ((("slip", (0.0, 0.0, 0.0)), ("slip", (-0.4, 0.0, 0.0))), (NOSL, ("velocity", (0.3, 0.0, 0.1))),
                     (TRAC, ("slip", (0.0, 0.2, 0.0)))),
+    # nonzero wall velocities on every side: ghosts at edges where a later dim's
+    # node assignment overrides an earlier dim's mirror image feed unfixed stresses
+    "velocity_box": ((("velocity", (0.1, 0.2, 0.3)), ("velocity", (-0.1, 0.05, 0.2))),
+                     (("velocity", (0.3, -0.2, 0.1)), ("velocity", (0.0, 0.4, -0.1))),
+                     (("velocity", (0.2, 0.1, -0.3)), ("velocity", (0.1, -0.1, 0.25)))),
 }
 SIZES3 = [(13, 7, 9), (33, 9, 10), (40, 17, 70)]
 
