@@ -54,6 +54,43 @@ __device__ __forceinline__ float sqrt_dev(float x) { return __fsqrt_rn(x); }
 __device__ __forceinline__ double div_dev(double a, double b) { return a / b; }
 __device__ __forceinline__ float div_dev(float a, float b) { return __fdiv_rn(a, b); }
 
+// Reciprocal by Newton-Raphson iteration r <- r + r (1 - b r) from the hardware
+// approximation (PTX rcp.approx.ftz): each step doubles the number of correct
+// bits, two steps in FP64 and one in FP32 reach the last bit or so.  Production
+// sweeps divide as a * rcp(b) (within a few ulp of the rounded quotient, no
+// special-case branches); FI_EXACT_ORDER builds keep the rounded division.
+__device__ __forceinline__ double rcp_nr(double b) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(b));
+    double e = fma(-b, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-b, r, 1.0);
+    return fma(r, e, r);
+}
+__device__ __forceinline__ float rcp_nr(float b) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(b));
+    const float e = fmaf(-b, r, 1.0f);
+    return fmaf(r, e, r);
+}
+template <typename T>
+__device__ __forceinline__ T div_fast(T a, T b) {
+#ifdef FI_EXACT_ORDER
+    return div_dev(a, b);
+#else
+    return a * rcp_nr(b);
+#endif
+}
+// x / 3 (the deviatoric split); production builds multiply by the rounded 1/3
+template <typename T>
+__device__ __forceinline__ T third(T x) {
+#ifdef FI_EXACT_ORDER
+    return x / T(3.0);
+#else
+    return x * T(1.0 / 3.0);
+#endif
+}
+
 // η_next from τII² = s2 (rheology(τII) with τII = sqrt(s2)).  Production builds
 // evaluate Glen's law with the integer exponent n = 3 as 0.5/(A s2) and its
 // viscoplastic regularisation as 1/(2 A s2 + 1/η_reg): the same function without
@@ -68,7 +105,7 @@ __device__ __forceinline__ T rheology_s2(const KParams &p, T A_const, T inv_reg,
     if (p.rheo_inner == FI_RHEO_POWER && p.rheo_n == 3 && p.rheo_relax == FI_RELAX_NONE) {
         T A = p.rheo_A_is_field ? Afield[I] : A_const;
         T As2 = A * s2;
-        return p.rheo_has_reg ? div_dev(T(1.0), T(2.0) * As2 + inv_reg) : div_dev(T(0.5), As2);
+        return p.rheo_has_reg ? rcp_nr(T(2.0) * As2 + inv_reg) : div_fast(T(0.5), As2);
     }
 #endif
     return rheology_dev(p, eta_lin, Afield, eta_cur, I, sqrt_dev(s2));

@@ -153,9 +153,33 @@ struct Ctx {
     long long sx, sxy;
     bool perx, pery;
     bool bnd_x, bnd_y;  // column touches an x / y boundary (needs fix-ups or ghost writes)
+    // Ring positions relative to the plane step sref: element offsets of the
+    // planes around sref inside three- and four-slot rings, computed once per plane
+    // step.  Every access names its plane as sref plus a constant, so after
+    // inlining the choice folds to one register (no modulo per access).
+    int sref;
+    int o3m, o30, o3p;                 // three-slot rings: planes sref-1, sref, sref+1
+    int o4m2, o4m, o40, o4p, o4p2;     // four-slot rings: planes sref-2 .. sref+2
 
+    __device__ __forceinline__ void set_plane(int s) {
+        sref = s;
+        const int m3 = s % 3, m4 = s & 3;
+        o30 = m3 * Lay::SLOT;
+        o3p = (m3 == 2 ? 0 : m3 + 1) * Lay::SLOT;
+        o3m = (m3 == 0 ? 2 : m3 - 1) * Lay::SLOT;
+        o4m2 = ((m4 + 2) & 3) * Lay::SLOT;
+        o4m = ((m4 + 3) & 3) * Lay::SLOT;
+        o40 = m4 * Lay::SLOT;
+        o4p = ((m4 + 1) & 3) * Lay::SLOT;
+        o4p2 = o4m2;
+    }
     __device__ __forceinline__ int at(int i, int j) const { return (j - j0 + 1) * Lay::BX + (i - i0 + Lay::XB); }
-    __device__ __forceinline__ T *slot(int base, int len, int p) const { return sm + (base + p % len) * Lay::SLOT; }
+    __device__ __forceinline__ T *slot(int base, int len, int p) const {
+        const int d = p - sref;
+        const int off = len == 3 ? (d < 0 ? o3m : d == 0 ? o30 : o3p)
+                                 : (d < -1 ? o4m2 : d == -1 ? o4m : d == 0 ? o40 : d == 1 ? o4p : o4p2);
+        return sm + base * Lay::SLOT + off;
+    }
     __device__ __forceinline__ T &P(int p, int i, int j) const { return slot(S_P, R_P, p)[at(i, j)]; }
     __device__ __forceinline__ T &Tzz(int p, int i, int j) const { return slot(S_ZZ, R_ZZ, p)[at(i, j)]; }
     __device__ __forceinline__ T &Txx(int p, int i, int j) const { return slot(S_XX, R_XX, p)[at(i, j)]; }
@@ -210,16 +234,18 @@ __device__ __forceinline__ void issue_group(const Ctx<T, TY> &c, const InMaps &m
 // raw stress update of plane s at (i, j): which components is a compile-time mask
 enum { F_P = 1, F_XX = 2, F_YY = 4, F_ZZ = 8, F_XY = 16, F_XZ = 32, F_YZ = 64, F_ALL = 127 };
 
-template <typename T, int TY>
+// XYI: the column and its ring lie inside every x / y range (no boundary column),
+// so only the z ranges are tested
+template <typename T, int TY, bool XYI>
 __device__ __forceinline__ void sigma_point(const Ctx<T, TY> &c, const KParams &p, const TConst<T> &q, int s, int i, int j, int mask,
                                             bool write_now, const Ptrs<T> &out) {
-    if (i > c.n0 + 2 || j > c.n1 + 2) return;
+    if (!XYI && (i > c.n0 + 2 || j > c.n1 + 2)) return;
     const T idx = q.inv_dx[0], idy = q.inv_dx[1], idz = q.inv_dx[2];
     const bool cz = s >= 1 && s <= c.n2, vz = s >= 1 && s <= c.n2 + 1;
-    const bool cx = (i >= 1 && i <= c.n0) || (c.perx && (i == 0 || i == c.n0 + 1));
-    const bool vx = i >= 1 && i <= c.n0 + 1;
-    const bool cy = (j >= 1 && j <= c.n1) || (c.pery && (j == 0 || j == c.n1 + 1));
-    const bool vy = j >= 1 && j <= c.n1 + 1;
+    const bool cx = XYI || (i >= 1 && i <= c.n0) || (c.perx && (i == 0 || i == c.n0 + 1));
+    const bool vx = XYI || (i >= 1 && i <= c.n0 + 1);
+    const bool cy = XYI || (j >= 1 && j <= c.n1) || (c.pery && (j == 0 || j == c.n1 + 1));
+    const bool vy = XYI || (j >= 1 && j <= c.n1 + 1);
     const int a = c.at(i, j);
     if ((mask & (F_P | F_XX | F_YY | F_ZZ)) && cx && cy && cz) {
         const T *vxs = c.slot(S_VX, R_VX, s), *vys = c.slot(S_VY, R_VY, s);
@@ -234,15 +260,15 @@ __device__ __forceinline__ void sigma_point(const Ctx<T, TY> &c, const KParams &
         }
         if (mask & F_XX) {
             T &v = c.slot(S_XX, R_XX, s)[a];
-            v = v - (v - T(2.0) * etac * (exx - divV / T(3.0))) * q.dt_tau[0];
+            v = v - (v - T(2.0) * etac * (exx - third(divV))) * q.dt_tau[0];
         }
         if (mask & F_YY) {
             T &v = c.slot(S_YY, R_YY, s)[a];
-            v = v - (v - T(2.0) * etac * (eyy - divV / T(3.0))) * q.dt_tau[1];
+            v = v - (v - T(2.0) * etac * (eyy - third(divV))) * q.dt_tau[1];
         }
         if (mask & F_ZZ) {
             T &v = c.slot(S_ZZ, R_ZZ, s)[a];
-            v = v - (v - T(2.0) * etac * (ezz - divV / T(3.0))) * q.dt_tau[2];
+            v = v - (v - T(2.0) * etac * (ezz - third(divV))) * q.dt_tau[2];
         }
     }
     constexpr int BX = Ctx<T, TY>::Lay::BX;
@@ -320,18 +346,22 @@ __device__ __forceinline__ void sigma_plane(const Ctx<T, TY> &c, const KParams &
     const bool zb_plane = s == 1 || s == c.n2 + 1;
     const bool late = c.bnd_x || c.bnd_y || zb_plane;
     const bool own_s = s >= c.kb && s < c.ke;
-    // pass 1: the column, all components
-    sigma_point<T, TY>(c, p, q, s, c.i0 + (tid % TX), c.j0 + (tid / TX), F_ALL, own_s && !late, out);
-    // pass 2: the ring, only the components read there
+    // pass 1: the column, all components; pass 2: the ring, only the components read there
     constexpr int NR = 2 * TY + 2 * TX + 1;
+    int ri = 0, rj = 0, rmask = 0;
     if (tid < NR) {
-        int i, j, mask;
-        if (tid < TY) { i = c.i0 - 1; j = c.j0 + tid; mask = F_P | F_XX; }
-        else if (tid < 2 * TY) { i = c.i0 + TX; j = c.j0 + tid - TY; mask = F_XY | F_XZ; }
-        else if (tid < 2 * TY + TX) { i = c.i0 + tid - 2 * TY; j = c.j0 - 1; mask = F_P | F_YY; }
-        else if (tid < 2 * TY + 2 * TX) { i = c.i0 + tid - 2 * TY - TX; j = c.j0 + TY; mask = F_XY | F_YZ; }
-        else { i = c.i0 + TX; j = c.j0 + TY; mask = F_XY; }
-        sigma_point<T, TY>(c, p, q, s, i, j, mask, false, out);
+        if (tid < TY) { ri = c.i0 - 1; rj = c.j0 + tid; rmask = F_P | F_XX; }
+        else if (tid < 2 * TY) { ri = c.i0 + TX; rj = c.j0 + tid - TY; rmask = F_XY | F_XZ; }
+        else if (tid < 2 * TY + TX) { ri = c.i0 + tid - 2 * TY; rj = c.j0 - 1; rmask = F_P | F_YY; }
+        else if (tid < 2 * TY + 2 * TX) { ri = c.i0 + tid - 2 * TY - TX; rj = c.j0 + TY; rmask = F_XY | F_YZ; }
+        else { ri = c.i0 + TX; rj = c.j0 + TY; rmask = F_XY; }
+    }
+    if (!c.bnd_x && !c.bnd_y) {
+        sigma_point<T, TY, true>(c, p, q, s, c.i0 + (tid % TX), c.j0 + (tid / TX), F_ALL, own_s && !late, out);
+        if (tid < NR) sigma_point<T, TY, true>(c, p, q, s, ri, rj, rmask, false, out);
+    } else {
+        sigma_point<T, TY, false>(c, p, q, s, c.i0 + (tid % TX), c.j0 + (tid / TX), F_ALL, own_s && !late, out);
+        if (tid < NR) sigma_point<T, TY, false>(c, p, q, s, ri, rj, rmask, false, out);
     }
     __syncthreads();
     if (!late) return;
@@ -360,9 +390,9 @@ __device__ __forceinline__ void sigma_plane(const Ctx<T, TY> &c, const KParams &
             for (int r = tid; r < NREG; r += Lay::NT) {
                 const int i = c.i0 - 1 + r % (TX + 2), j = c.j0 - 1 + r / (TX + 2);
                 if (kind == FI_BC_TRACTION) {
-                    if (side == 0) {
-                        c.P(0, i, j) = tv - c.P(1, i, j);
-                        c.Tzz(0, i, j) = tv - c.Tzz(1, i, j);
+                    if (side == 0) {  // s == 1: ghost plane 0 from plane 1
+                        c.P(s - 1, i, j) = tv - c.P(s, i, j);
+                        c.Tzz(s - 1, i, j) = tv - c.Tzz(s, i, j);
                     } else {
                         c.P(s, i, j) = tv - c.P(s - 1, i, j);
                         c.Tzz(s, i, j) = tv - c.Tzz(s - 1, i, j);
@@ -391,8 +421,8 @@ __device__ __forceinline__ void sigma_plane(const Ctx<T, TY> &c, const KParams &
             }
             if (own_0) {
                 const long long I0 = c.gidx(i, j, 0);
-                out.P[I0] = c.P(0, i, j);
-                out.tzz[I0] = c.Tzz(0, i, j);
+                out.P[I0] = c.P(s - 1, i, j);  // own_0: s == 1, ghost plane 0
+                out.tzz[I0] = c.Tzz(s - 1, i, j);
             }
         }
     }
@@ -475,7 +505,7 @@ __device__ __forceinline__ T vx_raw(const Ctx<T, TY> &c, const KParams &p, const
     const T idx = q.inv_dx[0], idy = q.inv_dx[1], idz = q.inv_dx[2];
     T gx = (p.g_kind[0] == FI_G_FIELD ? in.gx[I] : q.g_val[0]);
     T ex = h(c.Eta(t, i - 1, j) + c.Eta(t, i, j));
-    return c.Vx(t, i, j) + div_dev(-(c.P(t, i, j) - c.P(t, i - 1, j)) * idx + (c.Txx(t, i, j) - c.Txx(t, i - 1, j)) * idx +
+    return c.Vx(t, i, j) + div_fast(-(c.P(t, i, j) - c.P(t, i - 1, j)) * idx + (c.Txx(t, i, j) - c.Txx(t, i - 1, j)) * idx +
                                        (c.Txy(t, i, j + 1) - c.Txy(t, i, j)) * idy +
                                        (c.Txz(t + 1, i, j) - c.Txz(t, i, j)) * idz - gx,
                                    ex) *
@@ -487,7 +517,7 @@ __device__ __forceinline__ T vy_raw(const Ctx<T, TY> &c, const KParams &p, const
     const T idx = q.inv_dx[0], idy = q.inv_dx[1], idz = q.inv_dx[2];
     T gy = (p.g_kind[1] == FI_G_FIELD ? in.gy[I] : q.g_val[1]);
     T ey = h(c.Eta(t, i, j - 1) + c.Eta(t, i, j));
-    return c.Vy(t, i, j) + div_dev(-(c.P(t, i, j) - c.P(t, i, j - 1)) * idy + (c.Tyy(t, i, j) - c.Tyy(t, i, j - 1)) * idy +
+    return c.Vy(t, i, j) + div_fast(-(c.P(t, i, j) - c.P(t, i, j - 1)) * idy + (c.Tyy(t, i, j) - c.Tyy(t, i, j - 1)) * idy +
                                        (c.Txy(t, i + 1, j) - c.Txy(t, i, j)) * idx +
                                        (c.Tyz(t + 1, i, j) - c.Tyz(t, i, j)) * idz - gy,
                                    ey) *
@@ -499,7 +529,7 @@ __device__ __forceinline__ T vz_raw(const Ctx<T, TY> &c, const KParams &p, const
     const T idx = q.inv_dx[0], idy = q.inv_dx[1], idz = q.inv_dx[2];
     T gz = (p.g_kind[2] == FI_G_FIELD ? in.gz[I] : q.g_val[2]);
     T ez = h(c.Eta(t - 1, i, j) + c.Eta(t, i, j));
-    return c.Vz(t, i, j) + div_dev(-(c.P(t, i, j) - c.P(t - 1, i, j)) * idz + (c.Tzz(t, i, j) - c.Tzz(t - 1, i, j)) * idz +
+    return c.Vz(t, i, j) + div_fast(-(c.P(t, i, j) - c.P(t - 1, i, j)) * idz + (c.Tzz(t, i, j) - c.Tzz(t - 1, i, j)) * idz +
                                        (c.Txz(t, i + 1, j) - c.Txz(t, i, j)) * idx +
                                        (c.Tyz(t, i, j + 1) - c.Tyz(t, i, j)) * idy - gz,
                                    ez) *
@@ -612,6 +642,7 @@ __global__ void __launch_bounds__(TX *TY, (TY >= 16 ? (sizeof(T) == 8 ? 1 : 2) :
     __syncthreads();
     const int f = max(c.kb - 1, 1), last = min(c.ke, c.n2 + 1);
     uint32_t phase = 0;  // bit b: parity of the next completion of bars[b]
+    c.set_plane(f);
     if (tid == 0) {
         issue_group<T, TY>(c, maps, f - 1, false, &bars[(f - 1) % kBars]);
         issue_group<T, TY>(c, maps, f, true, &bars[f % kBars]);
@@ -624,6 +655,7 @@ __global__ void __launch_bounds__(TX *TY, (TY >= 16 ? (sizeof(T) == 8 ? 1 : 2) :
     };
     bool ok = wait_group(f - 1);
     for (int s = f; s <= last && ok; s++) {
+        c.set_plane(s);
         if (tid == 0 && s + 1 <= last) {
             fence_proxy_async();
             issue_group<T, TY>(c, maps, s + 1, true, &bars[(s + 1) % kBars]);
@@ -635,7 +667,10 @@ __global__ void __launch_bounds__(TX *TY, (TY >= 16 ? (sizeof(T) == 8 ? 1 : 2) :
         __syncthreads();
     }
     if (ok) {
-        if (c.ke - 1 == last && last == c.n2 + 1) v_plane<T, TY>(c, p, q, in, out, last);
+        if (c.ke - 1 == last && last == c.n2 + 1) {
+            c.set_plane(last);
+            v_plane<T, TY>(c, p, q, in, out, last);
+        }
         return;
     }
     // bounded wait expired: record it and drain this CTA's own copies (bounded) before leaving
