@@ -38,9 +38,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 
 # DRAM bytes per cell of one fused-sweep launch: dram__bytes_read.sum +
 # dram__bytes_write.sum of one ncu-captured 255^3 launch (32x8 tiles, z-blocks of
-# 64, summarised in profiles/fused3d_slab255_ncu_full.md) divided by its cell
+# 64, summarised in profiles/fused3d_slab255_ncu_full.md, v4) divided by its cell
 # count; traffic grows with the cell count, so it scales to 511^3.
-TRAFFIC_BYTES_PER_CELL = {"f64": 231.7, "f32": None}
+TRAFFIC_BYTES_PER_CELL = {"f64": 236.0, "f32": None}
 
 
 def load_fastice():
@@ -227,6 +227,156 @@ def cpu_baseline(n, seconds=12.0, warm=1):
     return its, el, cores
 
 
+def _base_line(metric, value, unit, steps, warmup, ms, dtype, cfg, hib=True):
+    return {"metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": steps, "warmup": warmup,
+            "ms_per_step": ms, "higher_is_better": hib, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
+            "data": "synthetic", "config": cfg}
+
+
+def run_batched(args):
+    """Batched 2D solves: `instances` pure-shear inclusion problems (seeds 0..k-1,
+    63-511 cells per side, 1-16 inclusions, contrasts up to 1e4) in one batch:
+    autotuned tile shape, CUDA-graph replay of each check round, one step = one
+    check round.  value = instances solved / wall time of the solve."""
+    import torch
+    fi = load_fastice()
+    from fastice_b200 import scenarios
+    dtype = args.dtypes.split(",")[0] if args.dtypes != "f64,f32" else "f32"
+    tol = args.tol or (1e-4 if dtype == "f32" else 1e-6)
+    ncheck = 200
+    models = [scenarios.inclusion_model(s, dtype=dtype)[0] for s in range(args.instances)]
+    cells = sum(m.grid.dims[0] * m.grid.dims[1] for m in models)
+    batch = fi.BatchedStokes2D(models)
+    best, per = batch.autotune(iters=10)
+    esz = 8 if dtype == "f64" else 4
+    sweep_gbs = {k: 13 * esz * cells / (v * 1e-3) / 1e9 for k, v in per.items()}
+    clocks = ClockSampler(0)
+    clocks.start()
+    max_iter = args.rounds * ncheck if args.rounds > 0 else 400000
+    items, sec = batch.solve(max_iter=max_iter, ncheck=ncheck, tol=tol, window=100000, use_graph=True)
+    ck = clocks.stop()
+    batch.close()
+    status = {}
+    for it in items:
+        status[it["status"]] = status.get(it["status"], 0) + 1
+    iters = [it["iterations"] for it in items]
+    cell_sweeps = sum(it["iterations"] * m.grid.dims[0] * m.grid.dims[1] for it, m in zip(items, models))
+    for m in models:
+        m.close()
+    cfg = {"workload": f"{args.instances} independent 2D pure-shear inclusion problems (seeds 0..{args.instances - 1}, "
+                       "63-511 cells per side, 1-16 circles r~U(0.02,0.15), log-normal contrast clipped to 1e4, "
+                       "viscosity smoothed by 4 log-space passes, free-slip walls with pure shear)",
+           "instances": args.instances, "cells_total": cells, "tol": tol, "ncheck": ncheck,
+           "measure": "cell-scaled relative residual max(|r_V|inf h/max|P,tau|, |r_P|inf h/max|V|), FP64",
+           "storage": dtype, "tile_shape": list(per)[best], "graph": True}
+    line = _base_line(f"batched 2D PT solves/s ({args.instances} instances)", len(items) / sec, "solves/s",
+                      len(iters), 10 * 3, 1e3 * sec / max(1, max(iters) // ncheck), dtype, cfg)
+    line.update({"status": status, "iterations": {"min": min(iters), "max": max(iters), "mean": float(np.mean(iters))},
+                 "seconds": sec, "sweep_teff_gbs": sweep_gbs,
+                 "solve_teff_gbs": 13 * esz * cell_sweeps / sec / 1e9, "clocks": ck,
+                 "gpu_launches": "k sweeps + 4 bookkeeping kernels per check round, replayed as one graph"})
+    print(json.dumps(line))
+
+
+def _serving_requests(fi, scale, duration, rate, seed=0):
+    from fastice_b200 import scenarios, serving
+    rng = np.random.default_rng(seed)
+    t, reqs = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > duration:
+            break
+        rid = len(reqs)
+        if rng.random() < 0.7:
+            n = int(round(rng.integers(128, 1025) * scale))
+            n = (max(n, 16), max(n, 16))
+            build = (lambda s=rid, n=n: scenarios.inclusion_model(s, n=n, dtype="f64")[0])
+            reqs.append(serving.SolveRequest(rid=rid, arrival=t, kind="2d", build=build,
+                                             bytes=serving.footprint_2d(n, 8), tol=1e-6, max_iter=400000))
+        else:
+            n = max(int(round(rng.integers(64, 256) * scale)), 12)
+            build = (lambda s=rid, n=n: scenarios.bed_model(s, n)[0])
+            reqs.append(serving.SolveRequest(rid=rid, arrival=t, kind="3d", build=build,
+                                             bytes=serving.footprint_3d_ib((n, n, n), 8), tol=1e-6, max_iter=200000,
+                                             meta={"length_z": 0.6}))
+    return reqs
+
+
+def run_serving(args):
+    """Continuous-batching server against one-at-a-time solves on the same
+    seeded Poisson stream (70 % 2D inclusion problems, 30 % 3D immersed-boundary
+    glaciers; sizes scaled by --scale from 128-1024 and 64-255 cells per side),
+    admission by a 150 GB device-memory budget, every request to 1e-6.  value =
+    requests / makespan with every request available at once; the latencies come
+    from a run that releases requests at their Poisson arrival times."""
+    fi = load_fastice()
+    from fastice_b200 import serving
+    rate, budget = 50.0, 150 << 30
+    out = {}
+    for mode, kw in (("batched", {}), ("sequential", {"max_active": 1})):
+        srv = serving.SolveServer(budget_bytes=budget, ncheck=200, window=100000, realtime=False, **kw)
+        t0 = time.perf_counter()
+        done = srv.run(_serving_requests(fi, args.scale, args.duration, rate))
+        span = time.perf_counter() - t0
+        thr = serving.summarize(done, makespan=span)
+        srv = serving.SolveServer(budget_bytes=budget, ncheck=200, window=100000, realtime=True, **kw)
+        done_rt = srv.run(_serving_requests(fi, args.scale, args.duration, rate))
+        lat = serving.summarize(done_rt)
+        out[mode] = {"solves_per_s": thr["solves_per_s"], "makespan_s": span, "status": thr["status"],
+                     "p50_latency_s": lat["p50_latency_s"], "p99_latency_s": lat["p99_latency_s"],
+                     "peak_bytes": srv.peak_bytes, "requests": thr["requests"]}
+    cfg = {"workload": f"Poisson stream lambda={rate}/s for {args.duration} s: 70% 2D inclusion problems "
+                       f"(128-1024 cells per side x {args.scale}), 30% 3D immersed-boundary glaciers over a seeded "
+                       f"64-bump bed (64-255 cells per side x {args.scale}); FP64; stop at 1e-6",
+           "budget_bytes": budget, "ncheck": 200,
+           "scaled": "the full stream (60 s, unscaled sizes) needs about an hour of GPU time per arm at the "
+                     "reference PT scheme's iteration counts"}
+    b = out["batched"]
+    line = _base_line("serving solves/s (continuous batching, scaled Poisson stream)", b["solves_per_s"], "solves/s",
+                      b["requests"], 0, 1e3 * b["makespan_s"] / max(1, b["requests"]), "f64", cfg)
+    line.update({"batched": b, "sequential": out["sequential"],
+                 "speedup_vs_sequential": b["solves_per_s"] / out["sequential"]["solves_per_s"]})
+    print(json.dumps(line))
+
+
+def run_mixed(args):
+    """Mixed-precision refined solve against the plain FP64 solve on the 3D
+    manufactured solution (stokes_manufactured_solution_free_slip_3D.jl) at n^3,
+    both to the same tolerance; one step = one solve."""
+    fi = load_fastice()
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from helpers import mms3d_error, mms3d_model
+    n = args.n if args.n != 511 else 255
+    tol = args.tol or 1e-8
+    res = {}
+    for mode in ("plain", "mixed"):
+        grid, m = mms3d_model(fi, n)
+        m.solve(mode=mode, max_iter=2 * n, ncheck=n, tol=1e-30)  # warm-up (shadow, autotune-free shapes)
+        for f in ("P", "txx", "tyy", "tzz", "txy", "txz", "tyz", "Vx", "Vy", "Vz"):
+            m.set_field(f, 0.0)
+        m.set_field("eta", 1.0)
+        m.set_field("eta_next", 1.0)
+        m.apply_bcs()
+        m.synchronize()
+        t0 = time.perf_counter()
+        r = m.solve(mode=mode, max_iter=400 * n, ncheck=n, tol=tol)
+        sec = time.perf_counter() - t0
+        res[mode] = {"seconds": sec, "iterations": r["iterations"], "outer": r["outer"], "measure": r["measure"],
+                     "converged": bool(r["converged"]), "mms_l2_error": mms3d_error(fi, grid, m),
+                     "Vx": m.get_field("Vx")}
+        m.close()
+    dv = float(np.max(np.abs(res["mixed"]["Vx"] - res["plain"]["Vx"])) / np.max(np.abs(res["plain"]["Vx"])))
+    for r in res.values():
+        r.pop("Vx")
+    cfg = {"workload": f"3D free-slip manufactured solution (eta=1) on [-1,1]^3, {n}^3 cells, to |R|inf < {tol}",
+           "n": n, "tol": tol}
+    sp = res["plain"]["seconds"] / res["mixed"]["seconds"]
+    line = _base_line("mixed-precision solve speedup vs plain FP64", sp, "x", 1, 1, 1e3 * res["mixed"]["seconds"],
+                      "f32+f64", cfg)
+    line.update({"plain_fp64": res["plain"], "mixed": res["mixed"], "max_rel_diff_Vx_vs_fp64": dv})
+    print(json.dumps(line))
+
+
 def dist_setup():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -246,7 +396,18 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape (profiling runs)")
     ap.add_argument("--variant", type=int, default=None, help="fused launch shape index (implies --no-autotune)")
     ap.add_argument("--dtypes", default="f64,f32", help="precisions to time, FP64 first")
+    ap.add_argument("--workload", choices=("slab", "batched", "serving", "mixed"), default="slab",
+                    help="slab: the headline T_eff line; batched / serving / mixed: the batched 2D solves, the "
+                         "continuous-batching server and the mixed-precision solve, one JSON line each")
+    ap.add_argument("--instances", type=int, default=256, help="batched: number of 2D instances")
+    ap.add_argument("--tol", type=float, default=None, help="batched / serving / mixed: stop tolerance")
+    ap.add_argument("--scale", type=float, default=0.25, help="serving: linear size scale of the request stream")
+    ap.add_argument("--duration", type=float, default=2.0, help="serving: seconds of Poisson arrivals")
+    ap.add_argument("--rounds", type=int, default=0, help="batched: stop after this many check rounds (profiling)")
     args = ap.parse_args()
+    if args.workload != "slab":
+        {"batched": run_batched, "serving": run_serving, "mixed": run_mixed}[args.workload](args)
+        return
     n = (args.n, args.n, args.n)
     ws, rank, local = dist_setup()
     metric = "PT-Stokes T_eff GB/s (511^3, FP64)"

@@ -739,7 +739,7 @@ static fi_status solve_mixed(fi_model *m, const fi_solve_opts *o, fi_solve_repor
     fi_model *s = m->shadow;
     const long long n = (long long)m->elems;
     const int nd = m->d.grid.nd;
-    const double inner_red = o->inner_reduction > 0 ? o->inner_reduction : 1e-5;
+    const double inner_red = o->inner_reduction > 0 ? o->inner_reduction : 1e-3;
     const int inner_max = o->inner_iter > 0 ? o->inner_iter : 50 * o->ncheck;
     // a stage that has not halved its best residual over this many sweeps has stalled
     int window = 0;
@@ -766,8 +766,8 @@ static fi_status solve_mixed(fi_model *m, const fi_solve_opts *o, fi_solve_repor
 
     // FP32 sweeps on the shadow, a check every ncheck, until (a) the FP64 tolerance
     // in the solve's measure (phase A only), (b) the four residual inf-norms drop to
-    // target, (c) they reach the FP32 rounding floor, (d) the best of them has not
-    // halved for `window` sweeps, or (e) max_sweeps
+    // target, (c) they reach the FP32 rounding floor (phase A only), (d) the best of
+    // them has not halved for `window` sweeps, or (e) max_sweeps
     auto stage = [&](bool phase_a, double target, int max_sweeps, const char *what) -> fi_status {
         double best = 1e300;
         int since = 0, done = 0;
@@ -792,7 +792,10 @@ static fi_status solve_mixed(fi_model *m, const fi_solve_opts *o, fi_solve_repor
                              r, target, fl_P, fl_V);
             if (phase_a && measure_of(s, o, nn) < o->tol) break;
             if (r <= target) break;
-            if (nn[0] <= fl_P && rv <= fl_V) break;
+            // the rounding floor ends the full-problem phase; a correction stops at its
+            // target or when it stalls (its own floor scales with the correction and
+            // would stop it before it has reduced anything)
+            if (phase_a && nn[0] <= fl_P && rv <= fl_V) break;
             if (r < 0.5 * best) {
                 best = r;
                 since = 0;
@@ -824,7 +827,7 @@ static fi_status solve_mixed(fi_model *m, const fi_solve_opts *o, fi_solve_repor
     FI_CHECK_CUDA(cudaStreamSynchronize(s->stream), "mixed sync");
 
     // ---- phase B: FP64 defect correction with FP32 correction sweeps
-    int outer = 0;
+    int outer = 0, outer_stale = 0;
     double best_outer = 1e300;
     while (true) {
         // viscosity from the current stresses (Picard step), then τ = 2η dev(ε̇(V)), BCs
@@ -846,12 +849,16 @@ static fi_status solve_mixed(fi_model *m, const fi_solve_opts *o, fi_solve_repor
             rep->outer = outer;
             return set_error("simulation failed: the defect correction diverged"), FI_ERR_DIVERGED;
         }
-        best_outer = std::min(best_outer, meas);
         if (meas < o->tol) {
             rep->converged = 1;
             break;
         }
         if (sweeps >= o->max_iter) break;
+        // three outer steps in a row without halving the FP64 measure: the
+        // correction no longer reaches the residual (stop, not converged)
+        if (meas < 0.5 * best_outer) outer_stale = 0;
+        else if (++outer_stale >= 3) break;
+        best_outer = std::min(best_outer, meas);
         // the correction problem on the shadow: frozen η, forcing r_P and -r_V, zero state
         if ((st = convert_field<double, float>(s->cur(FI_FIELD_ETA), m->cur(FI_FIELD_ETA), n, 1.0, m->stream)) != FI_OK)
             return st;

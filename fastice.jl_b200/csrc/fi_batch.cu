@@ -100,8 +100,8 @@ __device__ __forceinline__ void sigma2(const Tile<T, TY> &t, const BInst<T> &b, 
         T divV = exx + eyy;
         T etac = t.sEt[a];
         if (mask & M_P) t.sP[a] = t.sP[a] - divV * etac * b.dtP;
-        if (mask & M_XX) t.sXX[a] = t.sXX[a] - (t.sXX[a] - T(2.0) * etac * (exx - divV / T(3.0))) * b.dxx;
-        if (mask & M_YY) t.sYY[a] = t.sYY[a] - (t.sYY[a] - T(2.0) * etac * (eyy - divV / T(3.0))) * b.dyy;
+        if (mask & M_XX) t.sXX[a] = t.sXX[a] - (t.sXX[a] - T(2.0) * etac * (exx - third(divV))) * b.dxx;
+        if (mask & M_YY) t.sYY[a] = t.sYY[a] - (t.sYY[a] - T(2.0) * etac * (eyy - third(divV))) * b.dyy;
     }
     if ((mask & M_XY) && i >= 1 && i <= t.n0 + 1 && j >= 1 && j <= t.n1 + 1) {
         T exy = T(0.5) * ((t.sVy[a] - t.sVy[a - 1]) * b.idx + (t.sVx[a] - t.sVx[a - BW]) * b.idy);
@@ -123,22 +123,64 @@ __device__ __forceinline__ void center_ghosts(int q, int N, int kl, int kr, T cl
     if (q == N && kr == FI_BC_VELOCITY) { pos[1] = N + 1; val[1] = later_node ? v : T(2.0) * cr - v; ok[1] = true; }
 }
 
+// asynchronous global -> shared copy of one element (cp.async, sm_80+); valid == 0
+// zero-fills the destination without reading the source
+template <int S>
+__device__ __forceinline__ void cp_async_elem(void *dst, const void *src, bool valid) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src), "n"(S), "r"(valid ? S : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// stage tile w's box of the seven inputs into staging buffer buf (asynchronous)
+template <typename T, int TY>
+__device__ __forceinline__ void stage_tile(const BInst<T> *__restrict__ insts, const int4 *__restrict__ tiles, int w,
+                                           int src, T *buf) {
+    using TL = Tile<T, TY>;
+    const int4 d = tiles[w];
+    const BInst<T> &b = insts[d.x];
+    const long long sx = b.pitch;
+    const T *F[7] = {b.P[src], b.txx[src], b.tyy[src], b.txy[src], b.Vx[src], b.Vy[src], b.eta};
+    for (int r = threadIdx.x; r < TL::BOX; r += TL::NT) {
+        const int i = d.y - 1 + r % TL::BW, j = d.z - 1 + r / TL::BW;
+        const bool ok = i <= b.n0 + 2 && j <= b.n1 + 2;
+        const long long I = ok ? (long long)i + sx * (long long)j : 0;
+#pragma unroll
+        for (int f = 0; f < 7; f++) cp_async_elem<(int)sizeof(T)>(buf + f * TL::BOX + r, F[f] + I, ok);
+    }
+}
+
 template <typename T, int TY>
 __global__ void __launch_bounds__(BTX *TY) batch2d_sweep(const BInst<T> *__restrict__ insts, const int4 *__restrict__ tiles,
                                                          const int *__restrict__ ntiles, int src) {
     using TL = Tile<T, TY>;
-    __shared__ T smem[7 * TL::BOX];
+    // two staging buffers (dynamic shared memory, 2 x 7 boxes): the next tile of the
+    // work list is copied in while the current one is computed
+    extern __shared__ __align__(16) unsigned char batch_smem[];
+    T *const smem0 = reinterpret_cast<T *>(batch_smem);
     TL t;
-    t.sP = smem;
-    t.sXX = smem + TL::BOX;
-    t.sYY = smem + 2 * TL::BOX;
-    t.sXY = smem + 3 * TL::BOX;
-    t.sVx = smem + 4 * TL::BOX;
-    t.sVy = smem + 5 * TL::BOX;
-    t.sEt = smem + 6 * TL::BOX;
     const int tid = threadIdx.x, dst = src ^ 1;
     const int nt = *ntiles;
+    int cur = 0;
+    if ((int)blockIdx.x < nt) stage_tile<T, TY>(insts, tiles, blockIdx.x, src, smem0);
+    cp_async_commit();
     for (int w = blockIdx.x; w < nt; w += gridDim.x) {
+        const int nx = w + gridDim.x;
+        if (nx < nt) stage_tile<T, TY>(insts, tiles, nx, src, smem0 + (cur ^ 1) * 7 * TL::BOX);
+        cp_async_commit();
+        cp_async_wait_prev();  // this tile's copies (all but the group just committed) are done
+        __syncthreads();
+        T *sm = smem0 + cur * 7 * TL::BOX;
+        t.sP = sm;
+        t.sXX = sm + TL::BOX;
+        t.sYY = sm + 2 * TL::BOX;
+        t.sXY = sm + 3 * TL::BOX;
+        t.sVx = sm + 4 * TL::BOX;
+        t.sVy = sm + 5 * TL::BOX;
+        t.sEt = sm + 6 * TL::BOX;
+        cur ^= 1;
         const int4 d = tiles[w];
         const BInst<T> &b = insts[d.x];
         t.i0 = d.y;
@@ -146,17 +188,6 @@ __global__ void __launch_bounds__(BTX *TY) batch2d_sweep(const BInst<T> *__restr
         t.n0 = b.n0;
         t.n1 = b.n1;
         const long long sx = b.pitch;
-        const T *P = b.P[src], *XX = b.txx[src], *YY = b.tyy[src], *XY = b.txy[src], *VX = b.Vx[src], *VY = b.Vy[src];
-        for (int r = tid; r < TL::BOX; r += TL::NT) {
-            const int i = t.i0 - 1 + r % TL::BW, j = t.j0 - 1 + r / TL::BW;
-            T p = T(0), xx = T(0), yy = T(0), xy = T(0), vx = T(0), vy = T(0), et = T(0);
-            if (i <= t.n0 + 2 && j <= t.n1 + 2) {
-                const long long I = (long long)i + sx * (long long)j;
-                p = P[I]; xx = XX[I]; yy = YY[I]; xy = XY[I]; vx = VX[I]; vy = VY[I]; et = b.eta[I];
-            }
-            t.sP[r] = p; t.sXX[r] = xx; t.sYY[r] = yy; t.sXY[r] = xy; t.sVx[r] = vx; t.sVy[r] = vy; t.sEt[r] = et;
-        }
-        __syncthreads();
         const bool bnd_x = t.i0 == 1 || t.i0 + BTX >= t.n0 + 1;
         const bool bnd_y = t.j0 == 1 || t.j0 + TY >= t.n1 + 1;
         const bool late = bnd_x || bnd_y;
@@ -234,7 +265,7 @@ __global__ void __launch_bounds__(BTX *TY) batch2d_sweep(const BInst<T> *__restr
                 else {
                     const T gx = b.gkind[0] == FI_G_FIELD ? b.gx[Ic] : b.gval[0];
                     const T ex = T(0.5) * (t.sEt[a - 1] + t.sEt[a]);
-                    v = t.sVx[a] + div_dev(-(t.sP[a] - t.sP[a - 1]) * b.idx + (t.sXX[a] - t.sXX[a - 1]) * b.idx +
+                    v = t.sVx[a] + div_fast(-(t.sP[a] - t.sP[a - 1]) * b.idx + (t.sXX[a] - t.sXX[a - 1]) * b.idx +
                                                (t.sXY[a + BW] - t.sXY[a]) * b.idy - gx,
                                            ex) *
                                        b.dVx;
@@ -255,7 +286,7 @@ __global__ void __launch_bounds__(BTX *TY) batch2d_sweep(const BInst<T> *__restr
                 else {
                     const T gy = b.gkind[1] == FI_G_FIELD ? b.gy[Ic] : b.gval[1];
                     const T ey = T(0.5) * (t.sEt[a - BW] + t.sEt[a]);
-                    v = t.sVy[a] + div_dev(-(t.sP[a] - t.sP[a - BW]) * b.idy + (t.sYY[a] - t.sYY[a - BW]) * b.idy +
+                    v = t.sVy[a] + div_fast(-(t.sP[a] - t.sP[a - BW]) * b.idy + (t.sYY[a] - t.sYY[a - BW]) * b.idy +
                                                (t.sXY[a + 1] - t.sXY[a]) * b.idx - gy,
                                            ey) *
                                        b.dVy;
@@ -421,12 +452,21 @@ __global__ void batch_fill(int total, const int4 *__restrict__ all, const int *_
     }
 }
 
-// resident sweep CTAs per SM (queried once per instantiation, outside any capture)
+template <typename T, int TY>
+constexpr size_t sweep_smem() {
+    return 2 * 7 * (size_t)Tile<T, TY>::BOX * sizeof(T);
+}
+
+// resident sweep CTAs per SM (queried once per instantiation, outside any capture;
+// also lifts the dynamic shared-memory limit where the two staging buffers need it)
 template <typename T, int TY>
 int sweep_blocks_per_sm() {
     static const int nb = [] {
+        cudaFuncSetAttribute(batch2d_sweep<T, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sweep_smem<T, TY>());
         int v = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, batch2d_sweep<T, TY>, BTX * TY, 0) != cudaSuccess) v = 1;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, batch2d_sweep<T, TY>, BTX * TY, sweep_smem<T, TY>()) !=
+            cudaSuccess)
+            v = 1;
         return std::max(v, 1);
     }();
     return nb;
@@ -644,7 +684,7 @@ fi_status build_tiles(fi_batch *b, int ty) {
 template <typename T, int TY>
 cudaError_t launch_sweep_t(fi_batch *b, const int4 *list, const int *nt, int src) {
     const int grid = b->sms * sweep_blocks_per_sm<T, TY>();
-    batch2d_sweep<T, TY><<<grid, BTX * TY, 0, b->stream>>>((const BInst<T> *)b->d_inst, list, nt, src);
+    batch2d_sweep<T, TY><<<grid, BTX * TY, sweep_smem<T, TY>(), b->stream>>>((const BInst<T> *)b->d_inst, list, nt, src);
     return cudaGetLastError();
 }
 template <typename T>

@@ -325,7 +325,6 @@ class IsothermalImmersedBoundaryFullStokesModel(_StokesBase):
         L.check(self.lib, self.lib.fi_model_volfrac_from_levelset(self._h, {"na": 0, "ns": 1}[group], psi.ctypes.data))
 
 
-# -- free functions with the reference names ----------------------------------------
 class BatchedStokes2D:
     """Many independent 2D models solved together (fi_batch_* in the C ABI).
 
@@ -432,6 +431,7 @@ class BatchedStokes2D:
         return self._items(items), sec.value
 
 
+# -- free functions with the reference names ----------------------------------------
 def advance_iteration(model: _StokesBase, t: float = 0.0, dt: float = 1.0) -> None:
     """``advance_iteration!(model, t, Δt)`` (t and Δt are unused, as in the reference)."""
     model.advance(1)

@@ -109,6 +109,45 @@ def inclusion_model(seed: int, n=None, dtype: str = "f32", library: str = "fast"
     return m, prm
 
 
+def bed_model(seed: int, n: int, dtype: str = "f64", library: str = "fast", rheology=None, dem_cells=None):
+    """Build the immersed-boundary glacier of ``seed`` on the unit cube with n^3
+    cells: returns (model, params).  Bed and surface DEMs live on a 2D vertex grid
+    slightly wider than the cube; ψ.na comes from the surface DEM, ψ.ns from the
+    bed DEM inverted, and the volume fractions from ω_from_ψ!
+    (scripts_future_API/test_volume_fractions.jl:86-100).  Traction-free box
+    sides, ρg = (0, 0, 1), linear viscosity 1 unless ``rheology`` is given, and
+    that driver's PT steps (r = 0.9, re = 5π, factor 1.1)."""
+    from .levelsets import compute_levelset_from_dem
+    from .models import IsothermalImmersedBoundaryFullStokesModel
+    from .physics import TBC
+    prm = bed_params(seed, n)
+    grid = UniformGrid(origin=(0.0, 0.0, 0.0), extent=(1.0, 1.0, 1.0), dims=(n, n, n))
+    m2 = dem_cells or n + 1
+    dem_grid = UniformGrid(origin=(-0.05, -0.05), extent=(1.1, 1.1), dims=(m2, m2))
+    # vertex coordinates of the DEM grid in halo storage (index 0 is one spacing outside)
+    h = 1.1 / m2
+    xv = -0.05 + (np.arange(m2 + 3) - 1) * h
+    Y, X = np.meshgrid(xv, xv, indexing="ij")
+    bed = bed_height(prm, X, Y)
+    surf = 0.6 + 0.05 * np.sin(2.0 * math.pi * X)
+    psi_na = compute_levelset_from_dem(grid, dem_grid, surf, library=library)
+    psi_ns = compute_levelset_from_dem(grid, dem_grid, bed, invert=True, library=library)
+    free = TBC(0.0, 0.0, 0.0)
+    r, re_mech, factor = 0.9, 5 * math.pi, 1.1
+    sp = pt_params(grid, r=r, re_mech=re_mech, vdtau_factor=factor)
+    m = IsothermalImmersedBoundaryFullStokesModel(
+        grid=grid, boundary_conditions={"x": (free, free), "y": (free, free), "z": (free, free)},
+        gravity={"x": 0.0, "y": 0.0, "z": 1.0}, rheology=rheology or LinearViscousRheology(1.0),
+        solver_params=sp, dtype=dtype, library=library)
+    m.omega_from_psi("ns", psi_ns)
+    m.omega_from_psi("na", psi_na)
+    m.set_field("eta", 1.0)
+    m.set_field("eta_next", 1.0)
+    m.apply_bcs()
+    prm.update(thickness=0.6)
+    return m, prm
+
+
 def bed_params(seed: int, n: int, bumps: int = 64):
     """Seeded bed of ``bumps`` Gaussian bumps a·exp(-|x-c|^2/w^2), a~U(0,0.2),
     w~U(0.05,0.2), c~U([0,1]^2), and the surface z = 0.6 + 0.05 sin(2πx)."""
@@ -127,4 +166,4 @@ def bed_height(prm, x, y):
 
 
 __all__ = ["inclusion_params", "inclusion_viscosity", "inclusion_model", "smooth_log", "stiffness_ratio",
-           "bed_params", "bed_height", "INCLUSION_N_RANGE"]
+           "bed_model", "bed_params", "bed_height", "INCLUSION_N_RANGE"]

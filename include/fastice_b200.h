@@ -197,7 +197,7 @@ typedef struct {
     int32_t mode;           /* fi_solve_mode: MIXED = FP32 sweeps in FP64 defect correction */
     int32_t inner_iter;     /* MIXED: most FP32 sweeps per correction (0: 50 * ncheck) */
     double inner_reduction; /* MIXED: stop a correction once its residual dropped by this
-                               factor (0: 1e-5) or stopped halving over two checks */
+                               factor (0: 1e-3) or stopped halving for 2(n+1) sweeps */
 } fi_solve_opts;
 
 typedef struct {
