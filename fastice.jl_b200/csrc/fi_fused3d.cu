@@ -50,6 +50,9 @@ namespace {
 constexpr int TX = 32;
 constexpr long long kWaitCycles = 1ll << 31;
 
+// Launch shapes: tile height and z-block depth.  (Issuing the copies of plane s+1
+// after the stress barrier of step s instead, which saves the barrier closing each
+// step, measured 15-20 % slower at 511^3: the copies then lose half their lead.)
 struct Variant {
     int ty;
     int zb;
@@ -231,7 +234,10 @@ __device__ __forceinline__ void issue_group(const Ctx<T, TY> &c, const InMaps &m
     tma_load_3d(c.slot(S_ET, R_ET, p), &mp.m[10], x, y, p, bar);
 }
 
-// raw stress update of plane s at (i, j): which components is a compile-time mask
+// raw stress update of plane s at (i, j): which components is a compile-time mask.
+// Every shared-memory operand is loaded before the first store (the in-place stress
+// stores and the global writes go through pointers the compiler cannot separate from
+// the loads), so the seven updates form independent chains.
 enum { F_P = 1, F_XX = 2, F_YY = 4, F_ZZ = 8, F_XY = 16, F_XZ = 32, F_YZ = 64, F_ALL = 127 };
 
 // XYI: the column and its ring lie inside every x / y range (no boundary column),
@@ -240,6 +246,7 @@ template <typename T, int TY, bool XYI>
 __device__ __forceinline__ void sigma_point(const Ctx<T, TY> &c, const KParams &p, const TConst<T> &q, int s, int i, int j, int mask,
                                             bool write_now, const Ptrs<T> &out) {
     if (!XYI && (i > c.n0 + 2 || j > c.n1 + 2)) return;
+    constexpr int BX = Ctx<T, TY>::Lay::BX;
     const T idx = q.inv_dx[0], idy = q.inv_dx[1], idz = q.inv_dx[2];
     const bool cz = s >= 1 && s <= c.n2, vz = s >= 1 && s <= c.n2 + 1;
     const bool cx = XYI || (i >= 1 && i <= c.n0) || (c.perx && (i == 0 || i == c.n0 + 1));
@@ -247,61 +254,89 @@ __device__ __forceinline__ void sigma_point(const Ctx<T, TY> &c, const KParams &
     const bool cy = XYI || (j >= 1 && j <= c.n1) || (c.pery && (j == 0 || j == c.n1 + 1));
     const bool vy = XYI || (j >= 1 && j <= c.n1 + 1);
     const int a = c.at(i, j);
-    if ((mask & (F_P | F_XX | F_YY | F_ZZ)) && cx && cy && cz) {
-        const T *vxs = c.slot(S_VX, R_VX, s), *vys = c.slot(S_VY, R_VY, s);
+    const T *vxs = c.slot(S_VX, R_VX, s), *vys = c.slot(S_VY, R_VY, s), *vzs = c.slot(S_VZ, R_VZ, s);
+    const T *vxm = c.slot(S_VX, R_VX, s - 1), *vym = c.slot(S_VY, R_VY, s - 1), *vzp = c.slot(S_VZ, R_VZ, s + 1);
+    const T *et = c.slot(S_ET, R_ET, s), *etm = c.slot(S_ET, R_ET, s - 1);
+    T *sP = c.slot(S_P, R_P, s) + a, *sXX = c.slot(S_XX, R_XX, s) + a, *sYY = c.slot(S_YY, R_YY, s) + a;
+    T *sZZ = c.slot(S_ZZ, R_ZZ, s) + a, *sXY = c.slot(S_XY, R_XY, s) + a, *sXZ = c.slot(S_XZ, R_XZ, s) + a;
+    T *sYZ = c.slot(S_YZ, R_YZ, s) + a;
+    const bool dc = (mask & (F_P | F_XX | F_YY | F_ZZ)) && cx && cy && cz;
+    const bool dxy = (mask & F_XY) && vx && vy && cz;
+    const bool dxz = (mask & F_XZ) && vx && cy && vz;
+    const bool dyz = (mask & F_YZ) && cx && vy && vz;
+    // old values (all seven when the point is written out)
+    const int lmask = write_now ? F_ALL : mask;
+    T oP = T(0), oXX = T(0), oYY = T(0), oZZ = T(0), oXY = T(0), oXZ = T(0), oYZ = T(0);
+    if (lmask & F_P) oP = *sP;
+    if (lmask & F_XX) oXX = *sXX;
+    if (lmask & F_YY) oYY = *sYY;
+    if (lmask & F_ZZ) oZZ = *sZZ;
+    if (lmask & F_XY) oXY = *sXY;
+    if (lmask & F_XZ) oXZ = *sXZ;
+    if (lmask & F_YZ) oYZ = *sYZ;
+    T nP = oP, nXX = oXX, nYY = oYY, nZZ = oZZ, nXY = oXY, nXZ = oXZ, nYZ = oYZ;
+    if (dc) {
         T exx = (vxs[a + 1] - vxs[a]) * idx;
-        T eyy = (vys[a + Ctx<T, TY>::Lay::BX] - vys[a]) * idy;
-        T ezz = (c.slot(S_VZ, R_VZ, s + 1)[a] - c.slot(S_VZ, R_VZ, s)[a]) * idz;
+        T eyy = (vys[a + BX] - vys[a]) * idy;
+        T ezz = (vzp[a] - vzs[a]) * idz;
         T divV = exx + eyy + ezz;
-        T etac = c.slot(S_ET, R_ET, s)[a];
-        if (mask & F_P) {
-            T &v = c.slot(S_P, R_P, s)[a];
-            v = v - (p.p_forcing ? divV + __ldg(out.fP + c.gidx(i, j, s)) : divV) * etac * q.dt_P;
-        }
-        if (mask & F_XX) {
-            T &v = c.slot(S_XX, R_XX, s)[a];
-            v = v - (v - T(2.0) * etac * (exx - third(divV))) * q.dt_tau[0];
-        }
-        if (mask & F_YY) {
-            T &v = c.slot(S_YY, R_YY, s)[a];
-            v = v - (v - T(2.0) * etac * (eyy - third(divV))) * q.dt_tau[1];
-        }
-        if (mask & F_ZZ) {
-            T &v = c.slot(S_ZZ, R_ZZ, s)[a];
-            v = v - (v - T(2.0) * etac * (ezz - third(divV))) * q.dt_tau[2];
-        }
+        T etac = et[a];
+        if (mask & F_P) nP = oP - (p.p_forcing ? divV + __ldg(out.fP + c.gidx(i, j, s)) : divV) * etac * q.dt_P;
+        if (mask & F_XX) nXX = oXX - (oXX - T(2.0) * etac * (exx - third(divV))) * q.dt_tau[0];
+        if (mask & F_YY) nYY = oYY - (oYY - T(2.0) * etac * (eyy - third(divV))) * q.dt_tau[1];
+        if (mask & F_ZZ) nZZ = oZZ - (oZZ - T(2.0) * etac * (ezz - third(divV))) * q.dt_tau[2];
     }
-    constexpr int BX = Ctx<T, TY>::Lay::BX;
-    if ((mask & F_XY) && vx && vy && cz) {
-        const T *vxs = c.slot(S_VX, R_VX, s), *vys = c.slot(S_VY, R_VY, s), *et = c.slot(S_ET, R_ET, s);
+    if (dxy) {
         T exy = T(0.5) * ((vys[a] - vys[a - 1]) * idx + (vxs[a] - vxs[a - BX]) * idy);
         T e_xy = h(h(et[a - 1 - BX] + et[a - BX]) + h(et[a - 1] + et[a]));
-        T &v = c.slot(S_XY, R_XY, s)[a];
-        v = v - (v - T(2.0) * e_xy * exy) * q.dt_tau[3];
+        nXY = oXY - (oXY - T(2.0) * e_xy * exy) * q.dt_tau[3];
     }
-    if ((mask & F_XZ) && vx && cy && vz) {
-        const T *vzs = c.slot(S_VZ, R_VZ, s), *et = c.slot(S_ET, R_ET, s), *etm = c.slot(S_ET, R_ET, s - 1);
-        T exz = T(0.5) * ((vzs[a] - vzs[a - 1]) * idx + (c.slot(S_VX, R_VX, s)[a] - c.slot(S_VX, R_VX, s - 1)[a]) * idz);
+    if (dxz) {
+        T exz = T(0.5) * ((vzs[a] - vzs[a - 1]) * idx + (vxs[a] - vxm[a]) * idz);
         T e_xz = h(h(etm[a - 1] + etm[a]) + h(et[a - 1] + et[a]));
-        T &v = c.slot(S_XZ, R_XZ, s)[a];
-        v = v - (v - T(2.0) * e_xz * exz) * q.dt_tau[4];
+        nXZ = oXZ - (oXZ - T(2.0) * e_xz * exz) * q.dt_tau[4];
     }
-    if ((mask & F_YZ) && cx && vy && vz) {
-        const T *vzs = c.slot(S_VZ, R_VZ, s), *et = c.slot(S_ET, R_ET, s), *etm = c.slot(S_ET, R_ET, s - 1);
-        T eyz = T(0.5) * ((vzs[a] - vzs[a - BX]) * idy + (c.slot(S_VY, R_VY, s)[a] - c.slot(S_VY, R_VY, s - 1)[a]) * idz);
+    if (dyz) {
+        T eyz = T(0.5) * ((vzs[a] - vzs[a - BX]) * idy + (vys[a] - vym[a]) * idz);
         T e_yz = h(h(etm[a - BX] + etm[a]) + h(et[a - BX] + et[a]));
-        T &v = c.slot(S_YZ, R_YZ, s)[a];
-        v = v - (v - T(2.0) * e_yz * eyz) * q.dt_tau[5];
+        nYZ = oYZ - (oYZ - T(2.0) * e_yz * eyz) * q.dt_tau[5];
     }
+    if (dc) {
+        if (mask & F_P) *sP = nP;
+        if (mask & F_XX) *sXX = nXX;
+        if (mask & F_YY) *sYY = nYY;
+        if (mask & F_ZZ) *sZZ = nZZ;
+    }
+    if (dxy) *sXY = nXY;
+    if (dxz) *sXZ = nXZ;
+    if (dyz) *sYZ = nYZ;
     if (write_now) {
         const long long I = c.gidx(i, j, s);
-        out.P[I] = c.slot(S_P, R_P, s)[a];
-        out.txx[I] = c.slot(S_XX, R_XX, s)[a];
-        out.tyy[I] = c.slot(S_YY, R_YY, s)[a];
-        out.tzz[I] = c.slot(S_ZZ, R_ZZ, s)[a];
-        out.txy[I] = c.slot(S_XY, R_XY, s)[a];
-        out.txz[I] = c.slot(S_XZ, R_XZ, s)[a];
-        out.tyz[I] = c.slot(S_YZ, R_YZ, s)[a];
+        out.P[I] = nP;
+        out.txx[I] = nXX;
+        out.tyy[I] = nYY;
+        out.tzz[I] = nZZ;
+        out.txy[I] = nXY;
+        out.txz[I] = nXZ;
+        out.tyz[I] = nYZ;
+    }
+}
+
+// ring stresses of plane s (see sigma_plane); TX == 32 lanes span a row, TY < 32
+template <typename T, int TY, bool XYI>
+__device__ __forceinline__ void sigma_ring(const Ctx<T, TY> &c, const KParams &p, const TConst<T> &q, int s, const Ptrs<T> &out) {
+    constexpr int NW = Layout<T, TY>::NT / 32;
+    static_assert(TX == 32 && TY < 32 && NW >= 4, "one ring side per warp");
+    const int w = threadIdx.x / 32, lane = threadIdx.x % 32;
+    if (w == NW - 4) {
+        sigma_point<T, TY, XYI>(c, p, q, s, c.i0 + lane, c.j0 - 1, F_P | F_YY, false, out);
+    } else if (w == NW - 3) {
+        sigma_point<T, TY, XYI>(c, p, q, s, c.i0 + lane, c.j0 + TY, F_XY | F_YZ, false, out);
+    } else if (w == NW - 2) {
+        if (lane < TY) sigma_point<T, TY, XYI>(c, p, q, s, c.i0 - 1, c.j0 + lane, F_P | F_XX, false, out);
+    } else if (w == NW - 1) {
+        if (lane < TY) sigma_point<T, TY, XYI>(c, p, q, s, c.i0 + TX, c.j0 + lane, F_XY | F_XZ, false, out);
+        else if (lane == TY) sigma_point<T, TY, XYI>(c, p, q, s, c.i0 + TX, c.j0 + TY, F_XY, false, out);
     }
 }
 
@@ -346,22 +381,17 @@ __device__ __forceinline__ void sigma_plane(const Ctx<T, TY> &c, const KParams &
     const bool zb_plane = s == 1 || s == c.n2 + 1;
     const bool late = c.bnd_x || c.bnd_y || zb_plane;
     const bool own_s = s >= c.kb && s < c.ke;
-    // pass 1: the column, all components; pass 2: the ring, only the components read there
-    constexpr int NR = 2 * TY + 2 * TX + 1;
-    int ri = 0, rj = 0, rmask = 0;
-    if (tid < NR) {
-        if (tid < TY) { ri = c.i0 - 1; rj = c.j0 + tid; rmask = F_P | F_XX; }
-        else if (tid < 2 * TY) { ri = c.i0 + TX; rj = c.j0 + tid - TY; rmask = F_XY | F_XZ; }
-        else if (tid < 2 * TY + TX) { ri = c.i0 + tid - 2 * TY; rj = c.j0 - 1; rmask = F_P | F_YY; }
-        else if (tid < 2 * TY + 2 * TX) { ri = c.i0 + tid - 2 * TY - TX; rj = c.j0 + TY; rmask = F_XY | F_YZ; }
-        else { ri = c.i0 + TX; rj = c.j0 + TY; rmask = F_XY; }
-    }
+    // pass 1: the column, all components; pass 2: the ring, only the components read
+    // there, one ring side per warp on the last four warps (one per scheduler), so
+    // that every ring warp takes a single branch path: the row below (P, τyy), the
+    // row above (τxy, τyz), the column left (P, τxx), the column right (τxy, τxz)
+    // with the corner above it (τxy)
     if (!c.bnd_x && !c.bnd_y) {
         sigma_point<T, TY, true>(c, p, q, s, c.i0 + (tid % TX), c.j0 + (tid / TX), F_ALL, own_s && !late, out);
-        if (tid < NR) sigma_point<T, TY, true>(c, p, q, s, ri, rj, rmask, false, out);
+        sigma_ring<T, TY, true>(c, p, q, s, out);
     } else {
         sigma_point<T, TY, false>(c, p, q, s, c.i0 + (tid % TX), c.j0 + (tid / TX), F_ALL, own_s && !late, out);
-        if (tid < NR) sigma_point<T, TY, false>(c, p, q, s, ri, rj, rmask, false, out);
+        sigma_ring<T, TY, false>(c, p, q, s, out);
     }
     __syncthreads();
     if (!late) return;
@@ -554,10 +584,15 @@ __device__ __forceinline__ void v_plane(const Ctx<T, TY> &c, const KParams &p, c
     const long long I = c.gidx(i, j, t);
     const bool near = i <= 2 || i >= n0 || j <= 2 || j >= n1 || t <= 1 || t >= n2;
     if (!near) {
-        out.Vx[I] = vx_raw(c, p, q, in, t, i, j, I);
-        out.Vy[I] = vy_raw(c, p, q, in, t, i, j, I);
-        out.Vz[I] = vz_raw(c, p, q, in, t, i, j, I);
-        if (!p.freeze_eta) out.eta_next[I] = eta_raw(c, p, q, in, t, i, j, I);
+        // all four values before the first store (see sigma_point)
+        const T vxn = vx_raw(c, p, q, in, t, i, j, I);
+        const T vyn = vy_raw(c, p, q, in, t, i, j, I);
+        const T vzn = vz_raw(c, p, q, in, t, i, j, I);
+        const T etn = p.freeze_eta ? T(0) : eta_raw(c, p, q, in, t, i, j, I);
+        out.Vx[I] = vxn;
+        out.Vy[I] = vyn;
+        out.Vz[I] = vzn;
+        if (!p.freeze_eta) out.eta_next[I] = etn;
         return;
     }
     auto node_fixed = [](int kind) { return kind == FI_BC_SLIP || kind == FI_BC_VELOCITY; };

@@ -128,9 +128,10 @@ def test_3d_relaxation_log_scales(scale):
 
 @pytest.mark.parametrize("variant", range(7))
 @pytest.mark.parametrize("dtype", ["f64", "f32"])
-def test_every_fused_variant_bitwise(variant, dtype):
+@pytest.mark.parametrize("bc", ["mixed_values", "slab_periodic"])
+def test_every_fused_variant_bitwise(variant, dtype, bc):
     # each launch shape the autotuner may pick: tiles and z-blocks cut across the grid
-    p = Pair((70, 37, 150), BC3["mixed_values"], path="fused", library="strict", dtype=dtype, seed=13)
+    p = Pair((70, 37, 150), BC3[bc], path="fused", library="strict", dtype=dtype, seed=13)
     nv = p.model.lib.fi_fused_variant_count()
     if variant >= nv:
         p.close()
