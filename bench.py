@@ -377,6 +377,67 @@ def run_mixed(args):
     print(json.dumps(line))
 
 
+def ib_a_eff_elements(n):
+    """Minimum elements one immersed-boundary iteration moves: the 22 state passes
+    plus a read of the seven mask components of each of ω.na and ω.ns that the
+    masked kernels use (ccc, vcc, cvc, ccv, vvc, vcv, cvv), at their staggered sizes."""
+    nx, ny, nz = n
+    masks = nx * ny * nz + (nx + 1) * ny * nz + nx * (ny + 1) * nz + nx * ny * (nz + 1) + \
+        (nx + 1) * (ny + 1) * nz + (nx + 1) * ny * (nz + 1) + nx * (ny + 1) * (nz + 1)
+    return a_eff_elements(n) + 2 * masks
+
+
+def run_glacier(args):
+    """Immersed-boundary glacier: seeded 64-bump bed and the sinusoidal surface on
+    the unit cube at n^3 cells (383^3 by default), level sets from the DEMs, volume
+    fractions from the level sets, linear viscosity; one step = one PT iteration
+    (advance_iteration! of the immersed-boundary model).  value = T_eff over the
+    36 array passes of one iteration (FP64; FP32 in the same line)."""
+    import torch
+    fi = load_fastice()
+    from fastice_b200 import scenarios
+    n = args.n if args.n != 511 else 383
+    dims = (n, n, n)
+    A = ib_a_eff_elements(dims)
+    peak, peak_kind = measured_peak_hbm()
+    res = {}
+    clocks = None
+    for dtype in [d for d in args.dtypes.split(",") if d in ("f64", "f32")]:
+        t0 = time.perf_counter()
+        m, prm = scenarios.bed_model(0, n, dtype=dtype)
+        setup = time.perf_counter() - t0
+        m.advance(args.warmup)
+        m.synchronize()
+        sampler = ClockSampler(0) if dtype == "f64" else None
+        if sampler:
+            sampler.start()
+            time.sleep(0.15)
+        ms = time_advance(fi, m, args.steps, torch)
+        if sampler:
+            clocks = sampler.stop()
+        norms = m.residual_norms()
+        esz = 8 if dtype == "f64" else 4
+        res[dtype] = {"ms_per_step": ms / args.steps, "teff_gbs": A * esz / (ms / args.steps / 1e3) / 1e9,
+                      "path": m.path, "setup_s": setup, "finite": bool(norms[11] == 0.0)}
+        m.close()
+        torch.cuda.empty_cache()
+    d0 = res.get("f64") or next(iter(res.values()))
+    dt0 = "f64" if "f64" in res else next(iter(res))
+    cfg = {"workload": f"3D immersed-boundary glacier {n}^3 cells on the unit cube: bed = seeded sum of 64 Gaussian "
+                       "bumps (a~U(0,0.2), w~U(0.05,0.2), centres uniform), surface z = 0.6 + 0.05 sin(2 pi x), "
+                       "level sets from the DEMs, volume fractions from the level sets, traction-free box, "
+                       "one PT iteration per step", "grid": list(dims), "a_eff_arrays": 36,
+           "l2": "inputs exceed L2 (126 MB): no flush needed"}
+    line = _base_line(f"IB PT-Stokes T_eff GB/s ({n}^3, {dt0.upper()})", d0["teff_gbs"], "GB/s", args.steps,
+                      args.warmup, d0["ms_per_step"], dt0, cfg)
+    line.update({"kernel_path": d0["path"], "gpu_launches": None,
+                 "roofline": {"bound": "hbm", "achieved": d0["teff_gbs"], "peak": peak, "unit": "GB/s",
+                              "frac": d0["teff_gbs"] / peak, "peak_source": peak_kind,
+                              "algorithmic_bytes": A * (8 if dt0 == "f64" else 4)},
+                 "per_dtype": res, "clocks": clocks})
+    print(json.dumps(line))
+
+
 def dist_setup():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -396,9 +457,10 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape (profiling runs)")
     ap.add_argument("--variant", type=int, default=None, help="fused launch shape index (implies --no-autotune)")
     ap.add_argument("--dtypes", default="f64,f32", help="precisions to time, FP64 first")
-    ap.add_argument("--workload", choices=("slab", "batched", "serving", "mixed"), default="slab",
-                    help="slab: the headline T_eff line; batched / serving / mixed: the batched 2D solves, the "
-                         "continuous-batching server and the mixed-precision solve, one JSON line each")
+    ap.add_argument("--workload", choices=("slab", "batched", "serving", "mixed", "glacier"), default="slab",
+                    help="slab: the headline T_eff line; batched / serving / mixed / glacier: the batched 2D solves, "
+                         "the continuous-batching server, the mixed-precision solve and the immersed-boundary "
+                         "glacier sweep, one JSON line each")
     ap.add_argument("--instances", type=int, default=256, help="batched: number of 2D instances")
     ap.add_argument("--tol", type=float, default=None, help="batched / serving / mixed: stop tolerance")
     ap.add_argument("--scale", type=float, default=0.25, help="serving: linear size scale of the request stream")
@@ -406,7 +468,8 @@ def main():
     ap.add_argument("--rounds", type=int, default=0, help="batched: stop after this many check rounds (profiling)")
     args = ap.parse_args()
     if args.workload != "slab":
-        {"batched": run_batched, "serving": run_serving, "mixed": run_mixed}[args.workload](args)
+        {"batched": run_batched, "serving": run_serving, "mixed": run_mixed,
+         "glacier": run_glacier}[args.workload](args)
         return
     n = (args.n, args.n, args.n)
     ws, rank, local = dist_setup()

@@ -33,6 +33,7 @@
 
 #include "fi_device.cuh"
 #include "fi_model.h"
+#include "fi_tma.cuh"
 
 namespace fi {
 namespace {
@@ -43,7 +44,7 @@ constexpr int kBatchVariants = sizeof(kBatchTY) / sizeof(kBatchTY[0]);
 constexpr int kSlots = 4;  // per-instance check maxima: |r_P|, |r_V|, |P, τ|, |V|
 
 template <typename T>
-struct BInst {
+struct alignas(16) BInst {  // copied whole into shared memory (bulk copy: 16-byte granules)
     int n0, n1;
     long long pitch;
     T idx, idy, dtP, dxx, dyy, dxy, dVx, dVy;
@@ -69,12 +70,36 @@ struct BState {
 
 __device__ __forceinline__ bool node_fixed(int kind) { return kind == FI_BC_SLIP || kind == FI_BC_VELOCITY; }
 
+// TMA box width (elements) and the column's offset inside it: the box starts XB
+// positions left of the tile so that its x coordinate is 16-byte aligned
+template <typename T>
+struct BBox;
+template <>
+struct BBox<double> {
+    static constexpr int BX = 36, XB = 2;
+};
+template <>
+struct BBox<float> {
+    static constexpr int BX = 40, XB = 4;
+};
+
+// per-member tensor maps: [buffer][P, txx, tyy, txy, Vx, Vy, eta] (eta is the same
+// array for both buffers)
+struct alignas(128) BMaps {
+    unsigned char m[2][7][128];
+};
+
 template <typename T, int TY>
 struct Tile {
-    static constexpr int BW = BTX + 2, RY = TY + 2, BOX = BW * RY, NT = BTX * TY;
+    static constexpr int BX = BBox<T>::BX, XB = BBox<T>::XB, RW = BTX + 2, RY = TY + 2, NT = BTX * TY;
+    static constexpr int BOXB = BX * RY * (int)sizeof(T);
+    static constexpr int SLOTB = (BOXB + 127) / 128 * 128;
+    static constexpr int PARB = ((int)sizeof(BInst<T>) + 127) / 128 * 128;
+    static constexpr int STAGEB = 7 * SLOTB + PARB + 128;  // 7 boxes, the member's parameters, the tile descriptor
+    static constexpr uint32_t TX_BYTES = 7u * BOXB + (uint32_t)sizeof(BInst<T>);
     T *sP, *sXX, *sYY, *sXY, *sVx, *sVy, *sEt;
     int i0, j0, n0, n1;
-    __device__ __forceinline__ int at(int i, int j) const { return (j - j0 + 1) * BW + (i - i0 + 1); }
+    __device__ __forceinline__ int at(int i, int j) const { return (j - j0 + 1) * BX + (i - i0 + XB); }
     __device__ __forceinline__ bool own_x(int i) const {
         if (i >= 1 && i <= n0 + 1) return i >= i0 && i < i0 + BTX;
         if (i == 0) return i0 == 1;
@@ -89,24 +114,36 @@ struct Tile {
 
 enum { M_P = 1, M_XX = 2, M_YY = 4, M_XY = 8, M_ALL = 15 };
 
-// new stresses at (i, j) in shared memory (kernels_2d.jl:3-18), components in mask
+// new stresses at (i, j) in shared memory (kernels_2d.jl:3-18), components in mask;
+// all operands are loaded before the first store
 template <typename T, int TY>
 __device__ __forceinline__ void sigma2(const Tile<T, TY> &t, const BInst<T> &b, int i, int j, int mask) {
-    constexpr int BW = Tile<T, TY>::BW;
+    constexpr int BX = Tile<T, TY>::BX;
     const int a = t.at(i, j);
-    if ((mask & (M_P | M_XX | M_YY)) && i >= 1 && i <= t.n0 && j >= 1 && j <= t.n1) {
+    const bool dc = (mask & (M_P | M_XX | M_YY)) && i >= 1 && i <= t.n0 && j >= 1 && j <= t.n1;
+    const bool dxy = (mask & M_XY) && i >= 1 && i <= t.n0 + 1 && j >= 1 && j <= t.n1 + 1;
+    if (dc) {
+        const T oP = t.sP[a], oXX = t.sXX[a], oYY = t.sYY[a];
         T exx = (t.sVx[a + 1] - t.sVx[a]) * b.idx;
-        T eyy = (t.sVy[a + BW] - t.sVy[a]) * b.idy;
+        T eyy = (t.sVy[a + BX] - t.sVy[a]) * b.idy;
         T divV = exx + eyy;
         T etac = t.sEt[a];
-        if (mask & M_P) t.sP[a] = t.sP[a] - divV * etac * b.dtP;
-        if (mask & M_XX) t.sXX[a] = t.sXX[a] - (t.sXX[a] - T(2.0) * etac * (exx - third(divV))) * b.dxx;
-        if (mask & M_YY) t.sYY[a] = t.sYY[a] - (t.sYY[a] - T(2.0) * etac * (eyy - third(divV))) * b.dyy;
-    }
-    if ((mask & M_XY) && i >= 1 && i <= t.n0 + 1 && j >= 1 && j <= t.n1 + 1) {
-        T exy = T(0.5) * ((t.sVy[a] - t.sVy[a - 1]) * b.idx + (t.sVx[a] - t.sVx[a - BW]) * b.idy);
-        T e_xy = T(0.5) * (T(0.5) * (t.sEt[a - 1 - BW] + t.sEt[a - BW]) + T(0.5) * (t.sEt[a - 1] + t.sEt[a]));
-        t.sXY[a] = t.sXY[a] - (t.sXY[a] - T(2.0) * e_xy * exy) * b.dxy;
+        T nXY = T(0), oXY = T(0);
+        if (dxy) {
+            oXY = t.sXY[a];
+            T exy = T(0.5) * ((t.sVy[a] - t.sVy[a - 1]) * b.idx + (t.sVx[a] - t.sVx[a - BX]) * b.idy);
+            T e_xy = T(0.5) * (T(0.5) * (t.sEt[a - 1 - BX] + t.sEt[a - BX]) + T(0.5) * (t.sEt[a - 1] + t.sEt[a]));
+            nXY = oXY - (oXY - T(2.0) * e_xy * exy) * b.dxy;
+        }
+        if (mask & M_P) t.sP[a] = oP - divV * etac * b.dtP;
+        if (mask & M_XX) t.sXX[a] = oXX - (oXX - T(2.0) * etac * (exx - third(divV))) * b.dxx;
+        if (mask & M_YY) t.sYY[a] = oYY - (oYY - T(2.0) * etac * (eyy - third(divV))) * b.dyy;
+        if (dxy) t.sXY[a] = nXY;
+    } else if (dxy) {
+        const T oXY = t.sXY[a];
+        T exy = T(0.5) * ((t.sVy[a] - t.sVy[a - 1]) * b.idx + (t.sVx[a] - t.sVx[a - BX]) * b.idy);
+        T e_xy = T(0.5) * (T(0.5) * (t.sEt[a - 1 - BX] + t.sEt[a - BX]) + T(0.5) * (t.sEt[a - 1] + t.sEt[a]));
+        t.sXY[a] = oXY - (oXY - T(2.0) * e_xy * exy) * b.dxy;
     }
 }
 
@@ -123,66 +160,78 @@ __device__ __forceinline__ void center_ghosts(int q, int N, int kl, int kr, T cl
     if (q == N && kr == FI_BC_VELOCITY) { pos[1] = N + 1; val[1] = later_node ? v : T(2.0) * cr - v; ok[1] = true; }
 }
 
-// asynchronous global -> shared copy of one element (cp.async, sm_80+); valid == 0
-// zero-fills the destination without reading the source
-template <int S>
-__device__ __forceinline__ void cp_async_elem(void *dst, const void *src, bool valid) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
-                 "l"(src), "n"(S), "r"(valid ? S : 0)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
-
-// stage tile w's box of the seven inputs into staging buffer buf (asynchronous)
+// copies of tile d (member d.x, tile origin (d.y, d.z)) into one stage: the seven
+// input boxes (tensor maps of buffer src), the member's parameter block and the
+// descriptor itself (read by the other threads once the stage's barrier completes)
 template <typename T, int TY>
-__device__ __forceinline__ void stage_tile(const BInst<T> *__restrict__ insts, const int4 *__restrict__ tiles, int w,
-                                           int src, T *buf) {
+__device__ __forceinline__ void issue_tile(const BInst<T> *__restrict__ insts, const BMaps *__restrict__ maps, int4 d,
+                                           int src, unsigned char *stage, uint64_t *bar) {
     using TL = Tile<T, TY>;
-    const int4 d = tiles[w];
-    const BInst<T> &b = insts[d.x];
-    const long long sx = b.pitch;
-    const T *F[7] = {b.P[src], b.txx[src], b.tyy[src], b.txy[src], b.Vx[src], b.Vy[src], b.eta};
-    for (int r = threadIdx.x; r < TL::BOX; r += TL::NT) {
-        const int i = d.y - 1 + r % TL::BW, j = d.z - 1 + r / TL::BW;
-        const bool ok = i <= b.n0 + 2 && j <= b.n1 + 2;
-        const long long I = ok ? (long long)i + sx * (long long)j : 0;
+    *reinterpret_cast<int4 *>(stage + 7 * TL::SLOTB + TL::PARB) = d;
+    mbar_expect_tx(bar, TL::TX_BYTES);
+    const BMaps &mp = maps[d.x];
+    const int x = (int)kXOff + d.y - TL::XB, y = d.z - 1;
 #pragma unroll
-        for (int f = 0; f < 7; f++) cp_async_elem<(int)sizeof(T)>(buf + f * TL::BOX + r, F[f] + I, ok);
-    }
+    for (int f = 0; f < 7; f++) tma_load_2d(stage + f * TL::SLOTB, mp.m[src][f], x, y, bar);
+    bulk_load(stage + 7 * TL::SLOTB, insts + d.x, (uint32_t)sizeof(BInst<T>), bar);
 }
 
+// One PT iteration of every tile in the work list.  A persistent CTA strides over
+// the list with two stages: while tile w is computed, the copies of its next tile
+// (w + gridDim.x) land in the other stage; the descriptor of the tile after that is
+// fetched one step early, so the issuing thread never waits on it.
 template <typename T, int TY>
-__global__ void __launch_bounds__(BTX *TY) batch2d_sweep(const BInst<T> *__restrict__ insts, const int4 *__restrict__ tiles,
-                                                         const int *__restrict__ ntiles, int src) {
+__global__ void __launch_bounds__(BTX *TY) batch2d_sweep(const BInst<T> *__restrict__ insts,
+                                                         const BMaps *__restrict__ maps, const int4 *__restrict__ tiles,
+                                                         const int *__restrict__ ntiles, int src, int *err) {
     using TL = Tile<T, TY>;
-    // two staging buffers (dynamic shared memory, 2 x 7 boxes): the next tile of the
-    // work list is copied in while the current one is computed
-    extern __shared__ __align__(16) unsigned char batch_smem[];
-    T *const smem0 = reinterpret_cast<T *>(batch_smem);
+    extern __shared__ __align__(1024) unsigned char batch_smem[];
+    uint64_t *bars = reinterpret_cast<uint64_t *>(batch_smem + 2 * TL::STAGEB);
     TL t;
     const int tid = threadIdx.x, dst = src ^ 1;
-    const int nt = *ntiles;
+    const int nt = *ntiles, G = gridDim.x;
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    int4 dnext = make_int4(0, 1, 1, 0);
+    if (tid == 0) {
+        if ((int)blockIdx.x < nt) issue_tile<T, TY>(insts, maps, tiles[blockIdx.x], src, batch_smem, &bars[0]);
+        if ((int)blockIdx.x + G < nt) dnext = tiles[blockIdx.x + G];
+    }
+    uint32_t phase = 0;
     int cur = 0;
-    if ((int)blockIdx.x < nt) stage_tile<T, TY>(insts, tiles, blockIdx.x, src, smem0);
-    cp_async_commit();
-    for (int w = blockIdx.x; w < nt; w += gridDim.x) {
-        const int nx = w + gridDim.x;
-        if (nx < nt) stage_tile<T, TY>(insts, tiles, nx, src, smem0 + (cur ^ 1) * 7 * TL::BOX);
-        cp_async_commit();
-        cp_async_wait_prev();  // this tile's copies (all but the group just committed) are done
-        __syncthreads();
-        T *sm = smem0 + cur * 7 * TL::BOX;
+    for (int w = blockIdx.x; w < nt; w += G, cur ^= 1) {
+        if (tid == 0 && w + G < nt) {
+            fence_proxy_async();
+            issue_tile<T, TY>(insts, maps, dnext, src, batch_smem + (cur ^ 1) * TL::STAGEB, &bars[cur ^ 1]);
+            if (w + 2 * G < nt) dnext = tiles[w + 2 * G];
+        }
+        const bool ok = mbar_wait(&bars[cur], (phase >> cur) & 1u);
+        phase ^= 1u << cur;
+        if (__syncthreads_or(!ok)) {
+            // copies did not land within the bound: record it, drain this CTA's
+            // copies (bounded) and leave
+            if (tid == 0) {
+                atomicExch(err, (int)FI_ERR_TIMEOUT);
+                if (w + G < nt) mbar_wait(&bars[cur ^ 1], (phase >> (cur ^ 1)) & 1u);
+            }
+            return;
+        }
+        unsigned char *stage = batch_smem + cur * TL::STAGEB;
+        T *sm = reinterpret_cast<T *>(stage);
+        constexpr int SE = TL::SLOTB / (int)sizeof(T);
         t.sP = sm;
-        t.sXX = sm + TL::BOX;
-        t.sYY = sm + 2 * TL::BOX;
-        t.sXY = sm + 3 * TL::BOX;
-        t.sVx = sm + 4 * TL::BOX;
-        t.sVy = sm + 5 * TL::BOX;
-        t.sEt = sm + 6 * TL::BOX;
-        cur ^= 1;
-        const int4 d = tiles[w];
-        const BInst<T> &b = insts[d.x];
+        t.sXX = sm + SE;
+        t.sYY = sm + 2 * SE;
+        t.sXY = sm + 3 * SE;
+        t.sVx = sm + 4 * SE;
+        t.sVy = sm + 5 * SE;
+        t.sEt = sm + 6 * SE;
+        const BInst<T> &b = *reinterpret_cast<const BInst<T> *>(stage + 7 * TL::SLOTB);
+        const int4 d = *reinterpret_cast<const int4 *>(stage + 7 * TL::SLOTB + TL::PARB);
         t.i0 = d.y;
         t.j0 = d.z;
         t.n0 = b.n0;
@@ -192,15 +241,19 @@ __global__ void __launch_bounds__(BTX *TY) batch2d_sweep(const BInst<T> *__restr
         const bool bnd_y = t.j0 == 1 || t.j0 + TY >= t.n1 + 1;
         const bool late = bnd_x || bnd_y;
         const int ci = t.i0 + tid % BTX, cj = t.j0 + tid / BTX;
-        // pass 1: the tile, every component; pass 2: the ring components the V update reads
+        // pass 1: the tile, every component; pass 2: the ring components the V update
+        // reads, one ring side per warp on the last four warps (one branch path per warp)
         sigma2<T, TY>(t, b, ci, cj, M_ALL);
-        if (tid < 2 * TY + 2 * BTX) {
-            int i, j, mask;
-            if (tid < TY) { i = t.i0 - 1; j = t.j0 + tid; mask = M_P | M_XX; }
-            else if (tid < 2 * TY) { i = t.i0 + BTX; j = t.j0 + tid - TY; mask = M_XY; }
-            else if (tid < 2 * TY + BTX) { i = t.i0 + tid - 2 * TY; j = t.j0 - 1; mask = M_P | M_YY; }
-            else { i = t.i0 + tid - 2 * TY - BTX; j = t.j0 + TY; mask = M_XY; }
-            if (i <= t.n0 + 2 && j <= t.n1 + 2) sigma2<T, TY>(t, b, i, j, mask);
+        {
+            constexpr int NW = TL::NT / 32;
+            static_assert(NW >= 4 && TY <= 32, "one ring side per warp");
+            const int wp = tid / 32, lane = tid % 32;
+            int i = 0, j = 0, mask = 0;
+            if (wp == NW - 4) { i = t.i0 - 1; j = t.j0 + lane; mask = lane < TY ? (M_P | M_XX) : 0; }
+            else if (wp == NW - 3) { i = t.i0 + lane; j = t.j0 - 1; mask = M_P | M_YY; }
+            else if (wp == NW - 2) { i = t.i0 + lane; j = t.j0 + TY; mask = M_XY; }
+            else if (wp == NW - 1) { i = t.i0 + BTX; j = t.j0 + lane; mask = lane < TY ? M_XY : 0; }
+            if (mask && i <= t.n0 + 2 && j <= t.n1 + 2) sigma2<T, TY>(t, b, i, j, mask);
         }
         __syncthreads();
         const long long Ic = (long long)ci + sx * (long long)cj;
@@ -211,19 +264,21 @@ __global__ void __launch_bounds__(BTX *TY) batch2d_sweep(const BInst<T> *__restr
             b.tyy[dst][Ic] = t.sYY[a];
             b.txy[dst][Ic] = t.sXY[a];
         } else {
+            constexpr int REG = TL::RW * TL::RY;
             // stress boundary conditions on the staged region, x faces then y faces
             for (int side = 0; side < 2 && bnd_x; side++) {
                 const int kind = b.bc_kind[0][side];
                 if (kind != FI_BC_TRACTION && kind != FI_BC_SLIP) continue;
                 const int ghost = side == 0 ? 0 : t.n0 + 1, adj = side == 0 ? 1 : t.n0, node = side == 0 ? 1 : t.n0 + 1;
-                for (int r = tid; r < TL::BOX; r += TL::NT) {
-                    const int i = t.i0 - 1 + r % TL::BW, j = t.j0 - 1 + r / TL::BW;
+                for (int r = tid; r < REG; r += TL::NT) {
+                    const int i = t.i0 - 1 + r % TL::RW, j = t.j0 - 1 + r / TL::RW;
+                    const int a = t.at(i, j);
                     if (kind == FI_BC_TRACTION && i == ghost && j >= 1 && j <= t.n1 && adj >= t.i0 - 1 && adj <= t.i0 + BTX) {
                         const T tv = T(2.0) * b.bc_val[0][side][0];
-                        t.sP[r] = tv - t.sP[t.at(adj, j)];
-                        t.sXX[r] = tv - t.sXX[t.at(adj, j)];
+                        t.sP[a] = tv - t.sP[t.at(adj, j)];
+                        t.sXX[a] = tv - t.sXX[t.at(adj, j)];
                     }
-                    if (i == node && j >= 1 && j <= t.n1 + 1) t.sXY[r] = b.bc_val[0][side][1];
+                    if (i == node && j >= 1 && j <= t.n1 + 1) t.sXY[a] = b.bc_val[0][side][1];
                 }
                 __syncthreads();
             }
@@ -231,31 +286,33 @@ __global__ void __launch_bounds__(BTX *TY) batch2d_sweep(const BInst<T> *__restr
                 const int kind = b.bc_kind[1][side];
                 if (kind != FI_BC_TRACTION && kind != FI_BC_SLIP) continue;
                 const int ghost = side == 0 ? 0 : t.n1 + 1, adj = side == 0 ? 1 : t.n1, node = side == 0 ? 1 : t.n1 + 1;
-                for (int r = tid; r < TL::BOX; r += TL::NT) {
-                    const int i = t.i0 - 1 + r % TL::BW, j = t.j0 - 1 + r / TL::BW;
+                for (int r = tid; r < REG; r += TL::NT) {
+                    const int i = t.i0 - 1 + r % TL::RW, j = t.j0 - 1 + r / TL::RW;
+                    const int a = t.at(i, j);
                     if (kind == FI_BC_TRACTION && j == ghost && adj >= t.j0 - 1 && adj <= t.j0 + TY) {
                         const T tv = T(2.0) * b.bc_val[1][side][1];
-                        t.sP[r] = tv - t.sP[t.at(i, adj)];
-                        t.sYY[r] = tv - t.sYY[t.at(i, adj)];
+                        t.sP[a] = tv - t.sP[t.at(i, adj)];
+                        t.sYY[a] = tv - t.sYY[t.at(i, adj)];
                     }
-                    if (j == node) t.sXY[r] = b.bc_val[1][side][0];
+                    if (j == node) t.sXY[a] = b.bc_val[1][side][0];
                 }
                 __syncthreads();
             }
-            for (int r = tid; r < TL::BOX; r += TL::NT) {
-                const int i = t.i0 - 1 + r % TL::BW, j = t.j0 - 1 + r / TL::BW;
+            for (int r = tid; r < REG; r += TL::NT) {
+                const int i = t.i0 - 1 + r % TL::RW, j = t.j0 - 1 + r / TL::RW;
                 if (i > t.n0 + 2 || j > t.n1 + 2 || !t.own_x(i) || !t.own_y(j)) continue;
+                const int a = t.at(i, j);
                 const long long I = (long long)i + sx * (long long)j;
-                b.P[dst][I] = t.sP[r];
-                b.txx[dst][I] = t.sXX[r];
-                b.tyy[dst][I] = t.sYY[r];
-                b.txy[dst][I] = t.sXY[r];
+                b.P[dst][I] = t.sP[a];
+                b.txx[dst][I] = t.sXX[a];
+                b.tyy[dst][I] = t.sYY[a];
+                b.txy[dst][I] = t.sXY[a];
             }
             __syncthreads();
         }
         // velocity update of the tile (kernels_2d.jl:20-29) with boundary values and ghost images
         if (ci <= t.n0 + 1 && cj <= t.n1 + 1) {
-            constexpr int BW = TL::BW;
+            constexpr int BX = TL::BX;
             const int a = t.at(ci, cj);
             const int xl = b.bc_kind[0][0], xr = b.bc_kind[0][1], yl = b.bc_kind[1][0], yr = b.bc_kind[1][1];
             if (cj <= t.n1) {
@@ -266,17 +323,17 @@ __global__ void __launch_bounds__(BTX *TY) batch2d_sweep(const BInst<T> *__restr
                     const T gx = b.gkind[0] == FI_G_FIELD ? b.gx[Ic] : b.gval[0];
                     const T ex = T(0.5) * (t.sEt[a - 1] + t.sEt[a]);
                     v = t.sVx[a] + div_fast(-(t.sP[a] - t.sP[a - 1]) * b.idx + (t.sXX[a] - t.sXX[a - 1]) * b.idx +
-                                               (t.sXY[a + BW] - t.sXY[a]) * b.idy - gx,
+                                               (t.sXY[a + BX] - t.sXY[a]) * b.idy - gx,
                                            ex) *
                                        b.dVx;
                 }
                 b.Vx[dst][Ic] = v;
                 int pos[2];
                 T val[2];
-                bool ok[2];
-                center_ghosts<T>(cj, t.n1, yl, yr, b.bc_val[1][0][0], b.bc_val[1][1][0], pos, val, ok, v, false);
+                bool okg[2];
+                center_ghosts<T>(cj, t.n1, yl, yr, b.bc_val[1][0][0], b.bc_val[1][1][0], pos, val, okg, v, false);
                 for (int q = 0; q < 2; q++)
-                    if (ok[q]) b.Vx[dst][(long long)ci + sx * (long long)pos[q]] = val[q];
+                    if (okg[q]) b.Vx[dst][(long long)ci + sx * (long long)pos[q]] = val[q];
             }
             if (ci <= t.n0) {
                 T v;
@@ -285,8 +342,8 @@ __global__ void __launch_bounds__(BTX *TY) batch2d_sweep(const BInst<T> *__restr
                 else if (cj == t.n1 + 1 && node_fixed(yr)) v = b.bc_val[1][1][1];
                 else {
                     const T gy = b.gkind[1] == FI_G_FIELD ? b.gy[Ic] : b.gval[1];
-                    const T ey = T(0.5) * (t.sEt[a - BW] + t.sEt[a]);
-                    v = t.sVy[a] + div_fast(-(t.sP[a] - t.sP[a - BW]) * b.idy + (t.sYY[a] - t.sYY[a - BW]) * b.idy +
+                    const T ey = T(0.5) * (t.sEt[a - BX] + t.sEt[a]);
+                    v = t.sVy[a] + div_fast(-(t.sP[a] - t.sP[a - BX]) * b.idy + (t.sYY[a] - t.sYY[a - BX]) * b.idy +
                                                (t.sXY[a + 1] - t.sXY[a]) * b.idx - gy,
                                            ey) *
                                        b.dVy;
@@ -294,13 +351,13 @@ __global__ void __launch_bounds__(BTX *TY) batch2d_sweep(const BInst<T> *__restr
                 b.Vy[dst][Ic] = v;
                 int pos[2];
                 T val[2];
-                bool ok[2];
-                center_ghosts<T>(ci, t.n0, xl, xr, b.bc_val[0][0][1], b.bc_val[0][1][1], pos, val, ok, v, y_node);
+                bool okg[2];
+                center_ghosts<T>(ci, t.n0, xl, xr, b.bc_val[0][0][1], b.bc_val[0][1][1], pos, val, okg, v, y_node);
                 for (int q = 0; q < 2; q++)
-                    if (ok[q]) b.Vy[dst][(long long)pos[q] + sx * (long long)cj] = val[q];
+                    if (okg[q]) b.Vy[dst][(long long)pos[q] + sx * (long long)cj] = val[q];
             }
         }
-        __syncthreads();  // the next tile reuses the staging buffers
+        __syncthreads();  // the stage is refilled at the start of the step after next
     }
 }
 
@@ -454,7 +511,7 @@ __global__ void batch_fill(int total, const int4 *__restrict__ all, const int *_
 
 template <typename T, int TY>
 constexpr size_t sweep_smem() {
-    return 2 * 7 * (size_t)Tile<T, TY>::BOX * sizeof(T);
+    return 2 * (size_t)Tile<T, TY>::STAGEB + 2 * sizeof(uint64_t);
 }
 
 // resident sweep CTAs per SM (queried once per instantiation, outside any capture;
@@ -489,6 +546,10 @@ struct fi_batch {
     int capacity = 0;
     cudaStream_t stream = nullptr;
     void *d_inst = nullptr;               // BInst<T>[capacity]
+    BMaps *d_maps = nullptr;              // per-member tensor maps [capacity]
+    std::vector<BMaps> h_maps;
+    int maps_ty = -1;
+    int *d_err = nullptr;                 // device error word (bounded waits)
     std::vector<unsigned char> h_inst;    // host image of the table
     int4 *d_all = nullptr, *d_work = nullptr;
     int tile_capacity = 0;
@@ -607,6 +668,7 @@ fi_status ensure_capacity(fi_batch *b) {
     if (b->d_inst) cudaFree(b->d_inst);
     b->d_inst = nullptr;
     FB_CHECK(cudaMalloc(&b->d_inst, esz * cap), "batch table");
+    FB_CHECK(grow(&b->d_maps, cap), "batch tensor maps");
     FB_CHECK(grow(&b->d_first, cap), "batch arrays");
     FB_CHECK(grow(&b->d_count, cap), "batch arrays");
     FB_CHECK(grow(&b->d_offset, cap), "batch arrays");
@@ -638,6 +700,28 @@ fi_status upload_table(fi_batch *b) {
         }
     }
     if (n == 0) return FI_OK;
+    // tensor maps of every member's buffers, box = one tile of the current variant
+    const int ty = kBatchTY[b->variant];
+    const int bx = b->f64 ? BBox<double>::BX : BBox<float>::BX;
+    const int ez = b->f64 ? 8 : 4;
+    b->h_maps.resize(n);
+    const int F[6] = {FI_FIELD_P, FI_FIELD_TXX, FI_FIELD_TYY, FI_FIELD_TXY, FI_FIELD_VX, FI_FIELD_VY};
+    for (int q = 0; q < n; q++) {
+        const fi_model *m = b->models[q];
+        const unsigned long long dims[2] = {(unsigned long long)m->g.pitch, (unsigned long long)m->g.rows};
+        const unsigned long long strides[1] = {(unsigned long long)(m->g.pitch * ez)};
+        const unsigned box[2] = {(unsigned)bx, (unsigned)(ty + 2)};
+        for (int buf = 0; buf < 2; buf++) {
+            for (int f = 0; f < 7; f++) {
+                void *ptr = f < 6 ? (buf == 0 ? m->cur(F[f]) : m->nxt(F[f])) : m->cur(FI_FIELD_ETA);
+                void *raw = (char *)ptr - kXOff * ez;
+                if (!tma_encode(raw, 2, dims, strides, box, ez, b->h_maps[q].m[buf][f]))
+                    return set_error("tensor map encoding failed (batch member)"), FI_ERR_CUDA;
+            }
+        }
+    }
+    b->maps_ty = ty;
+    FB_CHECK(cudaMemcpy(b->d_maps, b->h_maps.data(), sizeof(BMaps) * n, cudaMemcpyHostToDevice), "batch tensor maps");
     FB_CHECK(cudaMemcpy(b->d_inst, b->h_inst.data(), esz * n, cudaMemcpyHostToDevice), "batch table");
     FB_CHECK(cudaMemcpy(b->d_h, hs.data(), sizeof(double) * n, cudaMemcpyHostToDevice), "batch spacings");
     return FI_OK;
@@ -684,7 +768,8 @@ fi_status build_tiles(fi_batch *b, int ty) {
 template <typename T, int TY>
 cudaError_t launch_sweep_t(fi_batch *b, const int4 *list, const int *nt, int src) {
     const int grid = b->sms * sweep_blocks_per_sm<T, TY>();
-    batch2d_sweep<T, TY><<<grid, BTX * TY, sweep_smem<T, TY>(), b->stream>>>((const BInst<T> *)b->d_inst, list, nt, src);
+    batch2d_sweep<T, TY><<<grid, BTX * TY, sweep_smem<T, TY>(), b->stream>>>((const BInst<T> *)b->d_inst, b->d_maps,
+                                                                               list, nt, src, b->d_err);
     return cudaGetLastError();
 }
 template <typename T>
@@ -763,7 +848,7 @@ void free_batch(fi_batch *b) {
     if (!b) return;
     if (b->graph) cudaGraphExecDestroy(b->graph);
     void *ptrs[] = {b->d_inst, b->d_all, b->d_work, b->d_first, b->d_count, b->d_offset, b->d_ntiles,
-                    b->d_nactive, b->d_full_ntiles, b->d_h, b->d_slots, b->d_state};
+                    b->d_nactive, b->d_full_ntiles, b->d_h, b->d_slots, b->d_state, b->d_maps, b->d_err};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (b->h_nactive) cudaFreeHost(b->h_nactive);
@@ -776,6 +861,16 @@ void finish_sweeps(fi_batch *b, const std::vector<int> &sweeps) {
         if (sweeps[q] & 1) b->models[q]->parity ^= 1;
         b->models[q]->iterations += sweeps[q];
     }
+}
+
+// the sweep's error word (a bounded wait that expired), cleared after reading
+fi_status check_batch_err(fi_batch *b) {
+    int e = 0;
+    FB_CHECK(cudaMemcpy(&e, b->d_err, sizeof(int), cudaMemcpyDeviceToHost), "batch error word");
+    if (e == 0) return FI_OK;
+    cudaMemset(b->d_err, 0, sizeof(int));
+    set_error("batched sweep: a tile's copies did not arrive within the wait bound");
+    return (fi_status)e;
 }
 
 // check rounds until no member is active or max_rounds; items/nactive may be NULL
@@ -817,6 +912,7 @@ fi_status run_rounds(fi_batch *b, const fi_batch_opts *o, int max_rounds, fi_bat
     }
     std::vector<BState> fin(n);
     if (n > 0) FB_CHECK(cudaMemcpy(fin.data(), b->d_state, sizeof(BState) * n, cudaMemcpyDeviceToHost), "batch state");
+    const fi_status es = check_batch_err(b);
     std::vector<int> sw(n);
     for (int q = 0; q < n; q++) {
         if (items) {
@@ -828,7 +924,7 @@ fi_status run_rounds(fi_batch *b, const fi_batch_opts *o, int max_rounds, fi_bat
     }
     finish_sweeps(b, sw);
     if (nactive) *nactive = *b->h_nactive;
-    return FI_OK;
+    return es;
 }
 
 fi_status check_opts(const fi_batch_opts *o) {
@@ -873,6 +969,8 @@ fi_status fi_batch_create(fi_model *const *models, int32_t count, fi_batch **out
     if (e == cudaSuccess) e = cudaMalloc(&b->d_full_ntiles, sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_nactive, sizeof(int));
     if (e == cudaSuccess) e = cudaMallocHost(&b->h_nactive, sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(b->d_err, 0, sizeof(int));
     if (e != cudaSuccess) {
         fi_status st = cuda_fail(e, "batch allocation");
         free_batch(b);
@@ -931,7 +1029,7 @@ fi_status fi_batch_advance(fi_batch *b, int32_t niter) {
     for (int s = 0; s < niter; s++) FB_CHECK(launch_sweep(b, b->d_all, b->d_full_ntiles, s & 1), "batch sweep");
     FB_CHECK(cudaStreamSynchronize(b->stream), "batch sync");
     finish_sweeps(b, std::vector<int>(b->count(), niter));
-    return FI_OK;
+    return check_batch_err(b);
 }
 
 fi_status fi_batch_set_variant(fi_batch *b, int32_t v) {
@@ -973,6 +1071,7 @@ fi_status fi_batch_autotune(fi_batch *b, int32_t iters, int32_t *best, double *m
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (st != FI_OK) return st;
+    if ((st = check_batch_err(b)) != FI_OK) return st;
     b->variant = best_v;
     *best = best_v;
     return FI_OK;

@@ -42,13 +42,13 @@
 #include <cstdlib>
 
 #include "fi_device.cuh"
+#include "fi_tma.cuh"
 
 namespace fi {
 
 namespace {
 
 constexpr int TX = 32;
-constexpr long long kWaitCycles = 1ll << 31;
 
 // Launch shapes: tile height and z-block depth.  (Issuing the copies of plane s+1
 // after the stress barrier of step s instead, which saves the barrier closing each
@@ -102,45 +102,6 @@ struct Layout {
     static constexpr int NT = TX * TY;
     static constexpr size_t SMEM = (size_t)S_COUNT * SLOT * sizeof(T) + 128;
 };
-
-// ---- PTX helpers (sm_90+ mbarrier / bulk tensor copy; no multicast) -------------
-__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-// bounded wait; false on expiry
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
-    if (mbar_try_wait(bar, parity)) return true;
-    const long long t0 = clock64();
-    while (!mbar_try_wait(bar, parity)) {
-        if (clock64() - t0 > kWaitCycles) return false;
-    }
-    return true;
-}
-__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z, uint64_t *bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
-            smem_u32(dst)),
-        "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
-        : "memory");
-}
 
 // the eleven input maps of one sweep, in field order P, txx, tyy, tzz, txy, txz, tyz, Vx, Vy, Vz, eta
 struct InMaps {
@@ -759,6 +720,25 @@ bool fused3d_supported(const Geom &g, const KParams &p, bool ib) {
     if (g.nd != 3 || ib) return false;
     if (p.bc_kind[2][0] == FI_BC_PERIODIC) return false;
     return g.pitch >= kXOff + g.n[0] + 3;
+}
+
+// a 2D or 3D tiled tensor map (no interleave, no swizzle, zero fill out of range)
+// over `nd` dims of a field allocation; strides in bytes (dims 1..nd-1)
+bool tma_encode(void *raw_base, int nd, const unsigned long long *dims, const unsigned long long *strides,
+                const unsigned *box, int esz, void *map_out) {
+    PFN_cuTensorMapEncodeTiled_v12000 enc = get_encoder();
+    if (!enc || nd < 1 || nd > 3) return false;
+    cuuint64_t d[3], st[2];
+    cuuint32_t bx[3], estr[3] = {1, 1, 1};
+    for (int k = 0; k < nd; k++) {
+        d[k] = dims[k];
+        bx[k] = box[k];
+        if (k > 0) st[k - 1] = strides[k - 1];
+    }
+    CUresult r = enc((CUtensorMap *)map_out, esz == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                     nd, raw_base, d, st, bx, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
 }
 
 // one 3D tensor map over a field allocation (raw base, aligned), box = one plane of

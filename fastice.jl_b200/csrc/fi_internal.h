@@ -140,6 +140,9 @@ template <typename T>
 cudaError_t launch_fused3d(const Geom &g, const KParams &p, const Ptrs<T> &in, const Ptrs<T> &out, const void *maps11,
                            int variant, int *err, cudaStream_t s);
 bool fused3d_encode_map(void *raw_base, const Geom &g, int esz, int ty, void *map_out);
+// generic tiled tensor map (fi_fused3d.cu): nd dims, strides of dims 1..nd-1 in bytes
+bool tma_encode(void *raw_base, int nd, const unsigned long long *dims, const unsigned long long *strides,
+                const unsigned *box, int esz, void *map_out);
 int fused3d_num_variants();
 int fused3d_variant_ty(int v);
 const char *fused3d_variant_name(int v);
