@@ -177,48 +177,49 @@ __device__ __forceinline__ void issue_tile(const BInst<T> *__restrict__ insts, c
 }
 
 // One PT iteration of every tile in the work list.  A persistent CTA strides over
-// the list with two stages: while tile w is computed, the copies of its next tile
-// (w + gridDim.x) land in the other stage; the descriptor of the tile after that is
-// fetched one step early, so the issuing thread never waits on it.
+// the list through three stages: while tile k is computed, the copies of tiles
+// k+1 and k+2 of its stride are in flight, and the descriptor of tile k+3 is
+// fetched one step early, so the issuing thread never waits on it.  Tile k+2 is
+// issued into the stage tile k-1 used, right after the block barrier that follows
+// tile k's stress update: every thread passes that barrier only after finishing
+// tile k-1 (its velocity update included), so one barrier per interior tile
+// suffices.
+constexpr int kStages = 3;
+// 48 resident warps per SM in FP32 (at most 42 registers a thread), 32 in FP64
 template <typename T, int TY>
-__global__ void __launch_bounds__(BTX *TY) batch2d_sweep(const BInst<T> *__restrict__ insts,
+__global__ void __launch_bounds__(BTX *TY, (sizeof(T) == 8 ? 1024 : 1536) / (BTX * TY)) batch2d_sweep(const BInst<T> *__restrict__ insts,
                                                          const BMaps *__restrict__ maps, const int4 *__restrict__ tiles,
                                                          const int *__restrict__ ntiles, int src, int *err) {
     using TL = Tile<T, TY>;
     extern __shared__ __align__(1024) unsigned char batch_smem[];
-    uint64_t *bars = reinterpret_cast<uint64_t *>(batch_smem + 2 * TL::STAGEB);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(batch_smem + kStages * TL::STAGEB);
     TL t;
     const int tid = threadIdx.x, dst = src ^ 1;
     const int nt = *ntiles, G = gridDim.x;
     if (tid == 0) {
-        mbar_init(&bars[0], 1);
-        mbar_init(&bars[1], 1);
+        for (int q = 0; q < kStages; q++) mbar_init(&bars[q], 1);
         mbar_fence_init();
     }
     __syncthreads();
     int4 dnext = make_int4(0, 1, 1, 0);
     if (tid == 0) {
-        if ((int)blockIdx.x < nt) issue_tile<T, TY>(insts, maps, tiles[blockIdx.x], src, batch_smem, &bars[0]);
-        if ((int)blockIdx.x + G < nt) dnext = tiles[blockIdx.x + G];
+        for (int q = 0; q < kStages - 1; q++)
+            if ((int)blockIdx.x + q * G < nt)
+                issue_tile<T, TY>(insts, maps, tiles[blockIdx.x + q * G], src, batch_smem + q * TL::STAGEB, &bars[q]);
+        if ((int)blockIdx.x + (kStages - 1) * G < nt) dnext = tiles[blockIdx.x + (kStages - 1) * G];
     }
     uint32_t phase = 0;
+    bool failed = false;
     int cur = 0;
-    for (int w = blockIdx.x; w < nt; w += G, cur ^= 1) {
-        if (tid == 0 && w + G < nt) {
-            fence_proxy_async();
-            issue_tile<T, TY>(insts, maps, dnext, src, batch_smem + (cur ^ 1) * TL::STAGEB, &bars[cur ^ 1]);
-            if (w + 2 * G < nt) dnext = tiles[w + 2 * G];
-        }
-        const bool ok = mbar_wait(&bars[cur], (phase >> cur) & 1u);
+    for (int w = blockIdx.x; w < nt; w += G, cur = cur == kStages - 1 ? 0 : cur + 1) {
+        // a wait that expires is recorded and the remaining tiles are computed from
+        // whatever the stage holds (the solve reports FI_ERR_TIMEOUT); later waits
+        // of this thread are single polls, so the launch ends in bounded time
+        const bool ok = failed ? mbar_try_wait(&bars[cur], (phase >> cur) & 1u) : mbar_wait(&bars[cur], (phase >> cur) & 1u);
         phase ^= 1u << cur;
-        if (__syncthreads_or(!ok)) {
-            // copies did not land within the bound: record it, drain this CTA's
-            // copies (bounded) and leave
-            if (tid == 0) {
-                atomicExch(err, (int)FI_ERR_TIMEOUT);
-                if (w + G < nt) mbar_wait(&bars[cur ^ 1], (phase >> (cur ^ 1)) & 1u);
-            }
-            return;
+        if (!ok && !failed) {
+            failed = true;
+            atomicExch(err, (int)FI_ERR_TIMEOUT);
         }
         unsigned char *stage = batch_smem + cur * TL::STAGEB;
         T *sm = reinterpret_cast<T *>(stage);
@@ -256,6 +257,12 @@ __global__ void __launch_bounds__(BTX *TY) batch2d_sweep(const BInst<T> *__restr
             if (mask && i <= t.n0 + 2 && j <= t.n1 + 2) sigma2<T, TY>(t, b, i, j, mask);
         }
         __syncthreads();
+        if (tid == 0 && !failed && w + (kStages - 1) * G < nt) {
+            const int nx = cur == 0 ? kStages - 1 : cur - 1;  // the stage of tile k-1
+            fence_proxy_async();
+            issue_tile<T, TY>(insts, maps, dnext, src, batch_smem + nx * TL::STAGEB, &bars[nx]);
+            if (w + kStages * G < nt) dnext = tiles[w + kStages * G];
+        }
         const long long Ic = (long long)ci + sx * (long long)cj;
         if (!late) {
             const int a = t.at(ci, cj);
@@ -265,39 +272,57 @@ __global__ void __launch_bounds__(BTX *TY) batch2d_sweep(const BInst<T> *__restr
             b.txy[dst][Ic] = t.sXY[a];
         } else {
             constexpr int REG = TL::RW * TL::RY;
-            // stress boundary conditions on the staged region, x faces then y faces
-            for (int side = 0; side < 2 && bnd_x; side++) {
-                const int kind = b.bc_kind[0][side];
-                if (kind != FI_BC_TRACTION && kind != FI_BC_SLIP) continue;
-                const int ghost = side == 0 ? 0 : t.n0 + 1, adj = side == 0 ? 1 : t.n0, node = side == 0 ? 1 : t.n0 + 1;
+            // stress boundary conditions on the staged region: the x faces the tile
+            // touches (both sides in one pass: their writes and reads are disjoint),
+            // then the y faces
+            const bool fx[2] = {t.i0 == 1, t.i0 + BTX >= t.n0 + 1}, fy[2] = {t.j0 == 1, t.j0 + TY >= t.n1 + 1};
+            bool any_x = false, any_y = false;
+            for (int side = 0; side < 2; side++) {
+                const int kx = b.bc_kind[0][side], ky = b.bc_kind[1][side];
+                any_x |= fx[side] && (kx == FI_BC_TRACTION || kx == FI_BC_SLIP);
+                any_y |= fy[side] && (ky == FI_BC_TRACTION || ky == FI_BC_SLIP);
+            }
+            if (any_x) {
                 for (int r = tid; r < REG; r += TL::NT) {
                     const int i = t.i0 - 1 + r % TL::RW, j = t.j0 - 1 + r / TL::RW;
                     const int a = t.at(i, j);
-                    if (kind == FI_BC_TRACTION && i == ghost && j >= 1 && j <= t.n1 && adj >= t.i0 - 1 && adj <= t.i0 + BTX) {
-                        const T tv = T(2.0) * b.bc_val[0][side][0];
-                        t.sP[a] = tv - t.sP[t.at(adj, j)];
-                        t.sXX[a] = tv - t.sXX[t.at(adj, j)];
+                    for (int side = 0; side < 2; side++) {
+                        const int kind = b.bc_kind[0][side];
+                        if (!fx[side] || (kind != FI_BC_TRACTION && kind != FI_BC_SLIP)) continue;
+                        const int ghost = side == 0 ? 0 : t.n0 + 1, adj = side == 0 ? 1 : t.n0,
+                                  node = side == 0 ? 1 : t.n0 + 1;
+                        if (kind == FI_BC_TRACTION && i == ghost && j >= 1 && j <= t.n1 && adj >= t.i0 - 1 &&
+                            adj <= t.i0 + BTX) {
+                            const T tv = T(2.0) * b.bc_val[0][side][0];
+                            t.sP[a] = tv - t.sP[t.at(adj, j)];
+                            t.sXX[a] = tv - t.sXX[t.at(adj, j)];
+                        }
+                        if (i == node && j >= 1 && j <= t.n1 + 1) t.sXY[a] = b.bc_val[0][side][1];
                     }
-                    if (i == node && j >= 1 && j <= t.n1 + 1) t.sXY[a] = b.bc_val[0][side][1];
                 }
                 __syncthreads();
             }
-            for (int side = 0; side < 2 && bnd_y; side++) {
-                const int kind = b.bc_kind[1][side];
-                if (kind != FI_BC_TRACTION && kind != FI_BC_SLIP) continue;
-                const int ghost = side == 0 ? 0 : t.n1 + 1, adj = side == 0 ? 1 : t.n1, node = side == 0 ? 1 : t.n1 + 1;
+            if (any_y) {
                 for (int r = tid; r < REG; r += TL::NT) {
                     const int i = t.i0 - 1 + r % TL::RW, j = t.j0 - 1 + r / TL::RW;
                     const int a = t.at(i, j);
-                    if (kind == FI_BC_TRACTION && j == ghost && adj >= t.j0 - 1 && adj <= t.j0 + TY) {
-                        const T tv = T(2.0) * b.bc_val[1][side][1];
-                        t.sP[a] = tv - t.sP[t.at(i, adj)];
-                        t.sYY[a] = tv - t.sYY[t.at(i, adj)];
+                    for (int side = 0; side < 2; side++) {
+                        const int kind = b.bc_kind[1][side];
+                        if (!fy[side] || (kind != FI_BC_TRACTION && kind != FI_BC_SLIP)) continue;
+                        const int ghost = side == 0 ? 0 : t.n1 + 1, adj = side == 0 ? 1 : t.n1,
+                                  node = side == 0 ? 1 : t.n1 + 1;
+                        if (kind == FI_BC_TRACTION && j == ghost && adj >= t.j0 - 1 && adj <= t.j0 + TY) {
+                            const T tv = T(2.0) * b.bc_val[1][side][1];
+                            t.sP[a] = tv - t.sP[t.at(i, adj)];
+                            t.sYY[a] = tv - t.sYY[t.at(i, adj)];
+                        }
+                        if (j == node) t.sXY[a] = b.bc_val[1][side][0];
                     }
-                    if (j == node) t.sXY[a] = b.bc_val[1][side][0];
                 }
                 __syncthreads();
             }
+            // write-back of the owned region (reads only: the velocity update below
+            // reads the same final values, so no barrier in between)
             for (int r = tid; r < REG; r += TL::NT) {
                 const int i = t.i0 - 1 + r % TL::RW, j = t.j0 - 1 + r / TL::RW;
                 if (i > t.n0 + 2 || j > t.n1 + 2 || !t.own_x(i) || !t.own_y(j)) continue;
@@ -308,7 +333,6 @@ __global__ void __launch_bounds__(BTX *TY) batch2d_sweep(const BInst<T> *__restr
                 b.tyy[dst][I] = t.sYY[a];
                 b.txy[dst][I] = t.sXY[a];
             }
-            __syncthreads();
         }
         // velocity update of the tile (kernels_2d.jl:20-29) with boundary values and ghost images
         if (ci <= t.n0 + 1 && cj <= t.n1 + 1) {
@@ -357,7 +381,13 @@ __global__ void __launch_bounds__(BTX *TY) batch2d_sweep(const BInst<T> *__restr
                     if (okg[q]) b.Vy[dst][(long long)pos[q] + sx * (long long)cj] = val[q];
             }
         }
-        __syncthreads();  // the stage is refilled at the start of the step after next
+        // no closing barrier: the stage of this tile is refilled only after every
+        // thread has passed the stress barrier of the next tile
+    }
+    if (tid == 0 && failed) {
+        // drain (bounded) the copies whose wait expired before the stages are
+        // released: the last phase waited on per stage (an unused stage passes at once)
+        for (int q = 0; q < kStages; q++) mbar_wait(&bars[q], ((phase >> q) & 1u) ^ 1u);
     }
 }
 
@@ -511,7 +541,7 @@ __global__ void batch_fill(int total, const int4 *__restrict__ all, const int *_
 
 template <typename T, int TY>
 constexpr size_t sweep_smem() {
-    return 2 * (size_t)Tile<T, TY>::STAGEB + 2 * sizeof(uint64_t);
+    return kStages * (size_t)Tile<T, TY>::STAGEB + kStages * sizeof(uint64_t);
 }
 
 // resident sweep CTAs per SM (queried once per instantiation, outside any capture;

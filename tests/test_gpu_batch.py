@@ -79,6 +79,33 @@ def test_batch_members_bitwise_vs_oracle(dtype, variant):
     assert not bad, bad
 
 
+@pytest.mark.parametrize("dtype", ["f32", "f64"])
+@pytest.mark.parametrize("variant", [0, 1, 2])
+def test_batch_with_several_tiles_per_cta_matches_members_alone(dtype, variant):
+    # 12 members of 255^2 cells: about three and a half tiles per resident CTA, so
+    # every stage of the sweep's pipeline is reused within a launch; each member
+    # must equal its twin advanced alone on the reference-shaped path (no-FMA
+    # builds of both are bit-exact against the oracle)
+    fi, O = load_fastice(), load_oracle()
+    n = (255, 255)
+    members = [_pair(fi, O, n, CASES[k % len(CASES)][1], dtype, "strict", 100 + k)[0] for k in range(12)]
+    twins = [_pair(fi, O, n, CASES[k % len(CASES)][1], dtype, "strict", 100 + k)[0] for k in range(12)]
+    batch = fi.BatchedStokes2D(members)
+    batch.set_variant(variant)
+    batch.advance(6)
+    batch.close()
+    bad = []
+    for k, (m, t) in enumerate(zip(members, twins)):
+        t.advance(6)
+        for name in STATE:
+            a, b = m.get_field(name), t.get_field(name)
+            if not np.array_equal(_bits(a), _bits(b)):
+                bad.append((k, name, int(np.sum(a != b))))
+    for m in members + twins:
+        m.close()
+    assert not bad, bad
+
+
 def _inclusions(fi, seeds, n_range=(40, 96), library="fast", dtype="f32", max_contrast=100.0):
     # moderate contrasts keep the reference PT scheme's iteration counts small here
     from fastice_b200 import scenarios
