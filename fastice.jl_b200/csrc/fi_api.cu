@@ -827,14 +827,31 @@ static fi_status solve_mixed(fi_model *m, const fi_solve_opts *o, fi_solve_repor
     FI_CHECK_CUDA(cudaStreamSynchronize(s->stream), "mixed sync");
 
     // ---- phase B: FP64 defect correction with FP32 correction sweeps
+    //
+    // For a fixed viscosity one PT iteration is an affine map x -> M x + c, so PT
+    // continued on a correction y from an anchor a follows y -> M y + (M a + c - a).
+    // Its pressure and velocity parts are forced by r_P(a) and r_V(a); its stress
+    // part carries no forcing once the anchor's stresses are replaced by the
+    // viscous law of its velocities (the projection) and the correction's stresses
+    // start from the difference the projection removed (the constitutive defect
+    // d = τ_a - 2η dev ε̇(V_a), taken in FP64, then rounded).  The FP32 sweeps on y
+    // then continue the FP64 iteration instead of restarting it from rest.
     int outer = 0, outer_stale = 0;
     double best_outer = 1e300;
+    const int tau_f[6] = {FI_FIELD_TXX, FI_FIELD_TYY, FI_FIELD_TZZ, FI_FIELD_TXY, FI_FIELD_TXZ, FI_FIELD_TYZ};
+    if ((st = model_ensure_second_state(m)) != FI_OK) return st;
     while (true) {
-        // viscosity from the current stresses (Picard step), then τ = 2η dev(ε̇(V)), BCs
+        // viscosity from the current stresses (Picard step), then τ = 2η dev(ε̇(V)), BCs;
+        // the stresses before the projection are kept in the second state buffer
         Ptrs<double> f = m->ptrs<double>();
         FI_CHECK_CUDA(launch_eta_from_tau<double>(m->g, m->kp, f, m->stream), "eta refresh");
         m->eta_swapped = !m->eta_swapped;
         if ((st = run_eta_batch<double>(m, FI_FIELD_ETA)) != FI_OK) return st;
+        for (int q = 0; q < 6; q++)
+            if (field_used(m, tau_f[q]))
+                FI_CHECK_CUDA(cudaMemcpyAsync(field_raw(m->nxt(tau_f[q]), m->esz), field_raw(m->cur(tau_f[q]), m->esz),
+                                              (m->elems + 64) * m->esz, cudaMemcpyDeviceToDevice, m->stream),
+                              "stress copy");
         FI_CHECK_CUDA(launch_compute_tau<double>(m->g, m->kp, m->ptrs<double>(), m->stream), "projection");
         if ((st = run_batch<double>(m, stress_batch)) != FI_OK) return st;
         // FP64 residual fields and norms
@@ -873,6 +890,13 @@ static fi_status solve_mixed(fi_model *m, const fi_solve_opts *o, fi_solve_repor
                 FI_CHECK_CUDA(cudaMemsetAsync(field_raw(s->alt[fl], s->esz), 0, (s->elems + 64) * s->esz, m->stream),
                               "zero");
         }
+        // the correction's stresses start from the constitutive defect
+        for (int q = 0; q < 6; q++)
+            if (field_used(m, tau_f[q])) {
+                cudaError_t e = launch_diff<double, float>((const double *)m->nxt(tau_f[q]), (const double *)m->cur(tau_f[q]),
+                                                           (float *)s->cur(tau_f[q]), n, m->stream);
+                if (e != cudaSuccess) return cuda_fail(e, "constitutive defect");
+            }
         FI_CHECK_CUDA(cudaStreamSynchronize(m->stream), "mixed sync");
         s->kp = kc;
         // target: inner_reduction of r0, but no further than a third of the tolerance

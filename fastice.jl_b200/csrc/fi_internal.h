@@ -152,6 +152,8 @@ template <typename S, typename D>
 cudaError_t launch_convert(const S *src, D *dst, long long n, double scale, cudaStream_t s);
 template <typename D, typename S>
 cudaError_t launch_accumulate(D *x, const S *d, long long n, cudaStream_t s);
+template <typename S, typename D>
+cudaError_t launch_diff(const S *a, const S *b, D *out, long long n, cudaStream_t s);
 template <typename T>
 cudaError_t launch_eta_from_tau(const Geom &g, const KParams &p, const Ptrs<T> &f, cudaStream_t s);
 // max |value| over up to 8 FP32 arrays of n elements each, as float bits in *out_bits

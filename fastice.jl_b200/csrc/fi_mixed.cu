@@ -24,6 +24,13 @@ __global__ void accumulate_kernel(D *__restrict__ x, const S *__restrict__ d, lo
         x[t] += D(d[t]);
 }
 
+// out = (D)(a - b), the difference taken in the source precision
+template <typename S, typename D>
+__global__ void diff_kernel(const S *__restrict__ a, const S *__restrict__ b, D *__restrict__ out, long long n) {
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+        out[t] = D(a[t] - b[t]);
+}
+
 template <typename T>
 __device__ __forceinline__ T h(T x) { return T(0.5) * x; }
 
@@ -86,6 +93,13 @@ cudaError_t launch_accumulate(D *x, const S *d, long long n, cudaStream_t s) {
     accumulate_kernel<D, S><<<grid_1d(n), 256, 0, s>>>(x, d, n);
     return cudaGetLastError();
 }
+
+template <typename S, typename D>
+cudaError_t launch_diff(const S *a, const S *b, D *out, long long n, cudaStream_t s) {
+    diff_kernel<S, D><<<grid_1d(n), 256, 0, s>>>(a, b, out, n);
+    return cudaGetLastError();
+}
+template cudaError_t launch_diff<double, float>(const double *, const double *, float *, long long, cudaStream_t);
 
 template <typename T>
 cudaError_t launch_eta_from_tau(const Geom &g, const KParams &p, const Ptrs<T> &f, cudaStream_t s) {
