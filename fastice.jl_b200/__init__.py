@@ -13,6 +13,7 @@ from .models import (Arch, BatchedStokes2D, FieldRef, IsothermalFullStokesModel,
 from .physics import (ArrayField, BoundaryCondition, ConstantField, FunctionField, LinearViscousRheology, OneField,
                       PBC, Periodic, PowerLawRheology, Relaxation, SBC, Slip, TBC, Traction, VBC, ValueField, Velocity,
                       ViscoplasticRegularisation, ZeroField, glen_regularised)
+from . import scenarios  # noqa: E402  (seeded problem set-ups over the names above)
 
 __all__ = [
     "FastIceError", "BatchedStokes2D", "Center", "Vertex", "UniformGrid", "flip", "compute_levelset_from_dem", "omega_from_psi", "Arch",
@@ -20,7 +21,7 @@ __all__ = [
     "compute_residuals", "interior", "pt_params", "set_", "ArrayField", "BoundaryCondition", "ConstantField",
     "FunctionField", "LinearViscousRheology", "OneField", "PBC", "Periodic", "PowerLawRheology", "Relaxation", "SBC",
     "Slip", "TBC", "Traction", "VBC", "ValueField", "Velocity", "ViscoplasticRegularisation", "ZeroField",
-    "glen_regularised", "load_library",
+    "glen_regularised", "load_library", "scenarios",
 ]
 
 

@@ -597,8 +597,8 @@ fi_status fi_model_compute_tau(fi_model *m) {
     if (!m) return set_error("null model"), FI_ERR_ARG;
     if (m->ib) return set_error("compute_tau of the immersed-boundary model is broken in the reference"), FI_ERR_UNSUPPORTED;
     FI_CHECK_CUDA(cudaSetDevice(m->d.device), "cudaSetDevice");
-    cudaError_t e = m->is_f64() ? launch_compute_tau<double>(m->g, m->kp, m->ptrs<double>(), m->stream)
-                                : launch_compute_tau<float>(m->g, m->kp, m->ptrs<float>(), m->stream);
+    cudaError_t e = m->is_f64() ? launch_compute_tau<double>(m->g, m->kp, m->ptrs<double>(), false, m->stream)
+                                : launch_compute_tau<float>(m->g, m->kp, m->ptrs<float>(), false, m->stream);
     if (e != cudaSuccess) return cuda_fail(e, "compute_tau");
     return FI_OK;
 }
@@ -680,6 +680,7 @@ static fi_status make_shadow(fi_model *m) {
                 return cuda_fail(e, "shadow inputs");
             }
         }
+
     if (s->path == FI_PATH_FUSED && fused3d_num_variants() > 4) {
         s->fused_variant = 4;  // 32x16 tiles: the FP32 shape the autotuner prefers on the slab
         fi_status es = encode_maps(s);
@@ -693,6 +694,7 @@ static fi_status make_shadow(fi_model *m) {
         return cuda_fail(cudaGetLastError(), "shadow sync");
     }
     m->shadow = s;
+    m->shadow_kp = s->kp;
     return FI_OK;
 }
 
@@ -732,11 +734,17 @@ static fi_status fp32_floors(fi_model *s, const double *nn, double *fl_P, double
 
 static fi_status solve_mixed(fi_model *m, const fi_solve_opts *o, fi_solve_report *rep) {
     if (!m->is_f64()) return set_error("the mixed-precision solve refines an FP64 model"), FI_ERR_ARG;
-    if (m->ib) return set_error("the mixed-precision solve does not cover the immersed-boundary model"), FI_ERR_UNSUPPORTED;
     FI_CHECK_CUDA(cudaSetDevice(m->d.device), "cudaSetDevice");
     fi_status st = make_shadow(m);
     if (st != FI_OK) return st;
     fi_model *s = m->shadow;
+    // volume fractions (refreshed every solve: the caller may have recomputed them);
+    // the shadow sees the FP64 model's empty, valid and null-space points
+    for (int f = FI_FIELD_NA_CCC; f < FI_FIELD_NA_CCC + 16 && m->ib; f++)
+        if (field_used(m, f))
+            FI_CHECK_CUDA(launch_mask_to_f32((const double *)m->base[f], (float *)s->base[f], (long long)m->elems,
+                                             (float)s->kp.small, m->stream),
+                          "shadow volume fractions");
     const long long n = (long long)m->elems;
     const int nd = m->d.grid.nd;
     const double inner_red = o->inner_reduction > 0 ? o->inner_reduction : 1e-3;
@@ -745,7 +753,7 @@ static fi_status solve_mixed(fi_model *m, const fi_solve_opts *o, fi_solve_repor
     int window = 0;
     for (int c = 0; c < nd; c++) window = std::max(window, 2 * (m->d.grid.n[c] + 1));
     window = std::max(window, 2 * o->ncheck);
-    const KParams kbase = s->kp;
+    const KParams kbase = m->shadow_kp;  // not s->kp: a previous solve leaves its last stage's parameters there
     KParams ka = kbase;  // phase A: the full problem in FP32
     for (int c = 0; c < 3; c++) {
         ka.g_kind[c] = m->kp.g_kind[c];
@@ -841,21 +849,13 @@ static fi_status solve_mixed(fi_model *m, const fi_solve_opts *o, fi_solve_repor
     const int tau_f[6] = {FI_FIELD_TXX, FI_FIELD_TYY, FI_FIELD_TZZ, FI_FIELD_TXY, FI_FIELD_TXZ, FI_FIELD_TYZ};
     if ((st = model_ensure_second_state(m)) != FI_OK) return st;
     while (true) {
-        // viscosity from the current stresses (Picard step), then τ = 2η dev(ε̇(V)), BCs;
-        // the stresses before the projection are kept in the second state buffer
+        // viscosity from the current stresses (Picard step)
         Ptrs<double> f = m->ptrs<double>();
         FI_CHECK_CUDA(launch_eta_from_tau<double>(m->g, m->kp, f, m->stream), "eta refresh");
         m->eta_swapped = !m->eta_swapped;
         if ((st = run_eta_batch<double>(m, FI_FIELD_ETA)) != FI_OK) return st;
-        for (int q = 0; q < 6; q++)
-            if (field_used(m, tau_f[q]))
-                FI_CHECK_CUDA(cudaMemcpyAsync(field_raw(m->nxt(tau_f[q]), m->esz), field_raw(m->cur(tau_f[q]), m->esz),
-                                              (m->elems + 64) * m->esz, cudaMemcpyDeviceToDevice, m->stream),
-                              "stress copy");
-        FI_CHECK_CUDA(launch_compute_tau<double>(m->g, m->kp, m->ptrs<double>(), m->stream), "projection");
-        if ((st = run_batch<double>(m, stress_batch)) != FI_OK) return st;
-        // FP64 residual fields and norms
-        if ((st = residuals_t<double>(m)) != FI_OK) return st;
+        // FP64 residual norms of the iterate itself (its own stresses), the quantity
+        // the plain solve tests
         if ((st = norms_t<double>(m, norms)) != FI_OK) return st;
         double meas = measure_of(m, o, norms);
         if (trace) std::fprintf(stderr, "[fi mixed] outer=%d sweeps=%d fp64 measure=%.3e\n", outer, sweeps, meas);
@@ -876,6 +876,16 @@ static fi_status solve_mixed(fi_model *m, const fi_solve_opts *o, fi_solve_repor
         if (meas < 0.5 * best_outer) outer_stale = 0;
         else if (++outer_stale >= 3) break;
         best_outer = std::min(best_outer, meas);
+        // projection τ = 2η dev(ε̇(V)) with its BCs (the stresses before it are kept in
+        // the second state buffer) and the FP64 residual fields of the projected anchor
+        for (int q = 0; q < 6; q++)
+            if (field_used(m, tau_f[q]))
+                FI_CHECK_CUDA(cudaMemcpyAsync(field_raw(m->nxt(tau_f[q]), m->esz), field_raw(m->cur(tau_f[q]), m->esz),
+                                              (m->elems + 64) * m->esz, cudaMemcpyDeviceToDevice, m->stream),
+                              "stress copy");
+        FI_CHECK_CUDA(launch_compute_tau<double>(m->g, m->kp, m->ptrs<double>(), m->ib, m->stream), "projection");
+        if ((st = run_batch<double>(m, stress_batch)) != FI_OK) return st;
+        if ((st = residuals_t<double>(m)) != FI_OK) return st;
         // the correction problem on the shadow: frozen η, forcing r_P and -r_V, zero state
         if ((st = convert_field<double, float>(s->cur(FI_FIELD_ETA), m->cur(FI_FIELD_ETA), n, 1.0, m->stream)) != FI_OK)
             return st;

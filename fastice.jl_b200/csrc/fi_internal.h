@@ -122,7 +122,7 @@ cudaError_t launch_update_V(const Geom &g, const KParams &p, const Ptrs<T> &f, b
 template <typename T>
 cudaError_t launch_compute_residuals(const Geom &g, const KParams &p, const Ptrs<T> &f, bool ib, cudaStream_t s);
 template <typename T>
-cudaError_t launch_compute_tau(const Geom &g, const KParams &p, const Ptrs<T> &f, cudaStream_t s);
+cudaError_t launch_compute_tau(const Geom &g, const KParams &p, const Ptrs<T> &f, bool ib, cudaStream_t s);
 template <typename T>
 cudaError_t launch_bc_batch(const Geom &g, const BcBatch &b, cudaStream_t s);
 template <typename T>
@@ -154,6 +154,8 @@ template <typename D, typename S>
 cudaError_t launch_accumulate(D *x, const S *d, long long n, cudaStream_t s);
 template <typename S, typename D>
 cudaError_t launch_diff(const S *a, const S *b, D *out, long long n, cudaStream_t s);
+// FP64 volume fractions to FP32 keeping every emptiness test w < 1e-6 unchanged
+cudaError_t launch_mask_to_f32(const double *src, float *dst, long long n, float thr32, cudaStream_t s);
 template <typename T>
 cudaError_t launch_eta_from_tau(const Geom &g, const KParams &p, const Ptrs<T> &f, cudaStream_t s);
 // max |value| over up to 8 FP32 arrays of n elements each, as float bits in *out_bits

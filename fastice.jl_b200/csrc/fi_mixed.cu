@@ -31,6 +31,20 @@ __global__ void diff_kernel(const S *__restrict__ a, const S *__restrict__ b, D 
         out[t] = D(a[t] - b[t]);
 }
 
+// A volume fraction rounded to FP32 for a shadow model whose emptiness threshold
+// is thr32 (the smallest float >= 1e-6): values below 1e-6 stay below thr32 and
+// the others stay at or above it, so both precisions see the same empty, valid
+// and null-space points (rounding to nearest alone could lift a value just under
+// 1e-6 onto thr32)
+__global__ void mask_to_f32_kernel(const double *__restrict__ src, float *__restrict__ dst, long long n, float thr32) {
+    const float below = nextafterf(thr32, 0.0f);
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const double w = src[t];
+        const float r = (float)w;
+        dst[t] = w < 1e-6 ? fminf(r, below) : fmaxf(r, thr32);
+    }
+}
+
 template <typename T>
 __device__ __forceinline__ T h(T x) { return T(0.5) * x; }
 
@@ -91,6 +105,11 @@ cudaError_t launch_convert(const S *src, D *dst, long long n, double scale, cuda
 template <typename D, typename S>
 cudaError_t launch_accumulate(D *x, const S *d, long long n, cudaStream_t s) {
     accumulate_kernel<D, S><<<grid_1d(n), 256, 0, s>>>(x, d, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mask_to_f32(const double *src, float *dst, long long n, float thr32, cudaStream_t s) {
+    mask_to_f32_kernel<<<grid_1d(n), 256, 0, s>>>(src, dst, n, thr32);
     return cudaGetLastError();
 }
 

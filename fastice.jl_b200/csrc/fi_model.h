@@ -38,6 +38,7 @@ struct fi_model {
     int *d_err = nullptr;  // device error word written by bounded waits
     void *fP = nullptr;    // pressure forcing (defect-correction shadow models only)
     fi_model *shadow = nullptr;  // FP32 model of the mixed-precision solve (created on first use)
+    KParams shadow_kp{};         // the shadow's parameters as created (gravity as fields); each solve starts from them
     // TMA maps (128 bytes each) of every buffer the fused sweep reads
     alignas(64) unsigned char map_base[kState][128];
     alignas(64) unsigned char map_alt[kState][128];

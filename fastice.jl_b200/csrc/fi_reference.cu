@@ -334,6 +334,61 @@ __global__ void __launch_bounds__(256) compute_tau_kernel(Geom g, KParams p, Ptr
     f.tyz[I] = T(2.0) * e_yz * eyz;
 }
 
+// Masked projection τ = 2η dev ε̇(V) of the immersed-boundary model: the strain
+// rates, activity tests and zeroing of update_σ! (IB kernels_3d.jl:3-44) with the
+// relaxation replaced by the assignment.  The reference's own IB compute_τ!
+// (IB kernels_3d.jl:76-100) cannot run (it names the undefined `Pr`); this is its
+// evident intent, used by the mixed-precision solve's projection step.
+template <typename T>
+__global__ void __launch_bounds__(256) compute_tau_ib_kernel(Geom g, KParams p, Ptrs<T> f) {
+    Idx x = vertex_index(g);
+    if (!x.ok) return;
+    const long long I = x.I, sx = g.pitch, sxy = g.sxy;
+    const T idx = T(p.inv_dx[0]), idy = T(p.inv_dx[1]), idz = T(p.inv_dx[2]);
+    const T *Vx = f.Vx, *Vy = f.Vy, *Vz = f.Vz, *eta = f.eta;
+    const T *const *na = f.wna;
+    const T *const *ns = f.wns;
+    const T thr = T(p.small);
+    if (active_dev(na, ns, W_CCC, I, sx, sxy, thr)) {
+        T exx = (ns[W_VCC][I + 1] * Vx[I + 1] - ns[W_VCC][I] * Vx[I]) * idx;
+        T eyy = (ns[W_CVC][I + sx] * Vy[I + sx] - ns[W_CVC][I] * Vy[I]) * idy;
+        T ezz = (ns[W_CCV][I + sxy] * Vz[I + sxy] - ns[W_CCV][I] * Vz[I]) * idz;
+        T divV = exx + eyy + ezz;
+        T etac = eta[I];
+        f.txx[I] = T(2.0) * etac * (exx - divV / T(3.0));
+        f.tyy[I] = T(2.0) * etac * (eyy - divV / T(3.0));
+        f.tzz[I] = T(2.0) * etac * (ezz - divV / T(3.0));
+    } else {
+        f.txx[I] = T(0);
+        f.tyy[I] = T(0);
+        f.tzz[I] = T(0);
+    }
+    if (active_dev(na, ns, W_VVC, I, sx, sxy, thr)) {
+        T exy = T(0.5) * ((ns[W_CVC][I] * Vy[I] - ns[W_CVC][I - 1] * Vy[I - 1]) * idx +
+                          (ns[W_VCC][I] * Vx[I] - ns[W_VCC][I - sx] * Vx[I - sx]) * idy);
+        T e_xy = h(h(eta[I - 1 - sx] + eta[I - sx]) + h(eta[I - 1] + eta[I]));
+        f.txy[I] = T(2.0) * e_xy * exy;
+    } else {
+        f.txy[I] = T(0);
+    }
+    if (active_dev(na, ns, W_VCV, I, sx, sxy, thr)) {
+        T exz = T(0.5) * ((ns[W_CCV][I] * Vz[I] - ns[W_CCV][I - 1] * Vz[I - 1]) * idx +
+                          (ns[W_VCC][I] * Vx[I] - ns[W_VCC][I - sxy] * Vx[I - sxy]) * idz);
+        T e_xz = h(h(eta[I - 1 - sxy] + eta[I - sxy]) + h(eta[I - 1] + eta[I]));
+        f.txz[I] = T(2.0) * e_xz * exz;
+    } else {
+        f.txz[I] = T(0);
+    }
+    if (active_dev(na, ns, W_CVV, I, sx, sxy, thr)) {
+        T eyz = T(0.5) * ((ns[W_CCV][I] * Vz[I] - ns[W_CCV][I - sx] * Vz[I - sx]) * idy +
+                          (ns[W_CVC][I] * Vy[I] - ns[W_CVC][I - sxy] * Vy[I - sxy]) * idz);
+        T e_yz = h(h(eta[I - sx - sxy] + eta[I - sxy]) + h(eta[I - sx] + eta[I]));
+        f.tyz[I] = T(2.0) * e_yz * eyz;
+    } else {
+        f.tyz[I] = T(0);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Boundary-condition batch for one dimension: the face of dim d spans the full
 // storage range of the dims before d and the interior range of the dims after
@@ -555,10 +610,11 @@ cudaError_t launch_compute_residuals(const Geom &g, const KParams &p, const Ptrs
 }
 
 template <typename T>
-cudaError_t launch_compute_tau(const Geom &g, const KParams &p, const Ptrs<T> &f, cudaStream_t s) {
+cudaError_t launch_compute_tau(const Geom &g, const KParams &p, const Ptrs<T> &f, bool ib, cudaStream_t s) {
     dim3 blk(32, 8);
     dim3 grd = vertex_grid(g, blk);
     if (g.nd == 2) compute_tau_kernel<T, 2><<<grd, blk, 0, s>>>(g, p, f);
+    else if (ib) compute_tau_ib_kernel<T><<<grd, blk, 0, s>>>(g, p, f);
     else compute_tau_kernel<T, 3><<<grd, blk, 0, s>>>(g, p, f);
     return cudaGetLastError();
 }
@@ -599,7 +655,7 @@ cudaError_t launch_residual_norms(const Geom &g, const KParams &p, const Ptrs<T>
     template cudaError_t launch_update_V<T>(const Geom &, const KParams &, const Ptrs<T> &, bool, cudaStream_t);     \
     template cudaError_t launch_compute_residuals<T>(const Geom &, const KParams &, const Ptrs<T> &, bool,          \
                                                      cudaStream_t);                                               \
-    template cudaError_t launch_compute_tau<T>(const Geom &, const KParams &, const Ptrs<T> &, cudaStream_t);       \
+    template cudaError_t launch_compute_tau<T>(const Geom &, const KParams &, const Ptrs<T> &, bool, cudaStream_t);       \
     template cudaError_t launch_bc_batch<T>(const Geom &, const BcBatch &, cudaStream_t);                          \
     template cudaError_t launch_residual_norms<T>(const Geom &, const KParams &, const Ptrs<T> &, bool, double *,  \
                                                   int, double *, cudaStream_t);

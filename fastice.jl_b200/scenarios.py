@@ -165,5 +165,68 @@ def bed_height(prm, x, y):
     return h
 
 
-__all__ = ["inclusion_params", "inclusion_viscosity", "inclusion_model", "smooth_log", "stiffness_ratio",
+# ---- 3D manufactured solution (scripts_future_API/stokes_manufactured_solution_free_slip_3D.jl:25-48)
+def _mf(a, b):
+    return np.cos(math.pi * a) * (b ** 2 - 1) ** 2 - np.cos(math.pi * b) * (a ** 2 - 1) ** 2
+
+
+def _mp(a, b):
+    return np.cos(math.pi * b) * (1 - 3 * a ** 2) * 2 - np.cos(math.pi * a) * (1 - 3 * b ** 2) * 2
+
+
+def mms3d_gravity(grid, eta: float = 1.0):
+    """Body force of the 3D free-slip manufactured solution on [-1, 1]^3 (the
+    driver's ρg, evaluated at each velocity component's location)."""
+    from .physics import FunctionField
+    from .grids import Center, Vertex
+    V, Cc = Vertex(), Center()
+    return {"x": FunctionField(lambda x, y, z: -2 * eta * np.sin(math.pi * x) * (_mf(y, z) * math.pi ** 2 - _mp(y, z)),
+                               grid, (V, Cc, Cc)),
+            "y": FunctionField(lambda x, y, z: -2 * eta * np.sin(math.pi * y) * (_mf(z, x) * math.pi ** 2 - _mp(z, x)),
+                               grid, (Cc, V, Cc)),
+            "z": FunctionField(lambda x, y, z: -2 * eta * np.sin(math.pi * z) * (_mf(x, y) * math.pi ** 2 - _mp(x, y)),
+                               grid, (Cc, Cc, V))}
+
+
+def mms3d_exact(grid):
+    """Exact vx, vy, vz at their staggered interior locations (numpy (z, y, x) order)."""
+    from .grids import Center, Vertex
+    V, Cc = Vertex(), Center()
+    out = []
+    for comp, locs in (("x", (V, Cc, Cc)), ("y", (Cc, V, Cc)), ("z", (Cc, Cc, V))):
+        x, y, z = (grid.coords(locs[d], d) for d in range(3))
+        Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+        if comp == "x":
+            out.append(np.sin(math.pi * X) * _mf(Y, Z))
+        elif comp == "y":
+            out.append(np.sin(math.pi * Y) * _mf(Z, X))
+        else:
+            out.append(np.sin(math.pi * Z) * _mf(X, Y))
+    return out
+
+
+def mms3d_model(n: int, dtype: str = "f64", library: str = "fast"):
+    """The 3D manufactured-solution model (η = 1, free slip on every side, zero
+    initial state) at n^3 cells: returns (grid, model)."""
+    grid = UniformGrid(origin=(-1.0, -1.0, -1.0), extent=(2.0, 2.0, 2.0), dims=(n, n, n))
+    slip = SBC(0.0, 0.0, 0.0)
+    m = IsothermalFullStokesModel(grid=grid, boundary_conditions={"x": (slip, slip), "y": (slip, slip),
+                                                                 "z": (slip, slip)},
+                                  gravity=mms3d_gravity(grid), rheology=LinearViscousRheology(1.0),
+                                  solver_params=pt_params(grid), dtype=dtype, library=library)
+    m.set_field("eta", 1.0)
+    m.set_field("eta_next", 1.0)
+    m.apply_bcs()
+    return grid, m
+
+
+def mms3d_error(grid, m) -> float:
+    """Relative L2 error of the model's velocity against the manufactured solution."""
+    ex = mms3d_exact(grid)
+    num = sum(np.sum((m.get_field(f).astype(np.float64) - e) ** 2) for f, e in zip(("Vx", "Vy", "Vz"), ex))
+    den = sum(np.sum(e ** 2) for e in ex)
+    return math.sqrt(num / den)
+
+
+__all__ = ["mms3d_gravity", "mms3d_exact", "mms3d_model", "mms3d_error", "inclusion_params", "inclusion_viscosity", "inclusion_model", "smooth_log", "stiffness_ratio",
            "bed_model", "bed_params", "bed_height", "INCLUSION_N_RANGE"]

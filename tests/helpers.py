@@ -166,56 +166,18 @@ def mms2d_exact(grid):
     return vx, vy
 
 
-# ---- 3D manufactured solution (scripts_future_API/stokes_manufactured_solution_free_slip_3D.jl:25-48)
-def _mf(a, b):
-    return np.cos(math.pi * a) * (b ** 2 - 1) ** 2 - np.cos(math.pi * b) * (a ** 2 - 1) ** 2
-
-
-def _mp(a, b):
-    return np.cos(math.pi * b) * (1 - 3 * a ** 2) * 2 - np.cos(math.pi * a) * (1 - 3 * b ** 2) * 2
-
-
+# ---- 3D manufactured solution: the package's builders (fastice_b200.scenarios)
 def mms3d_gravity(fi, grid, eta=1.0):
-    V, Cc = fi.Vertex(), fi.Center()
-    return {"x": fi.FunctionField(lambda x, y, z: -2 * eta * np.sin(math.pi * x) * (_mf(y, z) * math.pi ** 2 - _mp(y, z)),
-                                  grid, (V, Cc, Cc)),
-            "y": fi.FunctionField(lambda x, y, z: -2 * eta * np.sin(math.pi * y) * (_mf(z, x) * math.pi ** 2 - _mp(z, x)),
-                                  grid, (Cc, V, Cc)),
-            "z": fi.FunctionField(lambda x, y, z: -2 * eta * np.sin(math.pi * z) * (_mf(x, y) * math.pi ** 2 - _mp(x, y)),
-                                  grid, (Cc, Cc, V))}
+    return fi.scenarios.mms3d_gravity(grid, eta)
 
 
 def mms3d_exact(fi, grid):
-    """Exact vx, vy, vz at their staggered interior locations (numpy (z, y, x) order)."""
-    V, Cc = fi.Vertex(), fi.Center()
-    out = []
-    for comp, locs in (("x", (V, Cc, Cc)), ("y", (Cc, V, Cc)), ("z", (Cc, Cc, V))):
-        x, y, z = (grid.coords(locs[d], d) for d in range(3))
-        Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
-        if comp == "x":
-            out.append(np.sin(math.pi * X) * _mf(Y, Z))
-        elif comp == "y":
-            out.append(np.sin(math.pi * Y) * _mf(Z, X))
-        else:
-            out.append(np.sin(math.pi * Z) * _mf(X, Y))
-    return out
+    return fi.scenarios.mms3d_exact(grid)
 
 
 def mms3d_model(fi, n, dtype="f64", library="fast"):
-    grid = fi.UniformGrid(origin=(-1.0, -1.0, -1.0), extent=(2.0, 2.0, 2.0), dims=(n, n, n))
-    slip = fi.SBC(0.0, 0.0, 0.0)
-    m = fi.IsothermalFullStokesModel(grid=grid, boundary_conditions={"x": (slip, slip), "y": (slip, slip),
-                                                                    "z": (slip, slip)},
-                                     gravity=mms3d_gravity(fi, grid), rheology=fi.LinearViscousRheology(1.0),
-                                     solver_params=fi.pt_params(grid), dtype=dtype, library=library)
-    m.set_field("eta", 1.0)
-    m.set_field("eta_next", 1.0)
-    m.apply_bcs()
-    return grid, m
+    return fi.scenarios.mms3d_model(n, dtype=dtype, library=library)
 
 
 def mms3d_error(fi, grid, m):
-    ex = mms3d_exact(fi, grid)
-    num = sum(np.sum((m.get_field(f).astype(np.float64) - e) ** 2) for f, e in zip(("Vx", "Vy", "Vz"), ex))
-    den = sum(np.sum(e ** 2) for e in ex)
-    return math.sqrt(num / den)
+    return fi.scenarios.mms3d_error(grid, m)

@@ -53,3 +53,34 @@ def test_mixed_rejects_fp32_model():
     with pytest.raises(fi.FastIceError):
         m.solve(mode="mixed", max_iter=100, ncheck=10, tol=1e-8)
     m.close()
+
+
+def test_mixed_glacier_matches_fp64_solve():
+    # the immersed-boundary glacier (seeded 64-bump bed, sinusoidal surface):
+    # FP32 correction sweeps on volume fractions rounded so that every emptiness
+    # test agrees with FP64, masked stress projection, FP64 residuals
+    from fastice_b200 import scenarios
+    fi = load_fastice()
+    n = 24
+    kw = dict(max_iter=400 * n, ncheck=n, tol=1e-8, measure="rel_slab", rho_g_inf=1.0, length_z=0.6)
+    plain, _ = scenarios.bed_model(0, n)
+    rp = plain.solve(**kw)
+    mixed, _ = scenarios.bed_model(0, n)
+    # a first, short mixed solve ends inside the FP32 full-problem phase; the
+    # second solve (from the reset state) must still force its corrections with
+    # the FP64 residual, not with the full problem's body force
+    mixed.solve(mode="mixed", **dict(kw, max_iter=2 * n, tol=1e-30))
+    for f in ("P", "txx", "tyy", "tzz", "txy", "txz", "tyz", "Vx", "Vy", "Vz"):
+        mixed.set_field(f, 0.0)
+    mixed.set_field("eta", 1.0)
+    mixed.set_field("eta_next", 1.0)
+    mixed.apply_bcs()
+    rm = mixed.solve(mode="mixed", **kw)
+    assert rp["converged"] and rm["converged"], (rp, rm)
+    assert rm["measure"] < 1e-8 and rm["outer"] >= 1
+    vmax = max(np.max(np.abs(plain.get_field(c))) for c in ("Vx", "Vy", "Vz"))
+    for name in ("Vx", "Vy", "Vz"):
+        d = np.max(np.abs(mixed.get_field(name) - plain.get_field(name))) / vmax
+        assert d < 1e-6, (name, d)
+    plain.close()
+    mixed.close()
