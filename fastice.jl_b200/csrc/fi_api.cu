@@ -288,8 +288,19 @@ fi_status run_eta_batch(fi_model *m, int field) {
     return FI_OK;
 }
 
+// activity bytes of an immersed-boundary model, recomputed after its volume
+// fractions changed (set_field, ω_from_ψ!, a device pointer handed out)
+template <typename T>
+fi_status refresh_ibf(fi_model *m) {
+    if (!m->ib || !m->ibf_stale) return FI_OK;
+    FI_CHECK_CUDA(launch_ib_flags<T>(m->g, m->kp, m->ptrs<T>(), m->d_ibf, m->stream), "activity bytes");
+    m->ibf_stale = false;
+    return FI_OK;
+}
+
 template <typename T>
 fi_status advance_t(fi_model *m, int niter) {
+    if (fi_status st = refresh_ibf<T>(m); st != FI_OK) return st;
     for (int it = 0; it < niter; it++) {
         if (m->path == FI_PATH_FUSED) {
             Ptrs<T> in = m->ptrs<T>(false);
@@ -347,6 +358,7 @@ fi_status encode_maps(fi_model *m) {
 
 template <typename T>
 fi_status norms_t(fi_model *m, double *out) {
+    if (fi_status st = refresh_ibf<T>(m); st != FI_OK) return st;
     Ptrs<T> f = m->ptrs<T>();
     FI_CHECK_CUDA(launch_residual_norms<T>(m->g, m->kp, f, m->ib, m->d_partials, m->nblk, m->d_out, m->stream),
                   "residual norms");
@@ -369,6 +381,7 @@ template <typename T>
 fi_status residuals_t(fi_model *m) {
     fi_status st = ensure_residual_arrays(m);
     if (st != FI_OK) return st;
+    if ((st = refresh_ibf<T>(m)) != FI_OK) return st;
     Ptrs<T> f = m->ptrs<T>();
     FI_CHECK_CUDA(launch_compute_residuals<T>(m->g, m->kp, f, m->ib, m->stream), "compute_residuals");
     return run_batch<T>(m, residual_batch);
@@ -498,6 +511,8 @@ fi_status fi_model_create(const fi_model_desc *desc, fi_model **out) {
         }
     }
     if (cudaMalloc(&m->d_err, sizeof(int)) != cudaSuccess) return fail(cuda_fail(cudaGetLastError(), "error word"));
+    if (m->ib && cudaMalloc(&m->d_ibf, m->elems) != cudaSuccess)
+        return fail(cuda_fail(cudaGetLastError(), "activity bytes"));
     cudaMemsetAsync(m->d_err, 0, sizeof(int), m->stream);
     if (m->path == FI_PATH_FUSED) {
         fi_status es = encode_maps(m);
@@ -523,6 +538,7 @@ fi_status fi_model_destroy(fi_model *m) {
     for (int f = 0; f < FI_FIELD_COUNT; f++) field_free(m->base[f], m->esz);
     for (int f = 0; f < kState; f++) field_free(m->alt[f], m->esz);
     if (m->d_err) cudaFree(m->d_err);
+    if (m->d_ibf) cudaFree(m->d_ibf);
     field_free(m->fP, m->esz);
     if (m->shadow) fi_model_destroy(m->shadow);
     if (m->d_partials) cudaFree(m->d_partials);
@@ -551,6 +567,7 @@ fi_status fi_model_set_field(fi_model *m, int32_t field, const void *host, size_
     cudaMemcpy3DParms p = copy_params(m, field, m->cur(field), const_cast<void *>(host), true);
     FI_CHECK_CUDA(cudaMemcpy3DAsync(&p, m->stream), "set_field copy");
     FI_CHECK_CUDA(cudaStreamSynchronize(m->stream), "set_field sync");
+    if (field >= FI_FIELD_NA_CCC) m->ibf_stale = true;
     return FI_OK;
 }
 
@@ -610,6 +627,9 @@ fi_status fi_model_device_ptr(fi_model *m, int32_t field, void **dptr) {
         if (st != FI_OK) return st;
     }
     *dptr = m->cur(field);
+    // the caller may write volume fractions through the pointer: their activity
+    // bytes are recomputed before the next kernel that reads them
+    if (field >= FI_FIELD_NA_CCC) m->ibf_stale = true;
     return FI_OK;
 }
 
@@ -745,6 +765,10 @@ static fi_status solve_mixed(fi_model *m, const fi_solve_opts *o, fi_solve_repor
             FI_CHECK_CUDA(launch_mask_to_f32((const double *)m->base[f], (float *)s->base[f], (long long)m->elems,
                                              (float)s->kp.small, m->stream),
                           "shadow volume fractions");
+    if (m->ib) {
+        s->ibf_stale = true;
+        FI_CHECK_CUDA(cudaStreamSynchronize(m->stream), "shadow volume fractions");
+    }
     const long long n = (long long)m->elems;
     const int nd = m->d.grid.nd;
     const double inner_red = o->inner_reduction > 0 ? o->inner_reduction : 1e-3;
@@ -883,6 +907,7 @@ static fi_status solve_mixed(fi_model *m, const fi_solve_opts *o, fi_solve_repor
                 FI_CHECK_CUDA(cudaMemcpyAsync(field_raw(m->nxt(tau_f[q]), m->esz), field_raw(m->cur(tau_f[q]), m->esz),
                                               (m->elems + 64) * m->esz, cudaMemcpyDeviceToDevice, m->stream),
                               "stress copy");
+        if ((st = refresh_ibf<double>(m)) != FI_OK) return st;
         FI_CHECK_CUDA(launch_compute_tau<double>(m->g, m->kp, m->ptrs<double>(), m->ib, m->stream), "projection");
         if ((st = run_batch<double>(m, stress_batch)) != FI_OK) return st;
         if ((st = residuals_t<double>(m)) != FI_OK) return st;
@@ -1022,6 +1047,7 @@ fi_status fi_model_volfrac_from_levelset(fi_model *m, int32_t group, const doubl
     e = cudaStreamSynchronize(m->stream);
     cleanup();
     if (e != cudaSuccess) return cuda_fail(e, "volfrac sync");
+    m->ibf_stale = true;
     return FI_OK;
 }
 

@@ -158,4 +158,20 @@ __device__ __forceinline__ bool active_dev(const T *const a[8], const T *const b
     return valid && !small_dev(b[comp][I], thr);
 }
 
+// the activity byte at index I: precomputed when the model provides it, else the
+// seven predicates of null_spaces.jl:41-43 evaluated here
+template <typename T>
+__device__ __forceinline__ unsigned ib_flags_at(const Ptrs<T> &f, long long I, long long sx, long long sxy, T thr) {
+    if (f.ibf) return f.ibf[I];
+    unsigned b = 0;
+    if (active_dev(f.wna, f.wns, W_CCC, I, sx, sxy, thr)) b |= IBF_S_CCC;
+    if (active_dev(f.wna, f.wns, W_VVC, I, sx, sxy, thr)) b |= IBF_S_VVC;
+    if (active_dev(f.wna, f.wns, W_VCV, I, sx, sxy, thr)) b |= IBF_S_VCV;
+    if (active_dev(f.wna, f.wns, W_CVV, I, sx, sxy, thr)) b |= IBF_S_CVV;
+    if (active_dev(f.wns, f.wna, W_VCC, I, sx, sxy, thr)) b |= IBF_V_VCC;
+    if (active_dev(f.wns, f.wna, W_CVC, I, sx, sxy, thr)) b |= IBF_V_CVC;
+    if (active_dev(f.wns, f.wna, W_CCV, I, sx, sxy, thr)) b |= IBF_V_CCV;
+    return b;
+}
+
 }  // namespace fi

@@ -86,7 +86,14 @@ struct Ptrs {
     const T *fP;  // pressure forcing of the defect-correction problem (p_forcing)
     const T *wna[8];
     const T *wns[8];
+    // immersed-boundary activity bits per grid index (IbFlag), precomputed from the
+    // volume fractions; nullptr: the kernels evaluate the predicates themselves
+    const unsigned char *ibf;
 };
+// bits of the precomputed immersed-boundary activity byte: update_σ! points
+// (isvalid(na) && !isempty(ns)) at ccc, vvc, vcv, cvv and update_V! points
+// (isvalid(ns) && !isempty(na)) at vcc, cvc, ccv
+enum IbFlag { IBF_S_CCC = 1, IBF_S_VVC = 2, IBF_S_VCV = 4, IBF_S_CVV = 8, IBF_V_VCC = 16, IBF_V_CVC = 32, IBF_V_CCV = 64 };
 
 // one boundary-condition operation on a face (see kernel bc_dim_kernel)
 enum BcOp { BC_DIRICHLET = 0, BC_NEUMANN = 1, BC_PERIODIC = 2 };
@@ -123,6 +130,9 @@ template <typename T>
 cudaError_t launch_compute_residuals(const Geom &g, const KParams &p, const Ptrs<T> &f, bool ib, cudaStream_t s);
 template <typename T>
 cudaError_t launch_compute_tau(const Geom &g, const KParams &p, const Ptrs<T> &f, bool ib, cudaStream_t s);
+// the activity byte of every vertex-range index from the model's volume fractions
+template <typename T>
+cudaError_t launch_ib_flags(const Geom &g, const KParams &p, const Ptrs<T> &f, unsigned char *flags, cudaStream_t s);
 template <typename T>
 cudaError_t launch_bc_batch(const Geom &g, const BcBatch &b, cudaStream_t s);
 template <typename T>

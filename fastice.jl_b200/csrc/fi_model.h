@@ -36,6 +36,8 @@ struct fi_model {
     bool ib = false;
     long long iterations = 0;
     int *d_err = nullptr;  // device error word written by bounded waits
+    unsigned char *d_ibf = nullptr;  // immersed-boundary activity byte per grid index (IbFlag bits)
+    bool ibf_stale = true;           // the volume fractions changed since d_ibf was computed
     void *fP = nullptr;    // pressure forcing (defect-correction shadow models only)
     fi_model *shadow = nullptr;  // FP32 model of the mixed-precision solve (created on first use)
     KParams shadow_kp{};         // the shadow's parameters as created (gravity as fields); each solve starts from them
@@ -84,6 +86,7 @@ struct fi_model {
             f.wna[c] = (const T *)base[FI_FIELD_NA_CCC + c];
             f.wns[c] = (const T *)base[FI_FIELD_NS_CCC + c];
         }
+        f.ibf = ibf_stale ? nullptr : d_ibf;  // stale bytes are never read: the kernels evaluate the predicates
         return f;
     }
 };

@@ -83,9 +83,9 @@ __global__ void __launch_bounds__(256) update_sigma_kernel(Geom g, KParams p, Pt
         f.tyz[I] = f.tyz[I] - (f.tyz[I] - T(2.0) * e_yz * eyz) * T(p.dt_tau[5]);
         return;
     }
-    const T *const *na = f.wna;
     const T *const *ns = f.wns;
-    if (active_dev(na, ns, W_CCC, I, sx, sxy, thr)) {
+    const unsigned fl = ib_flags_at(f, I, sx, sxy, thr);
+    if (fl & IBF_S_CCC) {
         T exx = (ns[W_VCC][I + 1] * Vx[I + 1] - ns[W_VCC][I] * Vx[I]) * idx;
         T eyy = (ns[W_CVC][I + sx] * Vy[I + sx] - ns[W_CVC][I] * Vy[I]) * idy;
         T ezz = (ns[W_CCV][I + sxy] * Vz[I + sxy] - ns[W_CCV][I] * Vz[I]) * idz;
@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(256) update_sigma_kernel(Geom g, KParams p, Pt
         f.tyy[I] = T(0);
         f.tzz[I] = T(0);
     }
-    if (active_dev(na, ns, W_VVC, I, sx, sxy, thr)) {
+    if (fl & IBF_S_VVC) {
         T exy = T(0.5) * ((ns[W_CVC][I] * Vy[I] - ns[W_CVC][I - 1] * Vy[I - 1]) * idx +
                           (ns[W_VCC][I] * Vx[I] - ns[W_VCC][I - sx] * Vx[I - sx]) * idy);
         T e_xy = h(h(eta[I - 1 - sx] + eta[I - sx]) + h(eta[I - 1] + eta[I]));
@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(256) update_sigma_kernel(Geom g, KParams p, Pt
     } else {
         f.txy[I] = T(0);
     }
-    if (active_dev(na, ns, W_VCV, I, sx, sxy, thr)) {
+    if (fl & IBF_S_VCV) {
         T exz = T(0.5) * ((ns[W_CCV][I] * Vz[I] - ns[W_CCV][I - 1] * Vz[I - 1]) * idx +
                           (ns[W_VCC][I] * Vx[I] - ns[W_VCC][I - sxy] * Vx[I - sxy]) * idz);
         T e_xz = h(h(eta[I - 1 - sxy] + eta[I - sxy]) + h(eta[I - 1] + eta[I]));
@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(256) update_sigma_kernel(Geom g, KParams p, Pt
     } else {
         f.txz[I] = T(0);
     }
-    if (active_dev(na, ns, W_CVV, I, sx, sxy, thr)) {
+    if (fl & IBF_S_CVV) {
         T eyz = T(0.5) * ((ns[W_CCV][I] * Vz[I] - ns[W_CCV][I - sx] * Vz[I - sx]) * idy +
                           (ns[W_CVC][I] * Vy[I] - ns[W_CVC][I - sxy] * Vy[I - sxy]) * idz);
         T e_yz = h(h(eta[I - sx - sxy] + eta[I - sxy]) + h(eta[I - sx] + eta[I]));
@@ -177,7 +177,8 @@ __global__ void __launch_bounds__(256) update_V_kernel(Geom g, KParams p, Ptrs<T
         const T *const *ns = f.wns;
         const T thr = T(p.small);
         const T *wc = na[W_CCC], *wvvc = na[W_VVC], *wvcv = na[W_VCV], *wcvv = na[W_CVV];
-        if (active_dev(ns, na, W_VCC, I, sx, sxy, thr)) {
+        const unsigned fl = ib_flags_at(f, I, sx, sxy, thr);
+        if (fl & IBF_V_VCC) {
             T ex = h(eta[I - 1] + eta[I]);
             f.Vx[I] = f.Vx[I] + div_dev(div_dev(-(wc[I] * P[I] - wc[I - 1] * P[I - 1]) * idx +
                                                     (wc[I] * txx[I] - wc[I - 1] * txx[I - 1]) * idx +
@@ -189,7 +190,7 @@ __global__ void __launch_bounds__(256) update_V_kernel(Geom g, KParams p, Ptrs<T
         } else {
             f.Vx[I] = T(0);
         }
-        if (active_dev(ns, na, W_CVC, I, sx, sxy, thr)) {
+        if (fl & IBF_V_CVC) {
             T ey = h(eta[I - sx] + eta[I]);
             f.Vy[I] = f.Vy[I] + div_dev(div_dev(-(wc[I] * P[I] - wc[I - sx] * P[I - sx]) * idy +
                                                     (wc[I] * tyy[I] - wc[I - sx] * tyy[I - sx]) * idy +
@@ -201,7 +202,7 @@ __global__ void __launch_bounds__(256) update_V_kernel(Geom g, KParams p, Ptrs<T
         } else {
             f.Vy[I] = T(0);
         }
-        if (active_dev(ns, na, W_CCV, I, sx, sxy, thr)) {
+        if (fl & IBF_V_CCV) {
             T ez = h(eta[I - sxy] + eta[I]);
             f.Vz[I] = f.Vz[I] + div_dev(div_dev(-(wc[I] * P[I] - wc[I - sxy] * P[I - sxy]) * idz +
                                                     (wc[I] * tzz[I] - wc[I - sxy] * tzz[I - sxy]) * idz +
@@ -260,22 +261,23 @@ __device__ __forceinline__ Resid<T, ND, IB> residual_at(const Geom &g, const KPa
     const T *const *ns = f.wns;
     const T thr = T(p.small);
     const T *wc = na[W_CCC], *wvvc = na[W_VVC], *wvcv = na[W_VCV], *wcvv = na[W_CVV];
-    r.rP = active_dev(na, ns, W_CCC, I, sx, sxy, thr)
+    const unsigned fl = ib_flags_at(f, I, sx, sxy, thr);
+    r.rP = (fl & IBF_S_CCC)
                ? (ns[W_VCC][I + 1] * Vx[I + 1] - ns[W_VCC][I] * Vx[I]) * idx +
                      (ns[W_CVC][I + sx] * Vy[I + sx] - ns[W_CVC][I] * Vy[I]) * idy +
                      (ns[W_CCV][I + sxy] * Vz[I + sxy] - ns[W_CCV][I] * Vz[I]) * idz
                : T(0);
-    r.rVx = active_dev(ns, na, W_VCC, I, sx, sxy, thr)
+    r.rVx = (fl & IBF_V_VCC)
                 ? -(wc[I] * P[I] - wc[I - 1] * P[I - 1]) * idx + (wc[I] * txx[I] - wc[I - 1] * txx[I - 1]) * idx +
                       (wvvc[I + sx] * txy[I + sx] - wvvc[I] * txy[I]) * idy +
                       (wvcv[I + sxy] * txz[I + sxy] - wvcv[I] * txz[I]) * idz - gx
                 : T(0);
-    r.rVy = active_dev(ns, na, W_CVC, I, sx, sxy, thr)
+    r.rVy = (fl & IBF_V_CVC)
                 ? -(wc[I] * P[I] - wc[I - sx] * P[I - sx]) * idy + (wc[I] * tyy[I] - wc[I - sx] * tyy[I - sx]) * idy +
                       (wvvc[I + 1] * txy[I + 1] - wvvc[I] * txy[I]) * idx +
                       (wcvv[I + sxy] * tyz[I + sxy] - wcvv[I] * tyz[I]) * idz - gy
                 : T(0);
-    r.rVz = active_dev(ns, na, W_CCV, I, sx, sxy, thr)
+    r.rVz = (fl & IBF_V_CCV)
                 ? -(wc[I] * P[I] - wc[I - sxy] * P[I - sxy]) * idz + (wc[I] * tzz[I] - wc[I - sxy] * tzz[I - sxy]) * idz +
                       (wvcv[I + 1] * txz[I + 1] - wvcv[I] * txz[I]) * idx +
                       (wcvv[I + sx] * tyz[I + sx] - wcvv[I] * tyz[I]) * idy - gz
@@ -346,10 +348,10 @@ __global__ void __launch_bounds__(256) compute_tau_ib_kernel(Geom g, KParams p, 
     const long long I = x.I, sx = g.pitch, sxy = g.sxy;
     const T idx = T(p.inv_dx[0]), idy = T(p.inv_dx[1]), idz = T(p.inv_dx[2]);
     const T *Vx = f.Vx, *Vy = f.Vy, *Vz = f.Vz, *eta = f.eta;
-    const T *const *na = f.wna;
     const T *const *ns = f.wns;
     const T thr = T(p.small);
-    if (active_dev(na, ns, W_CCC, I, sx, sxy, thr)) {
+    const unsigned fl = ib_flags_at(f, I, sx, sxy, thr);
+    if (fl & IBF_S_CCC) {
         T exx = (ns[W_VCC][I + 1] * Vx[I + 1] - ns[W_VCC][I] * Vx[I]) * idx;
         T eyy = (ns[W_CVC][I + sx] * Vy[I + sx] - ns[W_CVC][I] * Vy[I]) * idy;
         T ezz = (ns[W_CCV][I + sxy] * Vz[I + sxy] - ns[W_CCV][I] * Vz[I]) * idz;
@@ -363,7 +365,7 @@ __global__ void __launch_bounds__(256) compute_tau_ib_kernel(Geom g, KParams p, 
         f.tyy[I] = T(0);
         f.tzz[I] = T(0);
     }
-    if (active_dev(na, ns, W_VVC, I, sx, sxy, thr)) {
+    if (fl & IBF_S_VVC) {
         T exy = T(0.5) * ((ns[W_CVC][I] * Vy[I] - ns[W_CVC][I - 1] * Vy[I - 1]) * idx +
                           (ns[W_VCC][I] * Vx[I] - ns[W_VCC][I - sx] * Vx[I - sx]) * idy);
         T e_xy = h(h(eta[I - 1 - sx] + eta[I - sx]) + h(eta[I - 1] + eta[I]));
@@ -371,7 +373,7 @@ __global__ void __launch_bounds__(256) compute_tau_ib_kernel(Geom g, KParams p, 
     } else {
         f.txy[I] = T(0);
     }
-    if (active_dev(na, ns, W_VCV, I, sx, sxy, thr)) {
+    if (fl & IBF_S_VCV) {
         T exz = T(0.5) * ((ns[W_CCV][I] * Vz[I] - ns[W_CCV][I - 1] * Vz[I - 1]) * idx +
                           (ns[W_VCC][I] * Vx[I] - ns[W_VCC][I - sxy] * Vx[I - sxy]) * idz);
         T e_xz = h(h(eta[I - 1 - sxy] + eta[I - sxy]) + h(eta[I - 1] + eta[I]));
@@ -379,7 +381,7 @@ __global__ void __launch_bounds__(256) compute_tau_ib_kernel(Geom g, KParams p, 
     } else {
         f.txz[I] = T(0);
     }
-    if (active_dev(na, ns, W_CVV, I, sx, sxy, thr)) {
+    if (fl & IBF_S_CVV) {
         T eyz = T(0.5) * ((ns[W_CCV][I] * Vz[I] - ns[W_CCV][I - sx] * Vz[I - sx]) * idy +
                           (ns[W_CVC][I] * Vy[I] - ns[W_CVC][I - sxy] * Vy[I - sxy]) * idz);
         T e_yz = h(h(eta[I - sx - sxy] + eta[I - sxy]) + h(eta[I - sx] + eta[I]));
@@ -609,6 +611,25 @@ cudaError_t launch_compute_residuals(const Geom &g, const KParams &p, const Ptrs
     return cudaGetLastError();
 }
 
+// activity bytes over the vertex range (null_spaces.jl:41-43 at the seven
+// locations the masked kernels test)
+template <typename T>
+__global__ void __launch_bounds__(256) ib_flags_kernel(Geom g, KParams p, Ptrs<T> f, unsigned char *flags) {
+    Idx x = vertex_index(g);
+    if (!x.ok) return;
+    Ptrs<T> q = f;
+    q.ibf = nullptr;
+    flags[x.I] = (unsigned char)ib_flags_at(q, x.I, g.pitch, g.sxy, T(p.small));
+}
+
+template <typename T>
+cudaError_t launch_ib_flags(const Geom &g, const KParams &p, const Ptrs<T> &f, unsigned char *flags, cudaStream_t s) {
+    dim3 blk(32, 8);
+    dim3 grd = vertex_grid(g, blk);
+    ib_flags_kernel<T><<<grd, blk, 0, s>>>(g, p, f, flags);
+    return cudaGetLastError();
+}
+
 template <typename T>
 cudaError_t launch_compute_tau(const Geom &g, const KParams &p, const Ptrs<T> &f, bool ib, cudaStream_t s) {
     dim3 blk(32, 8);
@@ -655,7 +676,8 @@ cudaError_t launch_residual_norms(const Geom &g, const KParams &p, const Ptrs<T>
     template cudaError_t launch_update_V<T>(const Geom &, const KParams &, const Ptrs<T> &, bool, cudaStream_t);     \
     template cudaError_t launch_compute_residuals<T>(const Geom &, const KParams &, const Ptrs<T> &, bool,          \
                                                      cudaStream_t);                                               \
-    template cudaError_t launch_compute_tau<T>(const Geom &, const KParams &, const Ptrs<T> &, bool, cudaStream_t);       \
+    template cudaError_t launch_compute_tau<T>(const Geom &, const KParams &, const Ptrs<T> &, bool, cudaStream_t);   \
+    template cudaError_t launch_ib_flags<T>(const Geom &, const KParams &, const Ptrs<T> &, unsigned char *, cudaStream_t);       \
     template cudaError_t launch_bc_batch<T>(const Geom &, const BcBatch &, cudaStream_t);                          \
     template cudaError_t launch_residual_norms<T>(const Geom &, const KParams &, const Ptrs<T> &, bool, double *,  \
                                                   int, double *, cudaStream_t);
