@@ -147,6 +147,35 @@ def test_immersed_boundary_bitwise_strict():
     np.testing.assert_array_equal(a[[0, 1, 2, 3]], b[[0, 1, 2, 3]])
 
 
+def test_immersed_boundary_activity_follows_new_volume_fractions():
+    # the kernels read per-index activity bytes computed from the volume
+    # fractions; recomputing the fractions between iterations (ω_from_ψ! on a
+    # moved bed) must be seen by the next iteration, bit for bit with the oracle
+    fi, O = load_fastice(), load_oracle()
+    n = (20, 14, 18)
+    ext = (1.0, 1.25, 1.5)
+    dx = tuple(e / c for e, c in zip(ext, n))
+    psi_ns = -_sphere_psi(n, dx, (0.5, 0.6, -0.3), 0.75)
+    psi_na = _sphere_psi(n, dx, (0.5, 0.6, 0.5), 0.8)
+    trac = ("traction", (0.0, 0.0, 0.0))
+    bcs = ((trac, trac), (trac, trac), (trac, trac))
+    p = Pair(n, bcs, path="reference", library="strict", seed=32, origin=(0.0, 0.0, 0.0), extent=ext,
+             immersed_psi={"na": psi_na, "ns": psi_ns})
+    p.advance(2)
+    moved = -_sphere_psi(n, dx, (0.45, 0.55, -0.2), 0.8)
+    p.model.omega_from_psi("ns", moved)
+    new = O.volfrac3d(n, dx, moved)
+    for k, c in enumerate(O.MASK_COMPONENTS):
+        p.oracle.masks["ns"][k][...] = new[c]
+    p.advance(3)
+    bad = p.bitwise_equal()
+    a = p.model.residual_norms()
+    b = p.oracle.residual_norms()
+    p.close()
+    assert not bad, bad
+    np.testing.assert_array_equal(a[[0, 1, 2, 3]], b[[0, 1, 2, 3]])
+
+
 def test_model_omega_from_psi_matches_standalone():
     fi = load_fastice()
     n, ext = (16, 12, 10), (1.0, 0.75, 0.6)
