@@ -298,9 +298,62 @@ fi_status refresh_ibf(fi_model *m) {
     return FI_OK;
 }
 
+// one reference-shaped iteration: update_σ!, stress BCs, update_V!, velocity BCs
+template <typename T>
+fi_status reference_iteration(fi_model *m) {
+    Ptrs<T> f = m->ptrs<T>();
+    FI_CHECK_CUDA(launch_update_sigma<T>(m->g, m->kp, f, m->ib, m->stream), "update_sigma");
+    fi_status st = run_batch<T>(m, stress_batch);
+    if (st != FI_OK) return st;
+    FI_CHECK_CUDA(launch_update_V<T>(m->g, m->kp, f, m->ib, m->stream), "update_V");
+    st = run_batch<T>(m, velocity_batch);
+    if (st != FI_OK) return st;
+    if (!m->kp.freeze_eta) m->eta_swapped = !m->eta_swapped;
+    return FI_OK;
+}
+
+// The reference-shaped iteration is 2 + 2·nd launches, most of them small
+// boundary batches: on small grids their launch cost exceeds their work.  Two
+// iterations bring η / η_next back to their roles, so a pair is captured once as a
+// CUDA graph (per starting parity of the η buffers, recaptured when the parameters
+// change) and replayed for long advances.
+template <typename T>
+fi_status reference_pairs(fi_model *m, int pairs) {
+    const int e = m->eta_swapped ? 1 : 0;
+    if (!m->pair_graph[e] || std::memcmp(&m->pair_kp[e], &m->kp, sizeof(KParams)) != 0) {
+        if (m->pair_graph[e]) cudaGraphExecDestroy(m->pair_graph[e]);
+        m->pair_graph[e] = nullptr;
+        const bool sw = m->eta_swapped;
+        FI_CHECK_CUDA(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal), "graph capture");
+        fi_status st = reference_iteration<T>(m);
+        if (st == FI_OK) st = reference_iteration<T>(m);
+        cudaGraph_t g = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(m->stream, &g);
+        m->eta_swapped = sw;  // capturing ran nothing
+        if (st != FI_OK) {
+            if (g) cudaGraphDestroy(g);
+            return st;
+        }
+        FI_CHECK_CUDA(ce, "graph capture");
+        const cudaError_t ie = cudaGraphInstantiate(&m->pair_graph[e], g, 0);
+        cudaGraphDestroy(g);
+        FI_CHECK_CUDA(ie, "graph instantiate");
+        m->pair_kp[e] = m->kp;
+    }
+    for (int q = 0; q < pairs; q++) FI_CHECK_CUDA(cudaGraphLaunch(m->pair_graph[e], m->stream), "graph launch");
+    return FI_OK;
+}
+constexpr int kPairGraphMin = 8;  // advances of at least this many iterations replay the graph
+
 template <typename T>
 fi_status advance_t(fi_model *m, int niter) {
     if (fi_status st = refresh_ibf<T>(m); st != FI_OK) return st;
+    if (m->path != FI_PATH_FUSED && niter >= kPairGraphMin) {
+        const int pairs = niter / 2;
+        if (fi_status st = reference_pairs<T>(m, pairs); st != FI_OK) return st;
+        m->iterations += 2LL * pairs;
+        niter -= 2 * pairs;
+    }
     for (int it = 0; it < niter; it++) {
         if (m->path == FI_PATH_FUSED) {
             Ptrs<T> in = m->ptrs<T>(false);
@@ -313,16 +366,11 @@ fi_status advance_t(fi_model *m, int niter) {
             FI_CHECK_CUDA(launch_fused3d<T>(m->g, m->kp, in, out, maps, m->fused_variant, m->d_err, m->stream),
                           "fused sweep");
             m->parity ^= 1;
+            if (!m->kp.freeze_eta) m->eta_swapped = !m->eta_swapped;
         } else {
-            Ptrs<T> f = m->ptrs<T>();
-            FI_CHECK_CUDA(launch_update_sigma<T>(m->g, m->kp, f, m->ib, m->stream), "update_sigma");
-            fi_status st = run_batch<T>(m, stress_batch);
-            if (st != FI_OK) return st;
-            FI_CHECK_CUDA(launch_update_V<T>(m->g, m->kp, f, m->ib, m->stream), "update_V");
-            st = run_batch<T>(m, velocity_batch);
+            fi_status st = reference_iteration<T>(m);
             if (st != FI_OK) return st;
         }
-        if (!m->kp.freeze_eta) m->eta_swapped = !m->eta_swapped;
         m->iterations++;
     }
     return FI_OK;
@@ -539,6 +587,8 @@ fi_status fi_model_destroy(fi_model *m) {
     for (int f = 0; f < kState; f++) field_free(m->alt[f], m->esz);
     if (m->d_err) cudaFree(m->d_err);
     if (m->d_ibf) cudaFree(m->d_ibf);
+    for (cudaGraphExec_t &g : m->pair_graph)
+        if (g) cudaGraphExecDestroy(g);
     field_free(m->fP, m->esz);
     if (m->shadow) fi_model_destroy(m->shadow);
     if (m->d_partials) cudaFree(m->d_partials);

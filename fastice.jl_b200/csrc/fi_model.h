@@ -37,6 +37,10 @@ struct fi_model {
     long long iterations = 0;
     int *d_err = nullptr;  // device error word written by bounded waits
     unsigned char *d_ibf = nullptr;  // immersed-boundary activity byte per grid index (IbFlag bits)
+    // reference-shaped path: two iterations captured as a CUDA graph, one per η
+    // buffer parity at the start of the pair, with the parameters they were captured with
+    cudaGraphExec_t pair_graph[2] = {nullptr, nullptr};
+    KParams pair_kp[2]{};
     bool ibf_stale = true;           // the volume fractions changed since d_ibf was computed
     void *fP = nullptr;    // pressure forcing (defect-correction shadow models only)
     fi_model *shadow = nullptr;  // FP32 model of the mixed-precision solve (created on first use)
