@@ -38,9 +38,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 
 # DRAM bytes per cell of one fused-sweep launch: dram__bytes_read.sum +
 # dram__bytes_write.sum of one ncu-captured 255^3 launch (32x8 tiles, z-blocks of
-# 64, summarised in profiles/fused3d_slab255_ncu_full.md, v4) divided by its cell
+# 32, summarised in profiles/fused3d_slab255_ncu_full.md, v6) divided by its cell
 # count; traffic grows with the cell count, so it scales to 511^3.
-TRAFFIC_BYTES_PER_CELL = {"f64": 236.0, "f32": None}
+TRAFFIC_BYTES_PER_CELL = {"f64": 233.3, "f32": None}
 # DRAM bytes per cell of one immersed-boundary iteration (update_σ!, update_V! and
 # their six boundary launches): dram__bytes_read.sum + dram__bytes_write.sum of
 # one ncu-captured iteration of the 191^3 glacier (FP64) divided by its cell
