@@ -21,6 +21,7 @@ FI_PATH_AUTO, FI_PATH_REFERENCE, FI_PATH_FUSED = 0, 1, 2
 FI_CONV_ABS_INF, FI_CONV_REL_SLAB = 0, 1
 FI_SOLVE_PLAIN, FI_SOLVE_MIXED = 0, 1
 FI_NORMS_LEN = 12
+FI_HALO_ITERATION, FI_HALO_STATE = 0, 1
 
 FIELD_NAMES = (
     "P", "txx", "tyy", "tzz", "txy", "txz", "tyz", "Vx", "Vy", "Vz", "eta", "eta_next",
@@ -153,6 +154,9 @@ SIGNATURES = [
     ("fi_batch_variant_name", C.c_char_p, [C.c_int32]),
     ("fi_batch_set_variant", C.c_int, [C.c_void_p, C.c_int32]),
     ("fi_batch_autotune", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
+    ("fi_model_halo_bytes", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_size_t)]),
+    ("fi_model_halo_pack", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p]),
+    ("fi_model_halo_unpack", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p]),
 ]
 
 _libs = {}

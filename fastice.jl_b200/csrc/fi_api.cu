@@ -445,6 +445,8 @@ bool fused_ok(const fi_model *m) {
 // Second state buffer of every state field, for drivers that double-buffer a
 // model whose own path updates in place (the batched 2D sweep); a new buffer
 // starts as a copy of the current state, ghosts included.
+bool model_field_used(const fi_model *m, int f) { return field_used(m, f); }
+
 fi_status model_ensure_second_state(fi_model *m) {
     for (int f = 0; f < kState; f++) {
         if (!field_used(m, f) || m->alt[f]) continue;

@@ -97,3 +97,5 @@ struct fi_model {
 
 // allocates the second buffer of every state field a model lacks (fi_api.cu)
 fi_status model_ensure_second_state(fi_model *m);
+// whether the model stores field f (fi_api.cu)
+bool model_field_used(const fi_model *m, int f);

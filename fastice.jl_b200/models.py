@@ -26,6 +26,7 @@ from .grids import UniformGrid
 from .physics import (ArrayField, BoundaryCondition, FunctionField, Periodic, ValueField, rheology_desc)
 
 _DTYPES = {"f64": (L.FI_F64, np.float64), "f32": (L.FI_F32, np.float32)}
+_HALO = {"iteration": L.FI_HALO_ITERATION, "state": L.FI_HALO_STATE}
 _PATHS = {"auto": L.FI_PATH_AUTO, "reference": L.FI_PATH_REFERENCE, "fused": L.FI_PATH_FUSED}
 
 
@@ -265,6 +266,25 @@ class _StokesBase:
         L.check(self.lib, self.lib.fi_model_autotune(self._h, int(iters), C.byref(best), ms))
         names = [self.lib.fi_fused_variant_name(v).decode() for v in range(nv)]
         return best.value, dict(zip(names, ms[:]))
+
+    # -- subdomain halo layers (fi_model_halo_*: a slab of a domain split along x or y)
+    def halo_bytes(self, dim: int, side: int, what: str = "iteration") -> int:
+        """Bytes of the halo message packed toward ``side`` (0 = low, 1 = high
+        neighbour) of the split dimension ``dim``; ``what`` is "iteration" (V, η)
+        or "state" (P, τ, V, η)."""
+        b = C.c_size_t()
+        L.check(self.lib, self.lib.fi_model_halo_bytes(self._h, int(dim), int(side), _HALO[what], C.byref(b)))
+        return b.value
+
+    def halo_pack(self, dim: int, side: int, dst_ptr: int, what: str = "iteration") -> None:
+        """Fill the device buffer at ``dst_ptr`` with the message for the neighbour on
+        ``side`` (on the model's stream)."""
+        L.check(self.lib, self.lib.fi_model_halo_pack(self._h, int(dim), int(side), _HALO[what], C.c_void_p(dst_ptr)))
+
+    def halo_unpack(self, dim: int, side: int, src_ptr: int, what: str = "iteration") -> None:
+        """Write the message received from the neighbour on ``side`` (device buffer at
+        ``src_ptr``) into this model's ghost layers (on the model's stream)."""
+        L.check(self.lib, self.lib.fi_model_halo_unpack(self._h, int(dim), int(side), _HALO[what], C.c_void_p(src_ptr)))
 
     @property
     def stream_ptr(self) -> int:

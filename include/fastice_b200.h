@@ -339,6 +339,29 @@ const char *fi_batch_variant_name(int32_t variant);
 fi_status fi_batch_set_variant(fi_batch *b, int32_t variant);
 fi_status fi_batch_autotune(fi_batch *b, int32_t iters, int32_t *best, double *ms);
 
+/* ---- subdomains: halo layers of a domain split into slabs ---------------------
+ * Replaces the halo exchange of the reference's distributed architecture
+ * (Chmy.Distributed exchange_halo! of V and η_next after update_V!,
+ * src/Models/FullStokes/Isothermal/Isothermal.jl:103-104).  A slab is a model of
+ * its own cells whose split dimension (x or y) is declared periodic; after each
+ * PT iteration the caller moves the halo messages between neighbouring slabs (over
+ * NCCL, MPI or a device copy) and unpacks them, replacing the ghost images the
+ * sweep wrote.  Messages are device buffers in the model's dtype.
+ *   fi_model_halo_bytes(m, dim, side, what, &b): size of the message packed toward
+ *       `side` (0 = low neighbour, 1 = high neighbour); the neighbour unpacks it
+ *       from its opposite side
+ *   fi_model_halo_pack(m, dim, side, what, dst): fill that message (on the model's stream)
+ *   fi_model_halo_unpack(m, dim, side, what, src): write the message received from
+ *       the neighbour on `side` into the ghost layers (on the model's stream)
+ * what: FI_HALO_ITERATION (V, η: after every iteration) or FI_HALO_STATE (P, τ, V,
+ * η: once, after the initial state is set).  Slabs run the fused sweep (it recomputes
+ * the ghost stresses from the exchanged velocities); reference-shaped and
+ * immersed-boundary models are rejected with FI_ERR_UNSUPPORTED. */
+typedef enum { FI_HALO_ITERATION = 0, FI_HALO_STATE = 1 } fi_halo_what;
+fi_status fi_model_halo_bytes(const fi_model *m, int32_t dim, int32_t side, int32_t what, size_t *bytes);
+fi_status fi_model_halo_pack(fi_model *m, int32_t dim, int32_t side, int32_t what, void *dst_dev);
+fi_status fi_model_halo_unpack(fi_model *m, int32_t dim, int32_t side, int32_t what, const void *src_dev);
+
 /* ---- level sets and volume fractions (setup path) --------------------------- */
 
 /* ω_from_ψ!(arch, launch, ω, ψ, grid) (LevelSets/volume_fractions_kernels.jl:101-110):

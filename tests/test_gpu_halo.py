@@ -1,0 +1,97 @@
+"""Domain split into slabs (fastice_b200.distributed): slabs of a domain periodic
+along the split dimension, advanced with a halo exchange of V and η after every
+iteration, reproduce the undivided model bit for bit (no-FMA build).  The ranks
+of the ring are emulated in one process: the messages move by device copies,
+through the same pack / unpack entry points a multi-GPU run uses."""
+import numpy as np
+import pytest
+
+from conftest import load_fastice
+from helpers import make_bcs
+
+pytestmark = pytest.mark.gpu
+
+STATE = ("P", "txx", "tyy", "tzz", "txy", "txz", "tyz", "Vx", "Vy", "Vz", "eta")
+PER = ("periodic", ())
+SLIP = ("slip", (0.0, 0.0, 0.0))
+TRAC = ("traction", (0.0, 0.0, 0.0))
+
+
+def _model(fi, n, extent, bcs, path, sp=None):
+    grid = fi.UniformGrid(origin=(0.0, 0.0, 0.0), extent=extent, dims=n)
+    rheo = fi.ViscoplasticRegularisation(fi.PowerLawRheology(1.0, 3), 50.0)
+    # a subdomain iterates with the PT steps of the whole domain (sp)
+    return fi.IsothermalFullStokesModel(grid=grid, boundary_conditions=make_bcs(fi, bcs, 3),
+                                        gravity={"x": -0.17, "y": 0.05, "z": 0.98}, rheology=rheo,
+                                        solver_params=sp or fi.pt_params(grid), dtype="f64", library="strict",
+                                        path=path)
+
+
+def _bits(a):
+    return a.view(np.uint64)
+
+
+@pytest.mark.parametrize("dim,ranks", [(0, 2), (0, 4), (1, 2)])
+def test_split_run_matches_undivided(dim, ranks):
+    path = "fused"
+    fi = load_fastice()
+    from fastice_b200 import distributed as D
+    nl = [24, 16, 14]
+    ng = list(nl)
+    ng[dim] = nl[dim] * ranks
+    ext = [1.0, 0.8, 0.3]
+    ext_l = list(ext)
+    ext_l[dim] = ext[dim] / ranks
+    bcs = ((PER, PER), (PER, PER), (SLIP, TRAC))
+    whole = _model(fi, tuple(ng), tuple(ext), bcs, path)
+    sp = fi.pt_params(whole.grid)
+    slabs = [_model(fi, tuple(nl), tuple(ext_l), bcs, path, sp) for _ in range(ranks)]
+    rng = np.random.default_rng(5 + dim + ranks)
+    for name in STATE:
+        shape = whole.field_shape(name)
+        vals = np.exp(0.3 * rng.standard_normal(shape)) if name == "eta" else 0.1 * rng.standard_normal(shape)
+        whole.set_field(name, vals)
+        loc = fi._lib.FIELD_LOC[name]
+        for r, s in enumerate(slabs):
+            s.set_field(name, np.ascontiguousarray(D.slab_of(vals, dim, r, ranks, loc[dim] == 1)))
+        if name == "eta":
+            whole.set_field("eta_next", vals)
+            for r, s in enumerate(slabs):
+                s.set_field("eta_next", np.ascontiguousarray(D.slab_of(vals, dim, r, ranks, False)))
+    whole.apply_bcs()
+    for s in slabs:
+        s.apply_bcs()
+    D.exchange_local(slabs, dim, "state")
+    for _ in range(6):
+        whole.advance(1)
+        for s in slabs:
+            s.advance(1)
+        D.exchange_local(slabs, dim, "iteration")
+    bad = []
+    for name in STATE:
+        g = whole.get_field(name)
+        loc = fi._lib.FIELD_LOC[name]
+        for r, s in enumerate(slabs):
+            a, b = s.get_field(name), np.ascontiguousarray(D.slab_of(g, dim, r, ranks, loc[dim] == 1))
+            if not np.array_equal(_bits(a), _bits(b)):
+                bad.append((name, r, int(np.sum(a != b))))
+    for m in slabs + [whole]:
+        m.close()
+    assert not bad, bad
+
+
+def test_halo_needs_a_periodic_split_dimension_and_the_fused_sweep():
+    fi = load_fastice()
+    m = _model(fi, (16, 12, 10), (1.0, 1.0, 0.3), ((SLIP, SLIP), (PER, PER), (SLIP, TRAC)), "auto")
+    with pytest.raises(fi.FastIceError):
+        m.halo_bytes(0, 0)
+    with pytest.raises(fi.FastIceError):
+        m.halo_bytes(2, 0)
+    # toward the low side a slab sends two node layers of the fields Vertex-located along y
+    assert m.halo_bytes(1, 0) > m.halo_bytes(1, 1) > 0
+    m.close()
+    # the reference-shaped path fills ghost stresses by the boundary copy: no split
+    r = _model(fi, (16, 12, 10), (1.0, 1.0, 0.3), ((PER, PER), (PER, PER), (SLIP, TRAC)), "reference")
+    with pytest.raises(fi.FastIceError):
+        r.halo_bytes(0, 0)
+    r.close()
