@@ -14,6 +14,10 @@ from .physics import (ArrayField, BoundaryCondition, ConstantField, FunctionFiel
                       PBC, Periodic, PowerLawRheology, Relaxation, SBC, Slip, TBC, Traction, VBC, ValueField, Velocity,
                       ViscoplasticRegularisation, ZeroField, glen_regularised)
 from . import scenarios  # noqa: E402  (seeded problem set-ups over the names above)
+from . import writers  # noqa: E402
+from . import heat  # noqa: E402
+from .heat import HeatDiffusionModel  # noqa: E402
+from .writers import write_h5, write_xdmf  # noqa: E402
 
 __all__ = [
     "FastIceError", "BatchedStokes2D", "Center", "Vertex", "UniformGrid", "flip", "compute_levelset_from_dem", "omega_from_psi", "Arch",
@@ -21,7 +25,7 @@ __all__ = [
     "compute_residuals", "interior", "pt_params", "set_", "ArrayField", "BoundaryCondition", "ConstantField",
     "FunctionField", "LinearViscousRheology", "OneField", "PBC", "Periodic", "PowerLawRheology", "Relaxation", "SBC",
     "Slip", "TBC", "Traction", "VBC", "ValueField", "Velocity", "ViscoplasticRegularisation", "ZeroField",
-    "glen_regularised", "load_library", "scenarios",
+    "glen_regularised", "load_library", "scenarios", "writers", "write_h5", "write_xdmf", "heat", "HeatDiffusionModel",
 ]
 
 

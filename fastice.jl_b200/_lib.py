@@ -22,6 +22,8 @@ FI_CONV_ABS_INF, FI_CONV_REL_SLAB = 0, 1
 FI_SOLVE_PLAIN, FI_SOLVE_MIXED = 0, 1
 FI_NORMS_LEN = 12
 FI_HALO_ITERATION, FI_HALO_STATE = 0, 1
+FI_HEAT_VALUE, FI_HEAT_FLUX = 0, 1
+FI_HEAT_FIELDS = {"T": 0, "T_o": 1, "qx": 2, "qy": 3, "qz": 4}
 
 FIELD_NAMES = (
     "P", "txx", "tyy", "tzz", "txy", "txz", "tyz", "Vx", "Vy", "Vz", "eta", "eta_next",
@@ -109,6 +111,12 @@ class FastIceError(RuntimeError):
         self.status = status
 
 
+class fi_heat_desc(C.Structure):
+    _fields_ = [("grid", fi_grid), ("kind", (C.c_int32 * 2) * 3), ("value", (C.c_double * 2) * 3),
+                ("lambda_rhocp", C.c_double), ("dtau_T", C.c_double), ("dtau_q", C.c_double),
+                ("dtype", C.c_int32), ("device", C.c_int32)]
+
+
 # (name, restype, argtypes) of every exported entry point declared in include/fastice_b200.h
 SIGNATURES = [
     ("fi_last_error", C.c_char_p, []),
@@ -154,6 +162,14 @@ SIGNATURES = [
     ("fi_batch_variant_name", C.c_char_p, [C.c_int32]),
     ("fi_batch_set_variant", C.c_int, [C.c_void_p, C.c_int32]),
     ("fi_batch_autotune", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
+    ("fi_heat_create", C.c_int, [C.POINTER(fi_heat_desc), C.POINTER(C.c_void_p)]),
+    ("fi_heat_destroy", C.c_int, [C.c_void_p]),
+    ("fi_heat_field_size", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_size_t)]),
+    ("fi_heat_set_field", C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_size_t]),
+    ("fi_heat_get_field", C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_size_t]),
+    ("fi_heat_apply_bcs", C.c_int, [C.c_void_p]),
+    ("fi_heat_advance", C.c_int, [C.c_void_p, C.c_int32, C.c_double]),
+    ("fi_heat_synchronize", C.c_int, [C.c_void_p]),
     ("fi_model_halo_bytes", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_size_t)]),
     ("fi_model_halo_pack", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p]),
     ("fi_model_halo_unpack", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p]),

@@ -362,6 +362,37 @@ fi_status fi_model_halo_bytes(const fi_model *m, int32_t dim, int32_t side, int3
 fi_status fi_model_halo_pack(fi_model *m, int32_t dim, int32_t side, int32_t what, void *dst_dev);
 fi_status fi_model_halo_unpack(fi_model *m, int32_t dim, int32_t side, int32_t what, const void *src_dev);
 
+/* ---- heat diffusion (src/Models/Diffusion/Heat/) -------------------------------
+ * HeatDiffusionModel(; grid, boundary_conditions, physics, iter_params) and
+ * advance_iteration!(model, t, Δt) (Heat.jl:26-61, kernels.jl:3-29): the
+ * pseudo-transient flux q and the implicit temperature step, one fused sweep per
+ * iteration.  Boundary kinds BoundaryCondition{Value}(v) (T ghost 2v - T) and
+ * BoundaryCondition{Flux}(v) (q on the boundary face = v), per (dim, side) in the
+ * order west/east, south/north, bottom/top.  Fields are interiors, x fastest: T and
+ * T_o n0 x n1 x n2, q_d with n_d + 1 faces along d.  3D only, as the reference. */
+typedef enum { FI_HEAT_VALUE = 0, FI_HEAT_FLUX = 1 } fi_heat_bc_kind;
+typedef enum { FI_HEAT_T = 0, FI_HEAT_T_OLD = 1, FI_HEAT_QX = 2, FI_HEAT_QY = 3, FI_HEAT_QZ = 4 } fi_heat_field;
+typedef struct {
+    fi_grid grid;
+    int32_t kind[3][2];    /* fi_heat_bc_kind */
+    double value[3][2];
+    double lambda_rhocp;   /* physics λ / (ρ Cp) */
+    double dtau_T, dtau_q; /* iter_params.Δτ.T, iter_params.Δτ.q */
+    int32_t dtype;         /* fi_dtype */
+    int32_t device;
+} fi_heat_desc;
+typedef struct fi_heat fi_heat;
+fi_status fi_heat_create(const fi_heat_desc *desc, fi_heat **out);
+fi_status fi_heat_destroy(fi_heat *h);
+fi_status fi_heat_field_size(const fi_heat *h, int32_t field, size_t *count);
+fi_status fi_heat_set_field(fi_heat *h, int32_t field, const void *host, size_t nbytes);
+fi_status fi_heat_get_field(fi_heat *h, int32_t field, void *host, size_t nbytes);
+/* the Flux faces of q, then the Value ghosts of T (after set_field, as the drivers' _apply_bcs!) */
+fi_status fi_heat_apply_bcs(fi_heat *h);
+/* niter PT iterations of the implicit step of length dt (asynchronous on the model's stream) */
+fi_status fi_heat_advance(fi_heat *h, int32_t niter, double dt);
+fi_status fi_heat_synchronize(fi_heat *h);
+
 /* ---- level sets and volume fractions (setup path) --------------------------- */
 
 /* ω_from_ψ!(arch, launch, ω, ψ, grid) (LevelSets/volume_fractions_kernels.jl:101-110):

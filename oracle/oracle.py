@@ -332,3 +332,58 @@ def levelset_from_dem(n3, o3, dx3, n2, o2, dx2, dem, R=None, cutoff=None):
 def invert_levelset(n3, psi):
     lib().fo_invert_levelset((C.c_int * 3)(*n3), psi.ctypes.data)
     return psi
+
+
+# ----------------------------------------------------------------------------
+# heat diffusion (src/Models/Diffusion/Heat/), oracle/heat.c
+# ----------------------------------------------------------------------------
+class _FoHeat(C.Structure):
+    _fields_ = [("n", C.c_int * 3), ("dx", C.c_double * 3), ("kind", (C.c_int * 2) * 3),
+                ("value", (C.c_double * 2) * 3), ("lam", C.c_double), ("dtau_T", C.c_double),
+                ("dtau_q", C.c_double), ("dt", C.c_double)]
+
+
+class OracleHeat:
+    """Heat state on the CPU oracle: halo-storage arrays T, T_o, qx, qy, qz
+    ((n2+3, n1+3, n0+3), x fastest); kinds 0 = Value, 1 = Flux per (dim, side)."""
+
+    def __init__(self, n, extent, kinds, values, lam, dtau_T, dtau_q, dtype="f64"):
+        self.n = tuple(int(v) for v in n)
+        self.np_dtype = np.float64 if dtype == "f64" else np.float32
+        self.suf = "_" + dtype
+        p = _FoHeat()
+        for k in range(3):
+            p.n[k] = self.n[k]
+            p.dx[k] = extent[k] / self.n[k]
+            for s in range(2):
+                p.kind[k][s] = int(kinds[k][s])
+                p.value[k][s] = float(values[k][s])
+        p.lam, p.dtau_T, p.dtau_q = float(lam), float(dtau_T), float(dtau_q)
+        self.p = p
+        shape = (self.n[2] + 3, self.n[1] + 3, self.n[0] + 3)
+        self.a = {k: np.zeros(shape, self.np_dtype) for k in ("T", "T_o", "qx", "qy", "qz")}
+
+    def _slices(self, name):
+        ext = list(self.n)
+        if name in ("qx", "qy", "qz"):
+            ext["xyz".index(name[1])] += 1
+        return tuple(slice(1, e + 1) for e in reversed(ext))
+
+    def set_interior(self, name, values):
+        self.a[name][self._slices(name)] = values
+
+    def interior(self, name):
+        return self.a[name][self._slices(name)].copy()
+
+    def _ptr(self, k):
+        return self.a[k].ctypes.data_as(C.c_void_p)
+
+    def apply_bcs(self):
+        L = lib()
+        getattr(L, "fo_heat_bc_flux" + self.suf)(C.byref(self.p), self._ptr("qx"), self._ptr("qy"), self._ptr("qz"))
+        getattr(L, "fo_heat_bc_value" + self.suf)(C.byref(self.p), self._ptr("T"))
+
+    def advance(self, niter, dt):
+        self.p.dt = float(dt)
+        getattr(lib(), "fo_heat_advance" + self.suf)(C.byref(self.p), self._ptr("T"), self._ptr("T_o"),
+                                                     self._ptr("qx"), self._ptr("qy"), self._ptr("qz"), int(niter))
