@@ -468,6 +468,62 @@ def run_glacier(args):
     print(json.dumps(line))
 
 
+def run_heat(args):
+    """Heat diffusion (src/Models/Diffusion/Heat/ restated): the implicit step of the
+    driver scripts_future_API/heat_wip.jl (Value sides south/north, Flux 0 elsewhere,
+    λ/(ρCp) = 1, Δt = 1, a Gaussian initial temperature) at n^3 cells; one step = one
+    PT iteration (one fused sweep).  value = T_eff over the 9 array passes of an
+    iteration (T and q(3) read and written, T_o read)."""
+    import torch
+    fi = load_fastice()
+    from fastice_b200 import heat
+    n = args.n
+    dims = (n, n, n)
+    grid = fi.UniformGrid(origin=(-0.5, -0.5, 0.0), extent=(1.0, 1.0, 1.0), dims=dims)
+    sides = {"west": heat.Flux(0.0), "east": heat.Flux(0.0), "south": heat.Value(-0.1), "north": heat.Value(0.3),
+             "bottom": heat.Flux(0.0), "top": heat.Flux(0.0)}
+    dtype = args.dtypes.split(",")[0]
+    m = heat.HeatDiffusionModel(grid=grid, boundary_conditions=sides, physics={"λ_ρCp": 1.0},
+                                iter_params=heat.heat_iter_params(grid, 1.0, 1.0), dtype=dtype)
+    zc = (np.arange(n) + 0.5) / n
+    xc = -0.5 + zc
+    Z, Y, X = np.meshgrid(zc, xc, xc, indexing="ij")
+    T0 = np.exp(-(X / 0.1) ** 2 - (Y / 0.1) ** 2 - ((Z - 0.5) / 0.1) ** 2)
+    m.set_field("T", T0)
+    m.set_field("T_o", T0)
+    for q in ("qx", "qy", "qz"):
+        m.set_field(q, 0.0)
+    m.apply_bcs()
+    m.advance(args.warmup, 1.0)
+    m.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    time.sleep(0.15)
+    stream = torch.cuda.ExternalStream(m.stream_ptr)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    m.advance(args.steps, 1.0)
+    e1.record(stream)
+    e1.synchronize()
+    sec = e0.elapsed_time(e1) / 1e3
+    ck = clocks.stop()
+    m.close()
+    esz = 8 if dtype == "f64" else 4
+    cells = n ** 3
+    a_eff = esz * (2 * cells + cells + 2 * 3 * (n + 1) * n * n)
+    teff = a_eff * args.steps / sec / 1e9
+    peak, peak_kind = measured_peak_hbm()
+    cfg = {"workload": f"heat diffusion {n}^3 cells, implicit step dt = 1 of heat_wip.jl (Value -0.1 / 0.3 on "
+                       "south / north, Flux 0 elsewhere, Gaussian initial temperature), one PT iteration per step",
+           "grid": list(dims), "a_eff_arrays": 9, "l2": "inputs exceed L2 (126 MB): no flush needed"}
+    line = _base_line(f"heat PT T_eff GB/s ({n}^3, {dtype.upper()})", teff, "GB/s", args.steps, args.warmup,
+                      1e3 * sec / args.steps, dtype, cfg)
+    line.update({"gpu_launches": args.steps, "clocks": ck,
+                 "roofline": {"bound": "hbm", "achieved": teff, "peak": peak, "unit": "GB/s", "frac": teff / peak,
+                              "peak_source": peak_kind, "algorithmic_bytes": a_eff}})
+    print(json.dumps(line))
+
+
 def dist_setup():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -487,7 +543,7 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape (profiling runs)")
     ap.add_argument("--variant", type=int, default=None, help="fused launch shape index (implies --no-autotune)")
     ap.add_argument("--dtypes", default="f64,f32", help="precisions to time, FP64 first")
-    ap.add_argument("--workload", choices=("slab", "batched", "serving", "mixed", "glacier"), default="slab",
+    ap.add_argument("--workload", choices=("slab", "batched", "serving", "mixed", "glacier", "heat"), default="slab",
                     help="slab: the headline T_eff line; batched / serving / mixed / glacier: the batched 2D solves, "
                          "the continuous-batching server, the mixed-precision solve and the immersed-boundary "
                          "glacier sweep, one JSON line each")
@@ -501,7 +557,7 @@ def main():
     args = ap.parse_args()
     if args.workload != "slab":
         {"batched": run_batched, "serving": run_serving, "mixed": run_mixed,
-         "glacier": run_glacier}[args.workload](args)
+         "glacier": run_glacier, "heat": run_heat}[args.workload](args)
         return
     n = (args.n, args.n, args.n)
     ws, rank, local = dist_setup()

@@ -170,6 +170,7 @@ SIGNATURES = [
     ("fi_heat_apply_bcs", C.c_int, [C.c_void_p]),
     ("fi_heat_advance", C.c_int, [C.c_void_p, C.c_int32, C.c_double]),
     ("fi_heat_synchronize", C.c_int, [C.c_void_p]),
+    ("fi_heat_stream", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     ("fi_model_halo_bytes", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_size_t)]),
     ("fi_model_halo_pack", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p]),
     ("fi_model_halo_unpack", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p]),

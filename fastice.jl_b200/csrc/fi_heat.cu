@@ -330,6 +330,12 @@ fi_status fi_heat_advance(fi_heat *h, int32_t niter, double dt) {
     return h->esz == 8 ? heat_advance_t<double>(h, niter, dt) : heat_advance_t<float>(h, niter, dt);
 }
 
+fi_status fi_heat_stream(const fi_heat *h, void **stream) {
+    if (!h || !stream) return set_error("bad argument"), FI_ERR_ARG;
+    *stream = (void *)h->stream;
+    return FI_OK;
+}
+
 fi_status fi_heat_synchronize(fi_heat *h) {
     if (!h) return set_error("null model"), FI_ERR_ARG;
     FI_CHECK_CUDA(cudaStreamSynchronize(h->stream), "heat sync");

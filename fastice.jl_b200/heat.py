@@ -103,6 +103,12 @@ class HeatDiffusionModel:
     def advance(self, niter: int, dt: float) -> None:
         L.check(self.lib, self.lib.fi_heat_advance(self._h, int(niter), float(dt)))
 
+    @property
+    def stream_ptr(self) -> int:
+        s = C.c_void_p()
+        L.check(self.lib, self.lib.fi_heat_stream(self._h, C.byref(s)))
+        return s.value or 0
+
     def synchronize(self) -> None:
         L.check(self.lib, self.lib.fi_heat_synchronize(self._h))
 

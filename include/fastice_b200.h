@@ -392,6 +392,8 @@ fi_status fi_heat_apply_bcs(fi_heat *h);
 /* niter PT iterations of the implicit step of length dt (asynchronous on the model's stream) */
 fi_status fi_heat_advance(fi_heat *h, int32_t niter, double dt);
 fi_status fi_heat_synchronize(fi_heat *h);
+/* cudaStream_t of the heat model, as void* */
+fi_status fi_heat_stream(const fi_heat *h, void **stream);
 
 /* ---- level sets and volume fractions (setup path) --------------------------- */
 
