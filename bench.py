@@ -41,11 +41,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 # 32, summarised in profiles/fused3d_slab255_ncu_full.md, v6) divided by its cell
 # count; traffic grows with the cell count, so it scales to 511^3.
 TRAFFIC_BYTES_PER_CELL = {"f64": 233.3, "f32": None}
-# DRAM bytes per cell of one immersed-boundary iteration (update_σ!, update_V! and
-# their six boundary launches): dram__bytes_read.sum + dram__bytes_write.sum of
-# one ncu-captured iteration of the 191^3 glacier (FP64) divided by its cell
-# count (profiles/ib_glacier191_dram.md); the same geometry scales to 383^3.
-IB_TRAFFIC_BYTES_PER_CELL = {"f64": 203.8, "f32": None}
+# DRAM bytes per cell of one steady-state immersed-boundary iteration (update_σ!,
+# update_V! and their six boundary launches, inactive zeros no longer stored,
+# block list in use): dram__bytes_read.sum + dram__bytes_write.sum of one
+# ncu-captured iteration of the 191^3 glacier divided by its cell count
+# (profiles/ib_glacier191_dram.md); the same geometry scales to 383^3.
+IB_TRAFFIC_BYTES_PER_CELL = {"f64": 109.5, "f32": 62.5}
 
 
 def load_fastice():

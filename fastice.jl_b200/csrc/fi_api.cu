@@ -9,6 +9,7 @@
 #include <cstring>
 #include <limits>
 #include <string>
+#include <algorithm>
 #include <vector>
 
 #include "fi_model.h"
@@ -294,6 +295,26 @@ template <typename T>
 fi_status refresh_ibf(fi_model *m) {
     if (!m->ib || !m->ibf_stale) return FI_OK;
     FI_CHECK_CUDA(launch_ib_flags<T>(m->g, m->kp, m->ptrs<T>(), m->d_ibf, m->stream), "activity bytes");
+    // the block list, in z, y, x order (neighbouring blocks run close in time)
+    FI_CHECK_CUDA(cudaMemsetAsync(m->d_bcount, 0, sizeof(int), m->stream), "block count");
+    FI_CHECK_CUDA(launch_ib_blocks(m->g, m->d_ibf, m->d_blist, m->d_bcount, m->stream), "block list");
+    int cnt = 0;
+    FI_CHECK_CUDA(cudaMemcpyAsync(&cnt, m->d_bcount, sizeof(int), cudaMemcpyDeviceToHost, m->stream), "block count");
+    FI_CHECK_CUDA(cudaStreamSynchronize(m->stream), "block count");
+    std::vector<uint2> ids((size_t)cnt);
+    if (cnt > 0) {
+        FI_CHECK_CUDA(cudaMemcpy(ids.data(), m->d_blist, cnt * sizeof(uint2), cudaMemcpyDeviceToHost), "block list");
+        std::sort(ids.begin(), ids.end(), [](const uint2 &a, const uint2 &b) {
+            if (a.y != b.y) return a.y < b.y;
+            if ((a.x >> 16) != (b.x >> 16)) return (a.x >> 16) < (b.x >> 16);
+            return (a.x & 0xffffu) < (b.x & 0xffffu);
+        });
+        FI_CHECK_CUDA(cudaMemcpy(m->d_blist, ids.data(), cnt * sizeof(uint2), cudaMemcpyHostToDevice), "block list");
+    }
+    m->n_blist = cnt;
+    // captured iteration pairs hold the old list's launch size
+    for (cudaGraphExec_t &g : m->pair_graph)
+        if (g) cudaGraphExecDestroy(g), g = nullptr;
     m->ibf_stale = false;
     return FI_OK;
 }
@@ -302,10 +323,15 @@ fi_status refresh_ibf(fi_model *m) {
 template <typename T>
 fi_status reference_iteration(fi_model *m) {
     Ptrs<T> f = m->ptrs<T>();
-    FI_CHECK_CUDA(launch_update_sigma<T>(m->g, m->kp, f, m->ib, m->stream), "update_sigma");
+    // once zeros hold, only the blocks with an active or a boundary point run
+    const BlockList bl{m->d_blist, m->n_blist};
+    // (a relaxed viscosity moves towards its target at every point, so it runs all)
+    const bool eta_moves = !m->kp.freeze_eta && m->kp.rheo_relax != FI_RELAX_NONE;
+    const BlockList *blp = (m->ib && m->kp.skip_zeros && !m->ibf_stale && m->n_blist > 0 && !eta_moves) ? &bl : nullptr;
+    FI_CHECK_CUDA(launch_update_sigma<T>(m->g, m->kp, f, m->ib, m->stream, blp), "update_sigma");
     fi_status st = run_batch<T>(m, stress_batch);
     if (st != FI_OK) return st;
-    FI_CHECK_CUDA(launch_update_V<T>(m->g, m->kp, f, m->ib, m->stream), "update_V");
+    FI_CHECK_CUDA(launch_update_V<T>(m->g, m->kp, f, m->ib, m->stream, blp), "update_V");
     st = run_batch<T>(m, velocity_batch);
     if (st != FI_OK) return st;
     if (!m->kp.freeze_eta) m->eta_swapped = !m->eta_swapped;
@@ -348,6 +374,21 @@ constexpr int kPairGraphMin = 8;  // advances of at least this many iterations r
 template <typename T>
 fi_status advance_t(fi_model *m, int niter) {
     if (fi_status st = refresh_ibf<T>(m); st != FI_OK) return st;
+    if (m->ib && m->path != FI_PATH_FUSED) {
+        // the first two iterations after the state changed write every point; later
+        // ones skip the zeros of the inactive strict interior and the blocks outside
+        // the block list
+        m->kp.skip_zeros = 0;
+        if (!m->state_ptr_out) {
+            while (m->full_iters < 2 && niter > 0) {
+                if (fi_status st = reference_iteration<T>(m); st != FI_OK) return st;
+                m->iterations++;
+                niter--;
+                m->full_iters++;
+            }
+            if (m->full_iters >= 2) m->kp.skip_zeros = 1;
+        }
+    }
     if (m->path != FI_PATH_FUSED && niter >= kPairGraphMin) {
         const int pairs = niter / 2;
         if (fi_status st = reference_pairs<T>(m, pairs); st != FI_OK) return st;
@@ -561,7 +602,9 @@ fi_status fi_model_create(const fi_model_desc *desc, fi_model **out) {
         }
     }
     if (cudaMalloc(&m->d_err, sizeof(int)) != cudaSuccess) return fail(cuda_fail(cudaGetLastError(), "error word"));
-    if (m->ib && cudaMalloc(&m->d_ibf, m->elems) != cudaSuccess)
+    if (m->ib && (cudaMalloc(&m->d_ibf, m->elems) != cudaSuccess ||
+                  cudaMalloc(&m->d_blist, vertex_grid_blocks(g) * sizeof(uint2)) != cudaSuccess ||
+                  cudaMalloc(&m->d_bcount, sizeof(int)) != cudaSuccess))
         return fail(cuda_fail(cudaGetLastError(), "activity bytes"));
     cudaMemsetAsync(m->d_err, 0, sizeof(int), m->stream);
     if (m->path == FI_PATH_FUSED) {
@@ -589,6 +632,8 @@ fi_status fi_model_destroy(fi_model *m) {
     for (int f = 0; f < kState; f++) field_free(m->alt[f], m->esz);
     if (m->d_err) cudaFree(m->d_err);
     if (m->d_ibf) cudaFree(m->d_ibf);
+    if (m->d_blist) cudaFree(m->d_blist);
+    if (m->d_bcount) cudaFree(m->d_bcount);
     for (cudaGraphExec_t &g : m->pair_graph)
         if (g) cudaGraphExecDestroy(g);
     field_free(m->fP, m->esz);
@@ -619,6 +664,7 @@ fi_status fi_model_set_field(fi_model *m, int32_t field, const void *host, size_
     cudaMemcpy3DParms p = copy_params(m, field, m->cur(field), const_cast<void *>(host), true);
     FI_CHECK_CUDA(cudaMemcpy3DAsync(&p, m->stream), "set_field copy");
     FI_CHECK_CUDA(cudaStreamSynchronize(m->stream), "set_field sync");
+    m->full_iters = 0;
     if (field >= FI_FIELD_NA_CCC) m->ibf_stale = true;
     return FI_OK;
 }
@@ -681,7 +727,9 @@ fi_status fi_model_device_ptr(fi_model *m, int32_t field, void **dptr) {
     *dptr = m->cur(field);
     // the caller may write volume fractions through the pointer: their activity
     // bytes are recomputed before the next kernel that reads them
-    if (field >= FI_FIELD_NA_CCC) m->ibf_stale = true;
+    if (field >= FI_FIELD_NA_CCC) m->ibf_stale = true, m->full_iters = 0;
+    // the caller may write the state through the pointer at any later time
+    if (field < kState) m->state_ptr_out = true;
     return FI_OK;
 }
 
@@ -805,6 +853,7 @@ static fi_status fp32_floors(fi_model *s, const double *nn, double *fl_P, double
 }
 
 static fi_status solve_mixed(fi_model *m, const fi_solve_opts *o, fi_solve_report *rep) {
+    m->full_iters = 0;  // the solve writes the FP64 state outside its sweeps
     if (!m->is_f64()) return set_error("the mixed-precision solve refines an FP64 model"), FI_ERR_ARG;
     FI_CHECK_CUDA(cudaSetDevice(m->d.device), "cudaSetDevice");
     fi_status st = make_shadow(m);
@@ -818,7 +867,7 @@ static fi_status solve_mixed(fi_model *m, const fi_solve_opts *o, fi_solve_repor
                                              (float)s->kp.small, m->stream),
                           "shadow volume fractions");
     if (m->ib) {
-        s->ibf_stale = true;
+        s->ibf_stale = true, s->full_iters = 0;
         FI_CHECK_CUDA(cudaStreamSynchronize(m->stream), "shadow volume fractions");
     }
     const long long n = (long long)m->elems;
@@ -856,6 +905,7 @@ static fi_status solve_mixed(fi_model *m, const fi_solve_opts *o, fi_solve_repor
         double best = 1e300;
         int since = 0, done = 0;
         double nn[FI_NORMS_LEN];
+        s->full_iters = 0;  // the shadow's state was set outside its sweeps
         while (done < max_sweeps && sweeps < o->max_iter) {
             int k = std::min(o->ncheck, o->max_iter - sweeps);
             fi_status e = fi_model_advance(s, k);
@@ -1099,7 +1149,7 @@ fi_status fi_model_volfrac_from_levelset(fi_model *m, int32_t group, const doubl
     e = cudaStreamSynchronize(m->stream);
     cleanup();
     if (e != cudaSuccess) return cuda_fail(e, "volfrac sync");
-    m->ibf_stale = true;
+    m->ibf_stale = true, m->full_iters = 0;
     return FI_OK;
 }
 

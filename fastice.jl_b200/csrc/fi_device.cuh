@@ -43,6 +43,12 @@ __device__ __forceinline__ T rheology_dev(const KParams &p, const T *eta_lin, co
     return inner;
 }
 
+// A linear viscosity with neither regularisation nor relaxation: the new
+// viscosity is the linear one, whatever the stresses (rheology_dev above).
+__device__ __forceinline__ bool linear_unrelaxed(const KParams &p) {
+    return p.rheo_inner == FI_RHEO_LINEAR && !p.rheo_has_reg && p.rheo_relax == FI_RELAX_NONE;
+}
+
 template <typename T>
 __device__ __forceinline__ T gravity_dev(const KParams &p, const T *arr, int c, long long I) {
     return p.g_kind[c] == FI_G_FIELD ? arr[I] : T(p.g_val[c]);

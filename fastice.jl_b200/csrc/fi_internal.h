@@ -48,6 +48,9 @@ struct KParams {
     double small;  // immersed-boundary emptiness threshold (1e-6, or the FP32 value equivalent to it)
     int freeze_eta;  // 1: η is held fixed (no η_next is computed or written)
     int p_forcing;   // 1: the pressure update and r_P carry the forcing field fP (defect correction)
+    int skip_zeros;  // 1: the immersed-boundary updates leave inactive points of the strict interior
+                     // (index 2..n in every dimension) unwritten: they hold zero since the last
+                     // iteration that wrote them (set by the model, never by a caller)
 };
 
 // the scalar parameters converted once to the compute type T (the conversion
@@ -107,6 +110,7 @@ struct BcOpDesc {
 struct BcBatch {
     int count;
     int dim;
+    int serial;  // set by launch_bc_batch: one thread applies every op in order
     BcOpDesc ops[kMaxBcOps];
 };
 
@@ -121,11 +125,29 @@ inline float small_threshold_f32() {
 void set_error(const std::string &msg);
 fi_status cuda_fail(cudaError_t e, const char *where);
 
+// Blocks (32x8 points of one z plane) of the vertex-range grid that an
+// immersed-boundary update must run once the inactive strict interior holds
+// zero: those with an active point or a point outside the strict interior.
+// Entry: x = block x | block y << 16, y = block z.
+struct BlockList {
+    const uint2 *ids;
+    int count;
+};
+
 // ---- launchers implemented in fi_reference.cu ----
+// bl: run only the listed blocks (immersed boundary with KParams::skip_zeros);
+// nullptr: the whole vertex-range grid
 template <typename T>
-cudaError_t launch_update_sigma(const Geom &g, const KParams &p, const Ptrs<T> &f, bool ib, cudaStream_t s);
+cudaError_t launch_update_sigma(const Geom &g, const KParams &p, const Ptrs<T> &f, bool ib, cudaStream_t s,
+                                const BlockList *bl = nullptr);
 template <typename T>
-cudaError_t launch_update_V(const Geom &g, const KParams &p, const Ptrs<T> &f, bool ib, cudaStream_t s);
+cudaError_t launch_update_V(const Geom &g, const KParams &p, const Ptrs<T> &f, bool ib, cudaStream_t s,
+                            const BlockList *bl = nullptr);
+// the block list of an immersed-boundary model from its activity bytes; *count
+// is device memory, the list unordered
+cudaError_t launch_ib_blocks(const Geom &g, const unsigned char *flags, uint2 *list, int *count, cudaStream_t s);
+// number of blocks of the vertex-range grid (the list's capacity)
+long long vertex_grid_blocks(const Geom &g);
 template <typename T>
 cudaError_t launch_compute_residuals(const Geom &g, const KParams &p, const Ptrs<T> &f, bool ib, cudaStream_t s);
 template <typename T>

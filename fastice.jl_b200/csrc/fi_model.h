@@ -37,11 +37,22 @@ struct fi_model {
     long long iterations = 0;
     int *d_err = nullptr;  // device error word written by bounded waits
     unsigned char *d_ibf = nullptr;  // immersed-boundary activity byte per grid index (IbFlag bits)
+    uint2 *d_blist = nullptr;        // blocks an immersed-boundary update runs once zeros hold (BlockList)
+    int *d_bcount = nullptr;
+    int n_blist = 0;
     // reference-shaped path: two iterations captured as a CUDA graph, one per η
     // buffer parity at the start of the pair, with the parameters they were captured with
     cudaGraphExec_t pair_graph[2] = {nullptr, nullptr};
     KParams pair_kp[2]{};
     bool ibf_stale = true;           // the volume fractions changed since d_ibf was computed
+    // Full immersed-boundary iterations since anything else wrote the state, η or
+    // the volume fractions.  After one, inactive strict-interior points of P, τ, V
+    // hold zero (boundary batches write only indices 0, 1, n+1, n+2 of their
+    // dimension, so they never break it); after two, both η buffers hold the
+    // viscosity of every point outside the block list.  A state pointer handed to
+    // a caller ends both for good.
+    int full_iters = 0;
+    bool state_ptr_out = false;
     void *fP = nullptr;    // pressure forcing (defect-correction shadow models only)
     fi_model *shadow = nullptr;  // FP32 model of the mixed-precision solve (created on first use)
     KParams shadow_kp{};         // the shadow's parameters as created (gravity as fields); each solve starts from them

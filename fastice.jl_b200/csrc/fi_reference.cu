@@ -22,14 +22,29 @@ struct Idx {
     bool ok;
 };
 
-__device__ __forceinline__ Idx vertex_index(const Geom &g) {
+__device__ __forceinline__ Idx vertex_index_of(const Geom &g, unsigned bx, unsigned by, unsigned bz) {
     Idx r;
-    r.i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    r.j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-    r.k = g.nd == 3 ? (int)blockIdx.z + 1 : 0;
+    r.i = bx * blockDim.x + threadIdx.x + 1;
+    r.j = by * blockDim.y + threadIdx.y + 1;
+    r.k = g.nd == 3 ? (int)bz + 1 : 0;
     r.ok = r.i <= g.n[0] + 1 && r.j <= g.n[1] + 1;
     r.I = (long long)r.i + g.pitch * ((long long)r.j + g.rows * (long long)r.k);
     return r;
+}
+
+__device__ __forceinline__ Idx vertex_index(const Geom &g) { return vertex_index_of(g, blockIdx.x, blockIdx.y, blockIdx.z); }
+
+// the point of this thread in a launch over the whole grid or over a block list
+__device__ __forceinline__ Idx vertex_index(const Geom &g, const BlockList &bl) {
+    if (!bl.ids) return vertex_index(g);
+    const uint2 b = bl.ids[blockIdx.x];
+    return vertex_index_of(g, b.x & 0xffffu, b.x >> 16, b.y);
+}
+
+// an inactive point whose zero need not be stored again (KParams::skip_zeros):
+// strictly inside in every dimension, where no boundary batch writes
+__device__ __forceinline__ bool skip_zero_store(const Geom &g, const KParams &p, const Idx &x) {
+    return p.skip_zeros && x.i >= 2 && x.i <= g.n[0] && x.j >= 2 && x.j <= g.n[1] && x.k >= 2 && x.k <= g.n[2];
 }
 
 dim3 vertex_grid(const Geom &g, dim3 blk) {
@@ -37,11 +52,113 @@ dim3 vertex_grid(const Geom &g, dim3 blk) {
 }
 
 // ---------------------------------------------------------------------------
-// update_σ!  (kernels_3d.jl:3-25, kernels_2d.jl:3-18; IB: IB kernels_3d.jl:3-44)
+// Immersed-boundary bodies of update_σ! and update_V! (IB kernels_3d.jl:3-74).
+// The activity byte gates each masked group; a group's stores come before the
+// next group's loads (the outputs may alias the inputs as far as the compiler
+// knows), so a thread makes several dependent round trips to memory with few
+// registers.  Forms that load every input first (per thread with predicated
+// loads, or per warp with unconditional loads) were measured slower in both
+// precisions: the extra registers cost more occupancy than the shorter chain
+// gains.
 // ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void ib_sigma(const KParams &p, const Ptrs<T> &f, long long I, long long sx,
+                                         long long sxy, T idx, T idy, T idz, bool skip0) {
+    const T *Vx = f.Vx, *Vy = f.Vy, *Vz = f.Vz, *eta = f.eta;
+    const T *const *ns = f.wns;
+    const unsigned fl = ib_flags_at(f, I, sx, sxy, T(p.small));
+    if (fl & IBF_S_CCC) {
+        T exx = (ns[W_VCC][I + 1] * Vx[I + 1] - ns[W_VCC][I] * Vx[I]) * idx;
+        T eyy = (ns[W_CVC][I + sx] * Vy[I + sx] - ns[W_CVC][I] * Vy[I]) * idy;
+        T ezz = (ns[W_CCV][I + sxy] * Vz[I + sxy] - ns[W_CCV][I] * Vz[I]) * idz;
+        T divV = exx + eyy + ezz;
+        T etac = eta[I];
+        f.P[I] = f.P[I] - (p.p_forcing ? divV + f.fP[I] : divV) * etac * T(p.dt_P);
+        f.txx[I] = f.txx[I] - (f.txx[I] - T(2.0) * etac * (exx - third(divV))) * T(p.dt_tau[0]);
+        f.tyy[I] = f.tyy[I] - (f.tyy[I] - T(2.0) * etac * (eyy - third(divV))) * T(p.dt_tau[1]);
+        f.tzz[I] = f.tzz[I] - (f.tzz[I] - T(2.0) * etac * (ezz - third(divV))) * T(p.dt_tau[2]);
+    } else if (!skip0) {
+        f.P[I] = T(0);
+        f.txx[I] = T(0);
+        f.tyy[I] = T(0);
+        f.tzz[I] = T(0);
+    }
+    if (fl & IBF_S_VVC) {
+        T exy = T(0.5) * ((ns[W_CVC][I] * Vy[I] - ns[W_CVC][I - 1] * Vy[I - 1]) * idx +
+                          (ns[W_VCC][I] * Vx[I] - ns[W_VCC][I - sx] * Vx[I - sx]) * idy);
+        T e_xy = h(h(eta[I - 1 - sx] + eta[I - sx]) + h(eta[I - 1] + eta[I]));
+        f.txy[I] = f.txy[I] - (f.txy[I] - T(2.0) * e_xy * exy) * T(p.dt_tau[3]);
+    } else if (!skip0) {
+        f.txy[I] = T(0);
+    }
+    if (fl & IBF_S_VCV) {
+        T exz = T(0.5) * ((ns[W_CCV][I] * Vz[I] - ns[W_CCV][I - 1] * Vz[I - 1]) * idx +
+                          (ns[W_VCC][I] * Vx[I] - ns[W_VCC][I - sxy] * Vx[I - sxy]) * idz);
+        T e_xz = h(h(eta[I - 1 - sxy] + eta[I - sxy]) + h(eta[I - 1] + eta[I]));
+        f.txz[I] = f.txz[I] - (f.txz[I] - T(2.0) * e_xz * exz) * T(p.dt_tau[4]);
+    } else if (!skip0) {
+        f.txz[I] = T(0);
+    }
+    if (fl & IBF_S_CVV) {
+        T eyz = T(0.5) * ((ns[W_CCV][I] * Vz[I] - ns[W_CCV][I - sx] * Vz[I - sx]) * idy +
+                          (ns[W_CVC][I] * Vy[I] - ns[W_CVC][I - sxy] * Vy[I - sxy]) * idz);
+        T e_yz = h(h(eta[I - sx - sxy] + eta[I - sxy]) + h(eta[I - sx] + eta[I]));
+        f.tyz[I] = f.tyz[I] - (f.tyz[I] - T(2.0) * e_yz * eyz) * T(p.dt_tau[5]);
+    } else if (!skip0) {
+        f.tyz[I] = T(0);
+    }
+}
+
+// update_V! of an immersed-boundary model: the velocities (the viscosity follows in the kernel)
+template <typename T>
+__device__ __forceinline__ void ib_V(const KParams &p, const Ptrs<T> &f, long long I, long long sx, long long sxy,
+                                     T idx, T idy, T idz, T gx, T gy, T gz, bool skip0) {
+    const T *P = f.P, *txx = f.txx, *tyy = f.tyy, *tzz = f.tzz, *txy = f.txy, *txz = f.txz, *tyz = f.tyz, *eta = f.eta;
+    const T *const *na = f.wna;
+    const T *const *ns = f.wns;
+    const T *wc = na[W_CCC], *wvvc = na[W_VVC], *wvcv = na[W_VCV], *wcvv = na[W_CVV];
+    const unsigned fl = ib_flags_at(f, I, sx, sxy, T(p.small));
+    if (fl & IBF_V_VCC) {
+        T ex = h(eta[I - 1] + eta[I]);
+        f.Vx[I] = f.Vx[I] + div_fast(div_fast(-(wc[I] * P[I] - wc[I - 1] * P[I - 1]) * idx +
+                                                  (wc[I] * txx[I] - wc[I - 1] * txx[I - 1]) * idx +
+                                                  (wvvc[I + sx] * txy[I + sx] - wvvc[I] * txy[I]) * idy +
+                                                  (wvcv[I + sxy] * txz[I + sxy] - wvcv[I] * txz[I]) * idz - gx,
+                                              ex),
+                                     ns[W_VCC][I]) *
+                                T(p.dt_V[0]);
+    } else if (!skip0) {
+        f.Vx[I] = T(0);
+    }
+    if (fl & IBF_V_CVC) {
+        T ey = h(eta[I - sx] + eta[I]);
+        f.Vy[I] = f.Vy[I] + div_fast(div_fast(-(wc[I] * P[I] - wc[I - sx] * P[I - sx]) * idy +
+                                                  (wc[I] * tyy[I] - wc[I - sx] * tyy[I - sx]) * idy +
+                                                  (wvvc[I + 1] * txy[I + 1] - wvvc[I] * txy[I]) * idx +
+                                                  (wcvv[I + sxy] * tyz[I + sxy] - wcvv[I] * tyz[I]) * idz - gy,
+                                              ey),
+                                     ns[W_CVC][I]) *
+                                T(p.dt_V[1]);
+    } else if (!skip0) {
+        f.Vy[I] = T(0);
+    }
+    if (fl & IBF_V_CCV) {
+        T ez = h(eta[I - sxy] + eta[I]);
+        f.Vz[I] = f.Vz[I] + div_fast(div_fast(-(wc[I] * P[I] - wc[I - sxy] * P[I - sxy]) * idz +
+                                                  (wc[I] * tzz[I] - wc[I - sxy] * tzz[I - sxy]) * idz +
+                                                  (wvcv[I + 1] * txz[I + 1] - wvcv[I] * txz[I]) * idx +
+                                                  (wcvv[I + sx] * tyz[I + sx] - wcvv[I] * tyz[I]) * idy - gz,
+                                              ez),
+                                     ns[W_CCV][I]) *
+                                T(p.dt_V[2]);
+    } else if (!skip0) {
+        f.Vz[I] = T(0);
+    }
+}
+
 template <typename T, int ND, bool IB>
-__global__ void __launch_bounds__(256) update_sigma_kernel(Geom g, KParams p, Ptrs<T> f) {
-    Idx x = vertex_index(g);
+__global__ void __launch_bounds__(256) update_sigma_kernel(Geom g, KParams p, Ptrs<T> f, BlockList bl) {
+    Idx x = vertex_index(g, bl);
     if (!x.ok) return;
     const long long I = x.I, sx = g.pitch, sxy = g.sxy;
     const T idx = T(p.inv_dx[0]), idy = T(p.inv_dx[1]);
@@ -53,8 +170,8 @@ __global__ void __launch_bounds__(256) update_sigma_kernel(Geom g, KParams p, Pt
         T divV = exx + eyy;
         T etac = eta[I];
         f.P[I] = f.P[I] - (p.p_forcing ? divV + f.fP[I] : divV) * etac * T(p.dt_P);
-        f.txx[I] = f.txx[I] - (f.txx[I] - T(2.0) * etac * (exx - divV / T(3.0))) * T(p.dt_tau[0]);
-        f.tyy[I] = f.tyy[I] - (f.tyy[I] - T(2.0) * etac * (eyy - divV / T(3.0))) * T(p.dt_tau[1]);
+        f.txx[I] = f.txx[I] - (f.txx[I] - T(2.0) * etac * (exx - third(divV))) * T(p.dt_tau[0]);
+        f.tyy[I] = f.tyy[I] - (f.tyy[I] - T(2.0) * etac * (eyy - third(divV))) * T(p.dt_tau[1]);
         T exy_eta = h(h(eta[I - 1 - sx] + eta[I - sx]) + h(eta[I - 1] + eta[I]));
         f.txy[I] = f.txy[I] - (f.txy[I] - T(2.0) * exy_eta * exy) * T(p.dt_tau[3]);
         return;
@@ -72,9 +189,9 @@ __global__ void __launch_bounds__(256) update_sigma_kernel(Geom g, KParams p, Pt
         T divV = exx + eyy + ezz;
         T etac = eta[I];
         f.P[I] = f.P[I] - (p.p_forcing ? divV + f.fP[I] : divV) * etac * T(p.dt_P);
-        f.txx[I] = f.txx[I] - (f.txx[I] - T(2.0) * etac * (exx - divV / T(3.0))) * T(p.dt_tau[0]);
-        f.tyy[I] = f.tyy[I] - (f.tyy[I] - T(2.0) * etac * (eyy - divV / T(3.0))) * T(p.dt_tau[1]);
-        f.tzz[I] = f.tzz[I] - (f.tzz[I] - T(2.0) * etac * (ezz - divV / T(3.0))) * T(p.dt_tau[2]);
+        f.txx[I] = f.txx[I] - (f.txx[I] - T(2.0) * etac * (exx - third(divV))) * T(p.dt_tau[0]);
+        f.tyy[I] = f.tyy[I] - (f.tyy[I] - T(2.0) * etac * (eyy - third(divV))) * T(p.dt_tau[1]);
+        f.tzz[I] = f.tzz[I] - (f.tzz[I] - T(2.0) * etac * (ezz - third(divV))) * T(p.dt_tau[2]);
         T e_xy = h(h(eta[I - 1 - sx] + eta[I - sx]) + h(eta[I - 1] + eta[I]));
         T e_xz = h(h(eta[I - 1 - sxy] + eta[I - sxy]) + h(eta[I - 1] + eta[I]));
         T e_yz = h(h(eta[I - sx - sxy] + eta[I - sxy]) + h(eta[I - sx] + eta[I]));
@@ -83,56 +200,21 @@ __global__ void __launch_bounds__(256) update_sigma_kernel(Geom g, KParams p, Pt
         f.tyz[I] = f.tyz[I] - (f.tyz[I] - T(2.0) * e_yz * eyz) * T(p.dt_tau[5]);
         return;
     }
-    const T *const *ns = f.wns;
-    const unsigned fl = ib_flags_at(f, I, sx, sxy, thr);
-    if (fl & IBF_S_CCC) {
-        T exx = (ns[W_VCC][I + 1] * Vx[I + 1] - ns[W_VCC][I] * Vx[I]) * idx;
-        T eyy = (ns[W_CVC][I + sx] * Vy[I + sx] - ns[W_CVC][I] * Vy[I]) * idy;
-        T ezz = (ns[W_CCV][I + sxy] * Vz[I + sxy] - ns[W_CCV][I] * Vz[I]) * idz;
-        T divV = exx + eyy + ezz;
-        T etac = eta[I];
-        f.P[I] = f.P[I] - (p.p_forcing ? divV + f.fP[I] : divV) * etac * T(p.dt_P);
-        f.txx[I] = f.txx[I] - (f.txx[I] - T(2.0) * etac * (exx - divV / T(3.0))) * T(p.dt_tau[0]);
-        f.tyy[I] = f.tyy[I] - (f.tyy[I] - T(2.0) * etac * (eyy - divV / T(3.0))) * T(p.dt_tau[1]);
-        f.tzz[I] = f.tzz[I] - (f.tzz[I] - T(2.0) * etac * (ezz - divV / T(3.0))) * T(p.dt_tau[2]);
-    } else {
-        f.P[I] = T(0);
-        f.txx[I] = T(0);
-        f.tyy[I] = T(0);
-        f.tzz[I] = T(0);
-    }
-    if (fl & IBF_S_VVC) {
-        T exy = T(0.5) * ((ns[W_CVC][I] * Vy[I] - ns[W_CVC][I - 1] * Vy[I - 1]) * idx +
-                          (ns[W_VCC][I] * Vx[I] - ns[W_VCC][I - sx] * Vx[I - sx]) * idy);
-        T e_xy = h(h(eta[I - 1 - sx] + eta[I - sx]) + h(eta[I - 1] + eta[I]));
-        f.txy[I] = f.txy[I] - (f.txy[I] - T(2.0) * e_xy * exy) * T(p.dt_tau[3]);
-    } else {
-        f.txy[I] = T(0);
-    }
-    if (fl & IBF_S_VCV) {
-        T exz = T(0.5) * ((ns[W_CCV][I] * Vz[I] - ns[W_CCV][I - 1] * Vz[I - 1]) * idx +
-                          (ns[W_VCC][I] * Vx[I] - ns[W_VCC][I - sxy] * Vx[I - sxy]) * idz);
-        T e_xz = h(h(eta[I - 1 - sxy] + eta[I - sxy]) + h(eta[I - 1] + eta[I]));
-        f.txz[I] = f.txz[I] - (f.txz[I] - T(2.0) * e_xz * exz) * T(p.dt_tau[4]);
-    } else {
-        f.txz[I] = T(0);
-    }
-    if (fl & IBF_S_CVV) {
-        T eyz = T(0.5) * ((ns[W_CCV][I] * Vz[I] - ns[W_CCV][I - sx] * Vz[I - sx]) * idy +
-                          (ns[W_CVC][I] * Vy[I] - ns[W_CVC][I - sxy] * Vy[I - sxy]) * idz);
-        T e_yz = h(h(eta[I - sx - sxy] + eta[I - sxy]) + h(eta[I - sx] + eta[I]));
-        f.tyz[I] = f.tyz[I] - (f.tyz[I] - T(2.0) * e_yz * eyz) * T(p.dt_tau[5]);
-    } else {
-        f.tyz[I] = T(0);
-    }
+    if constexpr (IB) ib_sigma(p, f, I, sx, sxy, idx, idy, idz, skip_zero_store(g, p, x));
 }
 
 // ---------------------------------------------------------------------------
 // update_V!  (kernels_3d.jl:27-40, kernels_2d.jl:20-29; IB kernels_3d.jl:46-74)
 // ---------------------------------------------------------------------------
+// resident blocks per SM asked of the compiler: 6 (40 registers) for the 2D and
+// immersed-boundary forms, 5 (48) for the plain 3D form
+template <int ND, bool IB>
+constexpr int update_V_min_blocks() { return (ND == 2 || IB) ? 6 : 5; }
+
 template <typename T, int ND, bool IB>
-__global__ void __launch_bounds__(256) update_V_kernel(Geom g, KParams p, Ptrs<T> f) {
-    Idx x = vertex_index(g);
+__global__ void __launch_bounds__(256, update_V_min_blocks<ND, IB>()) update_V_kernel(Geom g, KParams p, Ptrs<T> f,
+                                                                                   BlockList bl) {
+    Idx x = vertex_index(g, bl);
     if (!x.ok) return;
     const long long I = x.I, sx = g.pitch, sxy = g.sxy;
     const T idx = T(p.inv_dx[0]), idy = T(p.inv_dx[1]);
@@ -142,15 +224,19 @@ __global__ void __launch_bounds__(256) update_V_kernel(Geom g, KParams p, Ptrs<T
         T ex = h(eta[I - 1] + eta[I]);
         T ey = h(eta[I - sx] + eta[I]);
         f.Vx[I] = f.Vx[I] +
-                  div_dev(-(P[I] - P[I - 1]) * idx + (txx[I] - txx[I - 1]) * idx + (txy[I + sx] - txy[I]) * idy - gx, ex) *
+                  div_fast(-(P[I] - P[I - 1]) * idx + (txx[I] - txx[I - 1]) * idx + (txy[I + sx] - txy[I]) * idy - gx, ex) *
                       T(p.dt_V[0]);
         f.Vy[I] = f.Vy[I] +
-                  div_dev(-(P[I] - P[I - sx]) * idy + (tyy[I] - tyy[I - sx]) * idy + (txy[I + 1] - txy[I]) * idx - gy, ey) *
+                  div_fast(-(P[I] - P[I - sx]) * idy + (tyy[I] - tyy[I - sx]) * idy + (txy[I + 1] - txy[I]) * idx - gy, ey) *
                       T(p.dt_V[1]);
+        if (p.freeze_eta) return;
+        if (linear_unrelaxed(p)) {
+            f.eta_next[I] = p.rheo_eta_is_field ? f.eta_lin[I] : T(p.rheo_eta);
+            return;
+        }
         T lxy = h(h(txy[I] + txy[I + 1]) + h(txy[I + sx] + txy[I + sx + 1]));
         T s2 = T(0.5) * (txx[I] * txx[I] + tyy[I] * tyy[I]) + lxy * lxy;
-        if (!p.freeze_eta)
-            f.eta_next[I] = rheology_s2(p, T(p.rheo_A), T(p.rheo_inv_eta_reg), f.eta_lin, f.A, eta[I], I, s2);
+        f.eta_next[I] = rheology_s2(p, T(p.rheo_A), T(p.rheo_inv_eta_reg), f.eta_lin, f.A, eta[I], I, s2);
         return;
     }
     const T idz = T(p.inv_dx[2]);
@@ -160,66 +246,31 @@ __global__ void __launch_bounds__(256) update_V_kernel(Geom g, KParams p, Ptrs<T
         T ex = h(eta[I - 1] + eta[I]);
         T ey = h(eta[I - sx] + eta[I]);
         T ez = h(eta[I - sxy] + eta[I]);
-        f.Vx[I] = f.Vx[I] + div_dev(-(P[I] - P[I - 1]) * idx + (txx[I] - txx[I - 1]) * idx + (txy[I + sx] - txy[I]) * idy +
+        f.Vx[I] = f.Vx[I] + div_fast(-(P[I] - P[I - 1]) * idx + (txx[I] - txx[I - 1]) * idx + (txy[I + sx] - txy[I]) * idy +
                                         (txz[I + sxy] - txz[I]) * idz - gx,
                                     ex) *
                                 T(p.dt_V[0]);
-        f.Vy[I] = f.Vy[I] + div_dev(-(P[I] - P[I - sx]) * idy + (tyy[I] - tyy[I - sx]) * idy + (txy[I + 1] - txy[I]) * idx +
+        f.Vy[I] = f.Vy[I] + div_fast(-(P[I] - P[I - sx]) * idy + (tyy[I] - tyy[I - sx]) * idy + (txy[I + 1] - txy[I]) * idx +
                                         (tyz[I + sxy] - tyz[I]) * idz - gy,
                                     ey) *
                                 T(p.dt_V[1]);
-        f.Vz[I] = f.Vz[I] + div_dev(-(P[I] - P[I - sxy]) * idz + (tzz[I] - tzz[I - sxy]) * idz + (txz[I + 1] - txz[I]) * idx +
+        f.Vz[I] = f.Vz[I] + div_fast(-(P[I] - P[I - sxy]) * idz + (tzz[I] - tzz[I - sxy]) * idz + (txz[I + 1] - txz[I]) * idx +
                                         (tyz[I + sx] - tyz[I]) * idy - gz,
                                     ez) *
                                 T(p.dt_V[2]);
     } else {
-        const T *const *na = f.wna;
-        const T *const *ns = f.wns;
-        const T thr = T(p.small);
-        const T *wc = na[W_CCC], *wvvc = na[W_VVC], *wvcv = na[W_VCV], *wcvv = na[W_CVV];
-        const unsigned fl = ib_flags_at(f, I, sx, sxy, thr);
-        if (fl & IBF_V_VCC) {
-            T ex = h(eta[I - 1] + eta[I]);
-            f.Vx[I] = f.Vx[I] + div_dev(div_dev(-(wc[I] * P[I] - wc[I - 1] * P[I - 1]) * idx +
-                                                    (wc[I] * txx[I] - wc[I - 1] * txx[I - 1]) * idx +
-                                                    (wvvc[I + sx] * txy[I + sx] - wvvc[I] * txy[I]) * idy +
-                                                    (wvcv[I + sxy] * txz[I + sxy] - wvcv[I] * txz[I]) * idz - gx,
-                                                ex),
-                                        ns[W_VCC][I]) *
-                                    T(p.dt_V[0]);
-        } else {
-            f.Vx[I] = T(0);
-        }
-        if (fl & IBF_V_CVC) {
-            T ey = h(eta[I - sx] + eta[I]);
-            f.Vy[I] = f.Vy[I] + div_dev(div_dev(-(wc[I] * P[I] - wc[I - sx] * P[I - sx]) * idy +
-                                                    (wc[I] * tyy[I] - wc[I - sx] * tyy[I - sx]) * idy +
-                                                    (wvvc[I + 1] * txy[I + 1] - wvvc[I] * txy[I]) * idx +
-                                                    (wcvv[I + sxy] * tyz[I + sxy] - wcvv[I] * tyz[I]) * idz - gy,
-                                                ey),
-                                        ns[W_CVC][I]) *
-                                    T(p.dt_V[1]);
-        } else {
-            f.Vy[I] = T(0);
-        }
-        if (fl & IBF_V_CCV) {
-            T ez = h(eta[I - sxy] + eta[I]);
-            f.Vz[I] = f.Vz[I] + div_dev(div_dev(-(wc[I] * P[I] - wc[I - sxy] * P[I - sxy]) * idz +
-                                                    (wc[I] * tzz[I] - wc[I - sxy] * tzz[I - sxy]) * idz +
-                                                    (wvcv[I + 1] * txz[I + 1] - wvcv[I] * txz[I]) * idx +
-                                                    (wcvv[I + sx] * tyz[I + sx] - wcvv[I] * tyz[I]) * idy - gz,
-                                                ez),
-                                        ns[W_CCV][I]) *
-                                    T(p.dt_V[2]);
-        } else {
-            f.Vz[I] = T(0);
-        }
+        ib_V(p, f, I, sx, sxy, idx, idy, idz, gx, gy, gz, skip_zero_store(g, p, x));
+    }
+    if (p.freeze_eta) return;
+    if (linear_unrelaxed(p)) {  // the stress invariant is not needed
+        f.eta_next[I] = p.rheo_eta_is_field ? f.eta_lin[I] : T(p.rheo_eta);
+        return;
     }
     T lxy = h(h(txy[I] + txy[I + 1]) + h(txy[I + sx] + txy[I + sx + 1]));
     T lxz = h(h(txz[I] + txz[I + 1]) + h(txz[I + sxy] + txz[I + sxy + 1]));
     T lyz = h(h(tyz[I] + tyz[I + sx]) + h(tyz[I + sxy] + tyz[I + sxy + sx]));
     T s = T(0.5) * (txx[I] * txx[I] + tyy[I] * tyy[I] + tzz[I] * tzz[I]) + lxy * lxy + lxz * lxz + lyz * lyz;
-    if (!p.freeze_eta) f.eta_next[I] = rheology_s2(p, T(p.rheo_A), T(p.rheo_inv_eta_reg), f.eta_lin, f.A, eta[I], I, s);
+    f.eta_next[I] = rheology_s2(p, T(p.rheo_A), T(p.rheo_inv_eta_reg), f.eta_lin, f.A, eta[I], I, s);
 }
 
 // ---------------------------------------------------------------------------
@@ -395,6 +446,10 @@ __global__ void __launch_bounds__(256) compute_tau_ib_kernel(Geom g, KParams p, 
 // Boundary-condition batch for one dimension: the face of dim d spans the full
 // storage range of the dims before d and the interior range of the dims after
 // d (per field location); left and right sides of every field in the batch.
+// Each op of the batch has its own grid slice (blockIdx.z): the ops of a batch
+// touch distinct (field, side) pairs, whose reads and writes do not overlap
+// when the dimension has 3 or more cells, so they need no order among them;
+// otherwise (b.serial) one thread applies them all in the batch's order.
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void bc_dim_kernel(Geom g, BcBatch b) {
@@ -411,7 +466,8 @@ __global__ void bc_dim_kernel(Geom g, BcBatch b) {
     if (e2 >= 0 && c > g.n[e2] + 2) return;
     if (e2 < 0 && c > 0) return;
     const long long st[3] = {1, g.pitch, g.sxy};
-    for (int q = 0; q < b.count; q++) {
+    const int q0 = b.serial ? 0 : (int)blockIdx.z, q1 = b.serial ? b.count : q0 + 1;
+    for (int q = q0; q < q1; q++) {
         const BcOpDesc &op = b.ops[q];
         // range check for the other dims
         int pos[3] = {0, 0, 0};
@@ -582,22 +638,28 @@ int norm_blocks(const Geom &g) {
 }
 
 template <typename T>
-cudaError_t launch_update_sigma(const Geom &g, const KParams &p, const Ptrs<T> &f, bool ib, cudaStream_t s) {
+cudaError_t launch_update_sigma(const Geom &g, const KParams &p, const Ptrs<T> &f, bool ib, cudaStream_t s,
+                                const BlockList *bl) {
     dim3 blk(32, 8);
     dim3 grd = vertex_grid(g, blk);
-    if (g.nd == 2) update_sigma_kernel<T, 2, false><<<grd, blk, 0, s>>>(g, p, f);
-    else if (ib) update_sigma_kernel<T, 3, true><<<grd, blk, 0, s>>>(g, p, f);
-    else update_sigma_kernel<T, 3, false><<<grd, blk, 0, s>>>(g, p, f);
+    const BlockList none{nullptr, 0};
+    if (g.nd == 2) update_sigma_kernel<T, 2, false><<<grd, blk, 0, s>>>(g, p, f, none);
+    else if (ib && bl) update_sigma_kernel<T, 3, true><<<dim3(bl->count), blk, 0, s>>>(g, p, f, *bl);
+    else if (ib) update_sigma_kernel<T, 3, true><<<grd, blk, 0, s>>>(g, p, f, none);
+    else update_sigma_kernel<T, 3, false><<<grd, blk, 0, s>>>(g, p, f, none);
     return cudaGetLastError();
 }
 
 template <typename T>
-cudaError_t launch_update_V(const Geom &g, const KParams &p, const Ptrs<T> &f, bool ib, cudaStream_t s) {
+cudaError_t launch_update_V(const Geom &g, const KParams &p, const Ptrs<T> &f, bool ib, cudaStream_t s,
+                            const BlockList *bl) {
     dim3 blk(32, 8);
     dim3 grd = vertex_grid(g, blk);
-    if (g.nd == 2) update_V_kernel<T, 2, false><<<grd, blk, 0, s>>>(g, p, f);
-    else if (ib) update_V_kernel<T, 3, true><<<grd, blk, 0, s>>>(g, p, f);
-    else update_V_kernel<T, 3, false><<<grd, blk, 0, s>>>(g, p, f);
+    const BlockList none{nullptr, 0};
+    if (g.nd == 2) update_V_kernel<T, 2, false><<<grd, blk, 0, s>>>(g, p, f, none);
+    else if (ib && bl) update_V_kernel<T, 3, true><<<dim3(bl->count), blk, 0, s>>>(g, p, f, *bl);
+    else if (ib) update_V_kernel<T, 3, true><<<grd, blk, 0, s>>>(g, p, f, none);
+    else update_V_kernel<T, 3, false><<<grd, blk, 0, s>>>(g, p, f, none);
     return cudaGetLastError();
 }
 
@@ -630,6 +692,40 @@ cudaError_t launch_ib_flags(const Geom &g, const KParams &p, const Ptrs<T> &f, u
     return cudaGetLastError();
 }
 
+// Blocks that hold a point outside the strict interior (index 1 or n+1 in some
+// dimension: boundary batches write there) or a point p with an activity bit at
+// p + {0,1}^3.  The viscosity update at p reads τ at those eight points, and τ is
+// zero where no bit is set, so elsewhere η_next is the rheology of a zero
+// invariant: the same value every iteration.  The eight reads stay inside the
+// vertex range because p is strictly inside.
+__global__ void __launch_bounds__(256) ib_blocks_kernel(Geom g, const unsigned char *flags, uint2 *list, int *count) {
+    Idx x = vertex_index(g);
+    bool need = false;
+    if (x.ok) {
+        const bool inner = x.i >= 2 && x.i <= g.n[0] && x.j >= 2 && x.j <= g.n[1] && x.k >= 2 && x.k <= g.n[2];
+        if (!inner) {
+            need = true;
+        } else {
+            const long long I = x.I, sx = g.pitch, sxy = g.sxy;
+            need = (flags[I] | flags[I + 1] | flags[I + sx] | flags[I + sx + 1] | flags[I + sxy] | flags[I + sxy + 1] |
+                    flags[I + sxy + sx] | flags[I + sxy + sx + 1]) != 0;
+        }
+    }
+    if (__syncthreads_or(need) && threadIdx.x == 0 && threadIdx.y == 0)
+        list[atomicAdd(count, 1)] = make_uint2(blockIdx.x | (blockIdx.y << 16), blockIdx.z);
+}
+
+cudaError_t launch_ib_blocks(const Geom &g, const unsigned char *flags, uint2 *list, int *count, cudaStream_t s) {
+    dim3 blk(32, 8);
+    ib_blocks_kernel<<<vertex_grid(g, blk), blk, 0, s>>>(g, flags, list, count);
+    return cudaGetLastError();
+}
+
+long long vertex_grid_blocks(const Geom &g) {
+    dim3 grd = vertex_grid(g, dim3(32, 8));
+    return (long long)grd.x * grd.y * grd.z;
+}
+
 template <typename T>
 cudaError_t launch_compute_tau(const Geom &g, const KParams &p, const Ptrs<T> &f, bool ib, cudaStream_t s) {
     dim3 blk(32, 8);
@@ -650,9 +746,16 @@ cudaError_t launch_bc_batch(const Geom &g, const BcBatch &b, cudaStream_t s) {
         else e2 = e;
     }
     int na = g.n[e1] + 3, nc = e2 >= 0 ? g.n[e2] + 3 : 1;
+    BcBatch bb = b;
+    bb.serial = g.n[b.dim] < 3;
+    for (int q = 0; q < b.count && !bb.serial; q++)
+        for (int r = 0; r < q; r++)
+            if (b.ops[r].f == b.ops[q].f &&
+                (b.ops[r].side == b.ops[q].side || b.ops[r].op == BC_PERIODIC || b.ops[q].op == BC_PERIODIC))
+                bb.serial = 1;
     dim3 blk(32, 8);
-    dim3 grd((na + 31) / 32, (nc + 7) / 8);
-    bc_dim_kernel<T><<<grd, blk, 0, s>>>(g, b);
+    dim3 grd((na + 31) / 32, (nc + 7) / 8, bb.serial ? 1 : b.count);
+    bc_dim_kernel<T><<<grd, blk, 0, s>>>(g, bb);
     return cudaGetLastError();
 }
 
@@ -672,8 +775,10 @@ cudaError_t launch_residual_norms(const Geom &g, const KParams &p, const Ptrs<T>
 }
 
 #define FI_INST(T)                                                                                                \
-    template cudaError_t launch_update_sigma<T>(const Geom &, const KParams &, const Ptrs<T> &, bool, cudaStream_t); \
-    template cudaError_t launch_update_V<T>(const Geom &, const KParams &, const Ptrs<T> &, bool, cudaStream_t);     \
+    template cudaError_t launch_update_sigma<T>(const Geom &, const KParams &, const Ptrs<T> &, bool, cudaStream_t,   \
+                                                const BlockList *);                                               \
+    template cudaError_t launch_update_V<T>(const Geom &, const KParams &, const Ptrs<T> &, bool, cudaStream_t,       \
+                                            const BlockList *);                                                   \
     template cudaError_t launch_compute_residuals<T>(const Geom &, const KParams &, const Ptrs<T> &, bool,          \
                                                      cudaStream_t);                                               \
     template cudaError_t launch_compute_tau<T>(const Geom &, const KParams &, const Ptrs<T> &, bool, cudaStream_t);   \

@@ -176,6 +176,51 @@ def test_immersed_boundary_activity_follows_new_volume_fractions():
     np.testing.assert_array_equal(a[[0, 1, 2, 3]], b[[0, 1, 2, 3]])
 
 
+# power laws regularised at η = 1, so that the time steps of a unit viscosity stay stable
+@pytest.mark.parametrize("rheo", [{"kind": "linear", "eta": 1.0}, {"kind": "glen", "eta_reg": 1.0},
+                                  {"kind": "relax_glen", "eta_reg": 1.0}],
+                         ids=["linear", "glen", "relaxed_glen"])
+def test_immersed_boundary_zero_stores_skipped_after_full_iterations(rheo):
+    # after two full iterations the immersed-boundary updates stop rewriting the
+    # zeros of inactive strict-interior points and run only the listed blocks;
+    # state written from outside (here random values everywhere, inactive points
+    # included) must be zeroed again, boundary values (non-zero velocities and
+    # tractions) must not leak into skipped points, and the viscosity next to the
+    # ice (power law) or everywhere (relaxation) must keep moving -- bit for bit
+    # with the oracle, across single iterations and replayed iteration pairs
+    fi, O = load_fastice(), load_oracle()
+    n = (20, 14, 18)
+    ext = (1.0, 1.25, 1.5)
+    dx = tuple(e / c for e, c in zip(ext, n))
+    psi_ns = -_sphere_psi(n, dx, (0.5, 0.6, -0.3), 0.75)
+    psi_na = _sphere_psi(n, dx, (0.5, 0.6, 0.5), 0.8)
+    bcs = ((("velocity", (0.1, -0.2, 0.05)), ("traction", (0.3, 0.0, -0.1))),
+           (("slip", (0.0, 0.2, 0.0)), ("traction", (0.0, 0.0, 0.0))),
+           (("velocity", (0.0, 0.1, 0.0)), ("traction", (0.0, 0.2, 0.1))))
+    p = Pair(n, bcs, rheo=rheo, path="reference", library="strict", seed=33, origin=(0.0, 0.0, 0.0), extent=ext,
+             immersed_psi={"na": psi_na, "ns": psi_ns})
+    p.advance(11)
+    bad = p.bitwise_equal()
+    assert not bad, bad
+    rng = np.random.default_rng(5)
+    for name in ("P", "txy", "Vz", "eta"):
+        vals = rng.standard_normal(p.model.field_shape(name))
+        if name == "eta":
+            vals = 0.5 + np.abs(vals)
+        p.model.set_field(name, vals)
+        p.oracle.set_interior(name, vals)
+    p.advance(1)
+    p.advance(9)
+    bad = p.bitwise_equal()
+    finite = all(np.isfinite(p.oracle.interior(name)).all() for name in p.state)
+    a = p.model.residual_norms()
+    b = p.oracle.residual_norms()
+    p.close()
+    assert finite
+    assert not bad, bad
+    np.testing.assert_array_equal(a[[0, 1, 2, 3]], b[[0, 1, 2, 3]])
+
+
 def test_model_omega_from_psi_matches_standalone():
     fi = load_fastice()
     n, ext = (16, 12, 10), (1.0, 0.75, 0.6)
