@@ -356,19 +356,25 @@ def run_mixed(args):
     tol = args.tol or 1e-8
     res = {}
     fields = ("P", "txx", "tyy", "tzz", "txy", "txz", "tyz", "Vx", "Vy", "Vz")
+    rheo, eta0, rdesc, pt = glacier_rheology(fi, args.rheology)
+    if args.scenario == "mms":
+        eta0 = 1.0
     for mode in ("plain", "mixed"):
         if args.scenario == "mms":
             grid, m = scenarios.mms3d_model(n)
             kw = dict(max_iter=400 * n, ncheck=n, tol=tol)
         else:
-            m, _ = scenarios.bed_model(0, n)
+            m, _ = scenarios.bed_model(0, n, rheology=rheo, pt=pt)
+            m.set_field("eta", eta0)
+            m.set_field("eta_next", eta0)
+            m.apply_bcs()
             grid = m.grid
             kw = dict(max_iter=1000 * n, ncheck=n, tol=tol, measure="rel_slab", rho_g_inf=1.0, length_z=0.6)
         m.solve(mode=mode, **dict(kw, max_iter=2 * n, tol=1e-30))  # warm-up (shadow model, launch shapes)
         for f in fields:
             m.set_field(f, 0.0)
-        m.set_field("eta", 1.0)
-        m.set_field("eta_next", 1.0)
+        m.set_field("eta", eta0)
+        m.set_field("eta_next", eta0)
         m.apply_bcs()
         m.synchronize()
         t0 = time.perf_counter()
@@ -388,13 +394,27 @@ def run_mixed(args):
                "n": n, "tol": tol}
     else:
         cfg = {"workload": f"3D immersed-boundary glacier {n}^3 cells (seeded 64-bump bed, surface 0.6 + 0.05 "
-                           f"sin(2 pi x), traction-free box, linear viscosity) to relative residual < {tol}",
+                           f"sin(2 pi x), traction-free box, {rdesc}) to relative residual < {tol}",
                "n": n, "tol": tol, "measure": "max(|r_V|inf / |rho g|inf, |r_P|inf * 0.6 / max|V|)"}
     sp = res["plain"]["seconds"] / res["mixed"]["seconds"]
     line = _base_line("mixed-precision solve speedup vs plain FP64", sp, "x", 1, 1, 1e3 * res["mixed"]["seconds"],
                       "f32+f64", cfg)
     line.update({"plain_fp64": res["plain"], "mixed": res["mixed"], "max_rel_diff_V_vs_fp64": dv})
     print(json.dumps(line))
+
+
+def glacier_rheology(fi, kind):
+    """(rheology or None for the default linear viscosity 1, initial η, description,
+    PT steps (r, re, factor))."""
+    if kind in ("glen", "glen_relaxed"):
+        r = fi.glen_regularised(A=1.0, n=3, strain_rate_0=1e-6)
+        eta0 = r.eta_reg
+        desc = "Glen n=3, A=1, regularised at strain rate 1e-6"
+        if kind == "glen_relaxed":
+            r = fi.Relaxation(r, 0.1, scale="log")
+            desc += ", relaxed in log scale at rate 0.1"
+        return r, eta0, desc, (0.7, 8 * math.pi, 1.1)
+    return None, 1.0, "linear viscosity", (0.9, 5 * math.pi, 1.1)
 
 
 def ib_a_eff_elements(n):
@@ -426,9 +446,14 @@ def run_glacier(args):
     peak, peak_kind = measured_peak_hbm()
     res = {}
     clocks = None
+    rheo, eta0, rdesc, pt = glacier_rheology(fi, args.rheology)
     for dtype in [d for d in args.dtypes.split(",") if d in ("f64", "f32")]:
         t0 = time.perf_counter()
-        m, prm = scenarios.bed_model(0, n, dtype=dtype)
+        m, prm = scenarios.bed_model(0, n, dtype=dtype, rheology=rheo, pt=pt)
+        if rheo is not None:
+            m.set_field("eta", eta0)
+            m.set_field("eta_next", eta0)
+            m.apply_bcs()
         setup = time.perf_counter() - t0
         m.advance(args.warmup)
         m.synchronize()
@@ -450,7 +475,7 @@ def run_glacier(args):
     cfg = {"workload": f"3D immersed-boundary glacier {n}^3 cells on the unit cube: bed = seeded sum of 64 Gaussian "
                        "bumps (a~U(0,0.2), w~U(0.05,0.2), centres uniform), surface z = 0.6 + 0.05 sin(2 pi x), "
                        "level sets from the DEMs, volume fractions from the level sets, traction-free box, "
-                       "one PT iteration per step", "grid": list(dims), "a_eff_arrays": 36,
+                       f"{rdesc}, one PT iteration per step", "grid": list(dims), "a_eff_arrays": 36,
            "l2": "inputs exceed L2 (126 MB): no flush needed"}
     line = _base_line(f"IB PT-Stokes T_eff GB/s ({n}^3, {dt0.upper()}, 36-pass convention)", d0["teff_gbs"], "GB/s",
                       args.steps, args.warmup, d0["ms_per_step"], dt0, cfg)
@@ -555,6 +580,10 @@ def main():
     ap.add_argument("--rounds", type=int, default=0, help="batched: stop after this many check rounds (profiling)")
     ap.add_argument("--scenario", choices=("mms", "glacier"), default="mms",
                     help="mixed: the 3D manufactured solution or the immersed-boundary glacier")
+    ap.add_argument("--rheology", choices=("linear", "glen", "glen_relaxed"), default="linear",
+                    help="glacier workloads: linear viscosity 1 (the reference's glacier driver) or Glen's law "
+                         "n=3, A=1, regularised at strain rate 1e-6 (glen_relaxed: relaxed in log scale at rate "
+                         "0.1), with the slab's PT steps (r 0.7, re 8 pi)")
     args = ap.parse_args()
     if args.workload != "slab":
         {"batched": run_batched, "serving": run_serving, "mixed": run_mixed,

@@ -109,14 +109,15 @@ def inclusion_model(seed: int, n=None, dtype: str = "f32", library: str = "fast"
     return m, prm
 
 
-def bed_model(seed: int, n: int, dtype: str = "f64", library: str = "fast", rheology=None, dem_cells=None):
+def bed_model(seed: int, n: int, dtype: str = "f64", library: str = "fast", rheology=None, dem_cells=None,
+              pt=(0.9, 5 * math.pi, 1.1)):
     """Build the immersed-boundary glacier of ``seed`` on the unit cube with n^3
     cells: returns (model, params).  Bed and surface DEMs live on a 2D vertex grid
     slightly wider than the cube; ψ.na comes from the surface DEM, ψ.ns from the
     bed DEM inverted, and the volume fractions from ω_from_ψ!
     (scripts_future_API/test_volume_fractions.jl:86-100).  Traction-free box
     sides, ρg = (0, 0, 1), linear viscosity 1 unless ``rheology`` is given, and
-    that driver's PT steps (r = 0.9, re = 5π, factor 1.1)."""
+    that driver's PT steps (``pt`` = (r, re, factor) = (0.9, 5π, 1.1)) unless given."""
     from .levelsets import compute_levelset_from_dem
     from .models import IsothermalImmersedBoundaryFullStokesModel
     from .physics import TBC
@@ -133,7 +134,7 @@ def bed_model(seed: int, n: int, dtype: str = "f64", library: str = "fast", rheo
     psi_na = compute_levelset_from_dem(grid, dem_grid, surf, library=library)
     psi_ns = compute_levelset_from_dem(grid, dem_grid, bed, invert=True, library=library)
     free = TBC(0.0, 0.0, 0.0)
-    r, re_mech, factor = 0.9, 5 * math.pi, 1.1
+    r, re_mech, factor = pt
     sp = pt_params(grid, r=r, re_mech=re_mech, vdtau_factor=factor)
     m = IsothermalImmersedBoundaryFullStokesModel(
         grid=grid, boundary_conditions={"x": (free, free), "y": (free, free), "z": (free, free)},
