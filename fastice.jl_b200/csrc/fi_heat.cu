@@ -48,9 +48,30 @@ struct HeatArgs {
     int n[3];
     long long sx, sxy;
     T D[3], lam, dtq, dtT, dt;
+    T iD[3], idt;  // 1/D and 1/dt, rounded once on the host
     int kind[3][2];
     T val[3][2];
 };
+
+// x / D[d] and x / dt: production builds multiply by the rounded reciprocals
+// (within an ulp or so of the quotient, and no division sequence per cell);
+// FI_EXACT_ORDER builds divide as the reference does
+template <typename T>
+__device__ __forceinline__ T over_D(const HeatArgs<T> &a, T x, int d) {
+#ifdef FI_EXACT_ORDER
+    return x / a.D[d];
+#else
+    return x * a.iD[d];
+#endif
+}
+template <typename T>
+__device__ __forceinline__ T over_dt(const HeatArgs<T> &a, T x) {
+#ifdef FI_EXACT_ORDER
+    return x / a.dt;
+#else
+    return x * a.idt;
+#endif
+}
 
 template <typename T>
 __global__ void __launch_bounds__(256) heat_sweep(HeatArgs<T> a) {
@@ -69,12 +90,12 @@ __global__ void __launch_bounds__(256) heat_sweep(HeatArgs<T> a) {
     for (int d = 0; d < 3; d++) {
         const T Tm = a.T0[I - st[d]], Tp = a.T0[I + st[d]];
         const T qlo = q0[d][I], qhi = q0[d][I + st[d]];
-        const T dl = a.lam * (Tc - Tm) / a.D[d], dr = a.lam * (Tp - Tc) / a.D[d];
+        const T dl = over_D(a, a.lam * (Tc - Tm), d), dr = over_D(a, a.lam * (Tp - Tc), d);
         ql[d] = (ix[d] == 1 && a.kind[d][0] == FI_HEAT_FLUX) ? a.val[d][0] : qlo - (qlo + dl) * a.dtq;
         qr[d] = (ix[d] == a.n[d] && a.kind[d][1] == FI_HEAT_FLUX) ? a.val[d][1] : qhi - (qhi + dr) * a.dtq;
     }
-    const T gq = (qr[0] - ql[0]) / a.D[0] + (qr[1] - ql[1]) / a.D[1] + (qr[2] - ql[2]) / a.D[2];
-    const T Tn = Tc - ((Tc - a.To[I]) / a.dt + gq) * a.dtT;
+    const T gq = over_D(a, qr[0] - ql[0], 0) + over_D(a, qr[1] - ql[1], 1) + over_D(a, qr[2] - ql[2], 2);
+    const T Tn = Tc - (over_dt(a, Tc - a.To[I]) + gq) * a.dtT;
     a.T1[I] = Tn;
 #pragma unroll
     for (int d = 0; d < 3; d++) {
@@ -181,6 +202,7 @@ fi_status heat_advance_t(fi_heat *h, int niter, double dt) {
     for (int e = 0; e < 3; e++) {
         a.n[e] = h->d.grid.n[e];
         a.D[e] = T(h->d.grid.extent[e] / h->d.grid.n[e]);
+        a.iD[e] = T(1) / a.D[e];
         for (int s = 0; s < 2; s++) {
             a.kind[e][s] = h->d.kind[e][s];
             a.val[e][s] = T(h->d.value[e][s]);
@@ -192,6 +214,7 @@ fi_status heat_advance_t(fi_heat *h, int niter, double dt) {
     a.dtq = T(h->d.dtau_q);
     a.dtT = T(h->d.dtau_T);
     a.dt = T(dt);
+    a.idt = T(1) / a.dt;
     a.To = (const T *)h->To;
     const dim3 blk(32, 8), grd((a.n[0] + 31) / 32, (a.n[1] + 7) / 8, a.n[2]);
     for (int it = 0; it < niter; it++) {

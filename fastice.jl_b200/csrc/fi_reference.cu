@@ -549,11 +549,21 @@ __global__ void __launch_bounds__(kNormThreads) residual_norms_kernel(Geom g, KP
             int k = d < ND ? p.bc_kind[d][s] : FI_BC_TRACTION;
             wall0[d][s] = !(k == FI_BC_TRACTION || k == FI_BC_PERIODIC);
         }
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
-        int i = int(t % nx) + 1;
-        long long r2 = t / nx;
-        int j = int(r2 % ny) + 1;
-        int k = ND == 3 ? int(r2 / ny) + 1 : 0;
+    // grid-stride loop over the vertex range; the position (ii, jj, kk) steps by the
+    // stride's own decomposition with carries instead of two 64-bit divisions per point
+    const long long S = (long long)gridDim.x * blockDim.x;
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int ii = int(t % nx), jj = int((t / nx) % ny), kk = int(t / nx / ny);
+    const int si = int(S % nx), sj = int((S / nx) % ny), sk = int(S / nx / ny);
+    for (; t < total; t += S) {
+        const int i = ii + 1, j = jj + 1, k = ND == 3 ? kk + 1 : 0;
+        ii += si;
+        const int c1 = ii >= nx;
+        ii -= c1 ? int(nx) : 0;
+        jj += sj + c1;
+        const int c2 = jj >= ny;
+        jj -= c2 ? int(ny) : 0;
+        kk += sk + c2;
         long long I = (long long)i + g.pitch * ((long long)j + g.rows * (long long)k);
         Resid<T, ND, IB> r = residual_at<T, ND, IB>(g, p, f, I);
         if (p.p_forcing) r.rP = r.rP + f.fP[I];
