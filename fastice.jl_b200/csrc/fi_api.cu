@@ -297,7 +297,7 @@ fi_status refresh_ibf(fi_model *m) {
     FI_CHECK_CUDA(launch_ib_flags<T>(m->g, m->kp, m->ptrs<T>(), m->d_ibf, m->stream), "activity bytes");
     // the block list, in z, y, x order (neighbouring blocks run close in time)
     FI_CHECK_CUDA(cudaMemsetAsync(m->d_bcount, 0, sizeof(int), m->stream), "block count");
-    FI_CHECK_CUDA(launch_ib_blocks(m->g, m->d_ibf, m->d_blist, m->d_bcount, m->stream), "block list");
+    FI_CHECK_CUDA(launch_ib_blocks<T>(m->g, m->d_ibf, m->d_blist, m->d_bcount, m->stream), "block list");
     int cnt = 0;
     FI_CHECK_CUDA(cudaMemcpyAsync(&cnt, m->d_bcount, sizeof(int), cudaMemcpyDeviceToHost, m->stream), "block count");
     FI_CHECK_CUDA(cudaStreamSynchronize(m->stream), "block count");

@@ -125,10 +125,10 @@ inline float small_threshold_f32() {
 void set_error(const std::string &msg);
 fi_status cuda_fail(cudaError_t e, const char *where);
 
-// Blocks (32x8 points of one z plane) of the vertex-range grid that an
-// immersed-boundary update must run once the inactive strict interior holds
-// zero: those with an active point or a point outside the strict interior.
-// Entry: x = block x | block y << 16, y = block z.
+// Blocks (32·C x 8 points of one z plane, C points per thread) of the
+// immersed-boundary launch that must run once the inactive strict interior
+// holds zero: those with a point outside the strict interior or next to an
+// active one.  Entry: x = block x | block y << 16, y = block z.
 struct BlockList {
     const uint2 *ids;
     int count;
@@ -143,8 +143,9 @@ cudaError_t launch_update_sigma(const Geom &g, const KParams &p, const Ptrs<T> &
 template <typename T>
 cudaError_t launch_update_V(const Geom &g, const KParams &p, const Ptrs<T> &f, bool ib, cudaStream_t s,
                             const BlockList *bl = nullptr);
-// the block list of an immersed-boundary model from its activity bytes; *count
-// is device memory, the list unordered
+// the block list of an immersed-boundary model of precision T from its activity
+// bytes; *count is device memory, the list unordered
+template <typename T>
 cudaError_t launch_ib_blocks(const Geom &g, const unsigned char *flags, uint2 *list, int *count, cudaStream_t s);
 // number of blocks of the vertex-range grid (the list's capacity)
 long long vertex_grid_blocks(const Geom &g);

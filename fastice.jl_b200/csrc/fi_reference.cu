@@ -41,119 +41,287 @@ __device__ __forceinline__ Idx vertex_index(const Geom &g, const BlockList &bl) 
     return vertex_index_of(g, b.x & 0xffffu, b.x >> 16, b.y);
 }
 
-// an inactive point whose zero need not be stored again (KParams::skip_zeros):
-// strictly inside in every dimension, where no boundary batch writes
-__device__ __forceinline__ bool skip_zero_store(const Geom &g, const KParams &p, const Idx &x) {
-    return p.skip_zeros && x.i >= 2 && x.i <= g.n[0] && x.j >= 2 && x.j <= g.n[1] && x.k >= 2 && x.k <= g.n[2];
-}
-
 dim3 vertex_grid(const Geom &g, dim3 blk) {
     return dim3((g.n[0] + 1 + blk.x - 1) / blk.x, (g.n[1] + 1 + blk.y - 1) / blk.y, g.nd == 3 ? g.n[2] + 1 : 1);
 }
 
 // ---------------------------------------------------------------------------
-// Immersed-boundary bodies of update_σ! and update_V! (IB kernels_3d.jl:3-74).
-// The activity byte gates each masked group; a group's stores come before the
-// next group's loads (the outputs may alias the inputs as far as the compiler
-// knows), so a thread makes several dependent round trips to memory with few
-// registers.  Forms that load every input first (per thread with predicated
-// loads, or per warp with unconditional loads) were measured slower in both
+// Immersed-boundary update_σ! and update_V! (IB kernels_3d.jl:3-74).  A thread
+// owns C points of one row, 32 apart (x = i, i + 32, ...): one warp covers
+// 32·C consecutive positions and each load instruction stays coalesced, while
+// the loads of a masked group for all C points go out together.  The activity
+// byte gates each group; a group's stores come after its loads for all points
+// but before the next group's loads (the outputs may alias the inputs as far as
+// the compiler knows), so a thread makes several dependent round trips to
+// memory.  FP32 takes C = 2: its loads carry half the bytes of FP64 ones and one
+// point per thread keeps too few bytes in flight.  FP64 takes C = 1.
+// Loads for a point past the vertex range (the second point of the last block
+// of a row) stay inside the field's allocation (the row pitch, or the slack
+// after the last row) and are discarded; nothing is stored there.  Forms that
+// load every input of a point before any store (predicated loads, or one
+// decision per warp with unconditional loads) were measured slower in both
 // precisions: the extra registers cost more occupancy than the shorter chain
 // gains.
 // ---------------------------------------------------------------------------
 template <typename T>
-__device__ __forceinline__ void ib_sigma(const KParams &p, const Ptrs<T> &f, long long I, long long sx,
-                                         long long sxy, T idx, T idy, T idz, bool skip0) {
+constexpr int ib_points() { return sizeof(T) == 4 ? 2 : 1; }
+
+struct IbRow {
+    long long I;  // index of the first point
+    int i, j, k;  // its position
+};
+
+__device__ __forceinline__ IbRow ib_row(const Geom &g, const BlockList &bl, int C) {
+    unsigned bx = blockIdx.x, by = blockIdx.y, bz = blockIdx.z;
+    if (bl.ids) {
+        const uint2 b = bl.ids[blockIdx.x];
+        bx = b.x & 0xffffu, by = b.x >> 16, bz = b.y;
+    }
+    IbRow r;
+    r.i = bx * (32 * C) + threadIdx.x + 1;
+    r.j = by * blockDim.y + threadIdx.y + 1;
+    r.k = (int)bz + 1;
+    r.I = (long long)r.i + g.pitch * ((long long)r.j + g.rows * (long long)r.k);
+    return r;
+}
+
+dim3 ib_grid(const Geom &g, int C) {
+    return dim3((g.n[0] + 1 + 32 * C - 1) / (32 * C), (g.n[1] + 1 + 7) / 8, g.n[2] + 1);
+}
+
+template <typename T, int C>
+__global__ void __launch_bounds__(256) ib_sigma_kernel(Geom g, KParams p, Ptrs<T> f, BlockList bl) {
+    const IbRow r = ib_row(g, bl, C);
+    if (r.i > g.n[0] + 1 || r.j > g.n[1] + 1) return;
+    const long long sx = g.pitch, sxy = g.sxy;
+    const T idx = T(p.inv_dx[0]), idy = T(p.inv_dx[1]), idz = T(p.inv_dx[2]);
     const T *Vx = f.Vx, *Vy = f.Vy, *Vz = f.Vz, *eta = f.eta;
-    const T *const *ns = f.wns;
-    const unsigned fl = ib_flags_at(f, I, sx, sxy, T(p.small));
-    if (fl & IBF_S_CCC) {
-        T exx = (ns[W_VCC][I + 1] * Vx[I + 1] - ns[W_VCC][I] * Vx[I]) * idx;
-        T eyy = (ns[W_CVC][I + sx] * Vy[I + sx] - ns[W_CVC][I] * Vy[I]) * idy;
-        T ezz = (ns[W_CCV][I + sxy] * Vz[I + sxy] - ns[W_CCV][I] * Vz[I]) * idz;
-        T divV = exx + eyy + ezz;
-        T etac = eta[I];
-        f.P[I] = f.P[I] - (p.p_forcing ? divV + f.fP[I] : divV) * etac * T(p.dt_P);
-        f.txx[I] = f.txx[I] - (f.txx[I] - T(2.0) * etac * (exx - third(divV))) * T(p.dt_tau[0]);
-        f.tyy[I] = f.tyy[I] - (f.tyy[I] - T(2.0) * etac * (eyy - third(divV))) * T(p.dt_tau[1]);
-        f.tzz[I] = f.tzz[I] - (f.tzz[I] - T(2.0) * etac * (ezz - third(divV))) * T(p.dt_tau[2]);
-    } else if (!skip0) {
-        f.P[I] = T(0);
-        f.txx[I] = T(0);
-        f.tyy[I] = T(0);
-        f.tzz[I] = T(0);
+    const T *nx = f.wns[W_VCC], *ny = f.wns[W_CVC], *nz = f.wns[W_CCV];
+    const bool jk_inner = r.j >= 2 && r.j <= g.n[1] && r.k >= 2 && r.k <= g.n[2];
+    bool ok[C], skip0[C];
+    unsigned fl[C], any = 0;
+#pragma unroll
+    for (int c = 0; c < C; c++) {
+        const int i = r.i + 32 * c;
+        ok[c] = i <= g.n[0] + 1;
+        skip0[c] = p.skip_zeros && jk_inner && i >= 2 && i <= g.n[0];
+        fl[c] = ok[c] ? ib_flags_at(f, r.I + 32 * c, sx, sxy, T(p.small)) : 0u;
+        any |= fl[c];
     }
-    if (fl & IBF_S_VVC) {
-        T exy = T(0.5) * ((ns[W_CVC][I] * Vy[I] - ns[W_CVC][I - 1] * Vy[I - 1]) * idx +
-                          (ns[W_VCC][I] * Vx[I] - ns[W_VCC][I - sx] * Vx[I - sx]) * idy);
-        T e_xy = h(h(eta[I - 1 - sx] + eta[I - sx]) + h(eta[I - 1] + eta[I]));
-        f.txy[I] = f.txy[I] - (f.txy[I] - T(2.0) * e_xy * exy) * T(p.dt_tau[3]);
-    } else if (!skip0) {
-        f.txy[I] = T(0);
+    if (any & IBF_S_CCC) {
+        T nP[C], nxx[C], nyy[C], nzz[C];
+#pragma unroll
+        for (int c = 0; c < C; c++) {
+            const long long I = r.I + 32 * c;
+            T exx = (nx[I + 1] * Vx[I + 1] - nx[I] * Vx[I]) * idx;
+            T eyy = (ny[I + sx] * Vy[I + sx] - ny[I] * Vy[I]) * idy;
+            T ezz = (nz[I + sxy] * Vz[I + sxy] - nz[I] * Vz[I]) * idz;
+            T divV = exx + eyy + ezz;
+            T etac = eta[I];
+            nP[c] = f.P[I] - (p.p_forcing ? divV + f.fP[I] : divV) * etac * T(p.dt_P);
+            nxx[c] = f.txx[I] - (f.txx[I] - T(2.0) * etac * (exx - third(divV))) * T(p.dt_tau[0]);
+            nyy[c] = f.tyy[I] - (f.tyy[I] - T(2.0) * etac * (eyy - third(divV))) * T(p.dt_tau[1]);
+            nzz[c] = f.tzz[I] - (f.tzz[I] - T(2.0) * etac * (ezz - third(divV))) * T(p.dt_tau[2]);
+        }
+#pragma unroll
+        for (int c = 0; c < C; c++) {
+            const long long I = r.I + 32 * c;
+            const bool on = fl[c] & IBF_S_CCC;
+            if (on || (ok[c] && !skip0[c])) {
+                f.P[I] = on ? nP[c] : T(0);
+                f.txx[I] = on ? nxx[c] : T(0);
+                f.tyy[I] = on ? nyy[c] : T(0);
+                f.tzz[I] = on ? nzz[c] : T(0);
+            }
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < C; c++)
+            if (ok[c] && !skip0[c]) {
+                const long long I = r.I + 32 * c;
+                f.P[I] = T(0);
+                f.txx[I] = T(0);
+                f.tyy[I] = T(0);
+                f.tzz[I] = T(0);
+            }
     }
-    if (fl & IBF_S_VCV) {
-        T exz = T(0.5) * ((ns[W_CCV][I] * Vz[I] - ns[W_CCV][I - 1] * Vz[I - 1]) * idx +
-                          (ns[W_VCC][I] * Vx[I] - ns[W_VCC][I - sxy] * Vx[I - sxy]) * idz);
-        T e_xz = h(h(eta[I - 1 - sxy] + eta[I - sxy]) + h(eta[I - 1] + eta[I]));
-        f.txz[I] = f.txz[I] - (f.txz[I] - T(2.0) * e_xz * exz) * T(p.dt_tau[4]);
-    } else if (!skip0) {
-        f.txz[I] = T(0);
+    // the three shear components: edge viscosity from four centres, masked strain rate
+    if (any & IBF_S_VVC) {
+        T v[C];
+#pragma unroll
+        for (int c = 0; c < C; c++) {
+            const long long I = r.I + 32 * c;
+            T exy = T(0.5) * ((ny[I] * Vy[I] - ny[I - 1] * Vy[I - 1]) * idx + (nx[I] * Vx[I] - nx[I - sx] * Vx[I - sx]) * idy);
+            T e_xy = h(h(eta[I - 1 - sx] + eta[I - sx]) + h(eta[I - 1] + eta[I]));
+            v[c] = f.txy[I] - (f.txy[I] - T(2.0) * e_xy * exy) * T(p.dt_tau[3]);
+        }
+#pragma unroll
+        for (int c = 0; c < C; c++) {
+            const bool on = fl[c] & IBF_S_VVC;
+            if (on || (ok[c] && !skip0[c])) f.txy[r.I + 32 * c] = on ? v[c] : T(0);
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < C; c++)
+            if (ok[c] && !skip0[c]) f.txy[r.I + 32 * c] = T(0);
     }
-    if (fl & IBF_S_CVV) {
-        T eyz = T(0.5) * ((ns[W_CCV][I] * Vz[I] - ns[W_CCV][I - sx] * Vz[I - sx]) * idy +
-                          (ns[W_CVC][I] * Vy[I] - ns[W_CVC][I - sxy] * Vy[I - sxy]) * idz);
-        T e_yz = h(h(eta[I - sx - sxy] + eta[I - sxy]) + h(eta[I - sx] + eta[I]));
-        f.tyz[I] = f.tyz[I] - (f.tyz[I] - T(2.0) * e_yz * eyz) * T(p.dt_tau[5]);
-    } else if (!skip0) {
-        f.tyz[I] = T(0);
+    if (any & IBF_S_VCV) {
+        T v[C];
+#pragma unroll
+        for (int c = 0; c < C; c++) {
+            const long long I = r.I + 32 * c;
+            T exz = T(0.5) * ((nz[I] * Vz[I] - nz[I - 1] * Vz[I - 1]) * idx + (nx[I] * Vx[I] - nx[I - sxy] * Vx[I - sxy]) * idz);
+            T e_xz = h(h(eta[I - 1 - sxy] + eta[I - sxy]) + h(eta[I - 1] + eta[I]));
+            v[c] = f.txz[I] - (f.txz[I] - T(2.0) * e_xz * exz) * T(p.dt_tau[4]);
+        }
+#pragma unroll
+        for (int c = 0; c < C; c++) {
+            const bool on = fl[c] & IBF_S_VCV;
+            if (on || (ok[c] && !skip0[c])) f.txz[r.I + 32 * c] = on ? v[c] : T(0);
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < C; c++)
+            if (ok[c] && !skip0[c]) f.txz[r.I + 32 * c] = T(0);
+    }
+    if (any & IBF_S_CVV) {
+        T v[C];
+#pragma unroll
+        for (int c = 0; c < C; c++) {
+            const long long I = r.I + 32 * c;
+            T eyz = T(0.5) * ((nz[I] * Vz[I] - nz[I - sx] * Vz[I - sx]) * idy + (ny[I] * Vy[I] - ny[I - sxy] * Vy[I - sxy]) * idz);
+            T e_yz = h(h(eta[I - sx - sxy] + eta[I - sxy]) + h(eta[I - sx] + eta[I]));
+            v[c] = f.tyz[I] - (f.tyz[I] - T(2.0) * e_yz * eyz) * T(p.dt_tau[5]);
+        }
+#pragma unroll
+        for (int c = 0; c < C; c++) {
+            const bool on = fl[c] & IBF_S_CVV;
+            if (on || (ok[c] && !skip0[c])) f.tyz[r.I + 32 * c] = on ? v[c] : T(0);
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < C; c++)
+            if (ok[c] && !skip0[c]) f.tyz[r.I + 32 * c] = T(0);
     }
 }
 
-// update_V! of an immersed-boundary model: the velocities (the viscosity follows in the kernel)
-template <typename T>
-__device__ __forceinline__ void ib_V(const KParams &p, const Ptrs<T> &f, long long I, long long sx, long long sxy,
-                                     T idx, T idy, T idz, T gx, T gy, T gz, bool skip0) {
+// resident blocks per SM asked of the compiler: 6 (40 registers) for one point
+// per thread, 4 (64) for two
+template <typename T, int C>
+__global__ void __launch_bounds__(256, C == 1 ? 6 : 4) ib_V_kernel(Geom g, KParams p, Ptrs<T> f, BlockList bl) {
+    const IbRow r = ib_row(g, bl, C);
+    if (r.i > g.n[0] + 1 || r.j > g.n[1] + 1) return;
+    const long long sx = g.pitch, sxy = g.sxy;
+    const T idx = T(p.inv_dx[0]), idy = T(p.inv_dx[1]), idz = T(p.inv_dx[2]);
     const T *P = f.P, *txx = f.txx, *tyy = f.tyy, *tzz = f.tzz, *txy = f.txy, *txz = f.txz, *tyz = f.tyz, *eta = f.eta;
-    const T *const *na = f.wna;
-    const T *const *ns = f.wns;
-    const T *wc = na[W_CCC], *wvvc = na[W_VVC], *wvcv = na[W_VCV], *wcvv = na[W_CVV];
-    const unsigned fl = ib_flags_at(f, I, sx, sxy, T(p.small));
-    if (fl & IBF_V_VCC) {
-        T ex = h(eta[I - 1] + eta[I]);
-        f.Vx[I] = f.Vx[I] + div_fast(div_fast(-(wc[I] * P[I] - wc[I - 1] * P[I - 1]) * idx +
-                                                  (wc[I] * txx[I] - wc[I - 1] * txx[I - 1]) * idx +
-                                                  (wvvc[I + sx] * txy[I + sx] - wvvc[I] * txy[I]) * idy +
-                                                  (wvcv[I + sxy] * txz[I + sxy] - wvcv[I] * txz[I]) * idz - gx,
-                                              ex),
-                                     ns[W_VCC][I]) *
-                                T(p.dt_V[0]);
-    } else if (!skip0) {
-        f.Vx[I] = T(0);
+    const T *wc = f.wna[W_CCC], *wvvc = f.wna[W_VVC], *wvcv = f.wna[W_VCV], *wcvv = f.wna[W_CVV];
+    const bool jk_inner = r.j >= 2 && r.j <= g.n[1] && r.k >= 2 && r.k <= g.n[2];
+    bool ok[C], skip0[C];
+    unsigned fl[C], any = 0;
+#pragma unroll
+    for (int c = 0; c < C; c++) {
+        const int i = r.i + 32 * c;
+        ok[c] = i <= g.n[0] + 1;
+        skip0[c] = p.skip_zeros && jk_inner && i >= 2 && i <= g.n[0];
+        fl[c] = ok[c] ? ib_flags_at(f, r.I + 32 * c, sx, sxy, T(p.small)) : 0u;
+        any |= fl[c];
     }
-    if (fl & IBF_V_CVC) {
-        T ey = h(eta[I - sx] + eta[I]);
-        f.Vy[I] = f.Vy[I] + div_fast(div_fast(-(wc[I] * P[I] - wc[I - sx] * P[I - sx]) * idy +
-                                                  (wc[I] * tyy[I] - wc[I - sx] * tyy[I - sx]) * idy +
-                                                  (wvvc[I + 1] * txy[I + 1] - wvvc[I] * txy[I]) * idx +
-                                                  (wcvv[I + sxy] * tyz[I + sxy] - wcvv[I] * tyz[I]) * idz - gy,
-                                              ey),
-                                     ns[W_CVC][I]) *
-                                T(p.dt_V[1]);
-    } else if (!skip0) {
-        f.Vy[I] = T(0);
+    if (any & IBF_V_VCC) {
+        T v[C];
+#pragma unroll
+        for (int c = 0; c < C; c++) {
+            const long long I = r.I + 32 * c;
+            const T gx = gravity_dev(p, f.gx, 0, I);
+            T ex = h(eta[I - 1] + eta[I]);
+            v[c] = f.Vx[I] + div_fast(div_fast(-(wc[I] * P[I] - wc[I - 1] * P[I - 1]) * idx +
+                                                   (wc[I] * txx[I] - wc[I - 1] * txx[I - 1]) * idx +
+                                                   (wvvc[I + sx] * txy[I + sx] - wvvc[I] * txy[I]) * idy +
+                                                   (wvcv[I + sxy] * txz[I + sxy] - wvcv[I] * txz[I]) * idz - gx,
+                                               ex),
+                                      f.wns[W_VCC][I]) *
+                                 T(p.dt_V[0]);
+        }
+#pragma unroll
+        for (int c = 0; c < C; c++) {
+            const bool on = fl[c] & IBF_V_VCC;
+            if (on || (ok[c] && !skip0[c])) f.Vx[r.I + 32 * c] = on ? v[c] : T(0);
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < C; c++)
+            if (ok[c] && !skip0[c]) f.Vx[r.I + 32 * c] = T(0);
     }
-    if (fl & IBF_V_CCV) {
-        T ez = h(eta[I - sxy] + eta[I]);
-        f.Vz[I] = f.Vz[I] + div_fast(div_fast(-(wc[I] * P[I] - wc[I - sxy] * P[I - sxy]) * idz +
-                                                  (wc[I] * tzz[I] - wc[I - sxy] * tzz[I - sxy]) * idz +
-                                                  (wvcv[I + 1] * txz[I + 1] - wvcv[I] * txz[I]) * idx +
-                                                  (wcvv[I + sx] * tyz[I + sx] - wcvv[I] * tyz[I]) * idy - gz,
-                                              ez),
-                                     ns[W_CCV][I]) *
-                                T(p.dt_V[2]);
-    } else if (!skip0) {
-        f.Vz[I] = T(0);
+    if (any & IBF_V_CVC) {
+        T v[C];
+#pragma unroll
+        for (int c = 0; c < C; c++) {
+            const long long I = r.I + 32 * c;
+            const T gy = gravity_dev(p, f.gy, 1, I);
+            T ey = h(eta[I - sx] + eta[I]);
+            v[c] = f.Vy[I] + div_fast(div_fast(-(wc[I] * P[I] - wc[I - sx] * P[I - sx]) * idy +
+                                                   (wc[I] * tyy[I] - wc[I - sx] * tyy[I - sx]) * idy +
+                                                   (wvvc[I + 1] * txy[I + 1] - wvvc[I] * txy[I]) * idx +
+                                                   (wcvv[I + sxy] * tyz[I + sxy] - wcvv[I] * tyz[I]) * idz - gy,
+                                               ey),
+                                      f.wns[W_CVC][I]) *
+                                 T(p.dt_V[1]);
+        }
+#pragma unroll
+        for (int c = 0; c < C; c++) {
+            const bool on = fl[c] & IBF_V_CVC;
+            if (on || (ok[c] && !skip0[c])) f.Vy[r.I + 32 * c] = on ? v[c] : T(0);
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < C; c++)
+            if (ok[c] && !skip0[c]) f.Vy[r.I + 32 * c] = T(0);
     }
+    if (any & IBF_V_CCV) {
+        T v[C];
+#pragma unroll
+        for (int c = 0; c < C; c++) {
+            const long long I = r.I + 32 * c;
+            const T gz = gravity_dev(p, f.gz, 2, I);
+            T ez = h(eta[I - sxy] + eta[I]);
+            v[c] = f.Vz[I] + div_fast(div_fast(-(wc[I] * P[I] - wc[I - sxy] * P[I - sxy]) * idz +
+                                                   (wc[I] * tzz[I] - wc[I - sxy] * tzz[I - sxy]) * idz +
+                                                   (wvcv[I + 1] * txz[I + 1] - wvcv[I] * txz[I]) * idx +
+                                                   (wcvv[I + sx] * tyz[I + sx] - wcvv[I] * tyz[I]) * idy - gz,
+                                               ez),
+                                      f.wns[W_CCV][I]) *
+                                 T(p.dt_V[2]);
+        }
+#pragma unroll
+        for (int c = 0; c < C; c++) {
+            const bool on = fl[c] & IBF_V_CCV;
+            if (on || (ok[c] && !skip0[c])) f.Vz[r.I + 32 * c] = on ? v[c] : T(0);
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < C; c++)
+            if (ok[c] && !skip0[c]) f.Vz[r.I + 32 * c] = T(0);
+    }
+    // η_next at every point of the range (kernels_3d.jl:36-40)
+    if (p.freeze_eta) return;
+    if (linear_unrelaxed(p)) {  // the stress invariant is not needed
+#pragma unroll
+        for (int c = 0; c < C; c++)
+            if (ok[c]) f.eta_next[r.I + 32 * c] = p.rheo_eta_is_field ? f.eta_lin[r.I + 32 * c] : T(p.rheo_eta);
+        return;
+    }
+    T en[C];
+#pragma unroll
+    for (int c = 0; c < C; c++) {
+        const long long I = r.I + 32 * c;
+        T lxy = h(h(txy[I] + txy[I + 1]) + h(txy[I + sx] + txy[I + sx + 1]));
+        T lxz = h(h(txz[I] + txz[I + 1]) + h(txz[I + sxy] + txz[I + sxy + 1]));
+        T lyz = h(h(tyz[I] + tyz[I + sx]) + h(tyz[I + sxy] + tyz[I + sxy + sx]));
+        T s2 = T(0.5) * (txx[I] * txx[I] + tyy[I] * tyy[I] + tzz[I] * tzz[I]) + lxy * lxy + lxz * lxz + lyz * lyz;
+        en[c] = ok[c] ? rheology_s2(p, T(p.rheo_A), T(p.rheo_inv_eta_reg), f.eta_lin, f.A, eta[I], I, s2) : T(0);
+    }
+#pragma unroll
+    for (int c = 0; c < C; c++)
+        if (ok[c]) f.eta_next[r.I + 32 * c] = en[c];
 }
 
 template <typename T, int ND, bool IB>
@@ -200,16 +368,15 @@ __global__ void __launch_bounds__(256) update_sigma_kernel(Geom g, KParams p, Pt
         f.tyz[I] = f.tyz[I] - (f.tyz[I] - T(2.0) * e_yz * eyz) * T(p.dt_tau[5]);
         return;
     }
-    if constexpr (IB) ib_sigma(p, f, I, sx, sxy, idx, idy, idz, skip_zero_store(g, p, x));
 }
 
 // ---------------------------------------------------------------------------
 // update_V!  (kernels_3d.jl:27-40, kernels_2d.jl:20-29; IB kernels_3d.jl:46-74)
 // ---------------------------------------------------------------------------
-// resident blocks per SM asked of the compiler: 6 (40 registers) for the 2D and
-// immersed-boundary forms, 5 (48) for the plain 3D form
+// resident blocks per SM asked of the compiler: 6 (40 registers) for the 2D form,
+// 4 (64) for the 3D form
 template <int ND, bool IB>
-constexpr int update_V_min_blocks() { return (ND == 2 || IB) ? 6 : 5; }
+constexpr int update_V_min_blocks() { return ND == 2 ? 6 : 4; }
 
 template <typename T, int ND, bool IB>
 __global__ void __launch_bounds__(256, update_V_min_blocks<ND, IB>()) update_V_kernel(Geom g, KParams p, Ptrs<T> f,
@@ -258,8 +425,6 @@ __global__ void __launch_bounds__(256, update_V_min_blocks<ND, IB>()) update_V_k
                                         (tyz[I + sx] - tyz[I]) * idy - gz,
                                     ez) *
                                 T(p.dt_V[2]);
-    } else {
-        ib_V(p, f, I, sx, sxy, idx, idy, idz, gx, gy, gz, skip_zero_store(g, p, x));
     }
     if (p.freeze_eta) return;
     if (linear_unrelaxed(p)) {  // the stress invariant is not needed
@@ -653,9 +818,9 @@ cudaError_t launch_update_sigma(const Geom &g, const KParams &p, const Ptrs<T> &
     dim3 blk(32, 8);
     dim3 grd = vertex_grid(g, blk);
     const BlockList none{nullptr, 0};
+    constexpr int C = ib_points<T>();
     if (g.nd == 2) update_sigma_kernel<T, 2, false><<<grd, blk, 0, s>>>(g, p, f, none);
-    else if (ib && bl) update_sigma_kernel<T, 3, true><<<dim3(bl->count), blk, 0, s>>>(g, p, f, *bl);
-    else if (ib) update_sigma_kernel<T, 3, true><<<grd, blk, 0, s>>>(g, p, f, none);
+    else if (ib) ib_sigma_kernel<T, C><<<bl ? dim3(bl->count) : ib_grid(g, C), blk, 0, s>>>(g, p, f, bl ? *bl : none);
     else update_sigma_kernel<T, 3, false><<<grd, blk, 0, s>>>(g, p, f, none);
     return cudaGetLastError();
 }
@@ -666,9 +831,9 @@ cudaError_t launch_update_V(const Geom &g, const KParams &p, const Ptrs<T> &f, b
     dim3 blk(32, 8);
     dim3 grd = vertex_grid(g, blk);
     const BlockList none{nullptr, 0};
+    constexpr int C = ib_points<T>();
     if (g.nd == 2) update_V_kernel<T, 2, false><<<grd, blk, 0, s>>>(g, p, f, none);
-    else if (ib && bl) update_V_kernel<T, 3, true><<<dim3(bl->count), blk, 0, s>>>(g, p, f, *bl);
-    else if (ib) update_V_kernel<T, 3, true><<<grd, blk, 0, s>>>(g, p, f, none);
+    else if (ib) ib_V_kernel<T, C><<<bl ? dim3(bl->count) : ib_grid(g, C), blk, 0, s>>>(g, p, f, bl ? *bl : none);
     else update_V_kernel<T, 3, false><<<grd, blk, 0, s>>>(g, p, f, none);
     return cudaGetLastError();
 }
@@ -702,32 +867,39 @@ cudaError_t launch_ib_flags(const Geom &g, const KParams &p, const Ptrs<T> &f, u
     return cudaGetLastError();
 }
 
-// Blocks that hold a point outside the strict interior (index 1 or n+1 in some
-// dimension: boundary batches write there) or a point p with an activity bit at
-// p + {0,1}^3.  The viscosity update at p reads τ at those eight points, and τ is
-// zero where no bit is set, so elsewhere η_next is the rheology of a zero
-// invariant: the same value every iteration.  The eight reads stay inside the
-// vertex range because p is strictly inside.
+// Blocks of the immersed-boundary launch (32·C positions of a row by 8 rows, one
+// plane; C = ib_points) that hold a point outside the strict interior (index 1
+// or n+1 in some dimension: boundary batches write there) or a point p with an
+// activity bit at p + {0,1}^3.  The viscosity update at p reads τ at those eight
+// points, and τ is zero where no bit is set, so elsewhere η_next is the rheology
+// of a zero invariant: the same value every iteration.  The eight reads stay
+// inside the vertex range because p is strictly inside.
+template <int C>
 __global__ void __launch_bounds__(256) ib_blocks_kernel(Geom g, const unsigned char *flags, uint2 *list, int *count) {
-    Idx x = vertex_index(g);
+    const BlockList none{nullptr, 0};
+    const IbRow r = ib_row(g, none, C);
     bool need = false;
-    if (x.ok) {
-        const bool inner = x.i >= 2 && x.i <= g.n[0] && x.j >= 2 && x.j <= g.n[1] && x.k >= 2 && x.k <= g.n[2];
+#pragma unroll
+    for (int c = 0; c < C; c++) {
+        const int i = r.i + 32 * c;
+        if (i > g.n[0] + 1 || r.j > g.n[1] + 1) continue;
+        const bool inner = i >= 2 && i <= g.n[0] && r.j >= 2 && r.j <= g.n[1] && r.k >= 2 && r.k <= g.n[2];
         if (!inner) {
             need = true;
         } else {
-            const long long I = x.I, sx = g.pitch, sxy = g.sxy;
-            need = (flags[I] | flags[I + 1] | flags[I + sx] | flags[I + sx + 1] | flags[I + sxy] | flags[I + sxy + 1] |
-                    flags[I + sxy + sx] | flags[I + sxy + sx + 1]) != 0;
+            const long long I = r.I + 32 * c, sx = g.pitch, sxy = g.sxy;
+            need |= (flags[I] | flags[I + 1] | flags[I + sx] | flags[I + sx + 1] | flags[I + sxy] | flags[I + sxy + 1] |
+                     flags[I + sxy + sx] | flags[I + sxy + sx + 1]) != 0;
         }
     }
     if (__syncthreads_or(need) && threadIdx.x == 0 && threadIdx.y == 0)
         list[atomicAdd(count, 1)] = make_uint2(blockIdx.x | (blockIdx.y << 16), blockIdx.z);
 }
 
+template <typename T>
 cudaError_t launch_ib_blocks(const Geom &g, const unsigned char *flags, uint2 *list, int *count, cudaStream_t s) {
-    dim3 blk(32, 8);
-    ib_blocks_kernel<<<vertex_grid(g, blk), blk, 0, s>>>(g, flags, list, count);
+    constexpr int C = ib_points<T>();
+    ib_blocks_kernel<C><<<ib_grid(g, C), dim3(32, 8), 0, s>>>(g, flags, list, count);
     return cudaGetLastError();
 }
 
@@ -794,6 +966,7 @@ cudaError_t launch_residual_norms(const Geom &g, const KParams &p, const Ptrs<T>
     template cudaError_t launch_compute_tau<T>(const Geom &, const KParams &, const Ptrs<T> &, bool, cudaStream_t);   \
     template cudaError_t launch_ib_flags<T>(const Geom &, const KParams &, const Ptrs<T> &, unsigned char *, cudaStream_t);       \
     template cudaError_t launch_bc_batch<T>(const Geom &, const BcBatch &, cudaStream_t);                          \
+    template cudaError_t launch_ib_blocks<T>(const Geom &, const unsigned char *, uint2 *, int *, cudaStream_t);   \
     template cudaError_t launch_residual_norms<T>(const Geom &, const KParams &, const Ptrs<T> &, bool, double *,  \
                                                   int, double *, cudaStream_t);
 FI_INST(double)
