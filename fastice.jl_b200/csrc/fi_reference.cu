@@ -324,7 +324,7 @@ __global__ void __launch_bounds__(256, C == 1 ? 6 : 4) ib_V_kernel(Geom g, KPara
         if (ok[c]) f.eta_next[r.I + 32 * c] = en[c];
 }
 
-template <typename T, int ND, bool IB>
+template <typename T, int ND>
 __global__ void __launch_bounds__(256) update_sigma_kernel(Geom g, KParams p, Ptrs<T> f, BlockList bl) {
     Idx x = vertex_index(g, bl);
     if (!x.ok) return;
@@ -346,28 +346,24 @@ __global__ void __launch_bounds__(256) update_sigma_kernel(Geom g, KParams p, Pt
     }
     const T idz = T(p.inv_dx[2]);
     const T *Vz = f.Vz;
-    const T thr = T(p.small);
-    if (!IB) {
-        T exx = (Vx[I + 1] - Vx[I]) * idx;
-        T eyy = (Vy[I + sx] - Vy[I]) * idy;
-        T ezz = (Vz[I + sxy] - Vz[I]) * idz;
-        T exy = T(0.5) * ((Vy[I] - Vy[I - 1]) * idx + (Vx[I] - Vx[I - sx]) * idy);
-        T exz = T(0.5) * ((Vz[I] - Vz[I - 1]) * idx + (Vx[I] - Vx[I - sxy]) * idz);
-        T eyz = T(0.5) * ((Vz[I] - Vz[I - sx]) * idy + (Vy[I] - Vy[I - sxy]) * idz);
-        T divV = exx + eyy + ezz;
-        T etac = eta[I];
-        f.P[I] = f.P[I] - (p.p_forcing ? divV + f.fP[I] : divV) * etac * T(p.dt_P);
-        f.txx[I] = f.txx[I] - (f.txx[I] - T(2.0) * etac * (exx - third(divV))) * T(p.dt_tau[0]);
-        f.tyy[I] = f.tyy[I] - (f.tyy[I] - T(2.0) * etac * (eyy - third(divV))) * T(p.dt_tau[1]);
-        f.tzz[I] = f.tzz[I] - (f.tzz[I] - T(2.0) * etac * (ezz - third(divV))) * T(p.dt_tau[2]);
-        T e_xy = h(h(eta[I - 1 - sx] + eta[I - sx]) + h(eta[I - 1] + eta[I]));
-        T e_xz = h(h(eta[I - 1 - sxy] + eta[I - sxy]) + h(eta[I - 1] + eta[I]));
-        T e_yz = h(h(eta[I - sx - sxy] + eta[I - sxy]) + h(eta[I - sx] + eta[I]));
-        f.txy[I] = f.txy[I] - (f.txy[I] - T(2.0) * e_xy * exy) * T(p.dt_tau[3]);
-        f.txz[I] = f.txz[I] - (f.txz[I] - T(2.0) * e_xz * exz) * T(p.dt_tau[4]);
-        f.tyz[I] = f.tyz[I] - (f.tyz[I] - T(2.0) * e_yz * eyz) * T(p.dt_tau[5]);
-        return;
-    }
+    T exx = (Vx[I + 1] - Vx[I]) * idx;
+    T eyy = (Vy[I + sx] - Vy[I]) * idy;
+    T ezz = (Vz[I + sxy] - Vz[I]) * idz;
+    T exy = T(0.5) * ((Vy[I] - Vy[I - 1]) * idx + (Vx[I] - Vx[I - sx]) * idy);
+    T exz = T(0.5) * ((Vz[I] - Vz[I - 1]) * idx + (Vx[I] - Vx[I - sxy]) * idz);
+    T eyz = T(0.5) * ((Vz[I] - Vz[I - sx]) * idy + (Vy[I] - Vy[I - sxy]) * idz);
+    T divV = exx + eyy + ezz;
+    T etac = eta[I];
+    f.P[I] = f.P[I] - (p.p_forcing ? divV + f.fP[I] : divV) * etac * T(p.dt_P);
+    f.txx[I] = f.txx[I] - (f.txx[I] - T(2.0) * etac * (exx - third(divV))) * T(p.dt_tau[0]);
+    f.tyy[I] = f.tyy[I] - (f.tyy[I] - T(2.0) * etac * (eyy - third(divV))) * T(p.dt_tau[1]);
+    f.tzz[I] = f.tzz[I] - (f.tzz[I] - T(2.0) * etac * (ezz - third(divV))) * T(p.dt_tau[2]);
+    T e_xy = h(h(eta[I - 1 - sx] + eta[I - sx]) + h(eta[I - 1] + eta[I]));
+    T e_xz = h(h(eta[I - 1 - sxy] + eta[I - sxy]) + h(eta[I - 1] + eta[I]));
+    T e_yz = h(h(eta[I - sx - sxy] + eta[I - sxy]) + h(eta[I - sx] + eta[I]));
+    f.txy[I] = f.txy[I] - (f.txy[I] - T(2.0) * e_xy * exy) * T(p.dt_tau[3]);
+    f.txz[I] = f.txz[I] - (f.txz[I] - T(2.0) * e_xz * exz) * T(p.dt_tau[4]);
+    f.tyz[I] = f.tyz[I] - (f.tyz[I] - T(2.0) * e_yz * eyz) * T(p.dt_tau[5]);
 }
 
 // ---------------------------------------------------------------------------
@@ -375,12 +371,11 @@ __global__ void __launch_bounds__(256) update_sigma_kernel(Geom g, KParams p, Pt
 // ---------------------------------------------------------------------------
 // resident blocks per SM asked of the compiler: 6 (40 registers) for the 2D form,
 // 4 (64) for the 3D form
-template <int ND, bool IB>
+template <int ND>
 constexpr int update_V_min_blocks() { return ND == 2 ? 6 : 4; }
 
-template <typename T, int ND, bool IB>
-__global__ void __launch_bounds__(256, update_V_min_blocks<ND, IB>()) update_V_kernel(Geom g, KParams p, Ptrs<T> f,
-                                                                                   BlockList bl) {
+template <typename T, int ND>
+__global__ void __launch_bounds__(256, update_V_min_blocks<ND>()) update_V_kernel(Geom g, KParams p, Ptrs<T> f, BlockList bl) {
     Idx x = vertex_index(g, bl);
     if (!x.ok) return;
     const long long I = x.I, sx = g.pitch, sxy = g.sxy;
@@ -409,23 +404,21 @@ __global__ void __launch_bounds__(256, update_V_min_blocks<ND, IB>()) update_V_k
     const T idz = T(p.inv_dx[2]);
     const T *tzz = f.tzz, *txz = f.txz, *tyz = f.tyz;
     T gx = gravity_dev(p, f.gx, 0, I), gy = gravity_dev(p, f.gy, 1, I), gz = gravity_dev(p, f.gz, 2, I);
-    if (!IB) {
-        T ex = h(eta[I - 1] + eta[I]);
-        T ey = h(eta[I - sx] + eta[I]);
-        T ez = h(eta[I - sxy] + eta[I]);
-        f.Vx[I] = f.Vx[I] + div_fast(-(P[I] - P[I - 1]) * idx + (txx[I] - txx[I - 1]) * idx + (txy[I + sx] - txy[I]) * idy +
-                                        (txz[I + sxy] - txz[I]) * idz - gx,
-                                    ex) *
-                                T(p.dt_V[0]);
-        f.Vy[I] = f.Vy[I] + div_fast(-(P[I] - P[I - sx]) * idy + (tyy[I] - tyy[I - sx]) * idy + (txy[I + 1] - txy[I]) * idx +
-                                        (tyz[I + sxy] - tyz[I]) * idz - gy,
-                                    ey) *
-                                T(p.dt_V[1]);
-        f.Vz[I] = f.Vz[I] + div_fast(-(P[I] - P[I - sxy]) * idz + (tzz[I] - tzz[I - sxy]) * idz + (txz[I + 1] - txz[I]) * idx +
-                                        (tyz[I + sx] - tyz[I]) * idy - gz,
-                                    ez) *
-                                T(p.dt_V[2]);
-    }
+    T ex = h(eta[I - 1] + eta[I]);
+    T ey = h(eta[I - sx] + eta[I]);
+    T ez = h(eta[I - sxy] + eta[I]);
+    f.Vx[I] = f.Vx[I] + div_fast(-(P[I] - P[I - 1]) * idx + (txx[I] - txx[I - 1]) * idx + (txy[I + sx] - txy[I]) * idy +
+                                    (txz[I + sxy] - txz[I]) * idz - gx,
+                                ex) *
+                            T(p.dt_V[0]);
+    f.Vy[I] = f.Vy[I] + div_fast(-(P[I] - P[I - sx]) * idy + (tyy[I] - tyy[I - sx]) * idy + (txy[I + 1] - txy[I]) * idx +
+                                    (tyz[I + sxy] - tyz[I]) * idz - gy,
+                                ey) *
+                            T(p.dt_V[1]);
+    f.Vz[I] = f.Vz[I] + div_fast(-(P[I] - P[I - sxy]) * idz + (tzz[I] - tzz[I - sxy]) * idz + (txz[I + 1] - txz[I]) * idx +
+                                    (tyz[I + sx] - tyz[I]) * idy - gz,
+                                ez) *
+                            T(p.dt_V[2]);
     if (p.freeze_eta) return;
     if (linear_unrelaxed(p)) {  // the stress invariant is not needed
         f.eta_next[I] = p.rheo_eta_is_field ? f.eta_lin[I] : T(p.rheo_eta);
@@ -819,9 +812,9 @@ cudaError_t launch_update_sigma(const Geom &g, const KParams &p, const Ptrs<T> &
     dim3 grd = vertex_grid(g, blk);
     const BlockList none{nullptr, 0};
     constexpr int C = ib_points<T>();
-    if (g.nd == 2) update_sigma_kernel<T, 2, false><<<grd, blk, 0, s>>>(g, p, f, none);
+    if (g.nd == 2) update_sigma_kernel<T, 2><<<grd, blk, 0, s>>>(g, p, f, none);
     else if (ib) ib_sigma_kernel<T, C><<<bl ? dim3(bl->count) : ib_grid(g, C), blk, 0, s>>>(g, p, f, bl ? *bl : none);
-    else update_sigma_kernel<T, 3, false><<<grd, blk, 0, s>>>(g, p, f, none);
+    else update_sigma_kernel<T, 3><<<grd, blk, 0, s>>>(g, p, f, none);
     return cudaGetLastError();
 }
 
@@ -832,9 +825,9 @@ cudaError_t launch_update_V(const Geom &g, const KParams &p, const Ptrs<T> &f, b
     dim3 grd = vertex_grid(g, blk);
     const BlockList none{nullptr, 0};
     constexpr int C = ib_points<T>();
-    if (g.nd == 2) update_V_kernel<T, 2, false><<<grd, blk, 0, s>>>(g, p, f, none);
+    if (g.nd == 2) update_V_kernel<T, 2><<<grd, blk, 0, s>>>(g, p, f, none);
     else if (ib) ib_V_kernel<T, C><<<bl ? dim3(bl->count) : ib_grid(g, C), blk, 0, s>>>(g, p, f, bl ? *bl : none);
-    else update_V_kernel<T, 3, false><<<grd, blk, 0, s>>>(g, p, f, none);
+    else update_V_kernel<T, 3><<<grd, blk, 0, s>>>(g, p, f, none);
     return cudaGetLastError();
 }
 

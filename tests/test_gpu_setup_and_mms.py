@@ -221,6 +221,37 @@ def test_immersed_boundary_zero_stores_skipped_after_full_iterations(rheo):
     np.testing.assert_array_equal(a[[0, 1, 2, 3]], b[[0, 1, 2, 3]])
 
 
+def test_immersed_boundary_f32_two_points_per_thread():
+    # FP32 threads of the immersed-boundary sweeps own two points 32 apart in x.
+    # A row of 71 vertex positions fills one 64-wide block and part of a second,
+    # so threads with both points in the row and threads whose second point lies
+    # past the row's end both occur; bit for bit with the oracle in FP32, through
+    # full iterations and the steady state (zeros not stored, block list)
+    fi, O = load_fastice(), load_oracle()
+    n = (70, 12, 14)
+    ext = (1.0, 0.5, 0.6)
+    dx = tuple(e / c for e, c in zip(ext, n))
+    psi_ns = -_sphere_psi(n, dx, (0.5, 0.25, -0.2), 0.45)
+    psi_na = _sphere_psi(n, dx, (0.5, 0.25, 0.3), 0.45)
+    trac = ("traction", (0.0, 0.0, 0.0))
+    bcs = ((("velocity", (0.1, 0.0, 0.0)), trac), (trac, trac), (("slip", (0.0, 0.0, 0.0)), trac))
+    p = Pair(n, bcs, path="reference", library="strict", dtype="f32", seed=34, origin=(0.0, 0.0, 0.0), extent=ext,
+             immersed_psi={"na": psi_na, "ns": psi_ns})
+    # (an FP32 model rounds its FP64 volume fractions once, as the oracle does)
+    p.advance(3)
+    bad = p.bitwise_equal()
+    assert not bad, bad
+    p.advance(10)
+    bad = p.bitwise_equal()
+    finite = all(np.isfinite(p.oracle.interior(name)).all() for name in p.state)
+    a = p.model.residual_norms()
+    b = p.oracle.residual_norms()
+    p.close()
+    assert finite
+    assert not bad, bad
+    np.testing.assert_array_equal(a[[0, 1, 2, 3]], b[[0, 1, 2, 3]])
+
+
 def test_model_omega_from_psi_matches_standalone():
     fi = load_fastice()
     n, ext = (16, 12, 10), (1.0, 0.75, 0.6)
