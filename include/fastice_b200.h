@@ -212,7 +212,10 @@ typedef struct {
 fi_status fi_model_solve(fi_model *m, const fi_solve_opts *opts, fi_solve_report *rep);
 
 /* swap-free view of the model state for callers that manage device memory:
- * device pointer of a field's storage (uniform halo box, see fi_model_layout). */
+ * device pointer of a field's storage (uniform halo box, see fi_model_layout).
+ * The caller may write through it at any later time, so for an immersed-boundary
+ * model a pointer to P, τ or V turns off for good the iterations' skipping of
+ * zeros already stored at inactive points (results are the same either way). */
 fi_status fi_model_device_ptr(fi_model *m, int32_t field, void **dptr);
 /* storage box: pitch (elements per x row, >= n0+3), rows per plane (n1+3),
  * planes (n2+3, 1 in 2D); index (i,j,k) -> i + pitch*(j + rows*k), 0 = ghost. */
