@@ -46,7 +46,7 @@ TRAFFIC_BYTES_PER_CELL = {"f64": 233.3, "f32": None}
 # block list in use): dram__bytes_read.sum + dram__bytes_write.sum of one
 # ncu-captured iteration of the 191^3 glacier divided by its cell count
 # (profiles/ib_glacier191_dram.md); the same geometry scales to 383^3.
-IB_TRAFFIC_BYTES_PER_CELL = {"f64": 109.5, "f32": 62.5}
+IB_TRAFFIC_BYTES_PER_CELL = {"f64": 109.5, "f32": 74.9}
 
 
 def load_fastice():
