@@ -437,10 +437,10 @@ def run_glacier(args):
     fractions from the level sets, linear viscosity; one step = one PT iteration
     (advance_iteration! of the immersed-boundary model).  value = T_eff in the
     reference's convention: 36 array passes over the whole box per iteration (FP64;
-    FP32 in the same line).  About half of the box is ice-free, where the masked
-    kernels write zeros without reading their inputs, so this figure can exceed the
-    copy bandwidth; the DRAM bytes an iteration really moves (ncu) and the bandwidth
-    they imply are reported beside it."""
+    FP32 in the same line).  About three quarters of the box are ice-free, where the
+    masked kernels read only the activity byte and, once the zeros are stored, write
+    nothing, so this figure can exceed the copy bandwidth; the DRAM bytes an iteration
+    really moves (ncu) and the bandwidth they imply are reported beside it."""
     import torch
     fi = load_fastice()
     from fastice_b200 import scenarios

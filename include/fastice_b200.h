@@ -39,7 +39,7 @@ typedef enum {
     FI_ERR_DIVERGED = 3,    /* non-finite residual */
     FI_ERR_TIMEOUT = 4,     /* iteration budget or bounded wait exhausted */
     FI_ERR_CUDA = 5,        /* CUDA runtime error */
-    FI_ERR_UNSUPPORTED = 6, /* valid request this build does not implement */
+    FI_ERR_UNSUPPORTED = 6, /* valid request the library does not implement */
     FI_ERR_STATE = 7        /* call not valid in the object's current state */
 } fi_status;
 

@@ -1,4 +1,4 @@
-"""GPU parity for configs[0] (2D manufactured solution), the immersed-boundary
+"""GPU parity for the 2D manufactured solution (128^2 unit square), the immersed-boundary
 model, and the level-set / volume-fraction set-up kernels, against the oracle."""
 import math
 
@@ -36,8 +36,8 @@ def mms2d_oracle(fi, O, grid, gravity):
     return o
 
 
-def test_config1_bit_level_after_1000_iterations():
-    # configs[0]: 128^2 unit square, free slip, manufactured forcing; strict build vs oracle, bit for bit
+def test_mms2d_128_bit_level_after_1000_iterations():
+    # 128^2 unit square, free slip, manufactured forcing; strict build vs oracle, bit for bit
     fi, O = load_fastice(), load_oracle()
     grid, m = mms2d_model(fi, 128, library="strict")
     o = mms2d_oracle(fi, O, grid, mms2d_gravity(fi, grid))
@@ -49,8 +49,8 @@ def test_config1_bit_level_after_1000_iterations():
     m.close()
 
 
-def test_config1_converges_second_order():
-    # configs[0] solved to ||R||inf < 1e-8 on the GPU; L2 error vs the analytic field converges at O(h^2)
+def test_mms2d_converges_second_order():
+    # the 2D manufactured solution solved to ||R||inf < 1e-8 on the GPU; L2 error vs the analytic field converges at O(h^2)
     fi = load_fastice()
     errs = []
     for n in (32, 64, 128):

@@ -59,7 +59,7 @@ def test_coords(fi, chmy_grid):
     assert math.isclose(xs[1], -1.0) and math.isclose(xs[0], -1.4)
 
 
-# ---- manufactured solution (config 1 on the unit square) ---------------------------------
+# ---- 2D manufactured solution on the unit square ------------------------------------------
 def _mms2d_oracle(orc, n, max_iter_factor=60):
     ext, org = (1.0, 1.0), (0.0, 0.0)
     dx = ext[0] / n
