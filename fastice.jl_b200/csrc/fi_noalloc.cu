@@ -5,9 +5,11 @@
 // per-block partial results in a file-scope static device array instead of a
 // buffer allocated by a model.  Callers that cannot call cudaMalloc: a host
 // program whose device memory is owned by another runtime's allocator or pool
-// (a Julia or Python runtime that hands out device pointers), code that runs
-// while a stream is being captured into a CUDA graph (allocation calls are not
-// allowed there), and long-running services that forbid allocation after start-up.
+// (a Julia or Python runtime that hands out device pointers and counts every
+// byte), and long-running services that fix their device memory at start-up and
+// forbid allocation afterwards (an allocation there could fail or stall a loop).
+// The first call on a device looks up the array's device address
+// (cudaGetSymbolAddress); make that first call before any stream capture.
 //
 // Limits and sharing.  The array holds kNoAllocSlots per-block partials
 // (kNoAllocSlots * 12 doubles, 3 MiB), and every loaded device keeps its own

@@ -253,9 +253,9 @@ typedef struct {
 
 /* Residual norms that allocate nothing.  No counterpart in the reference: it is
  * fi_model_residual_norms for callers that cannot allocate device memory -- a
- * host program whose device memory belongs to another runtime's allocator, code
- * running while a stream is captured into a CUDA graph, services that forbid
- * allocation after start-up.  It computes the same FI_NORMS_LEN values for the
+ * host program whose device memory belongs to another runtime's allocator,
+ * services that fix their device memory at start-up and forbid allocation
+ * afterwards.  It computes the same FI_NORMS_LEN values for the
  * state in `state` (problem described by `desc`; desc->path and device are
  * ignored, the current device is used) into the caller's device buffer out_dev,
  * asynchronously on `stream` (a cudaStream_t, NULL for the default stream).

@@ -1,8 +1,8 @@
 """fi_residual_norms_noalloc: the residual-norm entry point that allocates nothing.
 
 It exists for callers that cannot call cudaMalloc -- a program whose device
-memory is owned by another runtime's allocator, code running inside a CUDA-graph
-stream capture, services that forbid allocation after start-up.  Its partial sums
+memory is owned by another runtime's allocator, services that forbid allocation
+after start-up.  Its partial sums
 live in a static device array, so it must give the same norms as the model's own
 entry point (fi_model_residual_norms), which keeps its partials in a buffer the
 model allocated.  This file is collected last so that a run stopping at the first
