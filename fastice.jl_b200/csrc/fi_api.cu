@@ -163,6 +163,54 @@ cudaMemcpy3DParms copy_params(const fi_model *m, int field, void *dev, void *hos
     return p;
 }
 
+// Host interior -> device halo box.  A pitched 3D copy from host memory runs at
+// about half the linear copy rate (rows of a few KB), so the interior goes over
+// as linear copies of whole z planes into a staging buffer (at most 64 MB, at
+// least one plane, never more than the field), each followed by a kernel that
+// writes the rows into the box; both are issued on the model's stream, so one
+// buffer suffices.
+template <typename E>
+__global__ void __launch_bounds__(256) scatter_rows(const E *__restrict__ src, E *__restrict__ dst, int nx, int ny,
+                                                    long long pitch, long long rows) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= nx) return;
+    const long long z = blockIdx.y;
+    for (int y = 0; y < ny; y++) dst[x + pitch * (y + rows * z)] = src[x + (long long)nx * (y + (long long)ny * z)];
+}
+
+fi_status upload_interior(fi_model *m, int field, const void *host) {
+    int loc[3];
+    field_loc(field, loc);
+    const int nd = m->d.grid.nd;
+    const int nx = m->d.grid.n[0] + loc[0], ny = m->d.grid.n[1] + loc[1], nz = nd == 3 ? m->d.grid.n[2] + loc[2] : 1;
+    const size_t plane = (size_t)nx * ny * m->esz;
+    const size_t want = std::max(plane, std::min((size_t)64 << 20, plane * nz));
+    if (m->stage_bytes < want) {
+        if (m->d_stage) cudaFree(m->d_stage);
+        m->d_stage = nullptr, m->stage_bytes = 0;
+        if (cudaMalloc(&m->d_stage, want) != cudaSuccess) return cuda_fail(cudaGetLastError(), "staging buffer");
+        m->stage_bytes = want;
+    }
+    const int per = (int)std::min<size_t>(65535, std::max<size_t>(1, m->stage_bytes / plane));  // grid.y limit
+    char *dev = (char *)m->cur(field) + (1 + m->g.pitch * (1 + m->g.rows * (nd == 3 ? 1 : 0))) * (long long)m->esz;
+    const char *src = (const char *)host;
+    for (int z0 = 0; z0 < nz; z0 += per) {
+        const int zc = std::min(per, nz - z0);
+        FI_CHECK_CUDA(cudaMemcpyAsync(m->d_stage, src + plane * z0, plane * zc, cudaMemcpyHostToDevice, m->stream),
+                      "set_field copy");
+        char *d = dev + (long long)z0 * m->g.sxy * (long long)m->esz;
+        const dim3 grd((nx + 255) / 256, zc);
+        if (m->esz == 8)
+            scatter_rows<unsigned long long><<<grd, 256, 0, m->stream>>>(
+                (const unsigned long long *)m->d_stage, (unsigned long long *)d, nx, ny, m->g.pitch, m->g.rows);
+        else
+            scatter_rows<unsigned int><<<grd, 256, 0, m->stream>>>((const unsigned int *)m->d_stage, (unsigned int *)d,
+                                                                   nx, ny, m->g.pitch, m->g.rows);
+        FI_CHECK_CUDA(cudaGetLastError(), "set_field rows");
+    }
+    return FI_OK;
+}
+
 // ---- boundary-condition batches (boundary_conditions.jl) -------------------
 void add_op(BcBatch &b, void *f, int field, int side, int op, double v) {
     BcOpDesc &o = b.ops[b.count++];
@@ -637,6 +685,7 @@ fi_status fi_model_destroy(fi_model *m) {
     for (cudaGraphExec_t &g : m->pair_graph)
         if (g) cudaGraphExecDestroy(g);
     field_free(m->fP, m->esz);
+    if (m->d_stage) cudaFree(m->d_stage);
     if (m->shadow) fi_model_destroy(m->shadow);
     if (m->d_partials) cudaFree(m->d_partials);
     if (m->d_out) cudaFree(m->d_out);
@@ -661,8 +710,8 @@ fi_status fi_model_set_field(fi_model *m, int32_t field, const void *host, size_
         fi_status st = ensure_residual_arrays(m);
         if (st != FI_OK) return st;
     }
-    cudaMemcpy3DParms p = copy_params(m, field, m->cur(field), const_cast<void *>(host), true);
-    FI_CHECK_CUDA(cudaMemcpy3DAsync(&p, m->stream), "set_field copy");
+    fi_status st = upload_interior(m, field, host);
+    if (st != FI_OK) return st;
     FI_CHECK_CUDA(cudaStreamSynchronize(m->stream), "set_field sync");
     m->full_iters = 0;
     if (field >= FI_FIELD_NA_CCC) m->ibf_stale = true;

@@ -54,6 +54,8 @@ struct fi_model {
     int full_iters = 0;
     bool state_ptr_out = false;
     void *fP = nullptr;    // pressure forcing (defect-correction shadow models only)
+    void *d_stage = nullptr;  // staging buffer of set_field (contiguous rows of host data)
+    size_t stage_bytes = 0;
     fi_model *shadow = nullptr;  // FP32 model of the mixed-precision solve (created on first use)
     KParams shadow_kp{};         // the shadow's parameters as created (gravity as fields); each solve starts from them
     // TMA maps (128 bytes each) of every buffer the fused sweep reads
