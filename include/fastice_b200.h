@@ -155,7 +155,9 @@ fi_status fi_model_create(const fi_model_desc *desc, fi_model **out);
 fi_status fi_model_destroy(fi_model *m);
 
 /* set!(field, array) / Array(interior(field)): interior values, x fastest, in the
- * model's dtype; nbytes must equal the field's interior size times sizeof(dtype). */
+ * model's dtype; nbytes must equal the field's interior size times sizeof(dtype).
+ * set_field stages the upload through a device buffer that the model keeps until
+ * it is destroyed (at most 64 MB, at least one z plane, at most one field). */
 fi_status fi_model_set_field(fi_model *m, int32_t field, const void *host, size_t nbytes);
 fi_status fi_model_get_field(fi_model *m, int32_t field, void *host, size_t nbytes);
 /* interior element count of a field (n or n+1 per dim by location) */
