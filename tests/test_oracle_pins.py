@@ -4,8 +4,8 @@ The reference's only tests touching the discretisation are the Chmy grid
 geometry checks of test/test_chmy_grids.jl; their expected values are restated
 here and checked against the host UniformGrid and the oracle's coordinate
 convention.  The operators are further anchored by the O(h^2) convergence of
-the manufactured solution of scripts_future_API/stokes_manufactured_solution_free_slip_2D.jl,
-and the cut-cell volumes by closed-form known answers.
+the manufactured solutions of scripts_future_API/stokes_manufactured_solution_free_slip_2D.jl
+and _3D.jl, and the cut-cell volumes by closed-form known answers.
 """
 import math
 
@@ -103,6 +103,59 @@ def test_oracle_mms2d_second_order(orc):
         errs.append(err)
     orders = [math.log2(errs[i] / errs[i + 1]) for i in range(len(errs) - 1)]
     assert all(1.9 < o < 2.1 for o in orders), orders
+
+
+# ---- 3D manufactured solution on [-1,1]^3 (stokes_manufactured_solution_free_slip_3D.jl:25-48) ----
+def _mf(a, b):
+    return np.cos(math.pi * a) * (b ** 2 - 1) ** 2 - np.cos(math.pi * b) * (a ** 2 - 1) ** 2
+
+
+def _mp(a, b):
+    return np.cos(math.pi * b) * (1 - 3 * a ** 2) * 2 - np.cos(math.pi * a) * (1 - 3 * b ** 2) * 2
+
+
+def _mms3d_oracle(fi, orc, n, max_iter_factor=80):
+    ext, org = (2.0, 2.0, 2.0), (-1.0, -1.0, -1.0)
+    dx = ext[0] / n
+    dt = fi.pt_params(fi.UniformGrid(origin=org, extent=ext, dims=(n, n, n)))["Δτ"]
+    taus = ("xx", "yy", "zz", "xy", "xz", "yz")
+    slip = (orc.BC_SLIP, (0, 0, 0))
+    spec = orc.Spec(nd=3, n=(n, n, n), extent=ext, origin=org, bcs=((slip, slip),) * 3, dt_P=dt["Pr"],
+                    dt_tau=tuple(dt["τ"][k] for k in taus), dt_V=tuple(dt["V"][k] for k in "xyz"))
+    sh = spec.storage_shape()
+    k, j, i = np.meshgrid(np.arange(sh[0]), np.arange(sh[1]), np.arange(sh[2]), indexing="ij")
+    v = lambda q: org[0] + (q - 1) * dx  # noqa: E731  (vertex coordinate of index q)
+    c = lambda q: org[0] + (q - 0.5) * dx  # noqa: E731  (centre coordinate of index q)
+    gx = -2 * np.sin(math.pi * v(i)) * (_mf(c(j), c(k)) * math.pi ** 2 - _mp(c(j), c(k)))
+    gy = -2 * np.sin(math.pi * v(j)) * (_mf(c(k), c(i)) * math.pi ** 2 - _mp(c(k), c(i)))
+    gz = -2 * np.sin(math.pi * v(k)) * (_mf(c(i), c(j)) * math.pi ** 2 - _mp(c(i), c(j)))
+    m = orc.OracleStokes(spec, gravity_arrays={"gx": gx, "gy": gy, "gz": gz})
+    m.a["eta"][:] = 1.0
+    m.a["eta_next"][:] = 1.0
+    m.apply_initial_bcs()
+    it = 0
+    while it < max_iter_factor * n:
+        m.advance(n)
+        it += n
+        nr = m.residual_norms()
+        if max(nr[:4]) < 1e-8:
+            break
+    ex = (np.sin(math.pi * v(i)) * _mf(c(j), c(k)))[1:n + 1, 1:n + 1, 1:n + 2]
+    ey = (np.sin(math.pi * v(j)) * _mf(c(k), c(i)))[1:n + 1, 1:n + 2, 1:n + 1]
+    ez = (np.sin(math.pi * v(k)) * _mf(c(i), c(j)))[1:n + 2, 1:n + 1, 1:n + 1]
+    num = sum(np.sum((m.interior(f) - e) ** 2) for f, e in (("Vx", ex), ("Vy", ey), ("Vz", ez)))
+    den = sum(np.sum(e ** 2) for e in (ex, ey, ez))
+    return math.sqrt(num / den), it, max(nr[:4])
+
+
+def test_oracle_mms3d_second_order(fi, orc):
+    errs = []
+    for n in (8, 16, 32):
+        err, it, res = _mms3d_oracle(fi, orc, n)
+        assert res < 1e-8, (n, it, res)
+        errs.append(err)
+    orders = [math.log2(errs[i] / errs[i + 1]) for i in range(len(errs) - 1)]
+    assert 1.8 < orders[-1] < 2.2, (errs, orders)
 
 
 # ---- cut-cell volumes (volume_fractions.jl) -------------------------------------------------
