@@ -158,6 +158,35 @@ def test_oracle_mms3d_second_order(fi, orc):
     assert 1.8 < orders[-1] < 2.2, (errs, orders)
 
 
+# ---- hydrostatic column: sign of the pressure gradient against ρg, traction ghost of P --------
+def test_oracle_hydrostatic_column_is_steady(fi, orc):
+    # V = 0, τ = 0 and P = ρg_z (z_top - z) under a traction-free top: the residual
+    # r_V = -∇P + ∇·τ - ρg (kernels_3d.jl:66-75) vanishes, the top's Dirichlet ghost
+    # of P (boundary_conditions.jl:51-76) continues the line, and PT iterations leave
+    # the state where it is
+    n, ext, org = (6, 5, 12), (1.0, 0.8, 0.6), (0.0, 0.0, 0.0)
+    dt = fi.pt_params(fi.UniformGrid(origin=org, extent=ext, dims=n))["Δτ"]
+    taus = ("xx", "yy", "zz", "xy", "xz", "yz")
+    per = (orc.BC_PERIODIC, (0, 0, 0))
+    bcs = ((per, per), (per, per), ((orc.BC_SLIP, (0, 0, 0)), (orc.BC_TRACTION, (0, 0, 0))))
+    spec = orc.Spec(nd=3, n=n, extent=ext, origin=org, bcs=bcs, dt_P=dt["Pr"], dt_tau=tuple(dt["τ"][k] for k in taus),
+                    dt_V=tuple(dt["V"][k] for k in "xyz"), g_val=(0.0, 0.0, 1.0))
+    m = orc.OracleStokes(spec)
+    dz = ext[2] / n[2]
+    zc = org[2] + (np.arange(n[2]) + 0.5) * dz
+    P = np.broadcast_to((ext[2] - zc)[:, None, None], (n[2], n[1], n[0])).copy()
+    m.set_interior("P", P)
+    m.a["eta"][:] = 1.0
+    m.a["eta_next"][:] = 1.0
+    m.apply_initial_bcs()
+    nr = m.residual_norms()
+    assert max(nr[:4]) < 1e-12, nr[:4]
+    m.advance(50)
+    for f in ("Vx", "Vy", "Vz"):
+        assert np.max(np.abs(m.interior(f))) < 1e-12, f
+    np.testing.assert_allclose(m.interior("P"), P, rtol=0, atol=1e-12)
+
+
 # ---- cut-cell volumes (volume_fractions.jl) -------------------------------------------------
 def test_vol_box_full_and_empty(orc):
     d = (0.3, 0.2, 0.5)
