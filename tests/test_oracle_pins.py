@@ -187,6 +187,42 @@ def test_oracle_hydrostatic_column_is_steady(fi, orc):
     np.testing.assert_allclose(m.interior("P"), P, rtol=0, atol=1e-12)
 
 
+# ---- the immersed-boundary restatement with every volume fraction 1 is the plain model ----------
+@pytest.mark.parametrize("rheo", ["linear", "glen"])
+def test_oracle_immersed_boundary_with_full_fractions_is_the_plain_model(fi, orc, rheo):
+    # ω = 1 everywhere: every masked derivative (IB kernels_3d.jl:3-74) reduces to the
+    # plain one (kernels_3d.jl:3-40), every point is active, and the division by
+    # the face fraction is by 1, so the two restatements agree bit for bit
+    n, ext, org = (9, 7, 8), (1.0, 0.9, 0.8), (0.0, 0.0, 0.0)
+    dt = fi.pt_params(fi.UniformGrid(origin=org, extent=ext, dims=n))["Δτ"]
+    taus = ("xx", "yy", "zz", "xy", "xz", "yz")
+    bcs = (((orc.BC_VELOCITY, (0.1, -0.2, 0.0)), (orc.BC_TRACTION, (0.0, 0.1, 0.0))),
+           ((orc.BC_SLIP, (0.0, 0.0, 0.0)), (orc.BC_SLIP, (0.0, 0.05, 0.0))),
+           ((orc.BC_SLIP, (0.0, 0.0, 0.0)), (orc.BC_TRACTION, (0.0, 0.0, 0.0))))
+    kw = dict(rheo_inner=orc.RHEO_POWER, rheo_has_reg=1, rheo_inv_eta_reg=1.0) if rheo == "glen" else {}
+    spec = orc.Spec(nd=3, n=n, extent=ext, origin=org, bcs=bcs, dt_P=dt["Pr"], dt_tau=tuple(dt["τ"][k] for k in taus),
+                    dt_V=tuple(dt["V"][k] for k in "xyz"), g_val=(0.2, -0.1, 1.0), **kw)
+    ones = {c: np.ones(spec.storage_shape()) for c in orc.MASK_COMPONENTS}
+    plain = orc.OracleStokes(spec)
+    ib = orc.OracleStokes(spec, masks={"na": ones, "ns": ones})
+    rng = np.random.default_rng(11)
+    names = ("P", "txx", "tyy", "tzz", "txy", "txz", "tyz", "Vx", "Vy", "Vz", "eta")
+    for name in names:
+        shape = plain.interior(name).shape
+        vals = 0.5 + rng.random(shape) if name == "eta" else 0.1 * rng.standard_normal(shape)
+        for m in (plain, ib):
+            m.set_interior(name, vals)
+            if name == "eta":
+                m.set_interior("eta_next", vals)
+    for m in (plain, ib):
+        m.apply_initial_bcs()
+        m.advance(20)
+    for name in names:
+        a, b = plain.interior(name), ib.interior(name)
+        assert np.isfinite(a).all(), name
+        assert np.array_equal(a.view(np.uint64), b.view(np.uint64)), name
+
+
 # ---- cut-cell volumes (volume_fractions.jl) -------------------------------------------------
 def test_vol_box_full_and_empty(orc):
     d = (0.3, 0.2, 0.5)
