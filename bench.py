@@ -176,7 +176,7 @@ def e2e_run(fi, n, dtype, device, steps, torch, variant=None):
         a = t.numpy().reshape(shape)
         a[...] = 0.0 if nm != "eta" else 5000.0
         host[nm] = (t, a)
-    h2d = sum(a.nbytes for _, a in host.values()) + host["eta"][1].nbytes
+    h2d = sum(a.nbytes for _, a in host.values())
     d2h = sum(a.nbytes for nm, (_, a) in host.items() if nm != "eta") + 8 * 12
     if variant is not None:
         m.set_variant(variant)
@@ -185,7 +185,7 @@ def e2e_run(fi, n, dtype, device, steps, torch, variant=None):
     t0 = time.perf_counter()
     for nm, (_, a) in host.items():
         m.set_field(nm, a)
-    m.set_field("eta_next", host["eta"][1])
+    m.copy_field("eta_next", "eta")  # η_next = η on the device, as drivers do before iterating
     m.apply_bcs()
     m.advance(steps)
     norms = m.residual_norms()
@@ -197,13 +197,15 @@ def e2e_run(fi, n, dtype, device, steps, torch, variant=None):
     return dt, h2d, d2h, norms
 
 
-def cpu_baseline(n, seconds=12.0, warm=1):
-    """The CPU oracle (C restatement, OpenMP) on the same workload: whole
-    iterations at the full grid, as many as fit in `seconds` (at least one)."""
+def load_oracle():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     O.build()
-    fi = load_fastice()
+    return O
+
+
+def oracle_slab(O, fi, n):
+    """The slab workload on the CPU oracle (C restatement), at its initial state."""
     grid, bcs, gravity, rheology, sp = slab_problem(fi, n)
     dt = sp["Δτ"]
     taus = ("xx", "yy", "zz", "xy", "xz", "yz")
@@ -216,6 +218,33 @@ def cpu_baseline(n, seconds=12.0, warm=1):
     m.a["eta"][...] = rheology.eta_reg
     m.a["eta_next"][...] = rheology.eta_reg
     m.apply_initial_bcs()
+    return m
+
+
+OMP_PIN = {"OMP_PROC_BIND": "close", "OMP_PLACES": "cores"}
+
+
+def cpu_baseline(n, seconds=12.0, warm=1):
+    """The CPU oracle (C restatement, OpenMP) on the same workload: whole
+    iterations at the full grid, as many as fit in `seconds` (at least one).
+    Runs in a fresh process with the OpenMP threads pinned (one per host core,
+    bound close), so that both arms of the benchmark time it the same way and no
+    runtime already initialised in this process (torch's) decides its threads."""
+    env = dict(os.environ)
+    env.update(OMP_PIN)
+    threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    env["OMP_NUM_THREADS"] = str(threads)
+    cmd = [sys.executable, os.path.abspath(__file__), "--cpu-baseline-only", "--n", str(n[0]),
+           "--cpu-seconds", str(seconds), "--warmup", str(warm)]
+    r = subprocess.run(cmd, env=env, capture_output=True, text=True, check=True)
+    d = json.loads(r.stdout.strip().splitlines()[-1])
+    return d["iterations"], d["seconds"], d["threads"]
+
+
+def _cpu_baseline_inproc(n, seconds, warm):
+    O = load_oracle()
+    fi = load_fastice()
+    m = oracle_slab(O, fi, n)
     for _ in range(warm):
         m.advance(1)
     its, t0 = 0, time.perf_counter()
@@ -231,6 +260,77 @@ def cpu_baseline(n, seconds=12.0, warm=1):
     except ValueError:
         pass
     return its, el, cores
+
+
+def oracle_parity(fi, n, device, variants, iters=3):
+    """Error of the GPU sweeps against the FP64 oracle at the workload's own size:
+    a fresh model of each precision and the oracle advance `iters` PT iterations
+    from the workload's initial state; per field, max |gpu - oracle| / max |oracle|
+    over the interior, and the worst field."""
+    O = load_oracle()
+    om = oracle_slab(O, fi, n)
+    om.advance(iters)
+    names = ("P", "txx", "tyy", "tzz", "txy", "txz", "tyz", "Vx", "Vy", "Vz", "eta")
+    out = {"iterations": iters, "oracle": "C restatement (FP64) of the reference's kernels"}
+    for dtype, variant in variants.items():
+        m = make_model(fi, n, dtype, device)
+        if variant is not None:
+            m.set_variant(variant)
+        m.advance(iters)
+        per = {}
+        for nm in names:
+            b = om.interior(nm)
+            a = m.get_field(nm).astype(np.float64)
+            a -= b
+            per[nm] = float(np.max(np.abs(a)) / max(float(np.max(np.abs(b))), 1e-300))
+            del a, b
+        m.close()
+        out[dtype] = {"max_rel_diff": max(per.values()), "per_field": per}
+    return out
+
+
+def mms_errors(fi):
+    """Manufactured-solution discretisation errors of this build: the 3D free-slip
+    solution (stokes_manufactured_solution_free_slip_3D.jl) at 127^3 and the 2D one of
+    the 128^2 unit-square case, each solved to |R|inf < 1e-8 in FP64; the 2D case
+    also runs 1000 iterations of the no-FMA build against the oracle, bit for bit."""
+    from fastice_b200 import scenarios
+    res = {}
+    grid, m = scenarios.mms3d_model(127)
+    r = m.solve(max_iter=400 * 127, ncheck=127, tol=1e-8)
+    res["mms3d_127"] = {"l2_rel_error": scenarios.mms3d_error(grid, m), "converged": bool(r["converged"]),
+                        "iterations": r["iterations"]}
+    m.close()
+    for lib_name in ("fast", "strict"):
+        grid, m, gravity = scenarios.mms2d_model(128, library=lib_name)
+        if lib_name == "fast":
+            r = m.solve(max_iter=200 * 128, ncheck=128, tol=1e-8)
+            res["mms2d_128"] = {"l2_rel_error": scenarios.mms2d_error(grid, m), "converged": bool(r["converged"]),
+                                "iterations": r["iterations"]}
+        else:
+            O = load_oracle()
+            om = scenarios_mms2d_oracle(fi, O, grid, gravity)
+            m.advance(1000)
+            om.advance(1000)
+            same = all(np.array_equal(m.get_field(nm).view(np.uint64), om.interior(nm).view(np.uint64))
+                       for nm in ("P", "txx", "tyy", "txy", "Vx", "Vy"))
+            res["mms2d_128"]["bitwise_vs_oracle_after_1000_iterations"] = bool(same)
+        m.close()
+    return res
+
+
+def scenarios_mms2d_oracle(fi, O, grid, gravity):
+    """The 2D manufactured-solution case on the CPU oracle."""
+    sp = fi.pt_params(grid)["Δτ"]
+    slip = (O.BC_SLIP, (0, 0, 0))
+    spec = O.Spec(nd=2, n=grid.dims, extent=grid.extent, origin=grid.origin, bcs=((slip, slip), (slip, slip)),
+                  dt_P=sp["Pr"], dt_tau=(sp["τ"]["xx"], sp["τ"]["yy"], 0.0, sp["τ"]["xy"], 0.0, 0.0),
+                  dt_V=(sp["V"]["x"], sp["V"]["y"], 0.0))
+    o = O.OracleStokes(spec, gravity_arrays={"gx": gravity["x"].sample(), "gy": gravity["y"].sample()})
+    o.a["eta"][...] = 1.0
+    o.a["eta_next"][...] = 1.0
+    o.apply_initial_bcs()
+    return o
 
 
 def _base_line(metric, value, unit, steps, warmup, ms, dtype, cfg, hib=True):
@@ -569,6 +669,10 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--n", type=int, default=511)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity", action="store_true", help="skip the oracle comparison and manufactured-solution "
+                                                            "errors (profiling runs)")
+    ap.add_argument("--cpu-baseline-only", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help=argparse.SUPPRESS)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape (profiling runs)")
     ap.add_argument("--variant", type=int, default=None, help="fused launch shape index (implies --no-autotune)")
@@ -589,6 +693,10 @@ def main():
                          "n=3, A=1, regularised at strain rate 1e-6 (glen_relaxed: relaxed in log scale at rate "
                          "0.1), with the slab's PT steps (r 0.7, re 8 pi)")
     args = ap.parse_args()
+    if args.cpu_baseline_only:
+        its, el, threads = _cpu_baseline_inproc((args.n,) * 3, args.cpu_seconds, args.warmup)
+        print(json.dumps({"iterations": its, "seconds": el, "threads": threads}))
+        return
     if args.workload != "slab":
         {"batched": run_batched, "serving": run_serving, "mixed": run_mixed,
          "glacier": run_glacier, "heat": run_heat}[args.workload](args)
@@ -612,7 +720,8 @@ def main():
                 "impl": "reference",
                 "cpu_baseline": {"value": v, "unit": "GB/s", "cores": cores, "kind": "port",
                                  "sample": f"{its} whole PT iterations at {n[0]}^3 (C restatement of the reference "
-                                           "CPU path, OpenMP; the Julia reference cannot run: no Julia toolchain)"},
+                                           "CPU path, OpenMP threads pinned one per core, OMP_PROC_BIND=close; the "
+                                           "Julia reference cannot run: no Julia toolchain)"},
                 "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return
@@ -678,6 +787,7 @@ def main():
         "launch_shape": {dt: (None if res[dt]["tuned"] is None else
                               list(res[dt]["tuned"]["ms_per_iter"])[res[dt]["tuned"]["variant"]]) for dt in res},
         "gpu_launches": args.steps,
+        "autotune_ms_per_iter": {dt: (res[dt]["tuned"]["ms_per_iter"] if res[dt]["tuned"] else None) for dt in res},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_kind, "traffic": (tr * n[0] * n[1] * n[2]) if tr else None,
                      "algorithmic_bytes": A * esz[prim]},
@@ -695,11 +805,23 @@ def main():
                        "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                        "includes": "pinned host->device upload of the state, K iterations through the C ABI, "
                                    "residual norms, device->host download of the state"}
+    if rank == 0 and ws == 1 and not args.no_parity:
+        variants = {dt: (res[dt]["tuned"]["variant"] if res[dt]["tuned"] else args.variant) for dt in res}
+        par = oracle_parity(fi, n, local, variants)
+        line["error_vs_oracle"] = par["f64"]["max_rel_diff"] if "f64" in par else None
+        line["fp32_error_vs_oracle"] = par["f32"]["max_rel_diff"] if "f32" in par else None
+        line["parity"] = dict(par, bar="FP64 <= 1e-10 relative (production build, FMA contraction)",
+                              pinned="partially: the reference is Julia and cannot run here; the oracle restates "
+                                     "its kernels (operators, interpolation and ghost rules of Chmy.jl adopted)")
+        mm = mms_errors(fi)
+        line["mms_error"] = mm["mms3d_127"]["l2_rel_error"]
+        line["mms"] = mm
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         its, el, cores = cpu_baseline(n, seconds=12.0)
         line["cpu_baseline"] = {"value": A * 8 * its / el / 1e9, "unit": "GB/s", "cores": cores, "kind": "port",
                                 "sample": f"{its} whole PT iterations at {n[0]}^3 in FP64 (C restatement of the "
-                                          "reference CPU path, OpenMP)"}
+                                          "reference CPU path, OpenMP threads pinned one per core, "
+                                          "OMP_PROC_BIND=close)"}
     if pg:
         pg.barrier()
         pg.destroy_process_group()

@@ -449,9 +449,10 @@ fi_status advance_t(fi_model *m, int niter) {
             Ptrs<T> out = m->ptrs<T>(true);
             out.eta = in.eta;
             out.eta_next = in.eta_next;
-            alignas(64) unsigned char maps[11][128];
+            alignas(64) unsigned char maps[18][128];
             for (int f = 0; f < kState; f++) std::memcpy(maps[f], m->parity ? m->map_alt[f] : m->map_base[f], 128);
             std::memcpy(maps[10], m->map_eta[m->eta_swapped ? 1 : 0], 128);
+            for (int f = 0; f < 7; f++) std::memcpy(maps[11 + f], m->parity ? m->tmap_alt[f] : m->tmap_base[f], 128);
             FI_CHECK_CUDA(launch_fused3d<T>(m->g, m->kp, in, out, maps, m->fused_variant, m->d_err, m->stream),
                           "fused sweep");
             m->parity ^= 1;
@@ -477,19 +478,23 @@ fi_status check_err_word(fi_model *m) {
 }
 
 // (re)encode the tensor maps of every buffer the fused sweep reads, for the
-// current variant's tile height
+// current variant's tile shape: full boxes of the eleven inputs and trimmed boxes
+// of the seven stresses, for both state buffers
 fi_status encode_maps(fi_model *m) {
-    int ty = fused3d_variant_ty(m->fused_variant);
-    if (ty == m->maps_ty) return FI_OK;
+    const int v = m->fused_variant, key = fused3d_variant_key(v), esz = (int)m->esz;
+    if (key == m->maps_key) return FI_OK;
     for (int f = 0; f < kState; f++) {
-        if (!fused3d_encode_map(field_raw(m->base[f], m->esz), m->g, (int)m->esz, ty, m->map_base[f]) ||
-            !fused3d_encode_map(field_raw(m->alt[f], m->esz), m->g, (int)m->esz, ty, m->map_alt[f]))
+        if (!fused3d_encode_map(field_raw(m->base[f], m->esz), m->g, esz, v, f, false, m->map_base[f]) ||
+            !fused3d_encode_map(field_raw(m->alt[f], m->esz), m->g, esz, v, f, false, m->map_alt[f]))
+            return set_error("cuTensorMapEncodeTiled failed"), FI_ERR_CUDA;
+        if (f < 7 && (!fused3d_encode_map(field_raw(m->base[f], m->esz), m->g, esz, v, f, true, m->tmap_base[f]) ||
+                      !fused3d_encode_map(field_raw(m->alt[f], m->esz), m->g, esz, v, f, true, m->tmap_alt[f])))
             return set_error("cuTensorMapEncodeTiled failed"), FI_ERR_CUDA;
     }
-    if (!fused3d_encode_map(field_raw(m->base[FI_FIELD_ETA], m->esz), m->g, (int)m->esz, ty, m->map_eta[0]) ||
-        !fused3d_encode_map(field_raw(m->base[FI_FIELD_ETA_NEXT], m->esz), m->g, (int)m->esz, ty, m->map_eta[1]))
+    if (!fused3d_encode_map(field_raw(m->base[FI_FIELD_ETA], m->esz), m->g, esz, v, 10, false, m->map_eta[0]) ||
+        !fused3d_encode_map(field_raw(m->base[FI_FIELD_ETA_NEXT], m->esz), m->g, esz, v, 10, false, m->map_eta[1]))
         return set_error("cuTensorMapEncodeTiled failed"), FI_ERR_CUDA;
-    m->maps_ty = ty;
+    m->maps_key = key;
     return FI_OK;
 }
 
@@ -727,6 +732,26 @@ fi_status fi_model_get_field(fi_model *m, int32_t field, void *host, size_t nbyt
     cudaMemcpy3DParms p = copy_params(m, field, m->cur(field), host, false);
     FI_CHECK_CUDA(cudaMemcpy3DAsync(&p, m->stream), "get_field copy");
     FI_CHECK_CUDA(cudaStreamSynchronize(m->stream), "get_field sync");
+    return FI_OK;
+}
+
+fi_status fi_model_copy_field(fi_model *m, int32_t dst, int32_t src) {
+    if (!m || dst < 0 || dst >= FI_FIELD_COUNT || src < 0 || src >= FI_FIELD_COUNT || dst == src)
+        return set_error("bad argument"), FI_ERR_ARG;
+    if (!field_used(m, dst) || !field_used(m, src)) return set_error("field not used by this model"), FI_ERR_ARG;
+    if (is_residual(dst) || is_residual(src)) return set_error("residual fields are outputs"), FI_ERR_ARG;
+    int ld[3], ls[3];
+    field_loc(dst, ld);
+    field_loc(src, ls);
+    if (ld[0] != ls[0] || ld[1] != ls[1] || ld[2] != ls[2])
+        return set_error("the two fields have different staggered locations"), FI_ERR_ARG;
+    FI_CHECK_CUDA(cudaSetDevice(m->d.device), "cudaSetDevice");
+    FI_CHECK_CUDA(cudaMemcpyAsync(field_raw(m->cur(dst), m->esz), field_raw(m->cur(src), m->esz),
+                                  (m->elems + 64) * m->esz, cudaMemcpyDeviceToDevice, m->stream),
+                  "copy_field");
+    FI_CHECK_CUDA(cudaStreamSynchronize(m->stream), "copy_field sync");
+    m->full_iters = 0;
+    if (dst >= FI_FIELD_NA_CCC) m->ibf_stale = true;
     return FI_OK;
 }
 
@@ -1208,6 +1233,8 @@ const char *fi_fused_variant_name(int32_t variant) { return fused3d_variant_name
 fi_status fi_model_set_variant(fi_model *m, int32_t variant) {
     if (!m || variant < 0 || variant >= fused3d_num_variants()) return set_error("bad argument"), FI_ERR_ARG;
     if (m->path != FI_PATH_FUSED) return set_error("the model does not run the fused sweep"), FI_ERR_STATE;
+    if (!fused3d_variant_fits(variant, (int)m->esz))
+        return set_error("this launch shape does not fit a CTA in the model's precision"), FI_ERR_UNSUPPORTED;
     FI_CHECK_CUDA(cudaSetDevice(m->d.device), "cudaSetDevice");
     FI_CHECK_CUDA(cudaStreamSynchronize(m->stream), "sync");
     m->fused_variant = variant;
@@ -1225,9 +1252,20 @@ fi_status fi_model_autotune(fi_model *m, int32_t iters, int32_t *best, double *m
     double bestms = 1e300;
     fi_status st = FI_OK;
     for (int v = 0; v < nv && st == FI_OK; v++) {
+        if (!fused3d_variant_fits(v, (int)m->esz)) {
+            if (ms) ms[v] = -1.0;  // not offered in this precision
+            continue;
+        }
         st = fi_model_set_variant(m, v);
         if (st != FI_OK) break;
         st = fi_model_advance(m, 1);  // warm-up of this launch shape
+        if (st == FI_ERR_CUDA && cudaGetLastError() == cudaSuccess && cudaStreamSynchronize(m->stream) == cudaSuccess) {
+            // the shape could not be launched here (e.g. no room for its cluster); the
+            // device is healthy: leave the shape out
+            if (ms) ms[v] = -1.0;
+            st = FI_OK;
+            continue;
+        }
         if (st != FI_OK) break;
         cudaEventRecord(e0, m->stream);
         st = fi_model_advance(m, iters);

@@ -6,17 +6,33 @@
 // kernels touch the state twice per iteration (33 array passes); this sweep
 // reads P, τ(6), V(3), η once and writes P, τ(6), V(3), η_next once (22 passes).
 //
-// Work decomposition.  A CTA owns a 32 x TY column of grid positions (x, y) and a
-// block of z planes.  It marches up in z.  For every plane s the tensor-memory
-// accelerator copies an (x, y) box covering the column plus a one-position ring
-// of all eleven input fields (old P, τ, V, η; V.z one plane higher) into
-// shared-memory plane rings, one plane ahead of the compute, signalled by an
-// mbarrier.  The new stresses of plane s are computed in place over the column
-// (all seven components) and over the ring (only the components the velocity
-// update reads there), the stress boundary conditions are applied to the plane
-// in shared memory, and V / η_next of plane s-1 are updated from the stress
-// planes s-2, s-1, s.  Neighbouring CTAs recompute each other's ring: no
-// grid-wide synchronisation is needed.
+// Work decomposition.  A CTA owns a TX x TY column of grid positions (x, y) and a
+// block of z planes (TX = 32 or 64: one or two x positions per thread, 32·TY
+// threads).  It marches up in z.  For every plane s the tensor-memory
+// accelerator copies an (x, y) box of each of the eleven input fields (old P, τ,
+// V, η; V.z one plane higher) into shared-memory plane rings, one plane ahead of
+// the compute, signalled by an mbarrier.  The new stresses of plane s are
+// computed in place over the column (all seven components) and over a
+// one-position ring (only the components the velocity update reads there), the
+// stress boundary conditions are applied to the plane in shared memory, and V /
+// η_next of plane s-1 are updated from the stress planes s-2, s-1, s.
+// Neighbouring CTAs recompute each other's ring: no grid-wide synchronisation.
+//
+// Boxes.  A CTA whose column touches an x or y boundary loads every field over the
+// column plus the whole one-position ring (the boundary fix-ups and ghost writes
+// reach all of it).  An interior CTA of a "trimmed" launch shape loads each
+// stress component only where the sweep reads it: the ring stresses the velocity
+// update needs are P and τxx left of the column, P and τyy below it, τxy and τxz
+// right of it, τxy and τyz above it (and τxy at the upper right corner); τzz needs
+// no ring at all.  V and η keep the full ring.  This cuts the DRAM sectors an
+// interior column reads per plane by about a sixth (the ring is re-read by the
+// neighbouring columns).
+//
+// Clusters.  A launch shape may group CTAs into thread-block clusters (2x2, ...)
+// purely for co-scheduling: cluster members start together on one GPC and march
+// through z at the same pace, so the ring rows one member reads are the rows its
+// neighbour reads at about the same time and the second read hits L2.  There is no
+// cross-CTA communication and no multicast; a CTA may leave the cluster at any time.
 //
 // Double buffering.  Stresses and velocities are read from `in` and written to
 // `out` (distinct buffers), so the pointwise in-place updates of the reference
@@ -36,6 +52,10 @@
 // expiry the CTA records FI_ERR_TIMEOUT in the model's error word, waits once
 // more (bounded) for its own copies in flight, and returns.
 #include <cuda.h>
+
+// Layout and box constants of shapes a precision does not launch are still instantiated by
+// the host-side box tables: their unreferenced members are expected.
+#pragma nv_diag_suppress 177
 #include <cudaTypedefs.h>
 
 #include <cstdio>
@@ -48,33 +68,31 @@ namespace fi {
 
 namespace {
 
-constexpr int TX = 32;
-
-// Launch shapes: tile height and z-block depth.  (Issuing the copies of plane s+1
-// after the stress barrier of step s instead, which saves the barrier closing each
-// step, measured 15-20 % slower at 511^3: the copies then lose half their lead.
-// Z-blocks of 16 and 24 planes on 32x8 tiles measured 3 % slower and equal to 32
-// planes at 511^3 in both precisions: shorter blocks refill their rings more often.)
+// Launch shapes: tile width and height, z-block depth, cluster shape (x, y) and
+// whether interior tiles load trimmed stress boxes.  (Issuing the copies of plane
+// s+1 after the stress barrier of step s instead, which saves the barrier closing
+// each step, measured 15-20 % slower at 511^3: the copies then lose half their
+// lead.  Z-blocks of 16 and 24 planes on 32x8 tiles measured 3 % slower and equal
+// to 32 planes at 511^3 in both precisions: shorter blocks refill their rings
+// more often.)  Shapes whose shared memory does not fit a CTA for a precision
+// are not offered for it.
 struct Variant {
-    int ty;
-    int zb;
+    int tx, ty, zb, cx, cy, trim;
 };
-constexpr Variant kVariants[] = {{8, 32}, {8, 64}, {8, 128}, {4, 64}, {16, 32}, {16, 64}, {16, 128}};
+constexpr Variant kVariants[] = {
+    {32, 8, 32, 1, 1, 0},  {32, 8, 64, 1, 1, 0},  {32, 8, 128, 1, 1, 0}, {32, 4, 64, 1, 1, 0},
+    {32, 16, 32, 1, 1, 0}, {32, 16, 64, 1, 1, 0}, {32, 16, 128, 1, 1, 0},
+    // trimmed interior boxes, clusters
+    {32, 8, 32, 1, 1, 1},  {32, 8, 32, 2, 2, 1},  {32, 8, 64, 2, 2, 1},  {32, 8, 32, 2, 1, 1},
+    {32, 8, 32, 1, 4, 1},  {32, 8, 32, 2, 2, 0},  {32, 16, 32, 1, 1, 1},
+    // 64-wide tiles (two x positions per thread)
+    {64, 8, 32, 1, 1, 0},  {64, 8, 32, 1, 1, 1},  {64, 8, 32, 2, 2, 1},  {64, 4, 32, 1, 1, 1},
+    {64, 4, 64, 2, 2, 1},  {64, 4, 32, 2, 2, 1}};
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
-// TMA box width (elements) and position of the column's first x inside the box:
-// the box starts XB positions left of the column so that its global x coordinate
-// times the element size is a multiple of 16 bytes.
-template <typename T>
-struct BoxX;
-template <>
-struct BoxX<double> {
-    static constexpr int BX = 36, XB = 2;
-};
-template <>
-struct BoxX<float> {
-    static constexpr int BX = 40, XB = 4;
-};
+// input fields in map order
+enum { M_P = 0, M_XX, M_YY, M_ZZ, M_XY, M_XZ, M_YZ, M_VX, M_VY, M_VZ, M_ET, M_COUNT };
+constexpr int kTrimmed = 7;  // fields with a trimmed box (the stresses)
 
 // shared-memory plane slots: ring base and length per field
 enum {
@@ -92,27 +110,51 @@ enum {
     S_COUNT = 37
 };
 constexpr int kBars = 3;
+constexpr int kSmemPerSM = 233472;  // bytes of shared memory per SM (228 KB)
 
-template <typename T, int TY>
+template <typename T, int TX, int TY>
 struct Layout {
-    static constexpr int BX = BoxX<T>::BX;
-    static constexpr int XB = BoxX<T>::XB;
+    // the box starts XB positions left of the column so that its global x
+    // coordinate times the element size is a multiple of 16 bytes
+    static constexpr int XB = 16 / (int)sizeof(T);
+    static constexpr int BX = ((TX + 1 + XB + XB - 1) / XB) * XB;  // full box width (column + ring, aligned)
     static constexpr int RY = TY + 2;
-    static constexpr int PLANE = BX * RY;  // elements in one box
+    static constexpr int PLANE = BX * RY;  // elements in one full box
     static constexpr int PLANE_BYTES = PLANE * (int)sizeof(T);
     static constexpr int SLOT = ((PLANE_BYTES + 127) / 128) * 128 / (int)sizeof(T);  // 128-byte aligned slots
-    static constexpr int NT = TX * TY;
+    static constexpr int NT = 32 * TY;
+    static constexpr int PX = TX / 32;  // x positions per thread
     static constexpr size_t SMEM = (size_t)S_COUNT * SLOT * sizeof(T) + 128;
+    static constexpr int MINB_RAW = kSmemPerSM / (int)(SMEM + 1024);
+    static constexpr int MINB = MINB_RAW < 1 ? 1 : (MINB_RAW > 4 ? 4 : MINB_RAW);
 };
 
-// the eleven input maps of one sweep, in field order P, txx, tyy, tzz, txy, txz, tyz, Vx, Vy, Vz, eta
+// Box of input field F relative to the column origin (i0, j0): x from i0 + ox,
+// width bw; y from j0 + oy, height bh.  Full boxes cover the ring on all sides;
+// trimmed boxes (stresses of interior CTAs) only the ring sides read there.
+template <typename T, int TX, int TY, bool TRIM, int F>
+struct FBox {
+    using L = Layout<T, TX, TY>;
+    static constexpr bool full = !TRIM || F >= kTrimmed;
+    static constexpr int ox = full ? -L::XB : ((F == M_P || F == M_XX) ? -L::XB : 0);
+    static constexpr int bw = full ? L::BX : ((F == M_ZZ || F == M_YY || F == M_YZ) ? TX : TX + L::XB);
+    static constexpr int oy = full ? -1 : ((F == M_P || F == M_YY) ? -1 : 0);
+    static constexpr int bh = full ? TY + 2 : ((F == M_XX || F == M_ZZ || F == M_XZ) ? TY : TY + 1);
+    static constexpr int bytes = bw * bh * (int)sizeof(T);
+    static_assert(bw * bh <= L::SLOT, "box fits its slot");
+    static_assert((bw * (int)sizeof(T)) % 16 == 0, "TMA box rows are whole 16-byte units");
+};
+
+// the input maps of one sweep: eleven full-box maps in map order, then the trimmed
+// maps of the seven stress fields (used by interior CTAs of trimmed shapes)
 struct InMaps {
-    CUtensorMap m[11];
+    CUtensorMap m[M_COUNT];
+    CUtensorMap t[kTrimmed];
 };
 
-template <typename T, int TY>
+template <typename T, int TX, int TY, bool TRIM>
 struct Ctx {
-    using Lay = Layout<T, TY>;
+    using Lay = Layout<T, TX, TY>;
     T *sm;
     int i0, j0, kb, ke;
     int n0, n1, n2;
@@ -139,24 +181,35 @@ struct Ctx {
         o4p = ((m4 + 1) & 3) * Lay::SLOT;
         o4p2 = o4m2;
     }
-    __device__ __forceinline__ int at(int i, int j) const { return (j - j0 + 1) * Lay::BX + (i - i0 + Lay::XB); }
+    // element index of (i, j) inside field F's box
+    template <int F>
+    __device__ __forceinline__ int ix(int i, int j) const {
+        using B = FBox<T, TX, TY, TRIM, F>;
+        return (j - j0 - B::oy) * B::bw + (i - i0 - B::ox);
+    }
+    template <int F>
+    __device__ __forceinline__ bool in_box(int i, int j) const {
+        using B = FBox<T, TX, TY, TRIM, F>;
+        const int a = i - i0 - B::ox, b = j - j0 - B::oy;
+        return a >= 0 && a < B::bw && b >= 0 && b < B::bh;
+    }
     __device__ __forceinline__ T *slot(int base, int len, int p) const {
         const int d = p - sref;
         const int off = len == 3 ? (d < 0 ? o3m : d == 0 ? o30 : o3p)
                                  : (d < -1 ? o4m2 : d == -1 ? o4m : d == 0 ? o40 : d == 1 ? o4p : o4p2);
         return sm + base * Lay::SLOT + off;
     }
-    __device__ __forceinline__ T &P(int p, int i, int j) const { return slot(S_P, R_P, p)[at(i, j)]; }
-    __device__ __forceinline__ T &Tzz(int p, int i, int j) const { return slot(S_ZZ, R_ZZ, p)[at(i, j)]; }
-    __device__ __forceinline__ T &Txx(int p, int i, int j) const { return slot(S_XX, R_XX, p)[at(i, j)]; }
-    __device__ __forceinline__ T &Tyy(int p, int i, int j) const { return slot(S_YY, R_YY, p)[at(i, j)]; }
-    __device__ __forceinline__ T &Txy(int p, int i, int j) const { return slot(S_XY, R_XY, p)[at(i, j)]; }
-    __device__ __forceinline__ T &Txz(int p, int i, int j) const { return slot(S_XZ, R_XZ, p)[at(i, j)]; }
-    __device__ __forceinline__ T &Tyz(int p, int i, int j) const { return slot(S_YZ, R_YZ, p)[at(i, j)]; }
-    __device__ __forceinline__ T Vx(int p, int i, int j) const { return slot(S_VX, R_VX, p)[at(i, j)]; }
-    __device__ __forceinline__ T Vy(int p, int i, int j) const { return slot(S_VY, R_VY, p)[at(i, j)]; }
-    __device__ __forceinline__ T Vz(int p, int i, int j) const { return slot(S_VZ, R_VZ, p)[at(i, j)]; }
-    __device__ __forceinline__ T Eta(int p, int i, int j) const { return slot(S_ET, R_ET, p)[at(i, j)]; }
+    __device__ __forceinline__ T &P(int p, int i, int j) const { return slot(S_P, R_P, p)[ix<M_P>(i, j)]; }
+    __device__ __forceinline__ T &Tzz(int p, int i, int j) const { return slot(S_ZZ, R_ZZ, p)[ix<M_ZZ>(i, j)]; }
+    __device__ __forceinline__ T &Txx(int p, int i, int j) const { return slot(S_XX, R_XX, p)[ix<M_XX>(i, j)]; }
+    __device__ __forceinline__ T &Tyy(int p, int i, int j) const { return slot(S_YY, R_YY, p)[ix<M_YY>(i, j)]; }
+    __device__ __forceinline__ T &Txy(int p, int i, int j) const { return slot(S_XY, R_XY, p)[ix<M_XY>(i, j)]; }
+    __device__ __forceinline__ T &Txz(int p, int i, int j) const { return slot(S_XZ, R_XZ, p)[ix<M_XZ>(i, j)]; }
+    __device__ __forceinline__ T &Tyz(int p, int i, int j) const { return slot(S_YZ, R_YZ, p)[ix<M_YZ>(i, j)]; }
+    __device__ __forceinline__ T Vx(int p, int i, int j) const { return slot(S_VX, R_VX, p)[ix<M_VX>(i, j)]; }
+    __device__ __forceinline__ T Vy(int p, int i, int j) const { return slot(S_VY, R_VY, p)[ix<M_VY>(i, j)]; }
+    __device__ __forceinline__ T Vz(int p, int i, int j) const { return slot(S_VZ, R_VZ, p)[ix<M_VZ>(i, j)]; }
+    __device__ __forceinline__ T Eta(int p, int i, int j) const { return slot(S_ET, R_ET, p)[ix<M_ET>(i, j)]; }
     __device__ __forceinline__ long long gidx(int i, int j, int k) const {
         return (long long)i + sx * (long long)j + sxy * (long long)k;
     }
@@ -175,54 +228,73 @@ struct Ctx {
 template <typename T>
 __device__ __forceinline__ T h(T x) { return T(0.5) * x; }
 
+// one box copy of field F of plane p into its ring slot
+template <int F, typename T, int TX, int TY, bool TRIM>
+__device__ __forceinline__ void load_box(const Ctx<T, TX, TY, TRIM> &c, const InMaps &mp, T *dst, int p, uint64_t *bar) {
+    using B = FBox<T, TX, TY, TRIM, F>;
+    const CUtensorMap *map = (TRIM && F < kTrimmed) ? &mp.t[F] : &mp.m[F];
+    tma_load_3d(dst, map, (int)kXOff + c.i0 + B::ox, c.j0 + B::oy, p, bar);
+}
+
 // issue the TMA copies of input group p (planes: σ_old(p), Vx(p), Vy(p), Vz(p+1), η(p))
-template <typename T, int TY>
-__device__ __forceinline__ void issue_group(const Ctx<T, TY> &c, const InMaps &mp, int p, bool full, uint64_t *bar) {
-    using Lay = Layout<T, TY>;
-    const int x = (int)kXOff + c.i0 - Lay::XB, y = c.j0 - 1;
-    const uint32_t bytes = (full ? 11u : 4u) * (uint32_t)Lay::PLANE_BYTES;
-    mbar_expect_tx(bar, bytes);
+template <typename T, int TX, int TY, bool TRIM>
+__device__ __forceinline__ void issue_group(const Ctx<T, TX, TY, TRIM> &c, const InMaps &mp, int p, bool full,
+                                            uint64_t *bar) {
+    constexpr uint32_t vbytes = FBox<T, TX, TY, TRIM, M_VX>::bytes + FBox<T, TX, TY, TRIM, M_VY>::bytes +
+                                FBox<T, TX, TY, TRIM, M_VZ>::bytes + FBox<T, TX, TY, TRIM, M_ET>::bytes;
+    constexpr uint32_t sbytes = FBox<T, TX, TY, TRIM, M_P>::bytes + FBox<T, TX, TY, TRIM, M_XX>::bytes +
+                                FBox<T, TX, TY, TRIM, M_YY>::bytes + FBox<T, TX, TY, TRIM, M_ZZ>::bytes +
+                                FBox<T, TX, TY, TRIM, M_XY>::bytes + FBox<T, TX, TY, TRIM, M_XZ>::bytes +
+                                FBox<T, TX, TY, TRIM, M_YZ>::bytes;
+    mbar_expect_tx(bar, full ? vbytes + sbytes : vbytes);
     if (full) {
-        tma_load_3d(c.slot(S_P, R_P, p), &mp.m[0], x, y, p, bar);
-        tma_load_3d(c.slot(S_XX, R_XX, p), &mp.m[1], x, y, p, bar);
-        tma_load_3d(c.slot(S_YY, R_YY, p), &mp.m[2], x, y, p, bar);
-        tma_load_3d(c.slot(S_ZZ, R_ZZ, p), &mp.m[3], x, y, p, bar);
-        tma_load_3d(c.slot(S_XY, R_XY, p), &mp.m[4], x, y, p, bar);
-        tma_load_3d(c.slot(S_XZ, R_XZ, p), &mp.m[5], x, y, p, bar);
-        tma_load_3d(c.slot(S_YZ, R_YZ, p), &mp.m[6], x, y, p, bar);
+        load_box<M_P>(c, mp, c.slot(S_P, R_P, p), p, bar);
+        load_box<M_XX>(c, mp, c.slot(S_XX, R_XX, p), p, bar);
+        load_box<M_YY>(c, mp, c.slot(S_YY, R_YY, p), p, bar);
+        load_box<M_ZZ>(c, mp, c.slot(S_ZZ, R_ZZ, p), p, bar);
+        load_box<M_XY>(c, mp, c.slot(S_XY, R_XY, p), p, bar);
+        load_box<M_XZ>(c, mp, c.slot(S_XZ, R_XZ, p), p, bar);
+        load_box<M_YZ>(c, mp, c.slot(S_YZ, R_YZ, p), p, bar);
     }
-    tma_load_3d(c.slot(S_VX, R_VX, p), &mp.m[7], x, y, p, bar);
-    tma_load_3d(c.slot(S_VY, R_VY, p), &mp.m[8], x, y, p, bar);
-    tma_load_3d(c.slot(S_VZ, R_VZ, p + 1), &mp.m[9], x, y, p + 1, bar);
-    tma_load_3d(c.slot(S_ET, R_ET, p), &mp.m[10], x, y, p, bar);
+    load_box<M_VX>(c, mp, c.slot(S_VX, R_VX, p), p, bar);
+    load_box<M_VY>(c, mp, c.slot(S_VY, R_VY, p), p, bar);
+    load_box<M_VZ>(c, mp, c.slot(S_VZ, R_VZ, p + 1), p + 1, bar);
+    load_box<M_ET>(c, mp, c.slot(S_ET, R_ET, p), p, bar);
 }
 
 // raw stress update of plane s at (i, j): which components is a compile-time mask.
 // Every shared-memory operand is loaded before the first store (the in-place stress
 // stores and the global writes go through pointers the compiler cannot separate from
-// the loads), so the seven updates form independent chains.
+// the loads), so the seven updates form independent chains.  A component outside the
+// mask is neither loaded nor stored (a trimmed box may not hold it at (i, j)).
 enum { F_P = 1, F_XX = 2, F_YY = 4, F_ZZ = 8, F_XY = 16, F_XZ = 32, F_YZ = 64, F_ALL = 127 };
 
 // XYI: the column and its ring lie inside every x / y range (no boundary column),
 // so only the z ranges are tested
-template <typename T, int TY, bool XYI>
-__device__ __forceinline__ void sigma_point(const Ctx<T, TY> &c, const KParams &p, const TConst<T> &q, int s, int i, int j, int mask,
-                                            bool write_now, const Ptrs<T> &out) {
+template <typename T, int TX, int TY, bool TRIM, bool XYI>
+__device__ __forceinline__ void sigma_point(const Ctx<T, TX, TY, TRIM> &c, const KParams &p, const TConst<T> &q, int s,
+                                            int i, int j, int mask, bool write_now, const Ptrs<T> &out) {
     if (!XYI && (i > c.n0 + 2 || j > c.n1 + 2)) return;
-    constexpr int BX = Ctx<T, TY>::Lay::BX;
+    using Cx = Ctx<T, TX, TY, TRIM>;
+    constexpr int BV = FBox<T, TX, TY, TRIM, M_VX>::bw;  // row pitch of the V and η boxes
     const T idx = q.inv_dx[0], idy = q.inv_dx[1], idz = q.inv_dx[2];
     const bool cz = s >= 1 && s <= c.n2, vz = s >= 1 && s <= c.n2 + 1;
     const bool cx = XYI || (i >= 1 && i <= c.n0) || (c.perx && (i == 0 || i == c.n0 + 1));
     const bool vx = XYI || (i >= 1 && i <= c.n0 + 1);
     const bool cy = XYI || (j >= 1 && j <= c.n1) || (c.pery && (j == 0 || j == c.n1 + 1));
     const bool vy = XYI || (j >= 1 && j <= c.n1 + 1);
-    const int a = c.at(i, j);
+    const int a = c.template ix<M_VX>(i, j);
     const T *vxs = c.slot(S_VX, R_VX, s), *vys = c.slot(S_VY, R_VY, s), *vzs = c.slot(S_VZ, R_VZ, s);
     const T *vxm = c.slot(S_VX, R_VX, s - 1), *vym = c.slot(S_VY, R_VY, s - 1), *vzp = c.slot(S_VZ, R_VZ, s + 1);
     const T *et = c.slot(S_ET, R_ET, s), *etm = c.slot(S_ET, R_ET, s - 1);
-    T *sP = c.slot(S_P, R_P, s) + a, *sXX = c.slot(S_XX, R_XX, s) + a, *sYY = c.slot(S_YY, R_YY, s) + a;
-    T *sZZ = c.slot(S_ZZ, R_ZZ, s) + a, *sXY = c.slot(S_XY, R_XY, s) + a, *sXZ = c.slot(S_XZ, R_XZ, s) + a;
-    T *sYZ = c.slot(S_YZ, R_YZ, s) + a;
+    T *sP = c.slot(S_P, R_P, s) + c.template ix<M_P>(i, j);
+    T *sXX = c.slot(S_XX, R_XX, s) + c.template ix<M_XX>(i, j);
+    T *sYY = c.slot(S_YY, R_YY, s) + c.template ix<M_YY>(i, j);
+    T *sZZ = c.slot(S_ZZ, R_ZZ, s) + c.template ix<M_ZZ>(i, j);
+    T *sXY = c.slot(S_XY, R_XY, s) + c.template ix<M_XY>(i, j);
+    T *sXZ = c.slot(S_XZ, R_XZ, s) + c.template ix<M_XZ>(i, j);
+    T *sYZ = c.slot(S_YZ, R_YZ, s) + c.template ix<M_YZ>(i, j);
+    (void)sizeof(Cx);
     const bool dc = (mask & (F_P | F_XX | F_YY | F_ZZ)) && cx && cy && cz;
     const bool dxy = (mask & F_XY) && vx && vy && cz;
     const bool dxz = (mask & F_XZ) && vx && cy && vz;
@@ -240,7 +312,7 @@ __device__ __forceinline__ void sigma_point(const Ctx<T, TY> &c, const KParams &
     T nP = oP, nXX = oXX, nYY = oYY, nZZ = oZZ, nXY = oXY, nXZ = oXZ, nYZ = oYZ;
     if (dc) {
         T exx = (vxs[a + 1] - vxs[a]) * idx;
-        T eyy = (vys[a + BX] - vys[a]) * idy;
+        T eyy = (vys[a + BV] - vys[a]) * idy;
         T ezz = (vzp[a] - vzs[a]) * idz;
         T divV = exx + eyy + ezz;
         T etac = et[a];
@@ -250,8 +322,8 @@ __device__ __forceinline__ void sigma_point(const Ctx<T, TY> &c, const KParams &
         if (mask & F_ZZ) nZZ = oZZ - (oZZ - T(2.0) * etac * (ezz - third(divV))) * q.dt_tau[2];
     }
     if (dxy) {
-        T exy = T(0.5) * ((vys[a] - vys[a - 1]) * idx + (vxs[a] - vxs[a - BX]) * idy);
-        T e_xy = h(h(et[a - 1 - BX] + et[a - BX]) + h(et[a - 1] + et[a]));
+        T exy = T(0.5) * ((vys[a] - vys[a - 1]) * idx + (vxs[a] - vxs[a - BV]) * idy);
+        T e_xy = h(h(et[a - 1 - BV] + et[a - BV]) + h(et[a - 1] + et[a]));
         nXY = oXY - (oXY - T(2.0) * e_xy * exy) * q.dt_tau[3];
     }
     if (dxz) {
@@ -260,8 +332,8 @@ __device__ __forceinline__ void sigma_point(const Ctx<T, TY> &c, const KParams &
         nXZ = oXZ - (oXZ - T(2.0) * e_xz * exz) * q.dt_tau[4];
     }
     if (dyz) {
-        T eyz = T(0.5) * ((vzs[a] - vzs[a - BX]) * idy + (vys[a] - vym[a]) * idz);
-        T e_yz = h(h(etm[a - BX] + etm[a]) + h(et[a - BX] + et[a]));
+        T eyz = T(0.5) * ((vzs[a] - vzs[a - BV]) * idy + (vys[a] - vym[a]) * idz);
+        T e_yz = h(h(etm[a - BV] + etm[a]) + h(et[a - BV] + et[a]));
         nYZ = oYZ - (oYZ - T(2.0) * e_yz * eyz) * q.dt_tau[5];
     }
     if (dc) {
@@ -285,27 +357,36 @@ __device__ __forceinline__ void sigma_point(const Ctx<T, TY> &c, const KParams &
     }
 }
 
-// ring stresses of plane s (see sigma_plane); TX == 32 lanes span a row, TY < 32
-template <typename T, int TY, bool XYI>
-__device__ __forceinline__ void sigma_ring(const Ctx<T, TY> &c, const KParams &p, const TConst<T> &q, int s, const Ptrs<T> &out) {
-    constexpr int NW = Layout<T, TY>::NT / 32;
-    static_assert(TX == 32 && TY < 32 && NW >= 4, "one ring side per warp");
+// ring stresses of plane s (see sigma_plane); a warp spans a row of 32 positions
+// (TX / 32 per lane), TY < 32
+template <typename T, int TX, int TY, bool TRIM, bool XYI>
+__device__ __forceinline__ void sigma_ring(const Ctx<T, TX, TY, TRIM> &c, const KParams &p, const TConst<T> &q, int s,
+                                           const Ptrs<T> &out) {
+    constexpr int NW = Layout<T, TX, TY>::NT / 32;
+    constexpr int PX = TX / 32;
+    static_assert(TY < 32 && NW >= 4, "one ring side per warp");
     const int w = threadIdx.x / 32, lane = threadIdx.x % 32;
     if (w == NW - 4) {
-        sigma_point<T, TY, XYI>(c, p, q, s, c.i0 + lane, c.j0 - 1, F_P | F_YY, false, out);
+#pragma unroll
+        for (int u = 0; u < PX; u++)
+            sigma_point<T, TX, TY, TRIM, XYI>(c, p, q, s, c.i0 + lane + 32 * u, c.j0 - 1, F_P | F_YY, false, out);
     } else if (w == NW - 3) {
-        sigma_point<T, TY, XYI>(c, p, q, s, c.i0 + lane, c.j0 + TY, F_XY | F_YZ, false, out);
+#pragma unroll
+        for (int u = 0; u < PX; u++)
+            sigma_point<T, TX, TY, TRIM, XYI>(c, p, q, s, c.i0 + lane + 32 * u, c.j0 + TY, F_XY | F_YZ, false, out);
     } else if (w == NW - 2) {
-        if (lane < TY) sigma_point<T, TY, XYI>(c, p, q, s, c.i0 - 1, c.j0 + lane, F_P | F_XX, false, out);
+        if (lane < TY) sigma_point<T, TX, TY, TRIM, XYI>(c, p, q, s, c.i0 - 1, c.j0 + lane, F_P | F_XX, false, out);
     } else if (w == NW - 1) {
-        if (lane < TY) sigma_point<T, TY, XYI>(c, p, q, s, c.i0 + TX, c.j0 + lane, F_XY | F_XZ, false, out);
-        else if (lane == TY) sigma_point<T, TY, XYI>(c, p, q, s, c.i0 + TX, c.j0 + TY, F_XY, false, out);
+        if (lane < TY) sigma_point<T, TX, TY, TRIM, XYI>(c, p, q, s, c.i0 + TX, c.j0 + lane, F_XY | F_XZ, false, out);
+        else if (lane == TY) sigma_point<T, TX, TY, TRIM, XYI>(c, p, q, s, c.i0 + TX, c.j0 + TY, F_XY, false, out);
     }
 }
 
 // stress boundary fix-ups of one face side on plane s at region point (i, j)
-template <typename T, int TY>
-__device__ __forceinline__ void fix_x(const Ctx<T, TY> &c, const KParams &p, const TConst<T> &q, int s, int i, int j, int side) {
+// (boundary columns only: full boxes)
+template <typename T, int TX, int TY, bool TRIM>
+__device__ __forceinline__ void fix_x(const Ctx<T, TX, TY, TRIM> &c, const KParams &p, const TConst<T> &q, int s, int i,
+                                      int j, int side) {
     const int kind = p.bc_kind[0][side];
     if (kind != FI_BC_TRACTION && kind != FI_BC_SLIP) return;
     const bool cz = s >= 1 && s <= c.n2, vz = s >= 1 && s <= c.n2 + 1;
@@ -320,8 +401,9 @@ __device__ __forceinline__ void fix_x(const Ctx<T, TY> &c, const KParams &p, con
         if (j >= 1 && j <= c.n1 && vz) c.Txz(s, i, j) = q.bc_val[0][side][2];
     }
 }
-template <typename T, int TY>
-__device__ __forceinline__ void fix_y(const Ctx<T, TY> &c, const KParams &p, const TConst<T> &q, int s, int i, int j, int side) {
+template <typename T, int TX, int TY, bool TRIM>
+__device__ __forceinline__ void fix_y(const Ctx<T, TX, TY, TRIM> &c, const KParams &p, const TConst<T> &q, int s, int i,
+                                      int j, int side) {
     const int kind = p.bc_kind[1][side];
     if (kind != FI_BC_TRACTION && kind != FI_BC_SLIP) return;
     const bool cz = s >= 1 && s <= c.n2, vz = s >= 1 && s <= c.n2 + 1;
@@ -337,10 +419,13 @@ __device__ __forceinline__ void fix_y(const Ctx<T, TY> &c, const KParams &p, con
     }
 }
 
-template <typename T, int TY>
-__device__ __forceinline__ void sigma_plane(const Ctx<T, TY> &c, const KParams &p, const TConst<T> &q, const Ptrs<T> &out, int s) {
-    using Lay = Layout<T, TY>;
-    const int tid = threadIdx.x;
+template <typename T, int TX, int TY, bool TRIM>
+__device__ __forceinline__ void sigma_plane(const Ctx<T, TX, TY, TRIM> &c, const KParams &p, const TConst<T> &q,
+                                            const Ptrs<T> &out, int s) {
+    using Lay = Layout<T, TX, TY>;
+    using Cx = Ctx<T, TX, TY, TRIM>;
+    constexpr int PX = Lay::PX;
+    const int tid = threadIdx.x, lane = tid % 32, row = tid / 32;
     const bool zb_plane = s == 1 || s == c.n2 + 1;
     const bool late = c.bnd_x || c.bnd_y || zb_plane;
     const bool own_s = s >= c.kb && s < c.ke;
@@ -349,31 +434,38 @@ __device__ __forceinline__ void sigma_plane(const Ctx<T, TY> &c, const KParams &
     // that every ring warp takes a single branch path: the row below (P, τyy), the
     // row above (τxy, τyz), the column left (P, τxx), the column right (τxy, τxz)
     // with the corner above it (τxy)
-    if (!c.bnd_x && !c.bnd_y) {
-        sigma_point<T, TY, true>(c, p, q, s, c.i0 + (tid % TX), c.j0 + (tid / TX), F_ALL, own_s && !late, out);
-        sigma_ring<T, TY, true>(c, p, q, s, out);
+    if (TRIM || (!c.bnd_x && !c.bnd_y)) {
+#pragma unroll
+        for (int u = 0; u < PX; u++)
+            sigma_point<T, TX, TY, TRIM, true>(c, p, q, s, c.i0 + lane + 32 * u, c.j0 + row, F_ALL, own_s && !late, out);
+        sigma_ring<T, TX, TY, TRIM, true>(c, p, q, s, out);
     } else {
-        sigma_point<T, TY, false>(c, p, q, s, c.i0 + (tid % TX), c.j0 + (tid / TX), F_ALL, own_s && !late, out);
-        sigma_ring<T, TY, false>(c, p, q, s, out);
+#pragma unroll
+        for (int u = 0; u < PX; u++)
+            sigma_point<T, TX, TY, TRIM, false>(c, p, q, s, c.i0 + lane + 32 * u, c.j0 + row, F_ALL, own_s && !late,
+                                                out);
+        sigma_ring<T, TX, TY, TRIM, false>(c, p, q, s, out);
     }
     __syncthreads();
     if (!late) return;
     constexpr int NREG = (TX + 2) * (TY + 2);
-    if (c.bnd_x && !c.perx) {
-        for (int r = tid; r < NREG; r += Lay::NT) {
-            const int i = c.i0 - 1 + r % (TX + 2), j = c.j0 - 1 + r / (TX + 2);
-            fix_x<T, TY>(c, p, q, s, i, j, 0);
-            fix_x<T, TY>(c, p, q, s, i, j, 1);
+    if constexpr (!TRIM) {
+        if (c.bnd_x && !c.perx) {
+            for (int r = tid; r < NREG; r += Lay::NT) {
+                const int i = c.i0 - 1 + r % (TX + 2), j = c.j0 - 1 + r / (TX + 2);
+                fix_x<T, TX, TY, TRIM>(c, p, q, s, i, j, 0);
+                fix_x<T, TX, TY, TRIM>(c, p, q, s, i, j, 1);
+            }
+            __syncthreads();
         }
-        __syncthreads();
-    }
-    if (c.bnd_y && !c.pery) {
-        for (int r = tid; r < NREG; r += Lay::NT) {
-            const int i = c.i0 - 1 + r % (TX + 2), j = c.j0 - 1 + r / (TX + 2);
-            fix_y<T, TY>(c, p, q, s, i, j, 0);
-            fix_y<T, TY>(c, p, q, s, i, j, 1);
+        if (c.bnd_y && !c.pery) {
+            for (int r = tid; r < NREG; r += Lay::NT) {
+                const int i = c.i0 - 1 + r % (TX + 2), j = c.j0 - 1 + r / (TX + 2);
+                fix_y<T, TX, TY, TRIM>(c, p, q, s, i, j, 0);
+                fix_y<T, TX, TY, TRIM>(c, p, q, s, i, j, 1);
+            }
+            __syncthreads();
         }
-        __syncthreads();
     }
     if (zb_plane) {
         const int side = s == 1 ? 0 : 1;
@@ -382,21 +474,23 @@ __device__ __forceinline__ void sigma_plane(const Ctx<T, TY> &c, const KParams &
             const T c0 = q.bc_val[2][side][0], c1 = q.bc_val[2][side][1], tv = T(2.0) * q.bc_val[2][side][2];
             for (int r = tid; r < NREG; r += Lay::NT) {
                 const int i = c.i0 - 1 + r % (TX + 2), j = c.j0 - 1 + r / (TX + 2);
+                // a trimmed box holds a component only where the sweep reads it
                 if (kind == FI_BC_TRACTION) {
                     if (side == 0) {  // s == 1: ghost plane 0 from plane 1
-                        c.P(s - 1, i, j) = tv - c.P(s, i, j);
-                        c.Tzz(s - 1, i, j) = tv - c.Tzz(s, i, j);
+                        if (c.template in_box<M_P>(i, j)) c.P(s - 1, i, j) = tv - c.P(s, i, j);
+                        if (c.template in_box<M_ZZ>(i, j)) c.Tzz(s - 1, i, j) = tv - c.Tzz(s, i, j);
                     } else {
-                        c.P(s, i, j) = tv - c.P(s - 1, i, j);
-                        c.Tzz(s, i, j) = tv - c.Tzz(s - 1, i, j);
+                        if (c.template in_box<M_P>(i, j)) c.P(s, i, j) = tv - c.P(s - 1, i, j);
+                        if (c.template in_box<M_ZZ>(i, j)) c.Tzz(s, i, j) = tv - c.Tzz(s - 1, i, j);
                     }
                 }
-                c.Txz(s, i, j) = c0;
-                c.Tyz(s, i, j) = c1;
+                if (c.template in_box<M_XZ>(i, j)) c.Txz(s, i, j) = c0;
+                if (c.template in_box<M_YZ>(i, j)) c.Tyz(s, i, j) = c1;
             }
             __syncthreads();
         }
     }
+    (void)sizeof(Cx);
     const bool own_0 = s == 1 && c.kb == 1 && p.bc_kind[2][0] == FI_BC_TRACTION;
     if (own_s || own_0) {
         for (int r = tid; r < NREG; r += Lay::NT) {
@@ -470,8 +564,8 @@ __device__ __forceinline__ Img<T> img_vertex(int q, int N, bool periodic) {
     return d;
 }
 
-template <typename T, int TY>
-__device__ __forceinline__ void write_images(const Ctx<T, TY> &c, T *f, T v, const Img<T> &ix, const Img<T> &iy,
+template <typename T, typename C>
+__device__ __forceinline__ void write_images(const C &c, T *f, T v, const Img<T> &ix, const Img<T> &iy,
                                              const Img<T> &iz) {
 #pragma unroll
     for (int a = 0; a < 3; a++) {
@@ -492,9 +586,9 @@ __device__ __forceinline__ void write_images(const Ctx<T, TY> &c, T *f, T v, con
 }
 
 // ---- velocity / η_next update of plane t on the column ----------------------------
-template <typename T, int TY>
-__device__ __forceinline__ T vx_raw(const Ctx<T, TY> &c, const KParams &p, const TConst<T> &q, const Ptrs<T> &in, int t, int i, int j,
-                                    long long I) {
+template <typename T, typename C>
+__device__ __forceinline__ T vx_raw(const C &c, const KParams &p, const TConst<T> &q, const Ptrs<T> &in, int t, int i,
+                                    int j, long long I) {
     const T idx = q.inv_dx[0], idy = q.inv_dx[1], idz = q.inv_dx[2];
     T gx = (p.g_kind[0] == FI_G_FIELD ? in.gx[I] : q.g_val[0]);
     T ex = h(c.Eta(t, i - 1, j) + c.Eta(t, i, j));
@@ -504,9 +598,9 @@ __device__ __forceinline__ T vx_raw(const Ctx<T, TY> &c, const KParams &p, const
                                    ex) *
                                q.dt_V[0];
 }
-template <typename T, int TY>
-__device__ __forceinline__ T vy_raw(const Ctx<T, TY> &c, const KParams &p, const TConst<T> &q, const Ptrs<T> &in, int t, int i, int j,
-                                    long long I) {
+template <typename T, typename C>
+__device__ __forceinline__ T vy_raw(const C &c, const KParams &p, const TConst<T> &q, const Ptrs<T> &in, int t, int i,
+                                    int j, long long I) {
     const T idx = q.inv_dx[0], idy = q.inv_dx[1], idz = q.inv_dx[2];
     T gy = (p.g_kind[1] == FI_G_FIELD ? in.gy[I] : q.g_val[1]);
     T ey = h(c.Eta(t, i, j - 1) + c.Eta(t, i, j));
@@ -516,9 +610,9 @@ __device__ __forceinline__ T vy_raw(const Ctx<T, TY> &c, const KParams &p, const
                                    ey) *
                                q.dt_V[1];
 }
-template <typename T, int TY>
-__device__ __forceinline__ T vz_raw(const Ctx<T, TY> &c, const KParams &p, const TConst<T> &q, const Ptrs<T> &in, int t, int i, int j,
-                                    long long I) {
+template <typename T, typename C>
+__device__ __forceinline__ T vz_raw(const C &c, const KParams &p, const TConst<T> &q, const Ptrs<T> &in, int t, int i,
+                                    int j, long long I) {
     const T idx = q.inv_dx[0], idy = q.inv_dx[1], idz = q.inv_dx[2];
     T gz = (p.g_kind[2] == FI_G_FIELD ? in.gz[I] : q.g_val[2]);
     T ez = h(c.Eta(t - 1, i, j) + c.Eta(t, i, j));
@@ -528,9 +622,9 @@ __device__ __forceinline__ T vz_raw(const Ctx<T, TY> &c, const KParams &p, const
                                    ez) *
                                q.dt_V[2];
 }
-template <typename T, int TY>
-__device__ __forceinline__ T eta_raw(const Ctx<T, TY> &c, const KParams &p, const TConst<T> &q, const Ptrs<T> &in, int t, int i, int j,
-                                     long long I) {
+template <typename T, typename C>
+__device__ __forceinline__ T eta_raw(const C &c, const KParams &p, const TConst<T> &q, const Ptrs<T> &in, int t, int i,
+                                     int j, long long I) {
     T xx = c.Txx(t, i, j), yy = c.Tyy(t, i, j), zz = c.Tzz(t, i, j);
     T lxy = h(h(c.Txy(t, i, j) + c.Txy(t, i + 1, j)) + h(c.Txy(t, i, j + 1) + c.Txy(t, i + 1, j + 1)));
     T lxz = h(h(c.Txz(t, i, j) + c.Txz(t, i + 1, j)) + h(c.Txz(t + 1, i, j) + c.Txz(t + 1, i + 1, j)));
@@ -539,9 +633,9 @@ __device__ __forceinline__ T eta_raw(const Ctx<T, TY> &c, const KParams &p, cons
     return rheology_s2(p, q.rheo_A, q.rheo_inv_eta_reg, in.eta_lin, in.A, c.Eta(t, i, j), I, s2);
 }
 
-template <typename T, int TY>
-__device__ __forceinline__ void v_plane(const Ctx<T, TY> &c, const KParams &p, const TConst<T> &q, const Ptrs<T> &in, const Ptrs<T> &out, int t) {
-    const int i = c.i0 + (threadIdx.x % TX), j = c.j0 + (threadIdx.x / TX);
+template <typename T, int TX, int TY, bool TRIM>
+__device__ __forceinline__ void v_point(const Ctx<T, TX, TY, TRIM> &c, const KParams &p, const TConst<T> &q,
+                                        const Ptrs<T> &in, const Ptrs<T> &out, int t, int i, int j) {
     const int n0 = c.n0, n1 = c.n1, n2 = c.n2;
     if (i > n0 + 1 || j > n1 + 1) return;
     const long long I = c.gidx(i, j, t);
@@ -610,15 +704,61 @@ __device__ __forceinline__ void v_plane(const Ctx<T, TY> &c, const KParams &p, c
     }
 }
 
-template <typename T, int TY>
-__global__ void __launch_bounds__(TX *TY, (TY >= 16 ? (sizeof(T) == 8 ? 1 : 2) : (sizeof(T) == 8 ? 2 : 3)))
-    fused3d_kernel(Geom g, KParams p, TConst<T> q, Ptrs<T> in, Ptrs<T> out, const __grid_constant__ InMaps maps, int zb,
-                   int *err) {
-    using Lay = Layout<T, TY>;
-    extern __shared__ __align__(1024) unsigned char smem_raw[];
-    Ctx<T, TY> c;
-    c.sm = reinterpret_cast<T *>(smem_raw);
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + (size_t)S_COUNT * Lay::SLOT * sizeof(T));
+template <typename T, int TX, int TY, bool TRIM>
+__device__ __forceinline__ void v_plane(const Ctx<T, TX, TY, TRIM> &c, const KParams &p, const TConst<T> &q,
+                                        const Ptrs<T> &in, const Ptrs<T> &out, int t) {
+    const int lane = threadIdx.x % 32, j = c.j0 + (int)(threadIdx.x / 32);
+#pragma unroll
+    for (int u = 0; u < TX / 32; u++) v_point(c, p, q, in, out, t, c.i0 + lane + 32 * u, j);
+}
+
+// the plane march of one CTA (TRIM: an interior column of a trimmed launch shape)
+template <typename T, int TX, int TY, bool TRIM>
+__device__ __forceinline__ void sweep(Ctx<T, TX, TY, TRIM> &c, const KParams &p, const TConst<T> &q, const Ptrs<T> &in,
+                                      const Ptrs<T> &out, const InMaps &maps, uint64_t *bars, int *err) {
+    const int tid = threadIdx.x;
+    const int f = max(c.kb - 1, 1), last = min(c.ke, c.n2 + 1);
+    uint32_t phase = 0;  // bit b: parity of the next completion of bars[b]
+    c.set_plane(f);
+    if (tid == 0) {
+        issue_group(c, maps, f - 1, false, &bars[(f - 1) % kBars]);
+        issue_group(c, maps, f, true, &bars[f % kBars]);
+    }
+    auto wait_group = [&](int pl) -> bool {
+        const int b = pl % kBars;
+        bool ok = mbar_wait(&bars[b], (phase >> b) & 1u);
+        phase ^= 1u << b;
+        return ok;
+    };
+    bool ok = wait_group(f - 1);
+    for (int s = f; s <= last && ok; s++) {
+        c.set_plane(s);
+        if (tid == 0 && s + 1 <= last) {
+            fence_proxy_async();
+            issue_group(c, maps, s + 1, true, &bars[(s + 1) % kBars]);
+        }
+        ok = wait_group(s);
+        if (!ok) break;
+        sigma_plane(c, p, q, out, s);
+        if (s - 1 >= c.kb && s - 1 < c.ke) v_plane(c, p, q, in, out, s - 1);
+        __syncthreads();
+    }
+    if (ok) {
+        if (c.ke - 1 == last && last == c.n2 + 1) {
+            c.set_plane(last);
+            v_plane(c, p, q, in, out, last);
+        }
+        return;
+    }
+    // bounded wait expired: record it and drain this CTA's own copies (bounded) before leaving
+    atomicExch(err, (int)FI_ERR_TIMEOUT);
+    for (int b = 0; b < kBars; b++) mbar_wait(&bars[b], (phase >> b) & 1u);
+}
+
+template <typename T, int TX, int TY, bool TRIM>
+__device__ __forceinline__ void init_ctx(Ctx<T, TX, TY, TRIM> &c, const Geom &g, const KParams &p, unsigned char *smem,
+                                         int zb) {
+    c.sm = reinterpret_cast<T *>(smem);
     c.i0 = 1 + blockIdx.x * TX;
     c.j0 = 1 + blockIdx.y * TY;
     c.kb = 1 + blockIdx.z * zb;
@@ -632,66 +772,70 @@ __global__ void __launch_bounds__(TX *TY, (TY >= 16 ? (sizeof(T) == 8 ? 1 : 2) :
     c.pery = p.bc_kind[1][0] == FI_BC_PERIODIC;
     c.bnd_x = c.i0 == 1 || c.i0 + TX >= c.n0 + 1;
     c.bnd_y = c.j0 == 1 || c.j0 + TY >= c.n1 + 1;
-    const int tid = threadIdx.x;
-    if (tid == 0) {
+}
+
+template <typename T, int TX, int TY>
+__global__ void __launch_bounds__(Layout<T, TX, TY>::NT, Layout<T, TX, TY>::MINB)
+    fused3d_kernel(Geom g, KParams p, TConst<T> q, Ptrs<T> in, Ptrs<T> out, const __grid_constant__ InMaps maps, int zb,
+                   int trim, int *err) {
+    using Lay = Layout<T, TX, TY>;
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    // the grid is padded to whole clusters: columns past the vertex range have no work
+    if (1 + (int)blockIdx.x * TX > g.n[0] + 1 || 1 + (int)blockIdx.y * TY > g.n[1] + 1) return;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + (size_t)S_COUNT * Lay::SLOT * sizeof(T));
+    if (threadIdx.x == 0) {
         for (int b = 0; b < kBars; b++) mbar_init(&bars[b], 1);
         mbar_fence_init();
     }
     __syncthreads();
-    const int f = max(c.kb - 1, 1), last = min(c.ke, c.n2 + 1);
-    uint32_t phase = 0;  // bit b: parity of the next completion of bars[b]
-    c.set_plane(f);
-    if (tid == 0) {
-        issue_group<T, TY>(c, maps, f - 1, false, &bars[(f - 1) % kBars]);
-        issue_group<T, TY>(c, maps, f, true, &bars[f % kBars]);
+    Ctx<T, TX, TY, false> c;
+    init_ctx(c, g, p, smem_raw, zb);
+    if (trim && !c.bnd_x && !c.bnd_y) {
+        Ctx<T, TX, TY, true> ct;
+        init_ctx(ct, g, p, smem_raw, zb);
+        sweep(ct, p, q, in, out, maps, bars, err);
+    } else {
+        sweep(c, p, q, in, out, maps, bars, err);
     }
-    auto wait_group = [&](int pl) -> bool {
-        const int b = pl % kBars;
-        bool ok = mbar_wait(&bars[b], (phase >> b) & 1u);
-        phase ^= 1u << b;
-        return ok;
-    };
-    bool ok = wait_group(f - 1);
-    for (int s = f; s <= last && ok; s++) {
-        c.set_plane(s);
-        if (tid == 0 && s + 1 <= last) {
-            fence_proxy_async();
-            issue_group<T, TY>(c, maps, s + 1, true, &bars[(s + 1) % kBars]);
-        }
-        ok = wait_group(s);
-        if (!ok) break;
-        sigma_plane<T, TY>(c, p, q, out, s);
-        if (s - 1 >= c.kb && s - 1 < c.ke) v_plane<T, TY>(c, p, q, in, out, s - 1);
-        __syncthreads();
-    }
-    if (ok) {
-        if (c.ke - 1 == last && last == c.n2 + 1) {
-            c.set_plane(last);
-            v_plane<T, TY>(c, p, q, in, out, last);
-        }
-        return;
-    }
-    // bounded wait expired: record it and drain this CTA's own copies (bounded) before leaving
-    atomicExch(err, (int)FI_ERR_TIMEOUT);
-    for (int b = 0; b < kBars; b++) mbar_wait(&bars[b], (phase >> b) & 1u);
 }
 
-template <typename T, int TY>
+template <typename T, int TX, int TY>
 cudaError_t launch_variant(const Geom &g, const KParams &p, const Ptrs<T> &in, const Ptrs<T> &out, const InMaps &maps,
-                           int zb, int *err, cudaStream_t s) {
-    using Lay = Layout<T, TY>;
+                           const Variant &v, int *err, cudaStream_t s) {
+    using Lay = Layout<T, TX, TY>;
     int dev = 0;
     cudaGetDevice(&dev);
     static bool attr_set[64] = {};
     if (dev < 64 && !attr_set[dev]) {
         cudaError_t e =
-            cudaFuncSetAttribute(fused3d_kernel<T, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lay::SMEM);
+            cudaFuncSetAttribute(fused3d_kernel<T, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lay::SMEM);
         if (e != cudaSuccess) return e;
         attr_set[dev] = true;
     }
-    dim3 grd((g.n[0] + 1 + TX - 1) / TX, (g.n[1] + 1 + TY - 1) / TY, (g.n[2] + 1 + zb - 1) / zb);
-    fused3d_kernel<T, TY><<<grd, Lay::NT, Lay::SMEM, s>>>(g, p, make_tconst<T>(p), in, out, maps, zb, err);
-    return cudaGetLastError();
+    auto up = [](int a, int b) { return (a + b - 1) / b * b; };
+    dim3 grd(up((g.n[0] + 1 + TX - 1) / TX, v.cx), up((g.n[1] + 1 + TY - 1) / TY, v.cy), (g.n[2] + 1 + v.zb - 1) / v.zb);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grd;
+    cfg.blockDim = dim3(Lay::NT);
+    cfg.dynamicSmemBytes = Lay::SMEM;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    if (v.cx * v.cy > 1) {
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = v.cx;
+        attr[0].val.clusterDim.y = v.cy;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+    }
+    const TConst<T> q = make_tconst<T>(p);
+    return cudaLaunchKernelEx(&cfg, fused3d_kernel<T, TX, TY>, g, p, q, in, out, maps, v.zb, v.trim, err);
+}
+
+template <typename T>
+size_t variant_smem(const Variant &v) {
+    if (v.tx == 64) return v.ty == 4 ? Layout<T, 64, 4>::SMEM : Layout<T, 64, 8>::SMEM;
+    return v.ty == 4 ? Layout<T, 32, 4>::SMEM : v.ty == 16 ? Layout<T, 32, 16>::SMEM : Layout<T, 32, 8>::SMEM;
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 get_encoder() {
@@ -706,16 +850,69 @@ PFN_cuTensorMapEncodeTiled_v12000 get_encoder() {
     return fn;
 }
 
+// box (width, height) of input field f for tile tx x ty (trimmed: the interior box)
+template <typename T, int TX, int TY>
+void box_of(int f, bool trimmed, int *bw, int *bh) {
+#define FI_BOX_CASE(F)                                      \
+    case F:                                                 \
+        if (trimmed) {                                      \
+            *bw = FBox<T, TX, TY, true, F>::bw;             \
+            *bh = FBox<T, TX, TY, true, F>::bh;             \
+        } else {                                            \
+            *bw = FBox<T, TX, TY, false, F>::bw;            \
+            *bh = FBox<T, TX, TY, false, F>::bh;            \
+        }                                                   \
+        return;
+    switch (f) {
+        FI_BOX_CASE(M_P)
+        FI_BOX_CASE(M_XX)
+        FI_BOX_CASE(M_YY)
+        FI_BOX_CASE(M_ZZ)
+        FI_BOX_CASE(M_XY)
+        FI_BOX_CASE(M_XZ)
+        FI_BOX_CASE(M_YZ)
+        default: FI_BOX_CASE(M_VX)
+    }
+#undef FI_BOX_CASE
+}
+
+template <typename T>
+void variant_box(const Variant &v, int f, bool trimmed, int *bw, int *bh) {
+    if (v.tx == 64) {
+        if (v.ty == 4) box_of<T, 64, 4>(f, trimmed, bw, bh);
+        else box_of<T, 64, 8>(f, trimmed, bw, bh);
+    } else if (v.ty == 4) {
+        box_of<T, 32, 4>(f, trimmed, bw, bh);
+    } else if (v.ty == 16) {
+        box_of<T, 32, 16>(f, trimmed, bw, bh);
+    } else {
+        box_of<T, 32, 8>(f, trimmed, bw, bh);
+    }
+}
+
 }  // namespace
 
 int fused3d_num_variants() { return kNumVariants; }
 const char *fused3d_variant_name(int v) {
-    static char buf[kNumVariants][32];
+    static char buf[kNumVariants][48];
     if (v < 0 || v >= kNumVariants) return "?";
-    snprintf(buf[v], sizeof(buf[v]), "tile32x%d_zb%d", kVariants[v].ty, kVariants[v].zb);
+    const Variant &w = kVariants[v];
+    int n = snprintf(buf[v], sizeof(buf[v]), "tile%dx%d_zb%d", w.tx, w.ty, w.zb);
+    if (w.trim) n += snprintf(buf[v] + n, sizeof(buf[v]) - n, "_trim");
+    if (w.cx * w.cy > 1) snprintf(buf[v] + n, sizeof(buf[v]) - n, "_cl%dx%d", w.cx, w.cy);
     return buf[v];
 }
-int fused3d_variant_ty(int v) { return kVariants[(v < 0 || v >= kNumVariants) ? 0 : v].ty; }
+int fused3d_variant_key(int v) {
+    const Variant &w = kVariants[(v < 0 || v >= kNumVariants) ? 0 : v];
+    return w.tx * 1000 + w.ty;
+}
+bool fused3d_variant_fits(int v, int esz) {
+    if (v < 0 || v >= kNumVariants) return false;
+    const size_t smem = esz == 8 ? variant_smem<double>(kVariants[v]) : variant_smem<float>(kVariants[v]);
+    // 64-wide FP64 tiles would hold one CTA per SM: not offered
+    if (esz == 8 && kVariants[v].tx == 64) return false;
+    return smem <= 227 * 1024;
+}
 
 template <typename T>
 bool fused3d_supported(const Geom &g, const KParams &p, bool ib) {
@@ -743,17 +940,20 @@ bool tma_encode(void *raw_base, int nd, const unsigned long long *dims, const un
     return r == CUDA_SUCCESS;
 }
 
-// one 3D tensor map over a field allocation (raw base, aligned), box = one plane of
-// the widened column for tile height ty
-bool fused3d_encode_map(void *raw_base, const Geom &g, int esz, int ty, void *map_out) {
+// the 3D tensor map of input field f (map order) over a field allocation (raw
+// base, aligned) for a launch shape: box = one plane of the field's full box, or
+// of its trimmed box (stress fields of interior columns)
+bool fused3d_encode_map(void *raw_base, const Geom &g, int esz, int variant, int field, bool trimmed, void *map_out) {
     PFN_cuTensorMapEncodeTiled_v12000 enc = get_encoder();
-    if (!enc) return false;
-    const int bx = esz == 8 ? BoxX<double>::BX : BoxX<float>::BX;
+    if (!enc || variant < 0 || variant >= kNumVariants || field < 0 || field >= M_COUNT) return false;
+    int bw = 0, bh = 0;
+    if (esz == 8) variant_box<double>(kVariants[variant], field, trimmed && field < kTrimmed, &bw, &bh);
+    else variant_box<float>(kVariants[variant], field, trimmed && field < kTrimmed, &bw, &bh);
     cuuint64_t dims[3] = {(cuuint64_t)g.pitch, (cuuint64_t)g.rows, (cuuint64_t)g.planes};
     cuuint64_t strides[2] = {(cuuint64_t)(g.pitch * esz), (cuuint64_t)(g.sxy * esz)};
-    cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)(ty + 2), 1};
+    cuuint32_t box[3] = {(cuuint32_t)bw, (cuuint32_t)bh, 1};
     cuuint32_t estr[3] = {1, 1, 1};
-    // L2 promotion of the box rows (rows are 160 / 288 bytes); FI_TMA_L2_PROMOTION=0/64/128/256 overrides
+    // L2 promotion of the box rows; FI_TMA_L2_PROMOTION=0/64/128/256 overrides
     CUtensorMapL2promotion promo = CU_TENSOR_MAP_L2_PROMOTION_L2_256B;
     if (const char *e = getenv("FI_TMA_L2_PROMOTION")) {
         int v = atoi(e);
@@ -768,15 +968,23 @@ bool fused3d_encode_map(void *raw_base, const Geom &g, int esz, int ty, void *ma
 }
 
 template <typename T>
-cudaError_t launch_fused3d(const Geom &g, const KParams &p, const Ptrs<T> &in, const Ptrs<T> &out, const void *maps11,
+cudaError_t launch_fused3d(const Geom &g, const KParams &p, const Ptrs<T> &in, const Ptrs<T> &out, const void *maps18,
                            int variant, int *err, cudaStream_t s) {
     if (variant < 0 || variant >= kNumVariants) variant = 0;
     const Variant v = kVariants[variant];
-    const InMaps &mp = *reinterpret_cast<const InMaps *>(maps11);
+    if (!fused3d_variant_fits(variant, (int)sizeof(T))) return cudaErrorInvalidConfiguration;
+    const InMaps &mp = *reinterpret_cast<const InMaps *>(maps18);
+    if (v.tx == 64) {
+        if constexpr (sizeof(T) == 4) {
+            if (v.ty == 4) return launch_variant<T, 64, 4>(g, p, in, out, mp, v, err, s);
+            return launch_variant<T, 64, 8>(g, p, in, out, mp, v, err, s);
+        }
+        return cudaErrorInvalidConfiguration;
+    }
     switch (v.ty) {
-        case 4: return launch_variant<T, 4>(g, p, in, out, mp, v.zb, err, s);
-        case 16: return launch_variant<T, 16>(g, p, in, out, mp, v.zb, err, s);
-        default: return launch_variant<T, 8>(g, p, in, out, mp, v.zb, err, s);
+        case 4: return launch_variant<T, 32, 4>(g, p, in, out, mp, v, err, s);
+        case 16: return launch_variant<T, 32, 16>(g, p, in, out, mp, v, err, s);
+        default: return launch_variant<T, 32, 8>(g, p, in, out, mp, v, err, s);
     }
 }
 

@@ -48,23 +48,25 @@ bool vertex_in(int field, int d) {
     }
 }
 
-// fields of a halo message, in message order
-int halo_fields(const fi_model *m, int what, int *out) {
+// fields of a halo message of an nd-dimensional model, in message order
+int halo_fields_nd(int nd, int what, int *out) {
     static const int order[] = {FI_FIELD_P,   FI_FIELD_TXX, FI_FIELD_TYY, FI_FIELD_TZZ, FI_FIELD_TXY, FI_FIELD_TXZ,
                                 FI_FIELD_TYZ, FI_FIELD_VX,  FI_FIELD_VY,  FI_FIELD_VZ,  FI_FIELD_ETA};
     int n = 0;
     for (int f : order) {
         const bool state_only = f <= FI_FIELD_TYZ;
         if (state_only && what != FI_HALO_STATE) continue;
-        if (!model_field_used(m, f)) continue;
+        const bool only_3d = f == FI_FIELD_TZZ || f == FI_FIELD_TXZ || f == FI_FIELD_TYZ || f == FI_FIELD_VZ;
+        if (only_3d && nd != 3) continue;
         out[n++] = f;
     }
     return n;
 }
+int halo_fields(const fi_model *m, int what, int *out) { return halo_fields_nd(m->d.grid.nd, what, out); }
 
-// layer indices along d: pack toward `side` (0 = low neighbour) or unpack from it
-int layers(const fi_model *m, int field, int d, int side, bool pack, int *idx) {
-    const int n = m->d.grid.n[d];
+// layer indices along d (n cells of the slab along d): pack toward `side`
+// (0 = low neighbour) or unpack from it
+int layers_n(int n, int field, int d, int side, bool pack, int *idx) {
     const bool v = vertex_in(field, d);
     if (pack) {
         if (side == 0) {
@@ -82,6 +84,9 @@ int layers(const fi_model *m, int field, int d, int side, bool pack, int *idx) {
     idx[0] = n + 1;
     if (v) idx[1] = n + 2;
     return v ? 2 : 1;
+}
+int layers(const fi_model *m, int field, int d, int side, bool pack, int *idx) {
+    return layers_n(m->d.grid.n[d], field, d, side, pack, idx);
 }
 
 // elements of one layer: the storage plane of the other dimensions
@@ -163,6 +168,29 @@ fi_status fi_model_halo_bytes(const fi_model *m, int32_t dim, int32_t side, int3
         layers_total += (size_t)layers(m, fl[q], dim, side, true, idx);
     }
     *bytes = layers_total * (size_t)layer_elems(m, dim) * m->esz;
+    return FI_OK;
+}
+
+fi_status fi_halo_plan(int32_t nd, const int32_t *n, int32_t dim, int32_t side, int32_t what, int32_t pack,
+                       int32_t *fields, int32_t *layer_index, int32_t cap, int32_t *count) {
+    if (!n || !count || (nd != 2 && nd != 3) || dim < 0 || dim > 1 || (side != 0 && side != 1) ||
+        (what != FI_HALO_ITERATION && what != FI_HALO_STATE) || cap < 0 || (cap > 0 && (!fields || !layer_index)))
+        return set_error("bad argument"), FI_ERR_ARG;
+    int fl[16];
+    const int nf = halo_fields_nd(nd, what, fl);
+    int k = 0;
+    for (int q = 0; q < nf; q++) {
+        int idx[2];
+        const int nl = layers_n(n[dim], fl[q], dim, side, pack != 0, idx);
+        for (int l = 0; l < nl; l++, k++) {
+            if (k < cap) {
+                fields[k] = fl[q];
+                layer_index[k] = idx[l];
+            }
+        }
+    }
+    *count = k;
+    if (k > cap && cap > 0) return set_error("plan longer than the arrays given"), FI_ERR_ARG;
     return FI_OK;
 }
 

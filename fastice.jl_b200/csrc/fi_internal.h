@@ -167,17 +167,22 @@ int norm_blocks(const Geom &g);
 // P,tau,V read from `in`, written to `out`; eta read from in.eta, eta_next written.
 template <typename T>
 bool fused3d_supported(const Geom &g, const KParams &p, bool ib);
-// maps11: the eleven input tensor maps (P, txx, tyy, tzz, txy, txz, tyz, Vx, Vy, Vz, eta),
-// 128 bytes each, encoded with fused3d_encode_map for the variant's tile height
+// maps18: the eleven full-box input tensor maps (P, txx, tyy, tzz, txy, txz, tyz, Vx,
+// Vy, Vz, eta) then the trimmed-box maps of the seven stresses, 128 bytes each,
+// encoded with fused3d_encode_map for the variant
 template <typename T>
-cudaError_t launch_fused3d(const Geom &g, const KParams &p, const Ptrs<T> &in, const Ptrs<T> &out, const void *maps11,
+cudaError_t launch_fused3d(const Geom &g, const KParams &p, const Ptrs<T> &in, const Ptrs<T> &out, const void *maps18,
                            int variant, int *err, cudaStream_t s);
-bool fused3d_encode_map(void *raw_base, const Geom &g, int esz, int ty, void *map_out);
+// field: index in the map order above (0..10); trimmed: the interior box of a stress
+bool fused3d_encode_map(void *raw_base, const Geom &g, int esz, int variant, int field, bool trimmed, void *map_out);
 // generic tiled tensor map (fi_fused3d.cu): nd dims, strides of dims 1..nd-1 in bytes
 bool tma_encode(void *raw_base, int nd, const unsigned long long *dims, const unsigned long long *strides,
                 const unsigned *box, int esz, void *map_out);
 int fused3d_num_variants();
-int fused3d_variant_ty(int v);
+// launch shapes with the same key read through the same tensor maps
+int fused3d_variant_key(int v);
+// whether launch shape v fits a CTA in precision esz (8 or 4 bytes)
+bool fused3d_variant_fits(int v, int esz);
 const char *fused3d_variant_name(int v);
 
 // ---- mixed-precision solve helpers (fi_mixed.cu) ----

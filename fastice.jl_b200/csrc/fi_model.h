@@ -32,7 +32,7 @@ struct fi_model {
     int nblk = 0;
     int path = FI_PATH_REFERENCE;
     int fused_variant = 0;
-    int maps_ty = -1;  // tile height the tensor maps were encoded for
+    int maps_key = -1;  // launch-shape key (fused3d_variant_key) the tensor maps were encoded for
     bool ib = false;
     long long iterations = 0;
     int *d_err = nullptr;  // device error word written by bounded waits
@@ -62,6 +62,9 @@ struct fi_model {
     alignas(64) unsigned char map_base[kState][128];
     alignas(64) unsigned char map_alt[kState][128];
     alignas(64) unsigned char map_eta[2][128];  // base[ETA], base[ETA_NEXT]
+    // trimmed-box maps of the seven stress fields (interior columns of trimmed launch shapes)
+    alignas(64) unsigned char tmap_base[7][128];
+    alignas(64) unsigned char tmap_alt[7][128];
 
     bool is_f64() const { return d.dtype == FI_F64; }
 

@@ -9,19 +9,25 @@
 // byte), and long-running services that fix their device memory at start-up and
 // forbid allocation afterwards (an allocation there could fail or stall a loop).
 // The first call on a device looks up the array's device address
-// (cudaGetSymbolAddress); make that first call before any stream capture.
+// (cudaGetSymbolAddress) and caches it; make that first call before any stream
+// capture.  The cache is per process: after cudaDeviceReset (or anything else
+// that unloads the library's module on a device) the cached address is stale,
+// so a program that resets a device must not call this entry point afterwards.
 //
-// Limits and sharing.  The array holds kNoAllocSlots per-block partials
-// (kNoAllocSlots * 12 doubles, 3 MiB), and every loaded device keeps its own
-// copy until the process exits.  Each block reduces up to kPointsPerBlock grid
-// indices, so a grid with more than kNoAllocSlots * kPointsPerBlock vertex-range
-// indices ((n0+1)(n1+1)(n2+1), e.g. more than 511^3 cells) is rejected with
-// FI_ERR_ARG.  All calls on a device share the one array: calls whose work
-// overlaps on the GPU (on different streams, or from several host threads)
-// race on it and must be serialised by the caller.  Every slot a call reads is
-// written by the same call first, so nothing needs clearing between calls.
+// Limits and sharing.  The reduction runs a grid-stride loop over
+// norm_blocks(grid) blocks (at most 148 * 8, whatever the grid size), the same
+// block count as the model's own entry point, so the two give identical bits.
+// The array holds kNoAllocSlots per-block partials (kNoAllocSlots * 12 doubles,
+// 192 KiB), and every loaded device keeps its own copy until the process exits;
+// a launch needing more blocks than slots would be rejected with FI_ERR_ARG (no
+// grid does with these constants).  All calls on a device share the one array:
+// calls whose work overlaps on the GPU (on different streams, or from several
+// host threads) race on it and must be serialised by the caller.  Every slot a
+// call reads is written by the same call first, so nothing needs clearing
+// between calls.
 #include <cuda_runtime.h>
 
+#include <mutex>
 #include <string>
 
 #include "fi_internal.h"
@@ -29,20 +35,22 @@
 namespace fi {
 namespace {
 
-constexpr int kNoAllocSlots = 32768;
-constexpr long long kPointsPerBlock = 256LL * 16;  // threads per block x grid indices per thread
+constexpr int kNoAllocSlots = 2048;
 constexpr int kMaxDevices = 64;
 
 // per-block partials (FI_NORMS_LEN-slot layout), one copy per device
 static __device__ __align__(256) double g_noalloc_partials[kNoAllocSlots * kNormSlots];
 // device address of g_noalloc_partials on each device, filled once per device
+// under g_partials_lock (host threads may make their first calls concurrently)
 static double *g_partials_addr[kMaxDevices] = {};
+static std::mutex g_partials_lock;
 
 fi_status scratch_for_current_device(double **out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
     if (dev < 0 || dev >= kMaxDevices) return set_error("device ordinal beyond the no-alloc table"), FI_ERR_UNSUPPORTED;
+    std::lock_guard<std::mutex> guard(g_partials_lock);
     if (!g_partials_addr[dev]) {
         void *ptr = nullptr;
         e = cudaGetSymbolAddress(&ptr, g_noalloc_partials);
@@ -78,17 +86,6 @@ extern "C" fi_status fi_residual_norms_noalloc(const fi_model_desc *desc, const 
         for (int c = 0; c < 8; c++)
             if (!state->na[c] || !state->ns[c]) return set_error("missing immersed-boundary mask"), FI_ERR_ARG;
 
-    const long long points = (long long)(gr.n[0] + 1) * (gr.n[1] + 1) * (three ? gr.n[2] + 1 : 1);
-    const long long blocks = (points + kPointsPerBlock - 1) / kPointsPerBlock;
-    if (blocks > kNoAllocSlots)
-        return set_error("grid too large for the no-alloc scratch: " + std::to_string(points) +
-                         " grid indices, at most " + std::to_string((long long)kNoAllocSlots * kPointsPerBlock)),
-               FI_ERR_ARG;
-
-    double *scratch = nullptr;
-    fi_status st = scratch_for_current_device(&scratch);
-    if (st != FI_OK) return st;
-
     Geom g{};
     g.nd = gr.nd;
     for (int k = 0; k < 3; k++) g.n[k] = k < gr.nd ? gr.n[k] : 0;
@@ -104,6 +101,16 @@ extern "C" fi_status fi_residual_norms_noalloc(const fi_model_desc *desc, const 
         for (int s = 0; s < 2; s++) kp.bc_kind[k][s] = k < gr.nd ? desc->bc[k][s].kind : FI_BC_TRACTION;
     }
     kp.small = desc->dtype == FI_F64 ? 1e-6 : (double)small_threshold_f32();
+    // the model's own block count: a grid-stride reduction whose partials fit the array
+    const int blocks = norm_blocks(g);
+    if (blocks > kNoAllocSlots)
+        return set_error("the reduction needs " + std::to_string(blocks) + " partial slots, the no-alloc scratch has " +
+                         std::to_string(kNoAllocSlots)),
+               FI_ERR_ARG;
+
+    double *scratch = nullptr;
+    fi_status st = scratch_for_current_device(&scratch);
+    if (st != FI_OK) return st;
 
     cudaStream_t s = (cudaStream_t)stream;
     cudaError_t e;
@@ -117,7 +124,7 @@ extern "C" fi_status fi_residual_norms_noalloc(const fi_model_desc *desc, const 
             f.wna[c] = (const double *)state->na[c];
             f.wns[c] = (const double *)state->ns[c];
         }
-        e = launch_residual_norms<double>(g, kp, f, desc->immersed != 0, scratch, (int)blocks, out_dev, s);
+        e = launch_residual_norms<double>(g, kp, f, desc->immersed != 0, scratch, blocks, out_dev, s);
     } else {
         Ptrs<float> f{};
         f.P = (float *)state->P; f.txx = (float *)state->txx; f.tyy = (float *)state->tyy; f.tzz = (float *)state->tzz;
@@ -128,7 +135,7 @@ extern "C" fi_status fi_residual_norms_noalloc(const fi_model_desc *desc, const 
             f.wna[c] = (const float *)state->na[c];
             f.wns[c] = (const float *)state->ns[c];
         }
-        e = launch_residual_norms<float>(g, kp, f, desc->immersed != 0, scratch, (int)blocks, out_dev, s);
+        e = launch_residual_norms<float>(g, kp, f, desc->immersed != 0, scratch, blocks, out_dev, s);
     }
     if (e != cudaSuccess) return cuda_fail(e, "no-alloc residual norms");
     return FI_OK;

@@ -20,12 +20,61 @@ pair of sends and receives is posted in that order (and tagged, for gloo).
 
 A slab needs an ``exchange`` step only when R > 1: with one rank the sweep's own
 periodic images are already the neighbour's values.
+
+Convergence.  The driver's check (tm_stokes_chmy.jl:283-305) takes the residual
+norms every ncheck iterations; the reference's distributed driver reduces them
+over the ranks with MPI.Allreduce(MAX) (tm_stokes_mpi_wip.jl:21-22,157-163).
+``reduce_norms`` does the same over the FI_NORMS_LEN slots: the ∞-norms of r_P and
+r_V, max|V| and the non-finite flag by maximum (each equals the undivided
+domain's value exactly), the L2 norms as the root of the summed squares (the node
+layer two slabs share along the split dimension then counts on both sides).
+``Slab.solve`` is the driver loop on top: every rank takes the same checks and, from
+the same reduced norms, the same decision.
+
+Streams.  With device buffers the pack, the point-to-point operations and the
+unpack are all ordered on the model's own stream (the transfers are issued with it
+as torch's current stream, and waiting on them orders that stream after them), so
+an exchange needs no host synchronisation.
 """
 from __future__ import annotations
 
+import math
 from typing import Callable, Optional
 
+import numpy as np
+
 TAG_TO_LOW, TAG_TO_HIGH = 11, 12
+NORMS_LEN = 12
+NORM_MAX_SLOTS = (0, 1, 2, 3, 8, 9, 10, 11)  # ∞-norms of r_P, r_Vx..z; max|V|; non-finite flag
+NORM_L2_SLOTS = (4, 5, 6, 7)                  # L2 norms of r_P, r_Vx..z
+
+
+def combine_norms(per_rank) -> np.ndarray:
+    """The norm vector of the whole domain from the ranks' vectors (what
+    ``TorchTransport.allreduce_norms`` computes with collectives)."""
+    per_rank = [np.asarray(r, dtype=np.float64) for r in per_rank]
+    out = np.zeros(NORMS_LEN)
+    for q in NORM_MAX_SLOTS:
+        out[q] = max(r[q] for r in per_rank)
+    for q in NORM_L2_SLOTS:
+        out[q] = math.sqrt(sum(r[q] * r[q] for r in per_rank))
+    return out
+
+
+def measure_of(norms, measure: str = "abs_inf", nd: int = 3, rho_g_inf: float = 1.0, length_z: float = 1.0) -> float:
+    """Convergence measure of a norm vector, as fi_model_solve computes it:
+    abs_inf = max ∞-norm of r_P and r_V; rel_slab = max(|r_V|∞ / |ρg|∞,
+    |r_P|∞ · L_z / max|V|)."""
+    n = norms
+    if measure == "rel_slab":
+        rv = max(n[1], n[2], n[3] if nd == 3 else 0.0)
+        vmax = max(n[8], n[9], n[10])
+        a = rv / (rho_g_inf if rho_g_inf > 0 else 1.0)
+        b = n[0] * length_z / vmax if vmax > 0 else n[0]
+        return max(a, b)
+    if measure != "abs_inf":
+        raise ValueError(measure)
+    return max(n[0], n[1], n[2], n[3])
 
 
 class TorchTransport:
@@ -44,9 +93,26 @@ class TorchTransport:
     def _global(self, r):
         return r if self.group is None else self.dist.get_global_rank(self.group, r)
 
+    def allreduce_norms(self, norms) -> np.ndarray:
+        """``combine_norms`` over the ranks: one MAX and one SUM all-reduce, taken
+        in the same order on every rank."""
+        import torch
+        d = self.dist
+        dev = "cuda" if d.get_backend(self.group) == "nccl" else "cpu"
+        n = np.asarray(norms, dtype=np.float64)
+        mx = torch.tensor([n[q] for q in NORM_MAX_SLOTS], dtype=torch.float64, device=dev)
+        sq = torch.tensor([n[q] * n[q] for q in NORM_L2_SLOTS], dtype=torch.float64, device=dev)
+        d.all_reduce(mx, op=d.ReduceOp.MAX, group=self.group)
+        d.all_reduce(sq, op=d.ReduceOp.SUM, group=self.group)
+        out = np.zeros(NORMS_LEN)
+        out[list(NORM_MAX_SLOTS)] = mx.cpu().numpy()
+        out[list(NORM_L2_SLOTS)] = np.sqrt(sq.cpu().numpy())
+        return out
+
     def exchange(self, send_low, send_high, recv_low, recv_high) -> None:
         """send_low -> low neighbour (its recv_high), send_high -> high neighbour
-        (its recv_low); blocks until all four operations completed."""
+        (its recv_low).  Waiting on the operations orders torch's current stream
+        after them (device tensors) or blocks until they completed (host tensors)."""
         d = self.dist
         low, high = (self._global(r) for r in self.neighbours())
         ops = [d.P2POp(d.isend, send_low, low, self.group, TAG_TO_LOW),
@@ -67,9 +133,9 @@ class Slab:
     address.
     """
 
-    def __init__(self, model, dim: int, transport, alloc: Optional[Callable] = None, stream_ctx=None):
+    def __init__(self, model, dim: int, transport, alloc: Optional[Callable] = None):
         self.model, self.dim, self.transport = model, int(dim), transport
-        self.stream_ctx = stream_ctx
+        self.iterations = 0
         if alloc is None:
             import torch
             dev = torch.device("cuda", torch.cuda.current_device())
@@ -85,27 +151,70 @@ class Slab:
         # a host-side model (halo_takes_tensors) packs into the tensor itself
         return t if getattr(self.model, "halo_takes_tensors", False) else t.data_ptr()
 
-    def exchange(self, what: str = "iteration") -> None:
-        if self.transport.size == 1:
-            return
+    def _steps(self, what):
         b, m, d = self.buf[what], self.model, self.dim
         m.halo_pack(d, 0, self._ptr(b["send_low"]), what)
         m.halo_pack(d, 1, self._ptr(b["send_high"]), what)
-        if self.stream_ctx is not None:
-            with self.stream_ctx():
-                self.transport.exchange(b["send_low"], b["send_high"], b["recv_low"], b["recv_high"])
-        else:
-            if hasattr(m, "synchronize"):
-                m.synchronize()
-            self.transport.exchange(b["send_low"], b["send_high"], b["recv_low"], b["recv_high"])
+        yield
+        self.transport.exchange(b["send_low"], b["send_high"], b["recv_low"], b["recv_high"])
         m.halo_unpack(d, 0, self._ptr(b["recv_low"]), what)
         m.halo_unpack(d, 1, self._ptr(b["recv_high"]), what)
+
+    def exchange(self, what: str = "iteration") -> None:
+        if self.transport.size == 1:
+            return
+        b, m = self.buf[what], self.model
+        on_device = hasattr(b["send_low"], "is_cuda") and b["send_low"].is_cuda and hasattr(m, "stream_ptr")
+        steps = self._steps(what)
+        if on_device:
+            # pack, transfers and unpack in order on the model's stream
+            import torch
+            with torch.cuda.stream(torch.cuda.ExternalStream(m.stream_ptr)):
+                for _ in steps:
+                    pass
+        else:
+            next(steps)
+            if hasattr(m, "synchronize"):
+                m.synchronize()  # the packed messages are complete before a host transport reads them
+            for _ in steps:
+                pass
 
     def advance(self, niter: int) -> None:
         """niter PT iterations, each followed by the halo exchange of V and η."""
         for _ in range(int(niter)):
             self.model.advance(1)
             self.exchange("iteration")
+            self.iterations += 1
+
+    def residual_norms(self) -> np.ndarray:
+        """The residual norms of the whole domain (every rank gets the same vector)."""
+        local = self.model.residual_norms()
+        if self.transport.size == 1:
+            return np.asarray(local, dtype=np.float64)
+        return self.transport.allreduce_norms(local)
+
+    def solve(self, *, max_iter: int, ncheck: int, tol: float, measure: str = "abs_inf", rho_g_inf: float = 1.0,
+              length_z: float = 1.0, nd: int = 3) -> dict:
+        """The driver loop (tm_stokes_chmy.jl:283-305) over the split domain: ncheck
+        iterations with their exchanges, then the reduced norms and the decision,
+        which every rank takes alike; stops on convergence (measure < tol), on a
+        non-finite residual or after max_iter iterations (as fi_model_solve)."""
+        it, rep = 0, {"converged": False, "diverged": False, "measure": float("nan"), "norms": None}
+        while it < max_iter:
+            k = min(ncheck, max_iter - it)
+            self.advance(k)
+            it += k
+            norms = self.residual_norms()
+            meas = measure_of(norms, measure, nd, rho_g_inf, length_z)
+            rep.update(measure=meas, norms=norms.tolist())
+            if norms[11] != 0.0 or not math.isfinite(meas):
+                rep["diverged"] = True
+                break
+            if meas < tol:
+                rep["converged"] = True
+                break
+        rep["iterations"] = it
+        return rep
 
 
 def exchange_local(slabs, dim: int, what: str = "iteration") -> None:
@@ -134,6 +243,49 @@ def exchange_local(slabs, dim: int, what: str = "iteration") -> None:
         m.synchronize()
 
 
+def halo_plan(nd: int, n, dim: int, side: int, what: str = "iteration", pack: bool = True, library: str = "fast"):
+    """The library's layer plan of a halo message (fi_halo_plan, host only): a list
+    of (field name, layer index along ``dim``) in message order, each one whole
+    storage plane of the other dimensions."""
+    import ctypes as C
+    from . import _lib as L
+    lib = L.load(library)
+    nn = (C.c_int32 * 3)(*(list(n) + [0] * (3 - len(n))))
+    w = {"iteration": 0, "state": 1}[what]
+    cnt = C.c_int32()
+    L.check(lib, lib.fi_halo_plan(nd, nn, dim, side, w, int(pack), None, None, 0, C.byref(cnt)))
+    f, l = (C.c_int32 * cnt.value)(), (C.c_int32 * cnt.value)()
+    L.check(lib, lib.fi_halo_plan(nd, nn, dim, side, w, int(pack), f, l, cnt.value, C.byref(cnt)))
+    return [(L.FIELD_NAMES[f[k]], l[k]) for k in range(cnt.value)]
+
+
+def solve_local(slabs, dim: int, *, max_iter: int, ncheck: int, tol: float, measure: str = "abs_inf",
+                rho_g_inf: float = 1.0, length_z: float = 1.0) -> dict:
+    """``Slab.solve`` for a ring of slabs held by one process (one device): the same
+    iterations, exchanges (``exchange_local``), norm reduction (``combine_norms``)
+    and decision as a multi-rank run."""
+    nd = slabs[0].grid.ndims if hasattr(slabs[0], "grid") else 3
+    it, rep = 0, {"converged": False, "diverged": False, "measure": float("nan"), "norms": None}
+    while it < max_iter:
+        k = min(ncheck, max_iter - it)
+        for _ in range(k):
+            for m in slabs:
+                m.advance(1)
+            exchange_local(slabs, dim)
+        it += k
+        norms = combine_norms([m.residual_norms() for m in slabs])
+        meas = measure_of(norms, measure, nd, rho_g_inf, length_z)
+        rep.update(measure=meas, norms=norms.tolist())
+        if norms[11] != 0.0 or not math.isfinite(meas):
+            rep["diverged"] = True
+            break
+        if meas < tol:
+            rep["converged"] = True
+            break
+    rep["iterations"] = it
+    return rep
+
+
 def slab_of(global_interior, dim: int, rank: int, size: int, vertex: bool):
     """The part of a global interior array (numpy order (z, y, x) / (y, x)) that
     slab ``rank`` of ``size`` holds along ``dim``: its n cells, or its n+1 nodes for
@@ -149,4 +301,4 @@ def slab_of(global_interior, dim: int, rank: int, size: int, vertex: bool):
     return global_interior[tuple(sl)]
 
 
-__all__ = ["TorchTransport", "Slab", "exchange_local", "slab_of"]
+__all__ = ["TorchTransport", "Slab", "exchange_local", "solve_local", "slab_of", "combine_norms", "measure_of", "halo_plan"]

@@ -23,7 +23,8 @@ import numpy as np
 
 from . import _lib as L
 from .grids import UniformGrid
-from .physics import (ArrayField, BoundaryCondition, FunctionField, Periodic, ValueField, rheology_desc)
+from .physics import (ArrayField, BoundaryCondition, FunctionField, IceRheology, Periodic, Relaxation, ValueField,
+                      rheology_desc)
 
 _DTYPES = {"f64": (L.FI_F64, np.float64), "f32": (L.FI_F32, np.float32)}
 _HALO = {"iteration": L.FI_HALO_ITERATION, "state": L.FI_HALO_STATE}
@@ -100,12 +101,34 @@ def _dtau(solver_params, nd):
     return p
 
 
+def effective_rheology(rheology: IceRheology, solver_params: dict, eta_rel: Optional[str] = None) -> IceRheology:
+    """The rheology a model iterates with.  Drivers pass an under-relaxation rate
+    ``η_rel`` in ``solver_params`` (stokes_manufactured_solution_free_slip_2D.jl:76,
+    tm_stokes_mpi_wip.jl:71) that the reference's kernels never read; by default it
+    is ignored here too, so results stay the reference's.  With ``eta_rel`` =
+    'log', 'log10' or 'lin' the rate is honoured as its evident intent: the new
+    viscosity relaxes from the current one toward the rheology's value,
+    Relaxation(η, rheology, η_rel; scale) of Physics.jl:28-47."""
+    rate = None
+    if solver_params:
+        rate = solver_params.get("η_rel", solver_params.get("eta_rel"))
+    if eta_rel is None or rate is None:
+        return rheology
+    if eta_rel not in ("log", "log10", "lin"):
+        raise ValueError("eta_rel must be None, 'log', 'log10' or 'lin'")
+    if isinstance(rheology, Relaxation):
+        raise ValueError("the rheology is a Relaxation already; η_rel would nest a second one")
+    return Relaxation(rheology, float(rate), scale=None if eta_rel == "lin" else eta_rel)
+
+
 class _StokesBase:
     immersed = False
 
     def __init__(self, *, grid: UniformGrid, boundary_conditions, gravity, rheology, solver_params, arch=None,
-                 dtype: str = "f64", path: str = "auto", outer_width=None, level_sets=None, library: str = "fast"):
+                 dtype: str = "f64", path: str = "auto", outer_width=None, level_sets=None, library: str = "fast",
+                 eta_rel: Optional[str] = None):
         self.lib = L.load(library)
+        rheology = effective_rheology(rheology, solver_params, eta_rel)
         self.grid = grid
         self.arch = arch or Arch()
         self.dtype = dtype
@@ -214,6 +237,11 @@ class _StokesBase:
             raise ValueError("out must be a contiguous array of the field's interior shape and the model's dtype")
         L.check(self.lib, self.lib.fi_model_get_field(self._h, L.FIELD_ID[name], arr.ctypes.data, arr.nbytes))
         return arr
+
+    def copy_field(self, dst: str, src: str) -> None:
+        """set!(dst, src) on the device between two fields at the same location
+        (e.g. η_next from η), ghosts included."""
+        L.check(self.lib, self.lib.fi_model_copy_field(self._h, L.FIELD_ID[dst], L.FIELD_ID[src]))
 
     def _upload_input(self, name, src):
         if isinstance(src, FunctionField):
@@ -473,7 +501,7 @@ def interior(field: FieldRef) -> np.ndarray:
 
 
 def pt_params(grid: UniformGrid, r: float = 0.7, re_mech: float = 8 * math.pi, vdtau_factor: float = 1.1,
-              use_center_spacing: bool = True) -> dict:
+              use_center_spacing: bool = True, eta_rel: Optional[float] = None) -> dict:
     """Pseudo-transient steps as the drivers compute them
     (stokes_manufactured_solution_free_slip_2D.jl:67-77; tm_stokes_chmy.jl:48-54 uses
     re_mech=2π and factor 1.5): returns solver_params with Δτ."""
@@ -484,4 +512,7 @@ def pt_params(grid: UniformGrid, r: float = 0.7, re_mech: float = 8 * math.pi, v
     dt_r = 1.0 / (theta + 1.0)
     nudt = vdtau * ltau
     taus = ("xx", "yy", "zz", "xy", "xz", "yz") if nd == 3 else ("xx", "yy", "xy")
-    return {"Δτ": {"Pr": r / theta, "τ": {k: dt_r for k in taus}, "V": {k: nudt for k in ("x", "y", "z")[:nd]}}}
+    sp = {"Δτ": {"Pr": r / theta, "τ": {k: dt_r for k in taus}, "V": {k: nudt for k in ("x", "y", "z")[:nd]}}}
+    if eta_rel is not None:
+        sp["η_rel"] = float(eta_rel)  # read only by models created with eta_rel=... (see effective_rheology)
+    return sp

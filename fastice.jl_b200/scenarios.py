@@ -118,21 +118,9 @@ def bed_model(seed: int, n: int, dtype: str = "f64", library: str = "fast", rheo
     (scripts_future_API/test_volume_fractions.jl:86-100).  Traction-free box
     sides, ρg = (0, 0, 1), linear viscosity 1 unless ``rheology`` is given, and
     that driver's PT steps (``pt`` = (r, re, factor) = (0.9, 5π, 1.1)) unless given."""
-    from .levelsets import compute_levelset_from_dem
     from .models import IsothermalImmersedBoundaryFullStokesModel
     from .physics import TBC
-    prm = bed_params(seed, n)
-    grid = UniformGrid(origin=(0.0, 0.0, 0.0), extent=(1.0, 1.0, 1.0), dims=(n, n, n))
-    m2 = dem_cells or n + 1
-    dem_grid = UniformGrid(origin=(-0.05, -0.05), extent=(1.1, 1.1), dims=(m2, m2))
-    # vertex coordinates of the DEM grid in halo storage (index 0 is one spacing outside)
-    h = 1.1 / m2
-    xv = -0.05 + (np.arange(m2 + 3) - 1) * h
-    Y, X = np.meshgrid(xv, xv, indexing="ij")
-    bed = bed_height(prm, X, Y)
-    surf = 0.6 + 0.05 * np.sin(2.0 * math.pi * X)
-    psi_na = compute_levelset_from_dem(grid, dem_grid, surf, library=library)
-    psi_ns = compute_levelset_from_dem(grid, dem_grid, bed, invert=True, library=library)
+    grid, psi_na, psi_ns, prm = bed_levelsets(seed, n, library=library, dem_cells=dem_cells)
     free = TBC(0.0, 0.0, 0.0)
     r, re_mech, factor = pt
     sp = pt_params(grid, r=r, re_mech=re_mech, vdtau_factor=factor)
@@ -147,6 +135,31 @@ def bed_model(seed: int, n: int, dtype: str = "f64", library: str = "fast", rheo
     m.apply_bcs()
     prm.update(thickness=0.6)
     return m, prm
+
+
+def bed_dems(seed: int, n: int, dem_cells=None):
+    """The glacier's DEMs on their 2D vertex grid (halo storage): returns
+    (dem_grid, bed heights, surface heights, params)."""
+    prm = bed_params(seed, n)
+    m2 = dem_cells or n + 1
+    dem_grid = UniformGrid(origin=(-0.05, -0.05), extent=(1.1, 1.1), dims=(m2, m2))
+    # vertex coordinates of the DEM grid in halo storage (index 0 is one spacing outside)
+    h = 1.1 / m2
+    xv = -0.05 + (np.arange(m2 + 3) - 1) * h
+    Y, X = np.meshgrid(xv, xv, indexing="ij")
+    return dem_grid, bed_height(prm, X, Y), 0.6 + 0.05 * np.sin(2.0 * math.pi * X), prm
+
+
+def bed_levelsets(seed: int, n: int, library: str = "fast", dem_cells=None):
+    """Level sets of the glacier of ``seed`` on the unit cube with n^3 cells, from
+    its DEMs on the device: returns (grid, ψ.na from the surface, ψ.ns from the bed
+    inverted, params)."""
+    from .levelsets import compute_levelset_from_dem
+    grid = UniformGrid(origin=(0.0, 0.0, 0.0), extent=(1.0, 1.0, 1.0), dims=(n, n, n))
+    dem_grid, bed, surf, prm = bed_dems(seed, n, dem_cells)
+    psi_na = compute_levelset_from_dem(grid, dem_grid, surf, library=library)
+    psi_ns = compute_levelset_from_dem(grid, dem_grid, bed, invert=True, library=library)
+    return grid, psi_na, psi_ns, prm
 
 
 def bed_params(seed: int, n: int, bumps: int = 64):
@@ -164,6 +177,54 @@ def bed_height(prm, x, y):
     for a, w, (cx, cy) in zip(prm["a"], prm["w"], prm["c"]):
         h = h + a * np.exp(-((x - cx) ** 2 + (y - cy) ** 2) / (w * w))
     return h
+
+
+# ---- 2D manufactured solution on the unit square (the 128^2 plain-method case):
+# forcing of scripts_future_API/stokes_manufactured_solution_free_slip_2D.jl:31-32
+def mms2d_gravity(grid, eta: float = 1.0):
+    """Body force of the 2D free-slip manufactured solution vx = sin πx cos πy,
+    vy = -cos πx sin πy, P = 0 (η = 1), at the velocity locations."""
+    from .physics import FunctionField
+    from .grids import Center, Vertex
+
+    def gx(x, y):
+        return -2 * eta * math.pi ** 2 * np.sin(math.pi * x) * np.cos(math.pi * y)
+
+    def gy(x, y):
+        return 2 * eta * math.pi ** 2 * np.cos(math.pi * x) * np.sin(math.pi * y)
+    return {"x": FunctionField(gx, grid, (Vertex(), Center())), "y": FunctionField(gy, grid, (Center(), Vertex()))}
+
+
+def mms2d_exact(grid):
+    """Exact vx, vy at their staggered interior locations (numpy (y, x) order)."""
+    from .grids import Center, Vertex
+    xv, xc = grid.coords(Vertex(), 0), grid.coords(Center(), 0)
+    yv, yc = grid.coords(Vertex(), 1), grid.coords(Center(), 1)
+    vx = np.sin(math.pi * xv)[None, :] * np.cos(math.pi * yc)[:, None]
+    vy = -np.cos(math.pi * xc)[None, :] * np.sin(math.pi * yv)[:, None]
+    return vx, vy
+
+
+def mms2d_model(n: int, dtype: str = "f64", library: str = "fast"):
+    """The 2D manufactured-solution model on the unit square with n^2 cells (η = 1,
+    free slip on every side, zero initial state): returns (grid, model, gravity)."""
+    grid = UniformGrid(origin=(0.0, 0.0), extent=(1.0, 1.0), dims=(n, n))
+    slip = SBC(0.0, 0.0)
+    gravity = mms2d_gravity(grid)
+    m = IsothermalFullStokesModel(grid=grid, boundary_conditions={"x": (slip, slip), "y": (slip, slip)},
+                                  gravity=gravity, rheology=LinearViscousRheology(1.0),
+                                  solver_params=pt_params(grid), dtype=dtype, library=library)
+    m.set_field("eta", 1.0)
+    m.set_field("eta_next", 1.0)
+    m.apply_bcs()
+    return grid, m, gravity
+
+
+def mms2d_error(grid, m) -> float:
+    """Relative L2 error of the model's velocity against the 2D manufactured solution."""
+    ex, ey = mms2d_exact(grid)
+    vx, vy = m.get_field("Vx").astype(np.float64), m.get_field("Vy").astype(np.float64)
+    return math.sqrt((np.sum((vx - ex) ** 2) + np.sum((vy - ey) ** 2)) / (np.sum(ex ** 2) + np.sum(ey ** 2)))
 
 
 # ---- 3D manufactured solution (scripts_future_API/stokes_manufactured_solution_free_slip_3D.jl:25-48)
@@ -229,5 +290,5 @@ def mms3d_error(grid, m) -> float:
     return math.sqrt(num / den)
 
 
-__all__ = ["mms3d_gravity", "mms3d_exact", "mms3d_model", "mms3d_error", "inclusion_params", "inclusion_viscosity", "inclusion_model", "smooth_log", "stiffness_ratio",
-           "bed_model", "bed_params", "bed_height", "INCLUSION_N_RANGE"]
+__all__ = ["mms2d_gravity", "mms2d_exact", "mms2d_model", "mms2d_error", "mms3d_gravity", "mms3d_exact", "mms3d_model", "mms3d_error", "inclusion_params", "inclusion_viscosity", "inclusion_model", "smooth_log", "stiffness_ratio",
+           "bed_model", "bed_params", "bed_height", "bed_dems", "bed_levelsets", "INCLUSION_N_RANGE"]

@@ -160,6 +160,10 @@ fi_status fi_model_destroy(fi_model *m);
  * it is destroyed (at most 64 MB, at least one z plane, at most one field). */
 fi_status fi_model_set_field(fi_model *m, int32_t field, const void *host, size_t nbytes);
 fi_status fi_model_get_field(fi_model *m, int32_t field, void *host, size_t nbytes);
+/* set!(dst, src) between two fields of the model at the same staggered location,
+ * on the device (the drivers' η_next = η before iterating, tm_stokes_chmy.jl:277-278):
+ * the whole halo box, ghosts included. */
+fi_status fi_model_copy_field(fi_model *m, int32_t dst, int32_t src);
 /* interior element count of a field (n or n+1 per dim by location) */
 fi_status fi_model_field_size(const fi_model *m, int32_t field, size_t *count);
 
@@ -228,13 +232,15 @@ fi_status fi_model_synchronize(fi_model *m);
 /* which kernel path the model runs (fi_path, never AUTO) */
 fi_status fi_model_path(const fi_model *m, int32_t *path);
 
-/* Tile shape and z-block depth of the fused sweep.  fi_model_autotune times
- * every variant for `iters` iterations on the model itself (so the model
- * advances by n_variants * iters PT iterations, like warm-up iterations), keeps
- * the fastest and writes its index and the per-variant milliseconds per
- * iteration to best / ms (ms may be NULL; it needs fi_fused_variant_count()
- * slots).  No counterpart in the reference (its launch shape is fixed by Chmy's
- * Launcher). */
+/* Launch shape of the fused sweep: tile width and height, z-block depth,
+ * thread-block cluster shape and trimmed interior boxes.  A shape that does not
+ * fit a CTA in the model's precision is rejected by fi_model_set_variant with
+ * FI_ERR_UNSUPPORTED.  fi_model_autotune times every shape offered in the model's
+ * precision for `iters` iterations on the model itself (so the model advances
+ * like warm-up iterations), keeps the fastest and writes its index and the
+ * per-variant milliseconds per iteration to best / ms (-1 for shapes not offered;
+ * ms may be NULL, else it needs fi_fused_variant_count() slots).  No counterpart
+ * in the reference (its launch shape is fixed by Chmy's Launcher). */
 int fi_fused_variant_count(void);
 const char *fi_fused_variant_name(int32_t variant);
 fi_status fi_model_set_variant(fi_model *m, int32_t variant);
@@ -261,13 +267,16 @@ typedef struct {
  * state in `state` (problem described by `desc`; desc->path and device are
  * ignored, the current device is used) into the caller's device buffer out_dev,
  * asynchronously on `stream` (a cudaStream_t, NULL for the default stream).
- * Per-block partial sums live in a static device array of 32768 slots (3 MiB,
- * held by every device that loads the library until the process exits); a grid
- * with more than 32768 * 4096 vertex-range indices ((n0+1)(n1+1)(n2+1), i.e.
- * more than 511^3 cells) is rejected with FI_ERR_ARG.  The first call on a
- * device looks up that array's device address (cudaGetSymbolAddress); make that
- * first call before any stream capture.  All calls on a device share the array:
- * calls that overlap on the GPU race and must be serialised by the caller. */
+ * Per-block partial sums live in a static device array of 2048 slots (192 KiB,
+ * held by every device that loads the library until the process exits); the
+ * reduction is a grid-stride loop over at most 148 * 8 blocks, the model's own
+ * block count, so any grid fits and the norms equal fi_model_residual_norms' bit
+ * for bit (a launch needing more slots would be rejected with FI_ERR_ARG).  The
+ * first call on a device looks up that array's device address
+ * (cudaGetSymbolAddress) and caches it for the process; make that first call
+ * before any stream capture, and do not call it on a device after
+ * cudaDeviceReset.  All calls on a device share the array: calls that overlap
+ * on the GPU race and must be serialised by the caller. */
 fi_status fi_residual_norms_noalloc(const fi_model_desc *desc, const fi_state_view *state, double *out_dev,
                                     void *stream);
 
@@ -366,6 +375,15 @@ typedef enum { FI_HALO_ITERATION = 0, FI_HALO_STATE = 1 } fi_halo_what;
 fi_status fi_model_halo_bytes(const fi_model *m, int32_t dim, int32_t side, int32_t what, size_t *bytes);
 fi_status fi_model_halo_pack(fi_model *m, int32_t dim, int32_t side, int32_t what, void *dst_dev);
 fi_status fi_model_halo_unpack(fi_model *m, int32_t dim, int32_t side, int32_t what, const void *src_dev);
+/* The layer plan of those messages, host only (no device, no model): for an
+ * nd-dimensional slab of n cells, the (field, layer index along dim) pairs of the
+ * message packed toward `side` (pack != 0) or unpacked from it, in message order;
+ * each pair is one whole storage plane of the other dimensions.  *count gets the
+ * plan's length (pass cap = 0 to query it).  The layer rules of Chmy.Distributed's
+ * exchange for the fields the reference exchanges; no counterpart of its own in
+ * the reference (its halo layout is implicit in Chmy). */
+fi_status fi_halo_plan(int32_t nd, const int32_t *n, int32_t dim, int32_t side, int32_t what, int32_t pack,
+                       int32_t *fields, int32_t *layer_index, int32_t cap, int32_t *count);
 
 /* ---- heat diffusion (src/Models/Diffusion/Heat/) -------------------------------
  * HeatDiffusionModel(; grid, boundary_conditions, physics, iter_params) and

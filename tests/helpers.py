@@ -65,7 +65,7 @@ class Pair:
     """Library model + oracle model for the same problem and initial state."""
 
     def __init__(self, n, bcs, rheo=None, gravity=(0.3, -0.2, 1.0), dtype="f64", path="auto", seed=0,
-                 extent=None, origin=None, library="fast", random_state=True, immersed_psi=None):
+                 extent=None, origin=None, library="fast", random_state=True, immersed_psi=None, pt=None):
         fi = load_fastice()
         O = load_oracle()
         nd = len(n)
@@ -74,7 +74,7 @@ class Pair:
         extent = extent or tuple(1.0 + 0.25 * d for d in range(nd))
         origin = origin or tuple(-0.1 * d for d in range(nd))
         grid = fi.UniformGrid(origin=origin, extent=extent, dims=n)
-        sp = fi.pt_params(grid)
+        sp = fi.pt_params(grid) if pt is None else fi.pt_params(grid, r=pt[0], re_mech=pt[1], vdtau_factor=pt[2])
         dt = sp["Δτ"]
         g = {nm: float(gravity[d]) for d, nm in enumerate(("x", "y", "z")[:nd])}
         cls = fi.IsothermalImmersedBoundaryFullStokesModel if immersed_psi is not None else fi.IsothermalFullStokesModel

@@ -54,6 +54,18 @@ class LineSlab:
         out.append((self.v, ((1, 2) if side == 0 else (n,)) if pack else ((0,) if side == 0 else (n + 1, n + 2))))
         return out
 
+    def residual_norms(self):
+        """A norm vector in the library's layout from the slab's own cells and nodes:
+        ∞-norms of c (slot 0) and v (slot 1), L2 of c (slot 4), max|v| (slot 8), flag."""
+        n = self.n
+        c, v = self.c[1:n + 1], self.v[1:n + 2]
+        out = np.zeros(12)
+        out[0], out[1] = np.max(np.abs(c)), np.max(np.abs(v))
+        out[4] = np.sqrt(np.sum(c * c))
+        out[8] = np.max(np.abs(v))
+        out[11] = 0.0 if np.isfinite(c).all() and np.isfinite(v).all() else 1.0
+        return out
+
     def halo_bytes(self, dim, side, what="iteration"):
         return 8 * sum(len(ix) for _, ix in self._layers(side, True, what))
 
@@ -70,10 +82,10 @@ class LineSlab:
                 q += 1
 
 
-def _globals(R):
+def _globals(R, scale=0.5):
     rng = np.random.default_rng(3)
     n = N_LOCAL * R
-    return 0.5 * rng.standard_normal(n), 0.5 * rng.standard_normal(n + 1)
+    return scale * rng.standard_normal(n), scale * rng.standard_normal(n + 1)
 
 
 def _rank(rank, R, port, out):
@@ -121,3 +133,181 @@ def test_gloo_ranks_reproduce_the_undivided_line(R):
     for r in range(R):
         np.testing.assert_array_equal(got[r][0], whole.c[1 + r * n:1 + (r + 1) * n])
         np.testing.assert_array_equal(got[r][1], whole.v[1 + r * n:2 + (r + 1) * n])
+
+
+# ---- the distributed driver loop: reduced norms, the same decision on every rank
+NCHECK = 3
+SOLVE_SCALE = 0.05  # small enough that the line's quadratic term keeps the 24 iterations finite
+
+
+class _Single:
+    size = 1
+
+
+def _whole_measures(R, checks):
+    load_fastice()
+    from fastice_b200 import distributed as D
+    c, v = _globals(R, SOLVE_SCALE)
+    whole = LineSlab(c, v)
+    out = []
+    for _ in range(checks):
+        whole.advance(NCHECK)
+        out.append(D.measure_of(whole.residual_norms(), "abs_inf"))
+    return out
+
+
+def _solve_rank(rank, R, port, tol, out):
+    import torch.distributed as dist
+    load_fastice()
+    from fastice_b200 import distributed as D
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=R)
+    try:
+        c, v = _globals(R, SOLVE_SCALE)
+        s = LineSlab(D.slab_of(c, 0, rank, R, False), D.slab_of(v, 0, rank, R, True))
+        slab = D.Slab(s, 0, D.TorchTransport(), alloc=lambda nb: torch.empty(nb, dtype=torch.uint8))
+        slab.exchange("state")
+        rep = slab.solve(max_iter=8 * NCHECK, ncheck=NCHECK, tol=tol, measure="abs_inf")
+        out.put((rank, rep["iterations"], rep["measure"], rep["converged"], rep["norms"]))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("R", [2, 3])
+def test_gloo_ranks_take_the_undivided_convergence_decision(R):
+    load_fastice()
+    from fastice_b200 import distributed as D
+    meas = _whole_measures(R, 8)
+    # converge at the first check whose measure is below the third check's (inclusive)
+    tol = meas[2] * (1 + 1e-12)
+    k = next(q for q, m in enumerate(meas) if m < tol)
+    # the same loop on the undivided line (one rank, no exchange) decides at check k
+    c, v = _globals(R, SOLVE_SCALE)
+    whole = D.Slab(LineSlab(c, v), 0, _Single(), alloc=lambda nb: torch.empty(nb, dtype=torch.uint8))
+    ref = whole.solve(max_iter=8 * NCHECK, ncheck=NCHECK, tol=tol, measure="abs_inf")
+    assert ref["converged"] and ref["iterations"] == (k + 1) * NCHECK
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_solve_rank, args=(r, R, port, tol, out)) for r in range(R)]
+    for p in procs:
+        p.start()
+    got = [out.get(timeout=120) for _ in range(R)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, its, m, conv, norms in got:
+        assert conv and its == ref["iterations"], (rank, its, ref)
+        assert m == ref["measure"]
+        # ∞-norms and max|V| reduce by maximum: equal to the undivided line's
+        np.testing.assert_array_equal(np.asarray(norms)[[0, 1, 8, 11]], np.asarray(ref["norms"])[[0, 1, 8, 11]])
+        # the L2 norm of the cells (no shared cells) is the root of the summed squares
+        np.testing.assert_allclose(norms[4], ref["norms"][4], rtol=1e-14)
+
+
+def test_combine_norms_slots():
+    load_fastice()
+    from fastice_b200 import distributed as D
+    a = np.arange(12, dtype=float)
+    b = a[::-1].copy()
+    c = D.combine_norms([a, b])
+    for q in (0, 1, 2, 3, 8, 9, 10, 11):
+        assert c[q] == max(a[q], b[q])
+    for q in (4, 5, 6, 7):
+        assert c[q] == pytest.approx(np.hypot(a[q], b[q]))
+
+
+# ---- the library's own halo layer plan (fi_halo_plan) over gloo ranks
+SHAPE_LOCAL = (6, 5, 4)
+
+
+def _field_global(name, dim, R, seed):
+    """Values of a periodic field: unique positions 1..N along dim (N = R * n),
+    every storage position (ghosts included) along the other dims."""
+    rng = np.random.default_rng(seed)
+    nl = list(SHAPE_LOCAL)
+    e = [x + 3 for x in nl]
+    e[dim] = nl[dim] * R
+    return rng.standard_normal(tuple(reversed(e)))  # numpy order (z, y, x)
+
+
+def _local_index(r, n, N, i):
+    return (r * n + i - 1) % N  # position index (0-based) in the global periodic array
+
+
+def _layer(a, dim, i):
+    return a[:, :, i] if dim == 0 else a[:, i, :]
+
+
+def _plan_rank(rank, R, dim, what, port, out):
+    import torch.distributed as dist
+    fi = load_fastice()
+    from fastice_b200 import distributed as D
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=R)
+    try:
+        n = SHAPE_LOCAL[dim]
+        N = n * R
+        plans = {(side, pk): D.halo_plan(3, SHAPE_LOCAL, dim, side, what, pack=pk) for side in (0, 1)
+                 for pk in (True, False)}
+        names = sorted({f for pl in plans.values() for f, _ in pl})
+        local = {}
+        for k, name in enumerate(names):
+            g = _field_global(name, dim, R, 100 + k)
+            vert = fi._lib.FIELD_LOC[name][dim] == 1
+            shape = list(reversed([x + 3 for x in SHAPE_LOCAL]))
+            a = np.full(shape, np.nan)
+            for i in range(1, n + (2 if vert else 1)):
+                _layer(a, dim, i)[...] = np.take(g, _local_index(rank, n, N, i), axis=2 - dim)
+            local[name] = a
+
+        class Host:
+            halo_takes_tensors = True
+
+            def halo_bytes(self, d, side, what_):
+                return 8 * len(plans[(side, True)]) * _layer(local[names[0]], d, 0).size
+
+            def halo_pack(self, d, side, buf, what_):
+                vals = np.concatenate([_layer(local[f], d, i).ravel() for f, i in plans[(side, True)]])
+                buf.view(torch.float64)[:] = torch.from_numpy(vals)
+
+            def halo_unpack(self, d, side, buf, what_):
+                vals = buf.view(torch.float64).numpy()
+                q = 0
+                for f, i in plans[(side, False)]:
+                    L = _layer(local[f], d, i)
+                    L[...] = vals[q:q + L.size].reshape(L.shape)
+                    q += L.size
+
+        slab = D.Slab(Host(), dim, D.TorchTransport(), alloc=lambda nb: torch.empty(nb, dtype=torch.uint8))
+        slab.exchange(what)
+        bad = []
+        for k, name in enumerate(names):
+            g = _field_global(name, dim, R, 100 + k)
+            vert = fi._lib.FIELD_LOC[name][dim] == 1
+            for i in range(0, n + (3 if vert else 2)):
+                want = np.take(g, _local_index(rank, n, N, i), axis=2 - dim)
+                if not np.array_equal(_layer(local[name], dim, i), want):
+                    bad.append((name, i))
+        out.put((rank, bad, names))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("R,dim,what", [(2, 0, "iteration"), (3, 0, "state"), (3, 1, "iteration"), (2, 1, "state")])
+def test_gloo_ranks_fill_ghost_layers_by_the_library_plan(R, dim, what):
+    # every slab's ghost layers (and node n+1, which the high neighbour owns) must
+    # hold the periodic domain's values after one exchange by the library's plan
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_plan_rank, args=(r, R, dim, what, port, out)) for r in range(R)]
+    for p in procs:
+        p.start()
+    got = [out.get(timeout=120) for _ in range(R)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, bad, names in got:
+        assert not bad, (rank, bad)
+        assert ("P" in names) == (what == "state") and "Vx" in names and "eta" in names

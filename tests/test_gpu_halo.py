@@ -80,6 +80,57 @@ def test_split_run_matches_undivided(dim, ranks):
     assert not bad, bad
 
 
+def test_split_solve_matches_undivided_solve():
+    # the driver loop over a split domain (ranks emulated on one device): the same
+    # checks, the norms reduced over the slabs, the same decision -- the iteration
+    # count and the measure equal the undivided model's own solve (fi_model_solve),
+    # and the final state equals it bit for bit (no-FMA build)
+    fi = load_fastice()
+    from fastice_b200 import distributed as D
+    dim, ranks = 0, 2
+    nl = [16, 12, 10]
+    ng = list(nl)
+    ng[dim] *= ranks
+    ext = [1.0, 0.75, 0.25]
+    ext_l = list(ext)
+    ext_l[dim] /= ranks
+    noslip = ("velocity", (0.0, 0.0, 0.0))
+    bcs = ((PER, PER), (PER, PER), (noslip, TRAC))
+
+    def model(n, e, sp=None):
+        grid = fi.UniformGrid(origin=(0.0, 0.0, 0.0), extent=e, dims=n)
+        return fi.IsothermalFullStokesModel(grid=grid, boundary_conditions=make_bcs(fi, bcs, 3),
+                                            gravity={"x": -0.17, "y": 0.0, "z": 0.98},
+                                            rheology=fi.LinearViscousRheology(1.0),
+                                            solver_params=sp or fi.pt_params(grid), dtype="f64", library="strict",
+                                            path="fused")
+    whole = model(tuple(ng), tuple(ext))
+    sp = fi.pt_params(whole.grid)
+    slabs = [model(tuple(nl), tuple(ext_l), sp) for _ in range(ranks)]
+    for m in slabs + [whole]:
+        m.set_field("eta", 1.0)
+        m.set_field("eta_next", 1.0)
+        m.apply_bcs()
+    D.exchange_local(slabs, dim, "state")
+    kw = dict(max_iter=20000, ncheck=100, tol=1e-9, measure="rel_slab", rho_g_inf=1.0, length_z=0.25)
+    ref = whole.solve(**kw)
+    rep = D.solve_local(slabs, dim, **kw)
+    assert ref["converged"] and rep["converged"], (ref, rep)
+    assert rep["iterations"] == ref["iterations"]
+    assert rep["measure"] == ref["measure"]
+    bad = []
+    for name in STATE:
+        g = whole.get_field(name)
+        loc = fi._lib.FIELD_LOC[name]
+        for r, s in enumerate(slabs):
+            a, b = s.get_field(name), np.ascontiguousarray(D.slab_of(g, dim, r, ranks, loc[dim] == 1))
+            if not np.array_equal(_bits(a), _bits(b)):
+                bad.append((name, r, int(np.sum(a != b))))
+    for m in slabs + [whole]:
+        m.close()
+    assert not bad, bad
+
+
 def test_halo_needs_a_periodic_split_dimension_and_the_fused_sweep():
     fi = load_fastice()
     m = _model(fi, (16, 12, 10), (1.0, 1.0, 0.3), ((SLIP, SLIP), (PER, PER), (SLIP, TRAC)), "auto")

@@ -4,6 +4,7 @@ the pure-shear inclusion instances of the batched and serving workloads and the
 import math
 
 import numpy as np
+import pytest
 
 from conftest import load_fastice
 
@@ -82,3 +83,20 @@ def test_bed_height_is_a_sum_of_gaussian_bumps():
     one_b = {k: v[1:] for k, v in two.items()}
     np.testing.assert_allclose(s.bed_height(two, X, Y), s.bed_height(one_a, X, Y) + s.bed_height(one_b, X, Y),
                                rtol=1e-15)
+
+
+def test_eta_rel_is_ignored_unless_asked_for():
+    # drivers pass η_rel in solver_params; the reference's kernels never read it
+    fi = load_fastice()
+    from fastice_b200 import models
+    g = fi.UniformGrid(origin=(0.0, 0.0), extent=(1.0, 1.0), dims=(8, 8))
+    sp = fi.pt_params(g, eta_rel=0.1)
+    assert sp["η_rel"] == 0.1
+    glen = fi.glen_regularised()
+    assert models.effective_rheology(glen, sp) is glen
+    r = models.effective_rheology(glen, sp, "log")
+    assert isinstance(r, fi.Relaxation) and r.rate == 0.1 and r.scale == "log" and r.target is glen
+    assert models.effective_rheology(glen, sp, "lin").scale is None
+    assert models.effective_rheology(glen, fi.pt_params(g), "log") is glen  # no rate given: nothing to honour
+    with pytest.raises(ValueError):
+        models.effective_rheology(fi.Relaxation(glen, 0.2), sp, "log")

@@ -23,8 +23,12 @@ PER = ("periodic", ())
 STATE = ("P", "txx", "tyy", "tzz", "txy", "txz", "tyz", "Vx", "Vy", "Vz")
 
 
+MASKS = ("ccc", "vvv", "vcc", "cvc", "ccv", "vvc", "vcv", "cvv")
+
+
 def state_view(fi, model):
-    """fi_state_view of the model's current device state."""
+    """fi_state_view of the model's current device state (gravity fields and
+    immersed-boundary masks included where the model has them)."""
     L = fi._lib
     v = L.fi_state_view()
     nd = model.grid.ndims
@@ -35,6 +39,10 @@ def state_view(fi, model):
     for c, name in enumerate(("gx", "gy", "gz")[:nd]):
         if model._desc.gravity.kind[c] == L.FI_G_FIELD:
             v.g[c] = model.device_ptr(name)
+    if model._desc.immersed:
+        for c, comp in enumerate(MASKS):
+            v.na[c] = model.device_ptr("na_" + comp)
+            v.ns[c] = model.device_ptr("ns_" + comp)
     v.pitch = model.layout()[0]
     return v
 
@@ -47,15 +55,44 @@ def noalloc_norms(fi, model, out_dev, stream):
 
 
 def compare(a, b):
-    # max-norms and max|V| are order independent; the L2 sums are added in a different block order
-    np.testing.assert_array_equal(a[[0, 1, 2, 3, 8, 9, 10, 11]], b[[0, 1, 2, 3, 8, 9, 10, 11]])
-    np.testing.assert_allclose(a[4:8], b[4:8], rtol=1e-12, atol=0.0)
+    # the same kernel over the same block count as the model's entry point: the
+    # same bits in every slot (the L2 sums are added in the same order)
+    np.testing.assert_array_equal(a, b)
+
+
+def _sphere_psi(n, dx, c, r):
+    """Signed distance to a sphere at the vertices, halo storage (numpy (z, y, x))."""
+    ax = [(np.arange(n[d] + 3) - 1) * dx[d] for d in range(3)]
+    Z, Y, X = np.meshgrid(ax[2], ax[1], ax[0], indexing="ij")
+    return np.sqrt((X - c[0]) ** 2 + (Y - c[1]) ** 2 + (Z - c[2]) ** 2) - r
+
+
+def _immersed_pair(seed):
+    n, ext = (24, 20, 22), (1.0, 0.8, 0.9)
+    dx = tuple(e / c for e, c in zip(ext, n))
+    psi_ns = -_sphere_psi(n, dx, (0.5, 0.4, -0.3), 0.75)
+    psi_na = _sphere_psi(n, dx, (0.5, 0.4, 0.45), 0.7)
+    bcs = ((TRAC, TRAC), (TRAC, TRAC), (TRAC, TRAC))
+    return Pair(n, bcs, seed=seed, path="reference", origin=(0.0, 0.0, 0.0), extent=ext,
+                immersed_psi={"na": psi_na, "ns": psi_ns})
+
+
+class _Gravity:
+    """The 3D manufactured solution: gravity given as fields (FI_G_FIELD)."""
+
+    def __init__(self, fi):
+        self.grid, self.model = fi.scenarios.mms3d_model(20)
+
+    def close(self):
+        self.model.close()
 
 
 CASES = [
     ("3d-fused-f64", (40, 17, 70), ((PER, PER), (PER, PER), (SLIP, TRAC)), "f64"),
     ("3d-fused-f32", (33, 20, 24), ((SLIP, SLIP), (SLIP, SLIP), (NOSL, TRAC)), "f32"),
     ("2d-f64", (45, 31), ((SLIP, SLIP), (NOSL, TRAC)), "f64"),
+    ("3d-immersed-f64", None, None, "f64"),
+    ("3d-gravity-field-f64", None, None, "f64"),
 ]
 
 
@@ -63,7 +100,12 @@ CASES = [
 @pytest.mark.parametrize("name,n,bcs,dtype", CASES, ids=[c[0] for c in CASES])
 def test_noalloc_matches_model_norms_twice(fi, name, n, bcs, dtype):
     import torch
-    p = Pair(n, bcs, dtype=dtype, seed=21)
+    if name == "3d-immersed-f64":
+        p = _immersed_pair(21)
+    elif name == "3d-gravity-field-f64":
+        p = _Gravity(fi)
+    else:
+        p = Pair(n, bcs, dtype=dtype, seed=21)
     m = p.model
     out = torch.empty(fi._lib.FI_NORMS_LEN, dtype=torch.float64, device="cuda")
     stream = torch.cuda.current_stream().cuda_stream
@@ -80,8 +122,8 @@ def test_noalloc_matches_model_norms_twice(fi, name, n, bcs, dtype):
     p.close()
 
 
-def test_noalloc_rejects_grids_beyond_its_scratch(fi):
-    # checked before any device work: runs without a GPU
+def test_noalloc_rejects_incomplete_views(fi):
+    # argument checks come before any device work: runs without a GPU
     L = fi._lib
     lib = fi.load_library()
     d = L.fi_model_desc()
@@ -91,9 +133,16 @@ def test_noalloc_rejects_grids_beyond_its_scratch(fi):
         d.grid.extent[k] = 1.0
     d.dtype = L.FI_F64
     v = L.fi_state_view()
-    for name in STATE:
-        setattr(v, name, 0x1000)  # never dereferenced: the size check comes first
+    for name in STATE[:-1]:
+        setattr(v, name, 0x1000)  # never dereferenced: Vz is missing
     v.pitch = 640
-    st = lib.fi_residual_norms_noalloc(C.byref(d), C.byref(v), C.c_void_p(0x2000), None)
-    assert st == L.FI_ERR_ARG
-    assert b"too large" in lib.fi_last_error()
+    assert lib.fi_residual_norms_noalloc(C.byref(d), C.byref(v), C.c_void_p(0x2000), None) == L.FI_ERR_ARG
+    assert b"missing state field" in lib.fi_last_error()
+    v.Vz = 0x1000
+    v.pitch = 500  # smaller than n0 + 3
+    assert lib.fi_residual_norms_noalloc(C.byref(d), C.byref(v), C.c_void_p(0x2000), None) == L.FI_ERR_ARG
+    assert b"pitch" in lib.fi_last_error()
+    v.pitch = 640
+    d.immersed = 1  # masks missing
+    assert lib.fi_residual_norms_noalloc(C.byref(d), C.byref(v), C.c_void_p(0x2000), None) == L.FI_ERR_ARG
+    assert b"mask" in lib.fi_last_error()
