@@ -175,6 +175,8 @@ SIGNATURES = [
     ("fi_model_halo_bytes", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_size_t)]),
     ("fi_model_halo_pack", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p]),
     ("fi_model_halo_unpack", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p]),
+    ("fi_model_advance_begin", C.c_int, [C.c_void_p, C.c_int32]),
+    ("fi_model_advance_end", C.c_int, [C.c_void_p]),
     ("fi_halo_plan", C.c_int, [C.c_int32, C.POINTER(C.c_int32), C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_int32, C.POINTER(C.c_int32)]),
 ]

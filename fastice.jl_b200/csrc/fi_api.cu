@@ -558,6 +558,54 @@ fi_status model_ensure_second_state(fi_model *m) {
     return FI_OK;
 }
 
+// An overlapped iteration (fi_model_advance_begin / _end) leaves its second half
+// on the model's second stream: every other entry point first orders the model's
+// stream after it, and refuses to run between the two halves.
+static fi_status join_overlap(fi_model *m) {
+    if (m->split_begun >= 0)
+        return set_error("an overlapped iteration is begun: call fi_model_advance_end first"), FI_ERR_STATE;
+    if (m->interior_pending) {
+        FI_CHECK_CUDA(cudaSetDevice(m->d.device), "cudaSetDevice");
+        FI_CHECK_CUDA(cudaStreamWaitEvent(m->stream, m->ev_int, 0), "join the second half");
+        m->interior_pending = false;
+    }
+    return FI_OK;
+}
+
+namespace {
+// the two halves of an overlapped fused iteration
+template <typename T>
+fi_status advance_half(fi_model *m, int dim, int part) {
+    if (part == 0) {
+        Ptrs<T> in = m->ptrs<T>(false);
+        Ptrs<T> out = m->ptrs<T>(true);
+        out.eta = in.eta;
+        out.eta_next = in.eta_next;
+        for (int f = 0; f < kState; f++) std::memcpy(m->pend_maps[f], m->parity ? m->map_alt[f] : m->map_base[f], 128);
+        std::memcpy(m->pend_maps[10], m->map_eta[m->eta_swapped ? 1 : 0], 128);
+        for (int f = 0; f < 7; f++)
+            std::memcpy(m->pend_maps[11 + f], m->parity ? m->tmap_alt[f] : m->tmap_base[f], 128);
+        static_assert(sizeof(Ptrs<T>) <= sizeof(m->pend_ptrs[0]), "pending pointers fit");
+        std::memcpy(m->pend_ptrs[0], &in, sizeof(in));
+        std::memcpy(m->pend_ptrs[1], &out, sizeof(out));
+        FI_CHECK_CUDA(launch_fused3d<T>(m->g, m->kp, in, out, m->pend_maps, m->fused_variant, m->d_err, m->stream, dim, 0),
+                      "fused sweep (split faces)");
+        FI_CHECK_CUDA(cudaEventRecord(m->ev_bnd, m->stream), "event");
+        m->parity ^= 1;
+        if (!m->kp.freeze_eta) m->eta_swapped = !m->eta_swapped;
+        return FI_OK;
+    }
+    Ptrs<T> in, out;
+    std::memcpy(&in, m->pend_ptrs[0], sizeof(in));
+    std::memcpy(&out, m->pend_ptrs[1], sizeof(out));
+    FI_CHECK_CUDA(cudaStreamWaitEvent(m->stream2, m->ev_bnd, 0), "wait first half");
+    FI_CHECK_CUDA(launch_fused3d<T>(m->g, m->kp, in, out, m->pend_maps, m->fused_variant, m->d_err, m->stream2, dim, 1),
+                  "fused sweep (interior)");
+    FI_CHECK_CUDA(cudaEventRecord(m->ev_int, m->stream2), "event");
+    return FI_OK;
+}
+}  // namespace
+
 extern "C" {
 
 const char *fi_last_error(void) { return g_last_error.c_str(); }
@@ -681,6 +729,7 @@ fi_status fi_model_destroy(fi_model *m) {
     if (!m) return FI_OK;
     cudaSetDevice(m->d.device);
     if (m->stream) cudaStreamSynchronize(m->stream);
+    if (m->stream2) cudaStreamSynchronize(m->stream2);
     for (int f = 0; f < FI_FIELD_COUNT; f++) field_free(m->base[f], m->esz);
     for (int f = 0; f < kState; f++) field_free(m->alt[f], m->esz);
     if (m->d_err) cudaFree(m->d_err);
@@ -695,6 +744,9 @@ fi_status fi_model_destroy(fi_model *m) {
     if (m->d_partials) cudaFree(m->d_partials);
     if (m->d_out) cudaFree(m->d_out);
     if (m->h_out) cudaFreeHost(m->h_out);
+    if (m->ev_bnd) cudaEventDestroy(m->ev_bnd);
+    if (m->ev_int) cudaEventDestroy(m->ev_int);
+    if (m->stream2) cudaStreamDestroy(m->stream2);
     if (m->stream) cudaStreamDestroy(m->stream);
     delete m;
     return FI_OK;
@@ -708,6 +760,7 @@ fi_status fi_model_field_size(const fi_model *m, int32_t field, size_t *count) {
 
 fi_status fi_model_set_field(fi_model *m, int32_t field, const void *host, size_t nbytes) {
     if (!m || !host || field < 0 || field >= FI_FIELD_COUNT) return set_error("bad argument"), FI_ERR_ARG;
+    if (fi_status js = join_overlap(m); js != FI_OK) return js;
     if (!field_used(m, field)) return set_error("field not used by this model"), FI_ERR_ARG;
     if (nbytes != interior_count(m, field) * m->esz) return set_error("byte count does not match the field's interior"), FI_ERR_ARG;
     FI_CHECK_CUDA(cudaSetDevice(m->d.device), "cudaSetDevice");
@@ -725,6 +778,7 @@ fi_status fi_model_set_field(fi_model *m, int32_t field, const void *host, size_
 
 fi_status fi_model_get_field(fi_model *m, int32_t field, void *host, size_t nbytes) {
     if (!m || !host || field < 0 || field >= FI_FIELD_COUNT) return set_error("bad argument"), FI_ERR_ARG;
+    if (fi_status js = join_overlap(m); js != FI_OK) return js;
     if (!field_used(m, field)) return set_error("field not used by this model"), FI_ERR_ARG;
     if (nbytes != interior_count(m, field) * m->esz) return set_error("byte count does not match the field's interior"), FI_ERR_ARG;
     if (is_residual(field) && !m->base[field]) return set_error("residuals not computed yet"), FI_ERR_STATE;
@@ -738,6 +792,7 @@ fi_status fi_model_get_field(fi_model *m, int32_t field, void *host, size_t nbyt
 fi_status fi_model_copy_field(fi_model *m, int32_t dst, int32_t src) {
     if (!m || dst < 0 || dst >= FI_FIELD_COUNT || src < 0 || src >= FI_FIELD_COUNT || dst == src)
         return set_error("bad argument"), FI_ERR_ARG;
+    if (fi_status js = join_overlap(m); js != FI_OK) return js;
     if (!field_used(m, dst) || !field_used(m, src)) return set_error("field not used by this model"), FI_ERR_ARG;
     if (is_residual(dst) || is_residual(src)) return set_error("residual fields are outputs"), FI_ERR_ARG;
     int ld[3], ls[3];
@@ -757,6 +812,7 @@ fi_status fi_model_copy_field(fi_model *m, int32_t dst, int32_t src) {
 
 fi_status fi_model_apply_bcs(fi_model *m) {
     if (!m) return set_error("null model"), FI_ERR_ARG;
+    if (fi_status js = join_overlap(m); js != FI_OK) return js;
     FI_CHECK_CUDA(cudaSetDevice(m->d.device), "cudaSetDevice");
     fi_status st = m->is_f64() ? apply_bcs_t<double>(m) : apply_bcs_t<float>(m);
     if (st != FI_OK) return st;
@@ -766,24 +822,59 @@ fi_status fi_model_apply_bcs(fi_model *m) {
 
 fi_status fi_model_advance(fi_model *m, int32_t niter) {
     if (!m || niter < 0) return set_error("bad argument"), FI_ERR_ARG;
+    if (fi_status js = join_overlap(m); js != FI_OK) return js;
     FI_CHECK_CUDA(cudaSetDevice(m->d.device), "cudaSetDevice");
     return m->is_f64() ? advance_t<double>(m, niter) : advance_t<float>(m, niter);
 }
 
+fi_status fi_model_advance_begin(fi_model *m, int32_t dim) {
+    if (!m || (dim != 0 && dim != 1)) return set_error("bad argument"), FI_ERR_ARG;
+    if (fi_status js = join_overlap(m); js != FI_OK) return js;
+    if (m->path != FI_PATH_FUSED) return set_error("an overlapped iteration needs the fused sweep"), FI_ERR_UNSUPPORTED;
+    if (dim >= m->d.grid.nd || m->d.bc[dim][0].kind != FI_BC_PERIODIC)
+        return set_error("the split dimension must be declared periodic on the subdomain model"), FI_ERR_STATE;
+    FI_CHECK_CUDA(cudaSetDevice(m->d.device), "cudaSetDevice");
+    if (!m->stream2) {
+        FI_CHECK_CUDA(cudaStreamCreateWithFlags(&m->stream2, cudaStreamNonBlocking), "second stream");
+        FI_CHECK_CUDA(cudaEventCreateWithFlags(&m->ev_bnd, cudaEventDisableTiming), "event");
+        FI_CHECK_CUDA(cudaEventCreateWithFlags(&m->ev_int, cudaEventDisableTiming), "event");
+    }
+    m->full_iters = 0;
+    fi_status st = m->is_f64() ? advance_half<double>(m, dim, 0) : advance_half<float>(m, dim, 0);
+    if (st == FI_OK) m->split_begun = dim;
+    return st;
+}
+
+fi_status fi_model_advance_end(fi_model *m) {
+    if (!m) return set_error("null model"), FI_ERR_ARG;
+    if (m->split_begun < 0) return set_error("no overlapped iteration is begun"), FI_ERR_STATE;
+    FI_CHECK_CUDA(cudaSetDevice(m->d.device), "cudaSetDevice");
+    const int dim = m->split_begun;
+    fi_status st = m->is_f64() ? advance_half<double>(m, dim, 1) : advance_half<float>(m, dim, 1);
+    if (st != FI_OK) return st;
+    m->split_begun = -1;
+    m->interior_pending = true;
+    m->iterations++;
+    return FI_OK;
+}
+
 fi_status fi_model_compute_residuals(fi_model *m) {
     if (!m) return set_error("null model"), FI_ERR_ARG;
+    if (fi_status js = join_overlap(m); js != FI_OK) return js;
     FI_CHECK_CUDA(cudaSetDevice(m->d.device), "cudaSetDevice");
     return m->is_f64() ? residuals_t<double>(m) : residuals_t<float>(m);
 }
 
 fi_status fi_model_residual_norms(fi_model *m, double *out) {
     if (!m || !out) return set_error("bad argument"), FI_ERR_ARG;
+    if (fi_status js = join_overlap(m); js != FI_OK) return js;
     FI_CHECK_CUDA(cudaSetDevice(m->d.device), "cudaSetDevice");
     return m->is_f64() ? norms_t<double>(m, out) : norms_t<float>(m, out);
 }
 
 fi_status fi_model_compute_tau(fi_model *m) {
     if (!m) return set_error("null model"), FI_ERR_ARG;
+    if (fi_status js = join_overlap(m); js != FI_OK) return js;
     if (m->ib) return set_error("compute_tau of the immersed-boundary model is broken in the reference"), FI_ERR_UNSUPPORTED;
     FI_CHECK_CUDA(cudaSetDevice(m->d.device), "cudaSetDevice");
     cudaError_t e = m->is_f64() ? launch_compute_tau<double>(m->g, m->kp, m->ptrs<double>(), false, m->stream)
@@ -794,6 +885,7 @@ fi_status fi_model_compute_tau(fi_model *m) {
 
 fi_status fi_model_device_ptr(fi_model *m, int32_t field, void **dptr) {
     if (!m || !dptr || field < 0 || field >= FI_FIELD_COUNT) return set_error("bad argument"), FI_ERR_ARG;
+    if (fi_status js = join_overlap(m); js != FI_OK) return js;
     if (is_residual(field)) {
         fi_status st = ensure_residual_arrays(m);
         if (st != FI_OK) return st;
@@ -823,6 +915,7 @@ fi_status fi_model_stream(const fi_model *m, void **stream) {
 
 fi_status fi_model_synchronize(fi_model *m) {
     if (!m) return set_error("null model"), FI_ERR_ARG;
+    if (fi_status js = join_overlap(m); js != FI_OK) return js;
     FI_CHECK_CUDA(cudaStreamSynchronize(m->stream), "synchronize");
     return check_err_word(m);
 }
@@ -1137,6 +1230,7 @@ extern "C" {
 
 fi_status fi_model_solve(fi_model *m, const fi_solve_opts *o, fi_solve_report *rep) {
     if (!m || !o || !rep) return set_error("bad argument"), FI_ERR_ARG;
+    if (fi_status js = join_overlap(m); js != FI_OK) return js;
     if (o->ncheck <= 0 || o->max_iter <= 0) return set_error("ncheck and max_iter must be positive"), FI_ERR_ARG;
     if (o->mode != FI_SOLVE_PLAIN && o->mode != FI_SOLVE_MIXED) return set_error("unknown solve mode"), FI_ERR_ARG;
     std::memset(rep, 0, sizeof(*rep));
@@ -1175,6 +1269,7 @@ fi_status fi_model_solve(fi_model *m, const fi_solve_opts *o, fi_solve_report *r
 
 fi_status fi_model_volfrac_from_levelset(fi_model *m, int32_t group, const double *psi_host) {
     if (!m || !psi_host || (group != 0 && group != 1)) return set_error("bad argument"), FI_ERR_ARG;
+    if (fi_status js = join_overlap(m); js != FI_OK) return js;
     if (!m->ib) return set_error("volume fractions need an immersed-boundary model"), FI_ERR_STATE;
     FI_CHECK_CUDA(cudaSetDevice(m->d.device), "cudaSetDevice");
     const Geom &g = m->g;
@@ -1232,6 +1327,7 @@ const char *fi_fused_variant_name(int32_t variant) { return fused3d_variant_name
 
 fi_status fi_model_set_variant(fi_model *m, int32_t variant) {
     if (!m || variant < 0 || variant >= fused3d_num_variants()) return set_error("bad argument"), FI_ERR_ARG;
+    if (fi_status js = join_overlap(m); js != FI_OK) return js;
     if (m->path != FI_PATH_FUSED) return set_error("the model does not run the fused sweep"), FI_ERR_STATE;
     if (!fused3d_variant_fits(variant, (int)m->esz))
         return set_error("this launch shape does not fit a CTA in the model's precision"), FI_ERR_UNSUPPORTED;
@@ -1243,6 +1339,7 @@ fi_status fi_model_set_variant(fi_model *m, int32_t variant) {
 
 fi_status fi_model_autotune(fi_model *m, int32_t iters, int32_t *best, double *ms) {
     if (!m || iters <= 0) return set_error("bad argument"), FI_ERR_ARG;
+    if (fi_status js = join_overlap(m); js != FI_OK) return js;
     if (m->path != FI_PATH_FUSED) return set_error("the model does not run the fused sweep"), FI_ERR_STATE;
     FI_CHECK_CUDA(cudaSetDevice(m->d.device), "cudaSetDevice");
     cudaEvent_t e0, e1;

@@ -755,12 +755,30 @@ __device__ __forceinline__ void sweep(Ctx<T, TX, TY, TRIM> &c, const KParams &p,
     for (int b = 0; b < kBars; b++) mbar_wait(&bars[b], (phase >> b) & 1u);
 }
 
+// Tiles of one launch along a split dimension: a launch runs either every tile, or
+// part of them (the overlapped halo exchange runs the tiles next to the split faces
+// first and the others while the halo moves).  Along `dim`, grid block b stands for
+// tile b + base + (b >= nlow ? shift : 0).
+struct TileMap {
+    int dim;  // 0: x, 1: y, -1: every tile
+    int base, nlow, shift;
+};
+
+__device__ __forceinline__ int tile_x(const TileMap &tm) {
+    const int b = (int)blockIdx.x;
+    return tm.dim == 0 ? b + tm.base + (b >= tm.nlow ? tm.shift : 0) : b;
+}
+__device__ __forceinline__ int tile_y(const TileMap &tm) {
+    const int b = (int)blockIdx.y;
+    return tm.dim == 1 ? b + tm.base + (b >= tm.nlow ? tm.shift : 0) : b;
+}
+
 template <typename T, int TX, int TY, bool TRIM>
 __device__ __forceinline__ void init_ctx(Ctx<T, TX, TY, TRIM> &c, const Geom &g, const KParams &p, unsigned char *smem,
-                                         int zb) {
+                                         int zb, const TileMap &tm) {
     c.sm = reinterpret_cast<T *>(smem);
-    c.i0 = 1 + blockIdx.x * TX;
-    c.j0 = 1 + blockIdx.y * TY;
+    c.i0 = 1 + tile_x(tm) * TX;
+    c.j0 = 1 + tile_y(tm) * TY;
     c.kb = 1 + blockIdx.z * zb;
     c.n0 = g.n[0];
     c.n1 = g.n[1];
@@ -777,11 +795,11 @@ __device__ __forceinline__ void init_ctx(Ctx<T, TX, TY, TRIM> &c, const Geom &g,
 template <typename T, int TX, int TY>
 __global__ void __launch_bounds__(Layout<T, TX, TY>::NT, Layout<T, TX, TY>::MINB)
     fused3d_kernel(Geom g, KParams p, TConst<T> q, Ptrs<T> in, Ptrs<T> out, const __grid_constant__ InMaps maps, int zb,
-                   int trim, int *err) {
+                   int trim, TileMap tm, int *err) {
     using Lay = Layout<T, TX, TY>;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     // the grid is padded to whole clusters: columns past the vertex range have no work
-    if (1 + (int)blockIdx.x * TX > g.n[0] + 1 || 1 + (int)blockIdx.y * TY > g.n[1] + 1) return;
+    if (1 + tile_x(tm) * TX > g.n[0] + 1 || 1 + tile_y(tm) * TY > g.n[1] + 1) return;
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + (size_t)S_COUNT * Lay::SLOT * sizeof(T));
     if (threadIdx.x == 0) {
         for (int b = 0; b < kBars; b++) mbar_init(&bars[b], 1);
@@ -789,10 +807,10 @@ __global__ void __launch_bounds__(Layout<T, TX, TY>::NT, Layout<T, TX, TY>::MINB
     }
     __syncthreads();
     Ctx<T, TX, TY, false> c;
-    init_ctx(c, g, p, smem_raw, zb);
+    init_ctx(c, g, p, smem_raw, zb, tm);
     if (trim && !c.bnd_x && !c.bnd_y) {
         Ctx<T, TX, TY, true> ct;
-        init_ctx(ct, g, p, smem_raw, zb);
+        init_ctx(ct, g, p, smem_raw, zb, tm);
         sweep(ct, p, q, in, out, maps, bars, err);
     } else {
         sweep(c, p, q, in, out, maps, bars, err);
@@ -801,7 +819,7 @@ __global__ void __launch_bounds__(Layout<T, TX, TY>::NT, Layout<T, TX, TY>::MINB
 
 template <typename T, int TX, int TY>
 cudaError_t launch_variant(const Geom &g, const KParams &p, const Ptrs<T> &in, const Ptrs<T> &out, const InMaps &maps,
-                           const Variant &v, int *err, cudaStream_t s) {
+                           Variant v, int *err, cudaStream_t s, int part_dim, int part) {
     using Lay = Layout<T, TX, TY>;
     int dev = 0;
     cudaGetDevice(&dev);
@@ -813,7 +831,29 @@ cudaError_t launch_variant(const Geom &g, const KParams &p, const Ptrs<T> &in, c
         attr_set[dev] = true;
     }
     auto up = [](int a, int b) { return (a + b - 1) / b * b; };
-    dim3 grd(up((g.n[0] + 1 + TX - 1) / TX, v.cx), up((g.n[1] + 1 + TY - 1) / TY, v.cy), (g.n[2] + 1 + v.zb - 1) / v.zb);
+    TileMap tm{-1, 0, 1 << 30, 0};
+    const int nbx = (g.n[0] + 1 + TX - 1) / TX, nby = (g.n[1] + 1 + TY - 1) / TY;
+    int gx = nbx, gy = nby;
+    if (part_dim == 0 || part_dim == 1) {
+        // part 0: the tiles of the split faces -- tile 0 (positions 1 and 2) and the
+        // tile of position n: the layers a slab sends and the ghost images it
+        // writes; part 1: every other tile.  No clusters in partial launches.
+        const int T_d = part_dim == 0 ? TX : TY, nb = part_dim == 0 ? nbx : nby;
+        const int last = (g.n[part_dim] - 1) / T_d;
+        int cnt;
+        if (part == 0) {
+            tm = {part_dim, 0, 1, last - 1};
+            cnt = last > 0 ? 2 : 1;
+        } else {
+            // tiles 1 .. last-1, then last+1 .. nb-1
+            tm = last > 0 ? TileMap{part_dim, 1, last - 1, 1} : TileMap{part_dim, 1, 1 << 30, 0};
+            cnt = nb - (last > 0 ? 2 : 1);
+            if (cnt <= 0) return cudaSuccess;
+        }
+        (part_dim == 0 ? gx : gy) = cnt;
+        v.cx = v.cy = 1;
+    }
+    dim3 grd(up(gx, v.cx), up(gy, v.cy), (g.n[2] + 1 + v.zb - 1) / v.zb);
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grd;
     cfg.blockDim = dim3(Lay::NT);
@@ -829,7 +869,7 @@ cudaError_t launch_variant(const Geom &g, const KParams &p, const Ptrs<T> &in, c
         cfg.numAttrs = 1;
     }
     const TConst<T> q = make_tconst<T>(p);
-    return cudaLaunchKernelEx(&cfg, fused3d_kernel<T, TX, TY>, g, p, q, in, out, maps, v.zb, v.trim, err);
+    return cudaLaunchKernelEx(&cfg, fused3d_kernel<T, TX, TY>, g, p, q, in, out, maps, v.zb, v.trim, tm, err);
 }
 
 template <typename T>
@@ -969,30 +1009,30 @@ bool fused3d_encode_map(void *raw_base, const Geom &g, int esz, int variant, int
 
 template <typename T>
 cudaError_t launch_fused3d(const Geom &g, const KParams &p, const Ptrs<T> &in, const Ptrs<T> &out, const void *maps18,
-                           int variant, int *err, cudaStream_t s) {
+                           int variant, int *err, cudaStream_t s, int part_dim, int part) {
     if (variant < 0 || variant >= kNumVariants) variant = 0;
     const Variant v = kVariants[variant];
     if (!fused3d_variant_fits(variant, (int)sizeof(T))) return cudaErrorInvalidConfiguration;
     const InMaps &mp = *reinterpret_cast<const InMaps *>(maps18);
     if (v.tx == 64) {
         if constexpr (sizeof(T) == 4) {
-            if (v.ty == 4) return launch_variant<T, 64, 4>(g, p, in, out, mp, v, err, s);
-            return launch_variant<T, 64, 8>(g, p, in, out, mp, v, err, s);
+            if (v.ty == 4) return launch_variant<T, 64, 4>(g, p, in, out, mp, v, err, s, part_dim, part);
+            return launch_variant<T, 64, 8>(g, p, in, out, mp, v, err, s, part_dim, part);
         }
         return cudaErrorInvalidConfiguration;
     }
     switch (v.ty) {
-        case 4: return launch_variant<T, 32, 4>(g, p, in, out, mp, v, err, s);
-        case 16: return launch_variant<T, 32, 16>(g, p, in, out, mp, v, err, s);
-        default: return launch_variant<T, 32, 8>(g, p, in, out, mp, v, err, s);
+        case 4: return launch_variant<T, 32, 4>(g, p, in, out, mp, v, err, s, part_dim, part);
+        case 16: return launch_variant<T, 32, 16>(g, p, in, out, mp, v, err, s, part_dim, part);
+        default: return launch_variant<T, 32, 8>(g, p, in, out, mp, v, err, s, part_dim, part);
     }
 }
 
 template bool fused3d_supported<double>(const Geom &, const KParams &, bool);
 template bool fused3d_supported<float>(const Geom &, const KParams &, bool);
 template cudaError_t launch_fused3d<double>(const Geom &, const KParams &, const Ptrs<double> &, const Ptrs<double> &,
-                                            const void *, int, int *, cudaStream_t);
+                                            const void *, int, int *, cudaStream_t, int, int);
 template cudaError_t launch_fused3d<float>(const Geom &, const KParams &, const Ptrs<float> &, const Ptrs<float> &,
-                                           const void *, int, int *, cudaStream_t);
+                                           const void *, int, int *, cudaStream_t, int, int);
 
 }  // namespace fi

@@ -170,9 +170,12 @@ bool fused3d_supported(const Geom &g, const KParams &p, bool ib);
 // maps18: the eleven full-box input tensor maps (P, txx, tyy, tzz, txy, txz, tyz, Vx,
 // Vy, Vz, eta) then the trimmed-box maps of the seven stresses, 128 bytes each,
 // encoded with fused3d_encode_map for the variant
+// part_dim -1: every tile; 0 / 1: the tiles of the split faces along x / y (part 0)
+// or every other tile (part 1) -- the two halves of an iteration whose halo
+// exchange overlaps the second half
 template <typename T>
 cudaError_t launch_fused3d(const Geom &g, const KParams &p, const Ptrs<T> &in, const Ptrs<T> &out, const void *maps18,
-                           int variant, int *err, cudaStream_t s);
+                           int variant, int *err, cudaStream_t s, int part_dim = -1, int part = 0);
 // field: index in the map order above (0..10); trimmed: the interior box of a stress
 bool fused3d_encode_map(void *raw_base, const Geom &g, int esz, int variant, int field, bool trimmed, void *map_out);
 // generic tiled tensor map (fi_fused3d.cu): nd dims, strides of dims 1..nd-1 in bytes

@@ -62,6 +62,15 @@ struct fi_model {
     alignas(64) unsigned char map_base[kState][128];
     alignas(64) unsigned char map_alt[kState][128];
     alignas(64) unsigned char map_eta[2][128];  // base[ETA], base[ETA_NEXT]
+    // overlapped iteration (fi_model_advance_begin / _end): the second half of an
+    // iteration (the tiles away from the split faces) runs on stream2 while the halo
+    // moves on `stream`; ev_int marks its end, ev_bnd the end of the first half
+    cudaStream_t stream2 = nullptr;
+    cudaEvent_t ev_bnd = nullptr, ev_int = nullptr;
+    bool interior_pending = false;  // stream2 work that `stream` has not waited for yet
+    int split_begun = -1;           // split dimension of a begun iteration awaiting its second half
+    alignas(64) unsigned char pend_maps[18][128];
+    unsigned char pend_ptrs[2][sizeof(fi::Ptrs<double>)];  // in / out of the begun iteration
     // trimmed-box maps of the seven stress fields (interior columns of trimmed launch shapes)
     alignas(64) unsigned char tmap_base[7][128];
     alignas(64) unsigned char tmap_alt[7][128];

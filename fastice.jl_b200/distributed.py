@@ -179,10 +179,17 @@ class Slab:
             for _ in steps:
                 pass
 
-    def advance(self, niter: int) -> None:
-        """niter PT iterations, each followed by the halo exchange of V and η."""
+    def advance(self, niter: int, overlap: bool = False) -> None:
+        """niter PT iterations, each followed by the halo exchange of V and η.  With
+        ``overlap`` (a library model) each iteration runs in two halves: the tiles of
+        the split faces, then the others on a second stream while the halo moves on
+        the model's stream (fi_model_advance_begin / _end)."""
         for _ in range(int(niter)):
-            self.model.advance(1)
+            if overlap and self.transport.size > 1:
+                self.model.advance_begin(self.dim)
+                self.model.advance_end()
+            else:
+                self.model.advance(1)
             self.exchange("iteration")
             self.iterations += 1
 
@@ -194,7 +201,7 @@ class Slab:
         return self.transport.allreduce_norms(local)
 
     def solve(self, *, max_iter: int, ncheck: int, tol: float, measure: str = "abs_inf", rho_g_inf: float = 1.0,
-              length_z: float = 1.0, nd: int = 3) -> dict:
+              length_z: float = 1.0, nd: int = 3, overlap: bool = False) -> dict:
         """The driver loop (tm_stokes_chmy.jl:283-305) over the split domain: ncheck
         iterations with their exchanges, then the reduced norms and the decision,
         which every rank takes alike; stops on convergence (measure < tol), on a
@@ -202,7 +209,7 @@ class Slab:
         it, rep = 0, {"converged": False, "diverged": False, "measure": float("nan"), "norms": None}
         while it < max_iter:
             k = min(ncheck, max_iter - it)
-            self.advance(k)
+            self.advance(k, overlap=overlap)
             it += k
             norms = self.residual_norms()
             meas = measure_of(norms, measure, nd, rho_g_inf, length_z)
@@ -215,6 +222,21 @@ class Slab:
                 break
         rep["iterations"] = it
         return rep
+
+
+def advance_local(slabs, dim: int, niter: int, overlap: bool = False) -> None:
+    """``Slab.advance`` for a ring of slabs held by one process (one device): every
+    slab's iteration (in two halves with ``overlap``), then ``exchange_local``."""
+    for _ in range(int(niter)):
+        for m in slabs:
+            if overlap:
+                m.advance_begin(dim)
+            else:
+                m.advance(1)
+        if overlap:
+            for m in slabs:
+                m.advance_end()
+        exchange_local(slabs, dim)
 
 
 def exchange_local(slabs, dim: int, what: str = "iteration") -> None:
@@ -260,7 +282,7 @@ def halo_plan(nd: int, n, dim: int, side: int, what: str = "iteration", pack: bo
 
 
 def solve_local(slabs, dim: int, *, max_iter: int, ncheck: int, tol: float, measure: str = "abs_inf",
-                rho_g_inf: float = 1.0, length_z: float = 1.0) -> dict:
+                rho_g_inf: float = 1.0, length_z: float = 1.0, overlap: bool = False) -> dict:
     """``Slab.solve`` for a ring of slabs held by one process (one device): the same
     iterations, exchanges (``exchange_local``), norm reduction (``combine_norms``)
     and decision as a multi-rank run."""
@@ -268,10 +290,7 @@ def solve_local(slabs, dim: int, *, max_iter: int, ncheck: int, tol: float, meas
     it, rep = 0, {"converged": False, "diverged": False, "measure": float("nan"), "norms": None}
     while it < max_iter:
         k = min(ncheck, max_iter - it)
-        for _ in range(k):
-            for m in slabs:
-                m.advance(1)
-            exchange_local(slabs, dim)
+        advance_local(slabs, dim, k, overlap=overlap)
         it += k
         norms = combine_norms([m.residual_norms() for m in slabs])
         meas = measure_of(norms, measure, nd, rho_g_inf, length_z)
@@ -301,4 +320,4 @@ def slab_of(global_interior, dim: int, rank: int, size: int, vertex: bool):
     return global_interior[tuple(sl)]
 
 
-__all__ = ["TorchTransport", "Slab", "exchange_local", "solve_local", "slab_of", "combine_norms", "measure_of", "halo_plan"]
+__all__ = ["TorchTransport", "Slab", "advance_local", "exchange_local", "solve_local", "slab_of", "combine_norms", "measure_of", "halo_plan"]

@@ -295,6 +295,13 @@ class _StokesBase:
         names = [self.lib.fi_fused_variant_name(v).decode() for v in range(nv)]
         return best.value, dict(zip(names, ms[:]))
 
+    # -- an iteration in two halves around the halo exchange (fi_model_advance_begin / _end)
+    def advance_begin(self, dim: int) -> None:
+        L.check(self.lib, self.lib.fi_model_advance_begin(self._h, int(dim)))
+
+    def advance_end(self) -> None:
+        L.check(self.lib, self.lib.fi_model_advance_end(self._h))
+
     # -- subdomain halo layers (fi_model_halo_*: a slab of a domain split along x or y)
     def halo_bytes(self, dim: int, side: int, what: str = "iteration") -> int:
         """Bytes of the halo message packed toward ``side`` (0 = low, 1 = high

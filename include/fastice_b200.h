@@ -375,6 +375,20 @@ typedef enum { FI_HALO_ITERATION = 0, FI_HALO_STATE = 1 } fi_halo_what;
 fi_status fi_model_halo_bytes(const fi_model *m, int32_t dim, int32_t side, int32_t what, size_t *bytes);
 fi_status fi_model_halo_pack(fi_model *m, int32_t dim, int32_t side, int32_t what, void *dst_dev);
 fi_status fi_model_halo_unpack(fi_model *m, int32_t dim, int32_t side, int32_t what, const void *src_dev);
+/* One PT iteration of a slab in two halves, so that its halo exchange overlaps
+ * the second (the reference hides the exchange behind the interior with
+ * outer_width, FullStokes/Isothermal/Isothermal.jl:72-76,101-107):
+ *   fi_model_advance_begin(m, dim): the tiles of the split faces (the layers the
+ *     slab sends and the ghost images it writes) on the model's stream; the model's
+ *     state is the new one from here on (its other points still being written);
+ *   then pack, exchange and unpack on the model's stream;
+ *   fi_model_advance_end(m): every other tile, on a second stream of the model,
+ *     after the first half; it runs while the halo moves.
+ * Every other entry point (and the next begin) first waits for the second half;
+ * between begin and end only the halo entry points may be called (FI_ERR_STATE
+ * otherwise).  Fused sweep only, split dimension declared periodic. */
+fi_status fi_model_advance_begin(fi_model *m, int32_t dim);
+fi_status fi_model_advance_end(fi_model *m);
 /* The layer plan of those messages, host only (no device, no model): for an
  * nd-dimensional slab of n cells, the (field, layer index along dim) pairs of the
  * message packed toward `side` (pack != 0) or unpacked from it, in message order;

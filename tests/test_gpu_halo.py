@@ -31,12 +31,17 @@ def _bits(a):
     return a.view(np.uint64)
 
 
-@pytest.mark.parametrize("dim,ranks", [(0, 2), (0, 4), (1, 2)])
-def test_split_run_matches_undivided(dim, ranks):
+@pytest.mark.parametrize("dim,ranks,overlap", [(0, 2, False), (0, 4, False), (1, 2, False), (0, 2, True),
+                                                (1, 4, True), (0, 4, True)])
+def test_split_run_matches_undivided(dim, ranks, overlap):
+    # overlap: each slab iteration in two halves (the tiles of the split faces, then
+    # the others on the model's second stream), the halo moved after the first half
     path = "fused"
     fi = load_fastice()
     from fastice_b200 import distributed as D
-    nl = [24, 16, 14]
+    # slabs wide enough along the split dimension for several tiles on each side of
+    # the tile of position n (the partition of an overlapped iteration)
+    nl = [80, 16, 14] if dim == 0 else [24, 40, 14]
     ng = list(nl)
     ng[dim] = nl[dim] * ranks
     ext = [1.0, 0.8, 0.3]
@@ -64,9 +69,7 @@ def test_split_run_matches_undivided(dim, ranks):
     D.exchange_local(slabs, dim, "state")
     for _ in range(6):
         whole.advance(1)
-        for s in slabs:
-            s.advance(1)
-        D.exchange_local(slabs, dim, "iteration")
+        D.advance_local(slabs, dim, 1, overlap=overlap)
     bad = []
     for name in STATE:
         g = whole.get_field(name)
@@ -114,7 +117,7 @@ def test_split_solve_matches_undivided_solve():
     D.exchange_local(slabs, dim, "state")
     kw = dict(max_iter=20000, ncheck=100, tol=1e-9, measure="rel_slab", rho_g_inf=1.0, length_z=0.25)
     ref = whole.solve(**kw)
-    rep = D.solve_local(slabs, dim, **kw)
+    rep = D.solve_local(slabs, dim, overlap=True, **kw)
     assert ref["converged"] and rep["converged"], (ref, rep)
     assert rep["iterations"] == ref["iterations"]
     assert rep["measure"] == ref["measure"]
