@@ -343,44 +343,91 @@ def run_batched(args):
     """Batched 2D solves: `instances` pure-shear inclusion problems (seeds 0..k-1,
     63-511 cells per side, 1-16 inclusions, contrasts up to 1e4) in one batch:
     autotuned tile shape, CUDA-graph replay of each check round, one step = one
-    check round.  value = instances solved / wall time of the solve."""
+    check round.  With --storage f32 (the default) every PT sweep runs on FP32
+    storage inside a per-member FP64 defect correction (FP64 solution and
+    residuals) to the FP64 measure --tol (1e-6); --storage f64 runs plain FP64
+    sweeps.  value = instances solved / wall time of the solve.  The same method
+    solving members one at a time (a batch of one each) is timed on the first
+    --alone members, and the first --errcheck members are compared with a plain
+    FP64 solve taken to 1e-9."""
     import torch
     fi = load_fastice()
     from fastice_b200 import scenarios
-    dtype = args.dtypes.split(",")[0] if args.dtypes != "f64,f32" else "f32"
-    tol = args.tol or (1e-4 if dtype == "f32" else 1e-6)
+    storage = args.storage
+    mode = "mixed" if storage == "f32" else "plain"
+    tol = args.tol or 1e-6
     ncheck = 200
-    models = [scenarios.inclusion_model(s, dtype=dtype)[0] for s in range(args.instances)]
+    window = args.window
+
+    def members(seeds):
+        return [scenarios.inclusion_model(s, dtype="f64", smooth=args.smooth)[0] for s in seeds]
+
+    models = members(range(args.instances))
     cells = sum(m.grid.dims[0] * m.grid.dims[1] for m in models)
     batch = fi.BatchedStokes2D(models)
     best, per = batch.autotune(iters=10)
-    esz = 8 if dtype == "f64" else 4
-    sweep_gbs = {k: 13 * esz * cells / (v * 1e-3) / 1e9 for k, v in per.items()}
+    sweep_gbs = {k: 13 * 8 * cells / (v * 1e-3) / 1e9 for k, v in per.items()}
     clocks = ClockSampler(0)
     clocks.start()
     max_iter = args.rounds * ncheck if args.rounds > 0 else 400000
-    items, sec = batch.solve(max_iter=max_iter, ncheck=ncheck, tol=tol, window=100000, use_graph=True)
+    items, sec = batch.solve(max_iter=max_iter, ncheck=ncheck, tol=tol, window=window, use_graph=True, mode=mode)
     ck = clocks.stop()
     batch.close()
     status = {}
     for it in items:
         status[it["status"]] = status.get(it["status"], 0) + 1
     iters = [it["iterations"] for it in items]
-    cell_sweeps = sum(it["iterations"] * m.grid.dims[0] * m.grid.dims[1] for it, m in zip(items, models))
+    done = sum(1 for it in items if it["status"] == "converged")
+    # one at a time: the same method, each member alone in its own batch
+    alone = {"members": 0, "seconds": 0.0, "status": {}}
+    for q in range(min(args.alone, len(models))):
+        mq = members([q])
+        b1 = fi.BatchedStokes2D(mq)
+        b1.set_variant(best)
+        it1, s1 = b1.solve(max_iter=max_iter, ncheck=ncheck, tol=tol, window=window, use_graph=True, mode=mode)
+        b1.close()
+        mq[0].close()
+        alone["members"] += 1
+        alone["seconds"] += s1
+        alone["status"][it1[0]["status"]] = alone["status"].get(it1[0]["status"], 0) + 1
+    alone["solves_per_s"] = alone["members"] / alone["seconds"] if alone["seconds"] > 0 else None
+    # error against a plain FP64 solve of the same members, to 1e-9
+    errs = []
+    if args.errcheck > 0:
+        k = min(args.errcheck, len(models))
+        ref = members(range(k))
+        rb = fi.BatchedStokes2D(ref)
+        ritems, _ = rb.solve(max_iter=4 * max_iter, ncheck=ncheck, tol=1e-9, window=0, use_graph=True)
+        rb.close()
+        for q in range(k):
+            if ritems[q]["status"] != "converged" or items[q]["status"] != "converged":
+                errs.append(None)
+                continue
+            vmax = max(float(np.max(np.abs(ref[q].get_field(c)))) for c in ("Vx", "Vy"))
+            d = max(float(np.max(np.abs(models[q].get_field(c) - ref[q].get_field(c)))) for c in ("Vx", "Vy"))
+            errs.append(d / vmax)
+        for m in ref:
+            m.close()
     for m in models:
         m.close()
+    smooth = f"viscosity smoothed by {args.smooth} log-space passes" if args.smooth else "sharp inclusions"
     cfg = {"workload": f"{args.instances} independent 2D pure-shear inclusion problems (seeds 0..{args.instances - 1}, "
                        "63-511 cells per side, 1-16 circles r~U(0.02,0.15), log-normal contrast clipped to 1e4, "
-                       "viscosity smoothed by 4 log-space passes, free-slip walls with pure shear)",
-           "instances": args.instances, "cells_total": cells, "tol": tol, "ncheck": ncheck,
+                       f"{smooth}, free-slip walls with pure shear)",
+           "instances": args.instances, "cells_total": cells, "tol": tol, "ncheck": ncheck, "window": window,
            "measure": "cell-scaled relative residual max(|r_V|inf h/max|P,tau|, |r_P|inf h/max|V|), FP64",
-           "storage": dtype, "tile_shape": list(per)[best], "graph": True}
-    line = _base_line(f"batched 2D PT solves/s ({args.instances} instances)", len(items) / sec, "solves/s",
-                      len(iters), 10 * 3, 1e3 * sec / max(1, max(iters) // ncheck), dtype, cfg)
+           "storage": "FP32 sweeps inside an FP64 defect correction (FP64 solution and residuals)" if mode == "mixed"
+           else "FP64", "tile_shape": list(per)[best], "graph": True}
+    line = _base_line(f"batched 2D PT solves/s ({args.instances} instances)", done / sec, "solves/s",
+                      len(iters), 10 * 3, 1e3 * sec / max(1, max(iters) // ncheck), "f32+f64" if mode == "mixed"
+                      else "f64", cfg)
     line.update({"status": status, "iterations": {"min": min(iters), "max": max(iters), "mean": float(np.mean(iters))},
-                 "seconds": sec, "sweep_teff_gbs": sweep_gbs,
-                 "solve_teff_gbs": 13 * esz * cell_sweeps / sec / 1e9, "clocks": ck,
-                 "gpu_launches": "k sweeps + 4 bookkeeping kernels per check round, replayed as one graph"})
+                 "seconds": sec, "sweep_teff_gbs_fp64_members": sweep_gbs, "clocks": ck,
+                 "one_at_a_time": alone,
+                 "speedup_vs_one_at_a_time": (done / sec) / alone["solves_per_s"] if alone["solves_per_s"] else None,
+                 "error_vs_fp64_solve": errs,
+                 "gpu_launches": "k sweeps + 4 bookkeeping kernels per check round, replayed as one graph; per outer "
+                                 "step of the defect correction a few FP64 kernels per member"})
     print(json.dumps(line))
 
 
@@ -686,6 +733,12 @@ def main():
     ap.add_argument("--scale", type=float, default=0.25, help="serving: linear size scale of the request stream")
     ap.add_argument("--duration", type=float, default=2.0, help="serving: seconds of Poisson arrivals")
     ap.add_argument("--rounds", type=int, default=0, help="batched: stop after this many check rounds (profiling)")
+    ap.add_argument("--storage", choices=("f32", "f64"), default="f32",
+                    help="batched: FP32 sweeps in an FP64 defect correction (f32) or plain FP64 sweeps")
+    ap.add_argument("--smooth", type=int, default=0, help="batched: log-space smoothing passes of the viscosity")
+    ap.add_argument("--window", type=int, default=20000, help="batched: stall window in sweeps")
+    ap.add_argument("--alone", type=int, default=16, help="batched: members timed one at a time")
+    ap.add_argument("--errcheck", type=int, default=4, help="batched: members compared with a plain FP64 solve")
     ap.add_argument("--scenario", choices=("mms", "glacier"), default="mms",
                     help="mixed: the 3D manufactured solution or the immersed-boundary glacier")
     ap.add_argument("--rheology", choices=("linear", "glen", "glen_relaxed"), default="linear",

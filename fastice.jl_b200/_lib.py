@@ -159,6 +159,7 @@ SIGNATURES = [
     ("fi_batch_solve", C.c_int, [C.c_void_p, C.POINTER(fi_batch_opts), C.POINTER(fi_batch_item),
                                  C.POINTER(C.c_double)]),
     ("fi_batch_measure", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    ("fi_batch_solve_mixed", C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.POINTER(C.c_double)]),
     ("fi_batch_variant_count", C.c_int, []),
     ("fi_batch_variant_name", C.c_char_p, [C.c_int32]),
     ("fi_batch_set_variant", C.c_int, [C.c_void_p, C.c_int32]),

@@ -1019,15 +1019,136 @@ static fi_status fp32_floors(fi_model *s, const double *nn, double *fl_P, double
     return FI_OK;
 }
 
-static fi_status solve_mixed(fi_model *m, const fi_solve_opts *o, fi_solve_report *rep) {
-    m->full_iters = 0;  // the solve writes the FP64 state outside its sweeps
+// ---- stages of the defect correction, shared by the single-model solve and the
+// batched one (fi_batch_solve_mixed) ------------------------------------------------
+static const int kGravF[3] = {FI_FIELD_GX, FI_FIELD_GY, FI_FIELD_GZ};
+static const int kResVF[3] = {FI_FIELD_RVX, FI_FIELD_RVY, FI_FIELD_RVZ};
+static const int kTauF[6] = {FI_FIELD_TXX, FI_FIELD_TYY, FI_FIELD_TZZ, FI_FIELD_TXY, FI_FIELD_TXZ, FI_FIELD_TYZ};
+
+// the shadow's parameters for the full problem (phase A: the model's own gravity and
+// boundary values) and for a correction (homogeneous boundary values, frozen η,
+// forcing r); built from the shadow's parameters as created (a previous solve leaves
+// its last stage's parameters in the shadow)
+static KParams mixed_kp(const fi_model *m, bool correction) {
+    KParams k = m->shadow_kp;
+    if (!correction) {
+        for (int c = 0; c < 3; c++) {
+            k.g_kind[c] = m->kp.g_kind[c];
+            k.g_val[c] = m->kp.g_val[c];
+        }
+        return k;
+    }
+    for (int d = 0; d < 3; d++)
+        for (int sd = 0; sd < 2; sd++)
+            for (int c = 0; c < 3; c++) k.bc_val[d][sd][c] = 0.0;
+    k.freeze_eta = 1;
+    k.p_forcing = 1;
+    return k;
+}
+
+// phase A: the FP64 state, viscosity and gravity fields rounded into the shadow,
+// which then runs the full problem
+fi_status mixed_phase_a_begin(fi_model *m) {
+    fi_model *s = m->shadow;
+    const long long n = (long long)m->elems;
+    fi_status st;
+    for (int f = 0; f < kState; f++)
+        if (field_used(m, f) && (st = convert_field<double, float>(s->cur(f), m->cur(f), n, 1.0, m->stream)) != FI_OK)
+            return st;
+    for (int f : {(int)FI_FIELD_ETA, (int)FI_FIELD_ETA_NEXT})
+        if ((st = convert_field<double, float>(s->cur(f), m->cur(f), n, 1.0, m->stream)) != FI_OK) return st;
+    for (int c = 0; c < m->d.grid.nd; c++)
+        if (m->kp.g_kind[c] == FI_G_FIELD &&
+            (st = convert_field<double, float>(s->base[kGravF[c]], m->base[kGravF[c]], n, 1.0, m->stream)) != FI_OK)
+            return st;
+    FI_CHECK_CUDA(cudaStreamSynchronize(m->stream), "mixed sync");
+    s->kp = mixed_kp(m, false);
+    return FI_OK;
+}
+
+// end of phase A: the shadow's state back into the FP64 model
+fi_status mixed_phase_a_end(fi_model *m) {
+    fi_model *s = m->shadow;
+    const long long n = (long long)m->elems;
+    fi_status st;
+    for (int f = 0; f < kState; f++)
+        if (field_used(m, f) && (st = convert_field<float, double>(m->cur(f), s->cur(f), n, 1.0, s->stream)) != FI_OK)
+            return st;
+    for (int f : {(int)FI_FIELD_ETA, (int)FI_FIELD_ETA_NEXT})
+        if ((st = convert_field<float, double>(m->cur(f), s->cur(f), n, 1.0, s->stream)) != FI_OK) return st;
+    FI_CHECK_CUDA(cudaStreamSynchronize(s->stream), "mixed sync");
+    return FI_OK;
+}
+
+// viscosity from the current stresses (Picard step)
+fi_status mixed_picard(fi_model *m) {
+    Ptrs<double> f = m->ptrs<double>();
+    FI_CHECK_CUDA(launch_eta_from_tau<double>(m->g, m->kp, f, m->stream), "eta refresh");
+    m->eta_swapped = !m->eta_swapped;
+    return run_eta_batch<double>(m, FI_FIELD_ETA);
+}
+
+// A correction: projection τ = 2η dev(ε̇(V)) with its BCs (the stresses before it kept
+// in the second state buffer), the FP64 residual fields of the projected anchor, and
+// the correction problem on the shadow -- frozen η, forcing r_P and -r_V, zero state,
+// stresses starting from the constitutive defect.
+fi_status mixed_correction_begin(fi_model *m) {
+    fi_model *s = m->shadow;
+    const long long n = (long long)m->elems;
+    const int nd = m->d.grid.nd;
+    fi_status st;
+    for (int q = 0; q < 6; q++)
+        if (field_used(m, kTauF[q]))
+            FI_CHECK_CUDA(cudaMemcpyAsync(field_raw(m->nxt(kTauF[q]), m->esz), field_raw(m->cur(kTauF[q]), m->esz),
+                                          (m->elems + 64) * m->esz, cudaMemcpyDeviceToDevice, m->stream),
+                          "stress copy");
+    if ((st = refresh_ibf<double>(m)) != FI_OK) return st;
+    FI_CHECK_CUDA(launch_compute_tau<double>(m->g, m->kp, m->ptrs<double>(), m->ib, m->stream), "projection");
+    if ((st = run_batch<double>(m, stress_batch)) != FI_OK) return st;
+    if ((st = residuals_t<double>(m)) != FI_OK) return st;
+    if ((st = convert_field<double, float>(s->cur(FI_FIELD_ETA), m->cur(FI_FIELD_ETA), n, 1.0, m->stream)) != FI_OK)
+        return st;
+    if ((st = convert_field<double, float>(s->fP, m->base[FI_FIELD_RP], n, 1.0, m->stream)) != FI_OK) return st;
+    for (int c = 0; c < nd; c++)
+        if ((st = convert_field<double, float>(s->base[kGravF[c]], m->base[kResVF[c]], n, -1.0, m->stream)) != FI_OK)
+            return st;
+    for (int fl = 0; fl < kState; fl++) {
+        if (!field_used(s, fl)) continue;
+        FI_CHECK_CUDA(cudaMemsetAsync(field_raw(s->base[fl], s->esz), 0, (s->elems + 64) * s->esz, m->stream), "zero");
+        if (s->alt[fl])
+            FI_CHECK_CUDA(cudaMemsetAsync(field_raw(s->alt[fl], s->esz), 0, (s->elems + 64) * s->esz, m->stream), "zero");
+    }
+    for (int q = 0; q < 6; q++)
+        if (field_used(m, kTauF[q])) {
+            cudaError_t e = launch_diff<double, float>((const double *)m->nxt(kTauF[q]), (const double *)m->cur(kTauF[q]),
+                                                       (float *)s->cur(kTauF[q]), n, m->stream);
+            if (e != cudaSuccess) return cuda_fail(e, "constitutive defect");
+        }
+    FI_CHECK_CUDA(cudaStreamSynchronize(m->stream), "mixed sync");
+    s->kp = mixed_kp(m, true);
+    s->full_iters = 0;
+    return FI_OK;
+}
+
+// x += δ in FP64
+fi_status mixed_correction_end(fi_model *m) {
+    fi_model *s = m->shadow;
+    const long long n = (long long)m->elems;
+    for (int fl = 0; fl < kState; fl++)
+        if (field_used(m, fl)) {
+            cudaError_t e = launch_accumulate<double, float>((double *)m->cur(fl), (const float *)s->cur(fl), n, m->stream);
+            if (e != cudaSuccess) return cuda_fail(e, "accumulate");
+        }
+    return FI_OK;
+}
+
+// the FP32 shadow of an FP64 model (created on first use, masks refreshed)
+fi_status mixed_shadow(fi_model *m) {
     if (!m->is_f64()) return set_error("the mixed-precision solve refines an FP64 model"), FI_ERR_ARG;
     FI_CHECK_CUDA(cudaSetDevice(m->d.device), "cudaSetDevice");
     fi_status st = make_shadow(m);
     if (st != FI_OK) return st;
     fi_model *s = m->shadow;
-    // volume fractions (refreshed every solve: the caller may have recomputed them);
-    // the shadow sees the FP64 model's empty, valid and null-space points
     for (int f = FI_FIELD_NA_CCC; f < FI_FIELD_NA_CCC + 16 && m->ib; f++)
         if (field_used(m, f))
             FI_CHECK_CUDA(launch_mask_to_f32((const double *)m->base[f], (float *)s->base[f], (long long)m->elems,
@@ -1037,7 +1158,16 @@ static fi_status solve_mixed(fi_model *m, const fi_solve_opts *o, fi_solve_repor
         s->ibf_stale = true, s->full_iters = 0;
         FI_CHECK_CUDA(cudaStreamSynchronize(m->stream), "shadow volume fractions");
     }
-    const long long n = (long long)m->elems;
+    return FI_OK;
+}
+
+static fi_status solve_mixed(fi_model *m, const fi_solve_opts *o, fi_solve_report *rep) {
+    m->full_iters = 0;  // the solve writes the FP64 state outside its sweeps
+    // the shadow, its volume fractions refreshed every solve (the caller may have
+    // recomputed them): it sees the FP64 model's empty, valid and null-space points
+    fi_status st = mixed_shadow(m);
+    if (st != FI_OK) return st;
+    fi_model *s = m->shadow;
     const int nd = m->d.grid.nd;
     const double inner_red = o->inner_reduction > 0 ? o->inner_reduction : 1e-3;
     const int inner_max = o->inner_iter > 0 ? o->inner_iter : 50 * o->ncheck;
@@ -1045,20 +1175,6 @@ static fi_status solve_mixed(fi_model *m, const fi_solve_opts *o, fi_solve_repor
     int window = 0;
     for (int c = 0; c < nd; c++) window = std::max(window, 2 * (m->d.grid.n[c] + 1));
     window = std::max(window, 2 * o->ncheck);
-    const KParams kbase = m->shadow_kp;  // not s->kp: a previous solve leaves its last stage's parameters there
-    KParams ka = kbase;  // phase A: the full problem in FP32
-    for (int c = 0; c < 3; c++) {
-        ka.g_kind[c] = m->kp.g_kind[c];
-        ka.g_val[c] = m->kp.g_val[c];
-    }
-    KParams kc = kbase;  // corrections: homogeneous boundary values, frozen η, forcing r
-    for (int d = 0; d < 3; d++)
-        for (int sd = 0; sd < 2; sd++)
-            for (int c = 0; c < 3; c++) kc.bc_val[d][sd][c] = 0.0;
-    kc.freeze_eta = 1;
-    kc.p_forcing = 1;
-    const int gf[3] = {FI_FIELD_GX, FI_FIELD_GY, FI_FIELD_GZ};
-    const int rf[3] = {FI_FIELD_RVX, FI_FIELD_RVY, FI_FIELD_RVZ};
     auto t0 = std::chrono::steady_clock::now();
     double norms[FI_NORMS_LEN];
     int sweeps = 0;
@@ -1108,24 +1224,9 @@ static fi_status solve_mixed(fi_model *m, const fi_solve_opts *o, fi_solve_repor
     };
 
     // ---- phase A: FP32 PT on the full problem down to the FP32 floor
-    for (int f = 0; f < kState; f++)
-        if (field_used(m, f) && (st = convert_field<double, float>(s->cur(f), m->cur(f), n, 1.0, m->stream)) != FI_OK)
-            return st;
-    for (int f : {(int)FI_FIELD_ETA, (int)FI_FIELD_ETA_NEXT})
-        if ((st = convert_field<double, float>(s->cur(f), m->cur(f), n, 1.0, m->stream)) != FI_OK) return st;
-    for (int c = 0; c < nd; c++)
-        if (m->kp.g_kind[c] == FI_G_FIELD &&
-            (st = convert_field<double, float>(s->base[gf[c]], m->base[gf[c]], n, 1.0, m->stream)) != FI_OK)
-            return st;
-    FI_CHECK_CUDA(cudaStreamSynchronize(m->stream), "mixed sync");
-    s->kp = ka;
+    if ((st = mixed_phase_a_begin(m)) != FI_OK) return st;
     if ((st = stage(true, 0.0, o->max_iter, "fp32 phase")) != FI_OK) return st;
-    for (int f = 0; f < kState; f++)
-        if (field_used(m, f) && (st = convert_field<float, double>(m->cur(f), s->cur(f), n, 1.0, s->stream)) != FI_OK)
-            return st;
-    for (int f : {(int)FI_FIELD_ETA, (int)FI_FIELD_ETA_NEXT})
-        if ((st = convert_field<float, double>(m->cur(f), s->cur(f), n, 1.0, s->stream)) != FI_OK) return st;
-    FI_CHECK_CUDA(cudaStreamSynchronize(s->stream), "mixed sync");
+    if ((st = mixed_phase_a_end(m)) != FI_OK) return st;
 
     // ---- phase B: FP64 defect correction with FP32 correction sweeps
     //
@@ -1139,14 +1240,9 @@ static fi_status solve_mixed(fi_model *m, const fi_solve_opts *o, fi_solve_repor
     // then continue the FP64 iteration instead of restarting it from rest.
     int outer = 0, outer_stale = 0;
     double best_outer = 1e300;
-    const int tau_f[6] = {FI_FIELD_TXX, FI_FIELD_TYY, FI_FIELD_TZZ, FI_FIELD_TXY, FI_FIELD_TXZ, FI_FIELD_TYZ};
     if ((st = model_ensure_second_state(m)) != FI_OK) return st;
     while (true) {
-        // viscosity from the current stresses (Picard step)
-        Ptrs<double> f = m->ptrs<double>();
-        FI_CHECK_CUDA(launch_eta_from_tau<double>(m->g, m->kp, f, m->stream), "eta refresh");
-        m->eta_swapped = !m->eta_swapped;
-        if ((st = run_eta_batch<double>(m, FI_FIELD_ETA)) != FI_OK) return st;
+        if ((st = mixed_picard(m)) != FI_OK) return st;
         // FP64 residual norms of the iterate itself (its own stresses), the quantity
         // the plain solve tests
         if ((st = norms_t<double>(m, norms)) != FI_OK) return st;
@@ -1169,40 +1265,7 @@ static fi_status solve_mixed(fi_model *m, const fi_solve_opts *o, fi_solve_repor
         if (meas < 0.5 * best_outer) outer_stale = 0;
         else if (++outer_stale >= 3) break;
         best_outer = std::min(best_outer, meas);
-        // projection τ = 2η dev(ε̇(V)) with its BCs (the stresses before it are kept in
-        // the second state buffer) and the FP64 residual fields of the projected anchor
-        for (int q = 0; q < 6; q++)
-            if (field_used(m, tau_f[q]))
-                FI_CHECK_CUDA(cudaMemcpyAsync(field_raw(m->nxt(tau_f[q]), m->esz), field_raw(m->cur(tau_f[q]), m->esz),
-                                              (m->elems + 64) * m->esz, cudaMemcpyDeviceToDevice, m->stream),
-                              "stress copy");
-        if ((st = refresh_ibf<double>(m)) != FI_OK) return st;
-        FI_CHECK_CUDA(launch_compute_tau<double>(m->g, m->kp, m->ptrs<double>(), m->ib, m->stream), "projection");
-        if ((st = run_batch<double>(m, stress_batch)) != FI_OK) return st;
-        if ((st = residuals_t<double>(m)) != FI_OK) return st;
-        // the correction problem on the shadow: frozen η, forcing r_P and -r_V, zero state
-        if ((st = convert_field<double, float>(s->cur(FI_FIELD_ETA), m->cur(FI_FIELD_ETA), n, 1.0, m->stream)) != FI_OK)
-            return st;
-        if ((st = convert_field<double, float>(s->fP, m->base[FI_FIELD_RP], n, 1.0, m->stream)) != FI_OK) return st;
-        for (int c = 0; c < nd; c++)
-            if ((st = convert_field<double, float>(s->base[gf[c]], m->base[rf[c]], n, -1.0, m->stream)) != FI_OK)
-                return st;
-        for (int fl = 0; fl < kState; fl++) {
-            if (!field_used(s, fl)) continue;
-            FI_CHECK_CUDA(cudaMemsetAsync(field_raw(s->base[fl], s->esz), 0, (s->elems + 64) * s->esz, m->stream), "zero");
-            if (s->alt[fl])
-                FI_CHECK_CUDA(cudaMemsetAsync(field_raw(s->alt[fl], s->esz), 0, (s->elems + 64) * s->esz, m->stream),
-                              "zero");
-        }
-        // the correction's stresses start from the constitutive defect
-        for (int q = 0; q < 6; q++)
-            if (field_used(m, tau_f[q])) {
-                cudaError_t e = launch_diff<double, float>((const double *)m->nxt(tau_f[q]), (const double *)m->cur(tau_f[q]),
-                                                           (float *)s->cur(tau_f[q]), n, m->stream);
-                if (e != cudaSuccess) return cuda_fail(e, "constitutive defect");
-            }
-        FI_CHECK_CUDA(cudaStreamSynchronize(m->stream), "mixed sync");
-        s->kp = kc;
+        if ((st = mixed_correction_begin(m)) != FI_OK) return st;
         // target: inner_reduction of r0, but no further than a third of the tolerance
         // (scaled from the solve's measure to the residual inf-norms)
         const double r0 = std::max(std::max(norms[0], norms[1]), std::max(norms[2], norms[3]));
@@ -1211,13 +1274,7 @@ static fi_status solve_mixed(fi_model *m, const fi_solve_opts *o, fi_solve_repor
             rep->outer = outer;
             return st;
         }
-        // x += δ in FP64
-        for (int fl = 0; fl < kState; fl++)
-            if (field_used(m, fl)) {
-                cudaError_t e = launch_accumulate<double, float>((double *)m->cur(fl), (const float *)s->cur(fl), n,
-                                                                 m->stream);
-                if (e != cudaSuccess) return cuda_fail(e, "accumulate");
-            }
+        if ((st = mixed_correction_end(m)) != FI_OK) return st;
         outer++;
     }
     rep->iterations = sweeps;

@@ -26,6 +26,7 @@
 // check-to-check step is a fixed launch sequence, captured once as a CUDA graph
 // and replayed; the host reads back one word (instances still active) per replay.
 #include <algorithm>
+#include <cmath>
 #include <chrono>
 #include <cstdio>
 #include <cstring>
@@ -55,6 +56,9 @@ struct alignas(16) BInst {  // copied whole into shared memory (bulk copy: 16-by
     T *P[2], *txx[2], *tyy[2], *txy[2], *Vx[2], *Vy[2];
     const T *eta;
     const T *gx, *gy;
+    const T *fP;  // pressure forcing of a defect-correction problem (pforce), else unused
+    int pforce;
+    int pad_;
     double h;  // smallest grid spacing (scales the check's measure)
 };
 
@@ -135,7 +139,11 @@ __device__ __forceinline__ void sigma2(const Tile<T, TY> &t, const BInst<T> &b, 
             T e_xy = T(0.5) * (T(0.5) * (t.sEt[a - 1 - BX] + t.sEt[a - BX]) + T(0.5) * (t.sEt[a - 1] + t.sEt[a]));
             nXY = oXY - (oXY - T(2.0) * e_xy * exy) * b.dxy;
         }
-        if (mask & M_P) t.sP[a] = oP - divV * etac * b.dtP;
+        if (mask & M_P) {
+            // the forced pressure update of a correction problem (as update_σ! with p_forcing)
+            const T dv = b.pforce ? divV + b.fP[(long long)i + b.pitch * (long long)j] : divV;
+            t.sP[a] = oP - dv * etac * b.dtP;
+        }
         if (mask & M_XX) t.sXX[a] = oXX - (oXX - T(2.0) * etac * (exx - third(divV))) * b.dxx;
         if (mask & M_YY) t.sYY[a] = oYY - (oYY - T(2.0) * etac * (eyy - third(divV))) * b.dyy;
         if (dxy) t.sXY[a] = nXY;
@@ -416,7 +424,8 @@ __global__ void __launch_bounds__(BTX *TY) batch2d_check(const BInst<T> *__restr
         if (i <= b.n0 + 1 && j <= b.n1 + 1) {
             const bool ci = i <= b.n0, cj = j <= b.n1;
             if (ci && cj) {
-                const double rP = ((double)VX[I + 1] - (double)VX[I]) * idx + ((double)VY[I + sx] - (double)VY[I]) * idy;
+                double rP = ((double)VX[I + 1] - (double)VX[I]) * idx + ((double)VY[I + sx] - (double)VY[I]) * idy;
+                if (b.pforce) rP = rP + (double)b.fP[I];
                 m[0] = fabs(rP);
                 m[2] = fmax(fmax(fabs((double)P[I]), fabs((double)XX[I])), fabs((double)YY[I]));
             }
@@ -650,6 +659,8 @@ void fill_inst(const fi_model *m, BInst<T> &b) {
     b.eta = (const T *)m->cur(FI_FIELD_ETA);
     b.gx = (const T *)m->base[FI_FIELD_GX];
     b.gy = (const T *)m->base[FI_FIELD_GY];
+    b.fP = (const T *)m->fP;
+    b.pforce = p.p_forcing && m->fP ? 1 : 0;
     b.h = std::min(1.0 / p.inv_dx[0], 1.0 / p.inv_dx[1]);
 }
 
@@ -1131,6 +1142,92 @@ fi_status fi_batch_step(fi_batch *b, const fi_batch_opts *o, int32_t max_rounds,
     if (st != FI_OK) return st;
     if ((st = prepare(b)) != FI_OK) return st;
     return run_rounds(b, o, max_rounds, items, nactive);
+}
+
+fi_status fi_batch_solve_mixed(fi_batch *b, const fi_batch_opts *o, double inner_tol, fi_batch_item *items,
+                               double *seconds) {
+    if (!b || !o || !items) return set_error("bad argument"), FI_ERR_ARG;
+    if (!b->f64) return set_error("the mixed-precision batch refines FP64 members"), FI_ERR_ARG;
+    fi_status st = check_opts(o);
+    if (st != FI_OK) return st;
+    const double corr_tol = inner_tol > 0 ? inner_tol : 1e-3;
+    auto t0 = std::chrono::steady_clock::now();
+    const int n = b->count();
+    if ((st = pull_state(b)) != FI_OK) return st;
+    std::vector<fi_model *> shadows(n);
+    for (int q = 0; q < n; q++) {
+        if ((st = mixed_shadow(b->models[q])) != FI_OK) return st;
+        shadows[q] = b->models[q]->shadow;
+    }
+    fi_batch *sb = nullptr;
+    if ((st = fi_batch_create(shadows.data(), n, &sb)) != FI_OK) return st;
+    struct Guard {
+        fi_batch *p;
+        ~Guard() { fi_batch_destroy(p); }
+    } guard{sb};
+    sb->variant = b->variant;
+    std::vector<int> sweeps(n, 0), status(n, FI_ITEM_ACTIVE), stale(n, 0);
+    std::vector<double> best(n, 1e300), meas(n, 0.0);
+    std::vector<fi_batch_item> it(n);
+    // phase A: every member's full problem in FP32 storage, batched, down to the FP32
+    // rounding floor (where the stall rule ends a member) or the tolerance
+    for (int q = 0; q < n; q++)
+        if ((st = mixed_phase_a_begin(b->models[q])) != FI_OK) return st;
+    if ((st = fi_batch_solve(sb, o, it.data(), nullptr)) != FI_OK) return st;
+    for (int q = 0; q < n; q++) {
+        sweeps[q] += it[q].iterations;
+        if ((st = mixed_phase_a_end(b->models[q])) != FI_OK) return st;
+        if (it[q].status == FI_ITEM_DIVERGED) {
+            status[q] = FI_ITEM_DIVERGED;
+            if ((st = fi_batch_remove(sb, shadows[q])) != FI_OK) return st;
+        }
+    }
+    // FP64 defect correction: every outer step measures the FP64 members, retires the
+    // converged ones and runs the corrections of the others as one FP32 batch
+    while (true) {
+        if ((st = fi_batch_measure(b, meas.data())) != FI_OK) return st;
+        std::vector<fi_model *> act;
+        for (int q = 0; q < n; q++) {
+            if (status[q] != FI_ITEM_ACTIVE) continue;
+            if (!std::isfinite(meas[q])) status[q] = FI_ITEM_DIVERGED;
+            else if (meas[q] < o->tol) status[q] = FI_ITEM_CONVERGED;
+            else if (sweeps[q] >= o->max_iter) status[q] = FI_ITEM_MAXITER;
+            else {
+                // three outer steps without halving the FP64 measure: the corrections no
+                // longer reach the residual
+                if (meas[q] < 0.5 * best[q]) stale[q] = 0;
+                else if (++stale[q] >= 3) status[q] = FI_ITEM_STALLED;
+                best[q] = std::min(best[q], meas[q]);
+            }
+            if (status[q] == FI_ITEM_ACTIVE) act.push_back(b->models[q]);
+            else if ((st = fi_batch_remove(sb, shadows[q])) != FI_OK && st != FI_ERR_ARG) return st;
+        }
+        if (act.empty()) break;
+        for (fi_model *m : act) {
+            if ((st = mixed_picard(m)) != FI_OK) return st;
+            if ((st = mixed_correction_begin(m)) != FI_OK) return st;
+        }
+        fi_batch_opts oc = *o;
+        oc.tol = corr_tol;
+        std::vector<fi_batch_item> ic(sb->count());
+        if ((st = fi_batch_solve(sb, &oc, ic.data(), nullptr)) != FI_OK) return st;
+        for (int k = 0; k < sb->count(); k++) {
+            int q = 0;
+            while (shadows[q] != sb->models[k]) q++;
+            sweeps[q] += ic[k].iterations;
+            if (ic[k].status == FI_ITEM_DIVERGED) status[q] = FI_ITEM_DIVERGED;
+        }
+        for (fi_model *m : act)
+            if ((st = mixed_correction_end(m)) != FI_OK) return st;
+        for (fi_model *m : act) FB_CHECK(cudaStreamSynchronize(m->stream), "accumulate");
+    }
+    for (int q = 0; q < n; q++) {
+        items[q].iterations = sweeps[q];
+        items[q].status = status[q];
+        items[q].measure = meas[q];
+    }
+    if (seconds) *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return FI_OK;
 }
 
 fi_status fi_batch_measure(fi_batch *b, double *out) {

@@ -120,6 +120,19 @@ struct fi_model {
     }
 };
 
+// Stages of the FP32-in-FP64 defect correction of an FP64 model (fi_api.cu), shared
+// by fi_model_solve (mode MIXED) and fi_batch_solve_mixed:
+//   mixed_shadow            the FP32 shadow (created on first use, masks refreshed)
+//   mixed_phase_a_begin/end the full problem rounded into the shadow / back
+//   mixed_picard            η from the FP64 stresses
+//   mixed_correction_begin  projection, FP64 residuals, the shadow's correction problem
+//   mixed_correction_end    x += δ
+fi_status mixed_shadow(fi_model *m);
+fi_status mixed_phase_a_begin(fi_model *m);
+fi_status mixed_phase_a_end(fi_model *m);
+fi_status mixed_picard(fi_model *m);
+fi_status mixed_correction_begin(fi_model *m);
+fi_status mixed_correction_end(fi_model *m);
 // allocates the second buffer of every state field a model lacks (fi_api.cu)
 fi_status model_ensure_second_state(fi_model *m);
 // whether the model stores field f (fi_api.cu)

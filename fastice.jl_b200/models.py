@@ -475,14 +475,23 @@ class BatchedStokes2D:
         names = [self.lib.fi_batch_variant_name(v).decode() for v in range(nv)]
         return best.value, dict(zip(names, list(ms)))
 
-    def solve(self, *, max_iter: int, ncheck: int, tol: float, use_graph: bool = True, window: int = 0):
+    def solve(self, *, max_iter: int, ncheck: int, tol: float, use_graph: bool = True, window: int = 0,
+              mode: str = "plain", inner_tol: float = 0.0):
         """Iterate every member until it converges (measure < tol), stalls, fails or
         reaches max_iter.  Returns (items, seconds); items[k] is a dict with
-        iterations, status and measure of member k."""
+        iterations, status and measure of member k.  ``mode="mixed"`` (FP64
+        members): FP32 batched sweeps inside a per-member FP64 defect correction
+        (fi_batch_solve_mixed); ``window`` then also ends the FP32 stages at their
+        rounding floor."""
         o = self._opts(max_iter, ncheck, tol, use_graph, window)
         items = (L.fi_batch_item * len(self.models))()
         sec = C.c_double()
-        L.check(self.lib, self.lib.fi_batch_solve(self._h, C.byref(o), items, C.byref(sec)))
+        if mode == "mixed":
+            L.check(self.lib, self.lib.fi_batch_solve_mixed(self._h, C.byref(o), float(inner_tol), items, C.byref(sec)))
+        elif mode == "plain":
+            L.check(self.lib, self.lib.fi_batch_solve(self._h, C.byref(o), items, C.byref(sec)))
+        else:
+            raise ValueError(mode)
         return self._items(items), sec.value
 
 

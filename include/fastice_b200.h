@@ -346,6 +346,19 @@ fi_status fi_batch_step(fi_batch *b, const fi_batch_opts *opts, int32_t max_roun
                         int32_t *nactive);
 /* current measure of every member (count doubles) */
 fi_status fi_batch_measure(fi_batch *b, double *out);
+/* FP32 PT sweeps inside an FP64 defect correction, batched: the members (FP64
+ * models) keep the solution and the FP64 residuals; their FP32 shadows run every
+ * sweep as one batch -- first the full problems down to the FP32 rounding floor
+ * (the stall window ends a member there), then, per outer step, the correction
+ * problems of the members whose FP64 measure is still >= tol (forcing r_P and
+ * -r_V of the projected iterate, homogeneous boundary values), each to the
+ * relative measure inner_tol (0: 1e-3), added to the FP64 state.  A member stops
+ * when its FP64 measure drops below tol (CONVERGED), after three outer steps that
+ * did not halve it (STALLED) or after max_iter FP32 sweeps (MAXITER); items get
+ * the FP32 sweeps, the status and the last FP64 measure.  The north-star
+ * precision pattern applied to the batch; no counterpart in the reference. */
+fi_status fi_batch_solve_mixed(fi_batch *b, const fi_batch_opts *opts, double inner_tol, fi_batch_item *items,
+                               double *seconds);
 /* tile shapes of the batched sweep; autotune times each for `iters` iterations on
  * the batch itself (the members advance by (2 + iters) * count_of_variants) */
 int fi_batch_variant_count(void);

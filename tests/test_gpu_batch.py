@@ -231,3 +231,29 @@ def test_batch_rejects_unsupported_members():
     batch.close()
     for m in (m3, glen, a, b64):
         m.close()
+
+
+def test_mixed_batch_reaches_fp64_tolerance_with_fp32_sweeps():
+    # FP32 storage for every sweep, FP64 residuals and solution: each member reaches
+    # the FP64 measure 1e-6 (below the FP32 floor near 1e-5) and agrees with the
+    # plain FP64 batched solve of the same members taken to 1e-9
+    fi = load_fastice()
+    seeds = range(30, 36)
+    ms = _inclusions(fi, seeds, dtype="f64")
+    batch = fi.BatchedStokes2D(ms)
+    items, _ = batch.solve(max_iter=80000, ncheck=200, tol=1e-6, window=6000, mode="mixed")
+    meas = batch.measures()
+    batch.close()
+    assert all(it["status"] == "converged" and it["measure"] < 1e-6 for it in items), items
+    assert np.all(meas < 1e-6)
+    ref = _inclusions(fi, seeds, dtype="f64")
+    rb = fi.BatchedStokes2D(ref)
+    ritems, _ = rb.solve(max_iter=200000, ncheck=200, tol=1e-9, window=0)
+    rb.close()
+    assert all(it["status"] == "converged" for it in ritems), ritems
+    for m, r in zip(ms, ref):
+        for c in ("Vx", "Vy"):
+            a, b = m.get_field(c), r.get_field(c)
+            assert np.max(np.abs(a - b)) <= 1e-4 * np.max(np.abs(b)), c
+    for m in ms + ref:
+        m.close()
