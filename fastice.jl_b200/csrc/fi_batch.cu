@@ -1144,6 +1144,8 @@ fi_status fi_batch_step(fi_batch *b, const fi_batch_opts *o, int32_t max_rounds,
     return run_rounds(b, o, max_rounds, items, nactive);
 }
 
+constexpr double kPhaseATol = 2e-4;
+
 fi_status fi_batch_solve_mixed(fi_batch *b, const fi_batch_opts *o, double inner_tol, fi_batch_item *items,
                                double *seconds) {
     if (!b || !o || !items) return set_error("bad argument"), FI_ERR_ARG;
@@ -1169,11 +1171,16 @@ fi_status fi_batch_solve_mixed(fi_batch *b, const fi_batch_opts *o, double inner
     std::vector<int> sweeps(n, 0), status(n, FI_ITEM_ACTIVE), stale(n, 0);
     std::vector<double> best(n, 1e300), meas(n, 0.0);
     std::vector<fi_batch_item> it(n);
-    // phase A: every member's full problem in FP32 storage, batched, down to the FP32
-    // rounding floor (where the stall rule ends a member) or the tolerance
+    // phase A: every member's full problem in FP32 storage, batched, to the measure
+    // kPhaseATol (above the FP32 rounding floor of these measures, 2e-5 at 255^2 and
+    // growing with the grid; the stall window ends a member that meets its floor
+    // first).  PT contracts the residual at a fixed rate per sweep, so stopping here
+    // and reducing the rest by corrections costs no more sweeps than going on.
     for (int q = 0; q < n; q++)
         if ((st = mixed_phase_a_begin(b->models[q])) != FI_OK) return st;
-    if ((st = fi_batch_solve(sb, o, it.data(), nullptr)) != FI_OK) return st;
+    fi_batch_opts oa = *o;
+    oa.tol = std::max(o->tol, kPhaseATol);
+    if ((st = fi_batch_solve(sb, &oa, it.data(), nullptr)) != FI_OK) return st;
     for (int q = 0; q < n; q++) {
         sweeps[q] += it[q].iterations;
         if ((st = mixed_phase_a_end(b->models[q])) != FI_OK) return st;

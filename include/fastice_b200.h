@@ -348,8 +348,9 @@ fi_status fi_batch_step(fi_batch *b, const fi_batch_opts *opts, int32_t max_roun
 fi_status fi_batch_measure(fi_batch *b, double *out);
 /* FP32 PT sweeps inside an FP64 defect correction, batched: the members (FP64
  * models) keep the solution and the FP64 residuals; their FP32 shadows run every
- * sweep as one batch -- first the full problems down to the FP32 rounding floor
- * (the stall window ends a member there), then, per outer step, the correction
+ * sweep as one batch -- first the full problems to the measure 2e-4 (above the
+ * FP32 rounding floor; the stall window ends a member that meets its floor
+ * first), then, per outer step, the correction
  * problems of the members whose FP64 measure is still >= tol (forcing r_P and
  * -r_V of the projected iterate, homogeneous boundary values), each to the
  * relative measure inner_tol (0: 1e-3), added to the FP64 state.  A member stops
