@@ -701,6 +701,36 @@ def run_heat(args):
     print(json.dumps(line))
 
 
+def run_shapes(args):
+    """Every launch shape of the fused sweep on the slab workload at n^3: 3 warm-up
+    iterations, then `steps` iterations timed with CUDA events on the model's stream,
+    per precision; one JSON line with ms per iteration and T_eff per shape."""
+    import torch
+    fi = load_fastice()
+    n = (args.n,) * 3
+    A = a_eff_elements(n)
+    out = {}
+    for dtype in [d for d in args.dtypes.split(",") if d in ("f64", "f32")]:
+        m = make_model(fi, n, dtype, 0)
+        res = {}
+        for v in range(m.lib.fi_fused_variant_count()):
+            try:
+                m.set_variant(v)
+            except fi.FastIceError as e:
+                if e.status == 6:  # not offered in this precision
+                    continue
+                raise
+            m.advance(3)
+            ms = time_advance(fi, m, args.steps, torch) / args.steps
+            res[m.lib.fi_fused_variant_name(v).decode()] = {"ms_per_iter": ms,
+                                                           "teff_gbs": A * (8 if dtype == "f64" else 4) / ms / 1e6}
+        m.close()
+        torch.cuda.empty_cache()
+        out[dtype] = res
+    print(json.dumps({"workload": f"launch shapes of the fused sweep, slab {n[0]}^3", "steps": args.steps,
+                      "shapes": out}))
+
+
 def dist_setup():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -724,7 +754,8 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape (profiling runs)")
     ap.add_argument("--variant", type=int, default=None, help="fused launch shape index (implies --no-autotune)")
     ap.add_argument("--dtypes", default="f64,f32", help="precisions to time, FP64 first")
-    ap.add_argument("--workload", choices=("slab", "batched", "serving", "mixed", "glacier", "heat"), default="slab",
+    ap.add_argument("--workload", choices=("slab", "batched", "serving", "mixed", "glacier", "heat", "shapes"),
+                    default="slab",
                     help="slab: the headline T_eff line; batched / serving / mixed / glacier: the batched 2D solves, "
                          "the continuous-batching server, the mixed-precision solve and the immersed-boundary "
                          "glacier sweep, one JSON line each")
@@ -752,7 +783,7 @@ def main():
         return
     if args.workload != "slab":
         {"batched": run_batched, "serving": run_serving, "mixed": run_mixed,
-         "glacier": run_glacier, "heat": run_heat}[args.workload](args)
+         "glacier": run_glacier, "heat": run_heat, "shapes": run_shapes}[args.workload](args)
         return
     n = (args.n, args.n, args.n)
     ws, rank, local = dist_setup()

@@ -79,15 +79,19 @@ namespace {
 struct Variant {
     int tx, ty, zb, cx, cy, trim;
 };
+// Measured at 511^3 (CUDA events, 30 iterations per shape, one box): the 32x8 tiles
+// with z-blocks of 32 lead in both precisions; trimmed interior boxes (5.23 against
+// 5.09 ms in FP64), clusters (5.39-5.90 ms) and 64-wide FP32 tiles (4.51-9.5 against
+// 3.40 ms) are slower, and their DRAM reads per cell at 255^3 are within 5 % of the
+// plain shape's (the ring sectors they save were L2 hits already).  They stay in the
+// table so that the autotuner re-checks them on every device.
 constexpr Variant kVariants[] = {
     {32, 8, 32, 1, 1, 0},  {32, 8, 64, 1, 1, 0},  {32, 8, 128, 1, 1, 0}, {32, 4, 64, 1, 1, 0},
     {32, 16, 32, 1, 1, 0}, {32, 16, 64, 1, 1, 0}, {32, 16, 128, 1, 1, 0},
     // trimmed interior boxes, clusters
-    {32, 8, 32, 1, 1, 1},  {32, 8, 32, 2, 2, 1},  {32, 8, 64, 2, 2, 1},  {32, 8, 32, 2, 1, 1},
-    {32, 8, 32, 1, 4, 1},  {32, 8, 32, 2, 2, 0},  {32, 16, 32, 1, 1, 1},
-    // 64-wide tiles (two x positions per thread)
-    {64, 8, 32, 1, 1, 0},  {64, 8, 32, 1, 1, 1},  {64, 8, 32, 2, 2, 1},  {64, 4, 32, 1, 1, 1},
-    {64, 4, 64, 2, 2, 1},  {64, 4, 32, 2, 2, 1}};
+    {32, 8, 32, 1, 1, 1},  {32, 8, 32, 1, 4, 1},  {32, 8, 32, 2, 2, 0},
+    // 64-wide tiles (two x positions per thread; FP32 only)
+    {64, 8, 32, 1, 1, 0},  {64, 8, 32, 1, 1, 1}};
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
 // input fields in map order
@@ -792,10 +796,12 @@ __device__ __forceinline__ void init_ctx(Ctx<T, TX, TY, TRIM> &c, const Geom &g,
     c.bnd_y = c.j0 == 1 || c.j0 + TY >= c.n1 + 1;
 }
 
-template <typename T, int TX, int TY>
+// TRIMK: the kernel holds the trimmed path for interior columns (shapes without it keep
+// one plane-march body, as small as before trimming existed)
+template <typename T, int TX, int TY, bool TRIMK>
 __global__ void __launch_bounds__(Layout<T, TX, TY>::NT, Layout<T, TX, TY>::MINB)
     fused3d_kernel(Geom g, KParams p, TConst<T> q, Ptrs<T> in, Ptrs<T> out, const __grid_constant__ InMaps maps, int zb,
-                   int trim, TileMap tm, int *err) {
+                   TileMap tm, int *err) {
     using Lay = Layout<T, TX, TY>;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     // the grid is padded to whole clusters: columns past the vertex range have no work
@@ -808,13 +814,15 @@ __global__ void __launch_bounds__(Layout<T, TX, TY>::NT, Layout<T, TX, TY>::MINB
     __syncthreads();
     Ctx<T, TX, TY, false> c;
     init_ctx(c, g, p, smem_raw, zb, tm);
-    if (trim && !c.bnd_x && !c.bnd_y) {
-        Ctx<T, TX, TY, true> ct;
-        init_ctx(ct, g, p, smem_raw, zb, tm);
-        sweep(ct, p, q, in, out, maps, bars, err);
-    } else {
-        sweep(c, p, q, in, out, maps, bars, err);
+    if constexpr (TRIMK) {
+        if (!c.bnd_x && !c.bnd_y) {
+            Ctx<T, TX, TY, true> ct;
+            init_ctx(ct, g, p, smem_raw, zb, tm);
+            sweep(ct, p, q, in, out, maps, bars, err);
+            return;
+        }
     }
+    sweep(c, p, q, in, out, maps, bars, err);
 }
 
 template <typename T, int TX, int TY>
@@ -823,12 +831,12 @@ cudaError_t launch_variant(const Geom &g, const KParams &p, const Ptrs<T> &in, c
     using Lay = Layout<T, TX, TY>;
     int dev = 0;
     cudaGetDevice(&dev);
-    static bool attr_set[64] = {};
-    if (dev < 64 && !attr_set[dev]) {
-        cudaError_t e =
-            cudaFuncSetAttribute(fused3d_kernel<T, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lay::SMEM);
+    static bool attr_set[2][64] = {};
+    if (dev < 64 && !attr_set[v.trim][dev]) {
+        cudaError_t e = cudaFuncSetAttribute(v.trim ? fused3d_kernel<T, TX, TY, true> : fused3d_kernel<T, TX, TY, false>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lay::SMEM);
         if (e != cudaSuccess) return e;
-        attr_set[dev] = true;
+        attr_set[v.trim][dev] = true;
     }
     auto up = [](int a, int b) { return (a + b - 1) / b * b; };
     TileMap tm{-1, 0, 1 << 30, 0};
@@ -869,7 +877,8 @@ cudaError_t launch_variant(const Geom &g, const KParams &p, const Ptrs<T> &in, c
         cfg.numAttrs = 1;
     }
     const TConst<T> q = make_tconst<T>(p);
-    return cudaLaunchKernelEx(&cfg, fused3d_kernel<T, TX, TY>, g, p, q, in, out, maps, v.zb, v.trim, tm, err);
+    if (v.trim) return cudaLaunchKernelEx(&cfg, fused3d_kernel<T, TX, TY, true>, g, p, q, in, out, maps, v.zb, tm, err);
+    return cudaLaunchKernelEx(&cfg, fused3d_kernel<T, TX, TY, false>, g, p, q, in, out, maps, v.zb, tm, err);
 }
 
 template <typename T>

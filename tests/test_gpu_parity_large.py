@@ -44,7 +44,7 @@ def slab_pair(n, dtype, library, variant_name=None):
     return p
 
 
-@pytest.mark.parametrize("variant", ["tile32x8_zb32", "tile32x8_zb32_trim_cl2x2"])
+@pytest.mark.parametrize("variant", ["tile32x8_zb32", "tile32x8_zb32_trim_cl1x4"])
 @pytest.mark.parametrize("library", ["fast", "strict"])
 def test_slab_255_fp64(variant, library):
     p = slab_pair(255, "f64", library, variant)
@@ -59,7 +59,7 @@ def test_slab_255_fp64(variant, library):
         assert max(err.values()) <= 1e-10, err
 
 
-@pytest.mark.parametrize("variant", ["tile32x8_zb32", "tile64x8_zb32_trim", "tile64x4_zb32_trim_cl2x2"])
+@pytest.mark.parametrize("variant", ["tile32x8_zb32", "tile64x8_zb32_trim", "tile32x8_zb32_cl2x2"])
 def test_slab_255_fp32_strict(variant):
     p = slab_pair(255, "f32", "strict", variant)
     p.advance(3)
@@ -79,7 +79,10 @@ def glacier_pair(n, dtype, library):
     dem_grid, bed, surf, _ = fi.scenarios.bed_dems(0, n)
     dx = grid.spacing()
     exp = O.levelset_from_dem((n, n, n), grid.origin, dx, dem_grid.dims, dem_grid.origin, dem_grid.spacing(), surf)
-    assert np.array_equal(exp, psi_na)
+    if library == "strict":
+        assert np.array_equal(exp, psi_na)
+    else:  # FMA contraction in the distance arithmetic
+        assert np.max(np.abs(exp - psi_na)) <= 1e-12 * np.max(np.abs(exp))
     trac = ("traction", (0.0, 0.0, 0.0))
     return Pair((n, n, n), ((trac, trac), (trac, trac), (trac, trac)), path="reference", library=library, dtype=dtype,
                 rheo={"kind": "linear", "eta": 1.0}, gravity=(0.0, 0.0, 1.0), extent=(1.0, 1.0, 1.0),
