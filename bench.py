@@ -506,6 +506,9 @@ def run_mixed(args):
     rheo, eta0, rdesc, pt = glacier_rheology(fi, args.rheology)
     if args.scenario == "mms":
         eta0 = 1.0
+    if args.scenario == "glacier" and args.rheology == "glen":
+        eta0 = 1.0  # the continuation starts from the linear problem
+        rdesc += "; solved by continuation: linear, then the cap 10, 100, 1000, 5000 (PT velocity step /4 from 1000)"
     for mode in ("plain", "mixed"):
         if args.scenario == "mms":
             grid, m = scenarios.mms3d_model(n)
@@ -525,10 +528,17 @@ def run_mixed(args):
         m.apply_bcs()
         m.synchronize()
         t0 = time.perf_counter()
-        r = m.solve(mode=mode, **kw)
+        if args.scenario == "glacier" and args.rheology == "glen":
+            # Glen's law needs a continuation: linear, then the viscosity cap raised stage by stage
+            stages = scenarios.glacier_glen_stages(grid, tol=tol)
+            r = m.solve_continuation(stages, mode=mode, **{k: v for k, v in kw.items() if k != "tol"})
+        else:
+            r = m.solve(mode=mode, **kw)
         sec = time.perf_counter() - t0
         res[mode] = {"seconds": sec, "iterations": r["iterations"], "outer": r["outer"], "measure": r["measure"],
                      "converged": bool(r["converged"]), "V": [m.get_field(c) for c in ("Vx", "Vy", "Vz")]}
+        if "stages" in r:
+            res[mode]["stages"] = r["stages"]
         if args.scenario == "mms":
             res[mode]["mms_l2_error"] = scenarios.mms3d_error(grid, m)
         m.close()
@@ -560,7 +570,7 @@ def glacier_rheology(fi, kind):
     if kind in ("glen", "glen_relaxed"):
         r = fi.glen_regularised(A=1.0, n=3, strain_rate_0=1e-6)
         eta0 = r.eta_reg
-        desc = "Glen n=3, A=1, regularised at strain rate 1e-6"
+        desc = "Glen n=3, A=1, regularised at strain rate 1e-6 (viscosity cap 5000)"
         if kind == "glen_relaxed":
             r = fi.Relaxation(r, 0.1, scale="log")
             desc += ", relaxed in log scale at rate 0.1"

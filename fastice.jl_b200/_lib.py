@@ -126,6 +126,7 @@ SIGNATURES = [
     ("fi_model_set_field", C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_size_t]),
     ("fi_model_get_field", C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_size_t]),
     ("fi_model_copy_field", C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
+    ("fi_model_set_params", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("fi_model_field_size", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_size_t)]),
     ("fi_model_apply_bcs", C.c_int, [C.c_void_p]),
     ("fi_model_advance", C.c_int, [C.c_void_p, C.c_int32]),

@@ -561,6 +561,23 @@ fi_status model_ensure_second_state(fi_model *m) {
 // An overlapped iteration (fi_model_advance_begin / _end) leaves its second half
 // on the model's second stream: every other entry point first orders the model's
 // stream after it, and refuses to run between the two halves.
+// the rheology and PT-step parameters of a model (set at creation and by fi_model_set_params)
+static void set_rheology_dtau(KParams &kp, const fi_rheology &r, const fi_pt_params &dt) {
+    kp.dt_P = dt.dt_P;
+    for (int k = 0; k < 6; k++) kp.dt_tau[k] = dt.dt_tau[k];
+    for (int k = 0; k < 3; k++) kp.dt_V[k] = dt.dt_V[k];
+    kp.rheo_inner = r.inner;
+    kp.rheo_eta_is_field = r.eta_is_field;
+    kp.rheo_A_is_field = r.A_is_field;
+    kp.rheo_n = r.n;
+    kp.rheo_has_reg = r.has_reg;
+    kp.rheo_relax = r.relax;
+    kp.rheo_eta = r.eta;
+    kp.rheo_A = r.A;
+    kp.rheo_inv_eta_reg = r.has_reg ? 1.0 / r.eta_reg : 0.0;  // Physics.jl:22 stores one(η_reg)/η_reg
+    kp.rheo_rate = r.rate;
+}
+
 static fi_status join_overlap(fi_model *m) {
     if (m->split_begun >= 0)
         return set_error("an overlapped iteration is begun: call fi_model_advance_end first"), FI_ERR_STATE;
@@ -638,24 +655,11 @@ fi_status fi_model_create(const fi_model_desc *desc, fi_model **out) {
 
     KParams &kp = m->kp;
     for (int k = 0; k < 3; k++) kp.inv_dx[k] = k < gr.nd ? 1.0 / (gr.extent[k] / gr.n[k]) : 0.0;
-    kp.dt_P = desc->dtau.dt_P;
-    for (int k = 0; k < 6; k++) kp.dt_tau[k] = desc->dtau.dt_tau[k];
-    for (int k = 0; k < 3; k++) kp.dt_V[k] = desc->dtau.dt_V[k];
     for (int k = 0; k < 3; k++) {
         kp.g_kind[k] = desc->gravity.kind[k];
         kp.g_val[k] = desc->gravity.value[k];
     }
-    const fi_rheology &r = desc->rheology;
-    kp.rheo_inner = r.inner;
-    kp.rheo_eta_is_field = r.eta_is_field;
-    kp.rheo_A_is_field = r.A_is_field;
-    kp.rheo_n = r.n;
-    kp.rheo_has_reg = r.has_reg;
-    kp.rheo_relax = r.relax;
-    kp.rheo_eta = r.eta;
-    kp.rheo_A = r.A;
-    kp.rheo_inv_eta_reg = r.has_reg ? 1.0 / r.eta_reg : 0.0;  // Physics.jl:22 stores one(η_reg)/η_reg
-    kp.rheo_rate = r.rate;
+    set_rheology_dtau(kp, desc->rheology, desc->dtau);
     for (int k = 0; k < 3; k++)
         for (int s = 0; s < 2; s++) {
             kp.bc_kind[k][s] = k < gr.nd ? desc->bc[k][s].kind : FI_BC_TRACTION;
@@ -825,6 +829,33 @@ fi_status fi_model_advance(fi_model *m, int32_t niter) {
     if (fi_status js = join_overlap(m); js != FI_OK) return js;
     FI_CHECK_CUDA(cudaSetDevice(m->d.device), "cudaSetDevice");
     return m->is_f64() ? advance_t<double>(m, niter) : advance_t<float>(m, niter);
+}
+
+fi_status fi_model_set_params(fi_model *m, const fi_rheology *rheology, const fi_pt_params *dtau) {
+    if (!m || !rheology || !dtau) return set_error("bad argument"), FI_ERR_ARG;
+    if (fi_status js = join_overlap(m); js != FI_OK) return js;
+    const fi_rheology &r = *rheology, &o = m->d.rheology;
+    // the fields a rheology reads were allocated for the model's own kinds
+    if (r.eta_is_field != o.eta_is_field || r.A_is_field != o.A_is_field)
+        return set_error("the new rheology must read the same fields (η, A) as the model's"), FI_ERR_ARG;
+    if (r.inner != FI_RHEO_LINEAR && r.inner != FI_RHEO_POWER) return set_error("unknown rheology"), FI_ERR_ARG;
+    if (r.has_reg && !(r.eta_reg > 0.0)) return set_error("the regularisation viscosity must be positive"), FI_ERR_ARG;
+    FI_CHECK_CUDA(cudaSetDevice(m->d.device), "cudaSetDevice");
+    FI_CHECK_CUDA(cudaStreamSynchronize(m->stream), "sync");
+    m->d.rheology = r;
+    m->d.dtau = *dtau;
+    set_rheology_dtau(m->kp, r, *dtau);
+    m->full_iters = 0;  // the viscosity far from the ice may change: every point runs again
+    if (m->shadow) {
+        // the FP32 shadow of the mixed-precision solve follows (its base parameters too)
+        fi_model *s = m->shadow;
+        s->d.rheology = r;
+        s->d.dtau = *dtau;
+        set_rheology_dtau(s->kp, r, *dtau);
+        set_rheology_dtau(m->shadow_kp, r, *dtau);
+        s->full_iters = 0;
+    }
+    return FI_OK;
 }
 
 fi_status fi_model_advance_begin(fi_model *m, int32_t dim) {

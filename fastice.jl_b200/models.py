@@ -238,6 +238,40 @@ class _StokesBase:
         L.check(self.lib, self.lib.fi_model_get_field(self._h, L.FIELD_ID[name], arr.ctypes.data, arr.nbytes))
         return arr
 
+    def set_params(self, rheology: IceRheology = None, solver_params: dict = None) -> None:
+        """New rheology and/or PT steps for the next iterations (fi_model_set_params);
+        the state is kept.  The rheology must read the same fields as the model's."""
+        rheology = self.rheology if rheology is None else rheology
+        solver_params = self.solver_params if solver_params is None else solver_params
+        rdesc, rfields = rheology_desc(rheology)
+        if rfields:
+            raise ValueError("set_params takes rheologies without field inputs; upload fields with set_field")
+        dt = _dtau(solver_params, self.grid.ndims)
+        L.check(self.lib, self.lib.fi_model_set_params(self._h, C.byref(rdesc), C.byref(dt)))
+        self.rheology, self.solver_params = rheology, solver_params
+
+    def solve_continuation(self, stages, **solve_kw) -> dict:
+        """A continuation driver: for each stage (rheology, solver_params, tol) set the
+        parameters and solve to that stage's tolerance from the previous stage's state
+        (e.g. a viscosity cap raised stage by stage for Glen's law).  Returns the last
+        stage's report with the sweeps, outer steps and seconds of every stage summed."""
+        total = {"iterations": 0, "outer": 0, "seconds": 0.0, "stages": []}
+        rep = None
+        for rheology, solver_params, tol in stages:
+            self.set_params(rheology, solver_params)
+            rep = self.solve(tol=tol, **solve_kw)
+            total["iterations"] += rep["iterations"]
+            total["outer"] += rep["outer"]
+            total["seconds"] += rep["seconds"]
+            total["stages"].append({"tol": tol, "iterations": rep["iterations"], "measure": rep["measure"],
+                                    "converged": rep["converged"]})
+            if not rep["converged"]:
+                break
+        out = dict(rep)
+        out.update(iterations=total["iterations"], outer=total["outer"], seconds=total["seconds"],
+                   stages=total["stages"])
+        return out
+
     def copy_field(self, dst: str, src: str) -> None:
         """set!(dst, src) on the device between two fields at the same location
         (e.g. η_next from η), ghosts included."""

@@ -162,6 +162,27 @@ def bed_levelsets(seed: int, n: int, library: str = "fast", dem_cells=None):
     return grid, psi_na, psi_ns, prm
 
 
+def glacier_glen_stages(grid, tol: float = 1e-8, stage_tol: float = 1e-6, n: int = 3, A: float = 1.0,
+                        cap: float = 5000.0):
+    """Continuation stages for Glen's law on the glacier (stages for
+    ``solve_continuation``): the linear solution with the glacier driver's PT steps,
+    then the regularised power law with its viscosity cap raised 10 -> 100 -> 1000 ->
+    ``cap`` (5000: the Glen viscosity at the strain rate 1e-6), each stage to
+    ``stage_tol`` and the last to ``tol``; from the cap of 1000 on, the velocity PT
+    step is four times smaller (factor 4.4 instead of 1.1), without which those
+    stages diverge (measured at 127^3).  The reference's PT iteration started from
+    rest with the cap of 5000 diverges on this geometry."""
+    from .physics import PowerLawRheology, ViscoplasticRegularisation
+    r, re = 0.9, 5 * math.pi
+    sp = lambda f: pt_params(grid, r=r, re_mech=re, vdtau_factor=f)
+    caps = [c for c in (10.0, 100.0, 1000.0) if c < cap] + [cap]
+    stages = [(LinearViscousRheology(1.0), sp(1.1), stage_tol)]
+    for c in caps:
+        stages.append((ViscoplasticRegularisation(PowerLawRheology(A, n), c), sp(1.1 if c < 1000.0 else 4.4),
+                       tol if c == caps[-1] else stage_tol))
+    return stages
+
+
 def bed_params(seed: int, n: int, bumps: int = 64):
     """Seeded bed of ``bumps`` Gaussian bumps a·exp(-|x-c|^2/w^2), a~U(0,0.2),
     w~U(0.05,0.2), c~U([0,1]^2), and the surface z = 0.6 + 0.05 sin(2πx)."""
@@ -291,4 +312,5 @@ def mms3d_error(grid, m) -> float:
 
 
 __all__ = ["mms2d_gravity", "mms2d_exact", "mms2d_model", "mms2d_error", "mms3d_gravity", "mms3d_exact", "mms3d_model", "mms3d_error", "inclusion_params", "inclusion_viscosity", "inclusion_model", "smooth_log", "stiffness_ratio",
-           "bed_model", "bed_params", "bed_height", "bed_dems", "bed_levelsets", "INCLUSION_N_RANGE"]
+           "bed_model", "bed_params", "bed_height", "bed_dems", "bed_levelsets", "glacier_glen_stages",
+           "INCLUSION_N_RANGE"]

@@ -167,6 +167,13 @@ fi_status fi_model_copy_field(fi_model *m, int32_t dst, int32_t src);
 /* interior element count of a field (n or n+1 per dim by location) */
 fi_status fi_model_field_size(const fi_model *m, int32_t field, size_t *count);
 
+/* New rheology parameters and PT steps for the next iterations (the model's
+ * `rheology` and `solver_params`, Isothermal.jl:27-35; a continuation driver changes
+ * them between solves, e.g. raising a viscosity cap stage by stage).  The new
+ * rheology must read the same fields as the model's (eta_is_field, A_is_field); the
+ * state is kept; the mixed-precision shadow, if any, follows. */
+fi_status fi_model_set_params(fi_model *m, const fi_rheology *rheology, const fi_pt_params *dtau);
+
 /* Ghost fill that drivers do after set!: stress and velocity BC batches and
  * Neumann on η / η_next (tm_stokes_chmy.jl:273-281). */
 fi_status fi_model_apply_bcs(fi_model *m);

@@ -84,3 +84,30 @@ def test_mixed_glacier_matches_fp64_solve():
         assert d < 1e-6, (name, d)
     plain.close()
     mixed.close()
+
+
+def test_glen_glacier_continuation_plain_and_mixed():
+    # Glen's law on the glacier by continuation (linear, then the viscosity cap raised
+    # 10 -> 100 -> 1000 -> 5000): both the plain FP64 and the mixed-precision solve
+    # reach the relative residual 1e-8 and agree
+    fi = load_fastice()
+    from fastice_b200 import scenarios
+    n = 47
+    out = {}
+    for mode in ("plain", "mixed"):
+        m, _ = scenarios.bed_model(0, n, rheology=fi.glen_regularised())
+        m.set_field("eta", 1.0)
+        m.set_field("eta_next", 1.0)
+        m.apply_bcs()
+        stages = scenarios.glacier_glen_stages(m.grid, tol=1e-8)
+        r = m.solve_continuation(stages, mode=mode, max_iter=2000 * n, ncheck=n, measure="rel_slab", rho_g_inf=1.0,
+                                 length_z=0.6)
+        assert r["converged"] and r["measure"] < 1e-8, (mode, r)
+        assert len(r["stages"]) == 5
+        out[mode] = [m.get_field(c) for c in ("Vx", "Vy", "Vz")]
+        eta = m.get_field("eta")
+        assert eta.max() <= 5000.0 and eta.min() > 0.0
+        m.close()
+    vmax = max(np.max(np.abs(v)) for v in out["plain"])
+    dv = max(np.max(np.abs(a - b)) for a, b in zip(out["mixed"], out["plain"]))
+    assert dv <= 1e-6 * vmax, dv / vmax
