@@ -8,7 +8,7 @@ from . import _lib
 from ._lib import FastIceError
 from .grids import Center, UniformGrid, Vertex, flip
 from .levelsets import compute_levelset_from_dem, omega_from_psi
-from .models import (Arch, BatchedStokes2D, FieldRef, IsothermalFullStokesModel, IsothermalImmersedBoundaryFullStokesModel,
+from .models import (Arch, BatchedIB3D, BatchedStokes2D, FieldRef, IsothermalFullStokesModel, IsothermalImmersedBoundaryFullStokesModel,
                      advance_iteration, compute_residuals, interior, pt_params, set_)
 from .physics import (ArrayField, BoundaryCondition, ConstantField, FunctionField, LinearViscousRheology, OneField,
                       PBC, Periodic, PowerLawRheology, Relaxation, SBC, Slip, TBC, Traction, VBC, ValueField, Velocity,
@@ -20,7 +20,7 @@ from .heat import HeatDiffusionModel  # noqa: E402
 from .writers import write_h5, write_xdmf  # noqa: E402
 
 __all__ = [
-    "FastIceError", "BatchedStokes2D", "Center", "Vertex", "UniformGrid", "flip", "compute_levelset_from_dem", "omega_from_psi", "Arch",
+    "FastIceError", "BatchedIB3D", "BatchedStokes2D", "Center", "Vertex", "UniformGrid", "flip", "compute_levelset_from_dem", "omega_from_psi", "Arch",
     "FieldRef", "IsothermalFullStokesModel", "IsothermalImmersedBoundaryFullStokesModel", "advance_iteration",
     "compute_residuals", "interior", "pt_params", "set_", "ArrayField", "BoundaryCondition", "ConstantField",
     "FunctionField", "LinearViscousRheology", "OneField", "PBC", "Periodic", "PowerLawRheology", "Relaxation", "SBC",

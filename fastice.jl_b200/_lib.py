@@ -161,6 +161,13 @@ SIGNATURES = [
                                  C.POINTER(C.c_double)]),
     ("fi_batch_measure", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     ("fi_batch_solve_mixed", C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.POINTER(C.c_double)]),
+    ("fi_ib_batch_create", C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_void_p)]),
+    ("fi_ib_batch_destroy", C.c_int, [C.c_void_p]),
+    ("fi_ib_batch_add", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("fi_ib_batch_remove", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("fi_ib_batch_size", C.c_int32, [C.c_void_p]),
+    ("fi_ib_batch_advance", C.c_int, [C.c_void_p, C.c_int32]),
+    ("fi_ib_batch_synchronize", C.c_int, [C.c_void_p]),
     ("fi_batch_variant_count", C.c_int, []),
     ("fi_batch_variant_name", C.c_char_p, [C.c_int32]),
     ("fi_batch_set_variant", C.c_int, [C.c_void_p, C.c_int32]),

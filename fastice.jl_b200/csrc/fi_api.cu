@@ -536,6 +536,10 @@ bool fused_ok(const fi_model *m) {
 
 }  // namespace
 
+BcBatch model_stress_batch(const fi_model *m, int d) { return stress_batch(m, d); }
+BcBatch model_velocity_batch(const fi_model *m, int d) { return velocity_batch(m, d); }
+fi_status model_refresh_ibf(fi_model *m) { return m->is_f64() ? refresh_ibf<double>(m) : refresh_ibf<float>(m); }
+
 // Second state buffer of every state field, for drivers that double-buffer a
 // model whose own path updates in place (the batched 2D sweep); a new buffer
 // starts as a copy of the current state, ghosts included.

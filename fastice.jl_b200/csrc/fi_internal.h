@@ -134,6 +134,20 @@ struct BlockList {
     int count;
 };
 
+// one model of a batched immersed-boundary launch: geometry, parameters and the field
+// pointers for both roles of its η buffers (f[0]: as when the batch table was built)
+template <typename T>
+struct IbMember {
+    Geom g;
+    KParams p;
+    Ptrs<T> f[2];
+};
+// one model's boundary batch of one dimension, for a batched boundary launch
+struct BcMember {
+    Geom g;
+    BcBatch b;
+};
+
 // ---- launchers implemented in fi_reference.cu ----
 // bl: run only the listed blocks (immersed boundary with KParams::skip_zeros);
 // nullptr: the whole vertex-range grid
@@ -162,6 +176,20 @@ template <typename T>
 cudaError_t launch_residual_norms(const Geom &g, const KParams &p, const Ptrs<T> &f, bool ib, double *partials,
                                   int nblocks, double *out_dev, cudaStream_t s);
 int norm_blocks(const Geom &g);
+// batched immersed-boundary update_σ! (velocity false) or update_V! (true) over work
+// items (member, block x | block y << 16, block z, 0)
+template <typename T>
+cudaError_t launch_ib_batched(const IbMember<T> *members, const uint4 *items, int nitems, int epar, bool velocity,
+                              cudaStream_t s);
+// batched boundary batches of one dimension; max_a / max_c: the largest face extents
+// (storage sizes of the two other dimensions) over the members
+template <typename T>
+cudaError_t launch_bc_batched(const BcMember *list, int count, int max_a, int max_c, cudaStream_t s);
+// work items of member q: its whole block grid (full) or its block list
+cudaError_t launch_ib_items(const Geom &g, bool full, const uint2 *list, int count, unsigned q, uint4 *out, bool f32,
+                            cudaStream_t s);
+long long ib_grid_blocks(const Geom &g, bool f32);
+void bc_set_serial(const Geom &g, BcBatch &b);
 
 // ---- fused 3D sweep (fi_fused3d.cu) ----
 // P,tau,V read from `in`, written to `out`; eta read from in.eta, eta_next written.

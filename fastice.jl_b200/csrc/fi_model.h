@@ -133,6 +133,11 @@ fi_status mixed_phase_a_end(fi_model *m);
 fi_status mixed_picard(fi_model *m);
 fi_status mixed_correction_begin(fi_model *m);
 fi_status mixed_correction_end(fi_model *m);
+// the boundary batches of the reference-shaped iteration (fi_api.cu) and the refresh of
+// an immersed-boundary model's activity bytes and block list when stale
+fi::BcBatch model_stress_batch(const fi_model *m, int d);
+fi::BcBatch model_velocity_batch(const fi_model *m, int d);
+fi_status model_refresh_ibf(fi_model *m);
 // allocates the second buffer of every state field a model lacks (fi_api.cu)
 fi_status model_ensure_second_state(fi_model *m);
 // whether the model stores field f (fi_api.cu)

@@ -7,6 +7,8 @@
 // operation (same grouping of sums and products), so a build without FMA
 // contraction reproduces the CPU oracle bit for bit.  They serve as the
 // FI_PATH_REFERENCE path and for the shapes the fused sweep does not cover.
+#include <algorithm>
+
 #include "fi_device.cuh"
 
 namespace fi {
@@ -73,12 +75,7 @@ struct IbRow {
     int i, j, k;  // its position
 };
 
-__device__ __forceinline__ IbRow ib_row(const Geom &g, const BlockList &bl, int C) {
-    unsigned bx = blockIdx.x, by = blockIdx.y, bz = blockIdx.z;
-    if (bl.ids) {
-        const uint2 b = bl.ids[blockIdx.x];
-        bx = b.x & 0xffffu, by = b.x >> 16, bz = b.y;
-    }
+__device__ __forceinline__ IbRow ib_row_at(const Geom &g, unsigned bx, unsigned by, unsigned bz, int C) {
     IbRow r;
     r.i = bx * (32 * C) + threadIdx.x + 1;
     r.j = by * blockDim.y + threadIdx.y + 1;
@@ -87,13 +84,21 @@ __device__ __forceinline__ IbRow ib_row(const Geom &g, const BlockList &bl, int 
     return r;
 }
 
+__device__ __forceinline__ IbRow ib_row(const Geom &g, const BlockList &bl, int C) {
+    unsigned bx = blockIdx.x, by = blockIdx.y, bz = blockIdx.z;
+    if (bl.ids) {
+        const uint2 b = bl.ids[blockIdx.x];
+        bx = b.x & 0xffffu, by = b.x >> 16, bz = b.y;
+    }
+    return ib_row_at(g, bx, by, bz, C);
+}
+
 dim3 ib_grid(const Geom &g, int C) {
     return dim3((g.n[0] + 1 + 32 * C - 1) / (32 * C), (g.n[1] + 1 + 7) / 8, g.n[2] + 1);
 }
 
 template <typename T, int C>
-__global__ void __launch_bounds__(256) ib_sigma_kernel(Geom g, KParams p, Ptrs<T> f, BlockList bl) {
-    const IbRow r = ib_row(g, bl, C);
+__device__ __forceinline__ void ib_sigma_body(const Geom &g, const KParams &p, const Ptrs<T> &f, const IbRow &r) {
     if (r.i > g.n[0] + 1 || r.j > g.n[1] + 1) return;
     const long long sx = g.pitch, sxy = g.sxy;
     const T idx = T(p.inv_dx[0]), idy = T(p.inv_dx[1]), idz = T(p.inv_dx[2]);
@@ -207,11 +212,13 @@ __global__ void __launch_bounds__(256) ib_sigma_kernel(Geom g, KParams p, Ptrs<T
     }
 }
 
-// resident blocks per SM asked of the compiler: 6 (40 registers) for one point
-// per thread, 4 (64) for two
 template <typename T, int C>
-__global__ void __launch_bounds__(256, C == 1 ? 6 : 4) ib_V_kernel(Geom g, KParams p, Ptrs<T> f, BlockList bl) {
-    const IbRow r = ib_row(g, bl, C);
+__global__ void __launch_bounds__(256) ib_sigma_kernel(Geom g, KParams p, Ptrs<T> f, BlockList bl) {
+    ib_sigma_body<T, C>(g, p, f, ib_row(g, bl, C));
+}
+
+template <typename T, int C>
+__device__ __forceinline__ void ib_V_body(const Geom &g, const KParams &p, const Ptrs<T> &f, const IbRow &r) {
     if (r.i > g.n[0] + 1 || r.j > g.n[1] + 1) return;
     const long long sx = g.pitch, sxy = g.sxy;
     const T idx = T(p.inv_dx[0]), idy = T(p.inv_dx[1]), idz = T(p.inv_dx[2]);
@@ -324,6 +331,67 @@ __global__ void __launch_bounds__(256, C == 1 ? 6 : 4) ib_V_kernel(Geom g, KPara
 #pragma unroll
     for (int c = 0; c < C; c++)
         if (ok[c]) f.eta_next[r.I + 32 * c] = en[c];
+}
+
+// resident blocks per SM asked of the compiler: 6 (40 registers) for one point
+// per thread, 4 (64) for two
+template <typename T, int C>
+__global__ void __launch_bounds__(256, C == 1 ? 6 : 4) ib_V_kernel(Geom g, KParams p, Ptrs<T> f, BlockList bl) {
+    ib_V_body<T, C>(g, p, f, ib_row(g, bl, C));
+}
+
+// ---------------------------------------------------------------------------
+// Batched immersed-boundary updates: one launch runs the blocks of several
+// models.  Work item = (member, block x | block y << 16, block z); the block
+// copies its member's geometry, parameters and field pointers into shared
+// memory and runs the same body as the single-model kernel, so each member's
+// arithmetic is exactly its own model's.  epar picks the member's η roles for
+// this iteration (f[0]: as when the table was built, f[1]: swapped).
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ const IbMember<T> &ib_member_smem(const IbMember<T> *members, unsigned q,
+                                                              IbMember<T> *sm) {
+    constexpr int W = (int)(sizeof(IbMember<T>) / 4);
+    const unsigned *src = reinterpret_cast<const unsigned *>(members + q);
+    unsigned *dst = reinterpret_cast<unsigned *>(sm);
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+    for (int w = tid; w < W; w += blockDim.x * blockDim.y) dst[w] = __ldg(src + w);
+    __syncthreads();
+    return *sm;
+}
+
+template <typename T, int C>
+__global__ void __launch_bounds__(256) ib_sigma_batched(const IbMember<T> *members, const uint4 *items, int epar) {
+    __shared__ __align__(16) IbMember<T> sm;
+    const uint4 it = items[blockIdx.x];
+    const IbMember<T> &m = ib_member_smem(members, it.x, &sm);
+    ib_sigma_body<T, C>(m.g, m.p, m.f[epar], ib_row_at(m.g, it.y & 0xffffu, it.y >> 16, it.z, C));
+}
+
+template <typename T, int C>
+__global__ void __launch_bounds__(256, C == 1 ? 5 : 4) ib_V_batched(const IbMember<T> *members, const uint4 *items,
+                                                                     int epar) {
+    __shared__ __align__(16) IbMember<T> sm;
+    const uint4 it = items[blockIdx.x];
+    const IbMember<T> &m = ib_member_smem(members, it.x, &sm);
+    ib_V_body<T, C>(m.g, m.p, m.f[epar], ib_row_at(m.g, it.y & 0xffffu, it.y >> 16, it.z, C));
+}
+
+// the work items of one member: its block list (uint2 x | y << 16, z) with the member index
+__global__ void ib_items_from_list(const uint2 *list, int count, unsigned q, uint4 *out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const uint2 b = list[i];
+        out[i] = make_uint4(q, b.x, b.y, 0u);
+    }
+}
+// or its whole grid of blocks (nbx x nby x nbz)
+__global__ void ib_items_full(int nbx, int nby, int nbz, unsigned q, uint4 *out) {
+    const long long total = (long long)nbx * nby * nbz;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const unsigned bx = (unsigned)(i % nbx), by = (unsigned)((i / nbx) % nby), bz = (unsigned)(i / ((long long)nbx * nby));
+        out[i] = make_uint4(q, bx | (by << 16), bz, 0u);
+    }
 }
 
 template <typename T, int ND>
@@ -612,7 +680,7 @@ __global__ void __launch_bounds__(256) compute_tau_ib_kernel(Geom g, KParams p, 
 // otherwise (b.serial) one thread applies them all in the batch's order.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void bc_dim_kernel(Geom g, BcBatch b) {
+__device__ __forceinline__ void bc_dim_body(const Geom &g, const BcBatch &b, int opz) {
     const int d = b.dim;
     int e1 = -1, e2 = -1;
     for (int e = 0; e < g.nd; e++) {
@@ -626,7 +694,7 @@ __global__ void bc_dim_kernel(Geom g, BcBatch b) {
     if (e2 >= 0 && c > g.n[e2] + 2) return;
     if (e2 < 0 && c > 0) return;
     const long long st[3] = {1, g.pitch, g.sxy};
-    const int q0 = b.serial ? 0 : (int)blockIdx.z, q1 = b.serial ? b.count : q0 + 1;
+    const int q0 = b.serial ? 0 : opz, q1 = b.serial ? b.count : q0 + 1;
     for (int q = q0; q < q1; q++) {
         const BcOpDesc &op = b.ops[q];
         // range check for the other dims
@@ -674,6 +742,21 @@ __global__ void bc_dim_kernel(Geom g, BcBatch b) {
         }
 #undef A
     }
+}
+
+template <typename T>
+__global__ void bc_dim_kernel(Geom g, BcBatch b) {
+    bc_dim_body<T>(g, b, (int)blockIdx.z);
+}
+
+// the boundary batch of one dimension for several models: grid slice z = member *
+// kMaxBcOps + op (a serial batch runs its ops in slice op 0)
+template <typename T>
+__global__ void bc_dim_batched(const BcMember *list) {
+    const int q = (int)blockIdx.z / kMaxBcOps, op = (int)blockIdx.z % kMaxBcOps;
+    const BcMember &m = list[q];
+    if (op >= (m.b.serial ? 1 : m.b.count)) return;
+    bc_dim_body<T>(m.g, m.b, op);
 }
 
 // ---------------------------------------------------------------------------
@@ -913,6 +996,17 @@ cudaError_t launch_compute_tau(const Geom &g, const KParams &p, const Ptrs<T> &f
     return cudaGetLastError();
 }
 
+// whether the ops of a batch must run in order by one thread (a dimension of fewer
+// than 3 cells, or two ops on one field whose faces may meet)
+void bc_set_serial(const Geom &g, BcBatch &b) {
+    b.serial = g.n[b.dim] < 3;
+    for (int q = 0; q < b.count && !b.serial; q++)
+        for (int r = 0; r < q; r++)
+            if (b.ops[r].f == b.ops[q].f &&
+                (b.ops[r].side == b.ops[q].side || b.ops[r].op == BC_PERIODIC || b.ops[q].op == BC_PERIODIC))
+                b.serial = 1;
+}
+
 template <typename T>
 cudaError_t launch_bc_batch(const Geom &g, const BcBatch &b, cudaStream_t s) {
     if (b.count == 0) return cudaSuccess;
@@ -924,12 +1018,7 @@ cudaError_t launch_bc_batch(const Geom &g, const BcBatch &b, cudaStream_t s) {
     }
     int na = g.n[e1] + 3, nc = e2 >= 0 ? g.n[e2] + 3 : 1;
     BcBatch bb = b;
-    bb.serial = g.n[b.dim] < 3;
-    for (int q = 0; q < b.count && !bb.serial; q++)
-        for (int r = 0; r < q; r++)
-            if (b.ops[r].f == b.ops[q].f &&
-                (b.ops[r].side == b.ops[q].side || b.ops[r].op == BC_PERIODIC || b.ops[q].op == BC_PERIODIC))
-                bb.serial = 1;
+    bc_set_serial(g, bb);
     dim3 blk(32, 8);
     dim3 grd((na + 31) / 32, (nc + 7) / 8, bb.serial ? 1 : b.count);
     bc_dim_kernel<T><<<grd, blk, 0, s>>>(g, bb);
@@ -951,6 +1040,41 @@ cudaError_t launch_residual_norms(const Geom &g, const KParams &p, const Ptrs<T>
     return cudaGetLastError();
 }
 
+template <typename T>
+cudaError_t launch_ib_batched(const IbMember<T> *members, const uint4 *items, int nitems, int epar, bool velocity,
+                              cudaStream_t s) {
+    if (nitems <= 0) return cudaSuccess;
+    constexpr int C = ib_points<T>();
+    if (velocity) ib_V_batched<T, C><<<nitems, dim3(32, 8), 0, s>>>(members, items, epar);
+    else ib_sigma_batched<T, C><<<nitems, dim3(32, 8), 0, s>>>(members, items, epar);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_bc_batched(const BcMember *list, int count, int max_a, int max_c, cudaStream_t s) {
+    if (count <= 0) return cudaSuccess;
+    dim3 blk(32, 8);
+    bc_dim_batched<T><<<dim3((max_a + 31) / 32, (max_c + 7) / 8, count * kMaxBcOps), blk, 0, s>>>(list);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ib_items(const Geom &g, bool full, const uint2 *list, int count, unsigned q, uint4 *out, bool f32,
+                            cudaStream_t s) {
+    if (full) {
+        const dim3 gr = ib_grid(g, f32 ? 2 : 1);
+        const long long total = (long long)gr.x * gr.y * gr.z;
+        ib_items_full<<<(int)std::min<long long>((total + 255) / 256, 4096), 256, 0, s>>>(gr.x, gr.y, gr.z, q, out);
+    } else if (count > 0) {
+        ib_items_from_list<<<std::min((count + 255) / 256, 4096), 256, 0, s>>>(list, count, q, out);
+    }
+    return cudaGetLastError();
+}
+
+long long ib_grid_blocks(const Geom &g, bool f32) {
+    const dim3 gr = ib_grid(g, f32 ? 2 : 1);
+    return (long long)gr.x * gr.y * gr.z;
+}
+
 #define FI_INST(T)                                                                                                \
     template cudaError_t launch_update_sigma<T>(const Geom &, const KParams &, const Ptrs<T> &, bool, cudaStream_t,   \
                                                 const BlockList *);                                               \
@@ -963,7 +1087,9 @@ cudaError_t launch_residual_norms(const Geom &g, const KParams &p, const Ptrs<T>
     template cudaError_t launch_bc_batch<T>(const Geom &, const BcBatch &, cudaStream_t);                          \
     template cudaError_t launch_ib_blocks<T>(const Geom &, const unsigned char *, uint2 *, int *, cudaStream_t);   \
     template cudaError_t launch_residual_norms<T>(const Geom &, const KParams &, const Ptrs<T> &, bool, double *,  \
-                                                  int, double *, cudaStream_t);
+                                                  int, double *, cudaStream_t);                                    \
+    template cudaError_t launch_ib_batched<T>(const IbMember<T> *, const uint4 *, int, int, bool, cudaStream_t);    \
+    template cudaError_t launch_bc_batched<T>(const BcMember *, int, int, int, cudaStream_t);
 FI_INST(double)
 FI_INST(float)
 #undef FI_INST

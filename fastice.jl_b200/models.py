@@ -414,6 +414,48 @@ class IsothermalImmersedBoundaryFullStokesModel(_StokesBase):
         L.check(self.lib, self.lib.fi_model_volfrac_from_levelset(self._h, {"na": 0, "ns": 1}[group], psi.ctypes.data))
 
 
+class BatchedIB3D:
+    """Several 3D immersed-boundary models advanced by shared launches
+    (fi_ib_batch_* in the C ABI): one iteration of every member is eight launches
+    whatever their number, and pairs of iterations replay as a CUDA graph.  Each
+    member's iteration is the one ``advance`` runs for it alone."""
+
+    def __init__(self, models=()):
+        models = list(models)
+        self.lib = models[0].lib if models else L.load()
+        self.models = []
+        arr = (C.c_void_p * max(1, len(models)))(*[m._h for m in models])
+        h = C.c_void_p()
+        L.check(self.lib, self.lib.fi_ib_batch_create(arr, len(models), C.byref(h)))
+        self._h = h
+        self.models = models
+
+    def add(self, m) -> None:
+        L.check(self.lib, self.lib.fi_ib_batch_add(self._h, m._h))
+        self.models.append(m)
+
+    def remove(self, m) -> None:
+        L.check(self.lib, self.lib.fi_ib_batch_remove(self._h, m._h))
+        self.models.remove(m)
+
+    def advance(self, niter: int) -> None:
+        L.check(self.lib, self.lib.fi_ib_batch_advance(self._h, int(niter)))
+
+    def synchronize(self) -> None:
+        L.check(self.lib, self.lib.fi_ib_batch_synchronize(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.fi_ib_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class BatchedStokes2D:
     """Many independent 2D models solved together (fi_batch_* in the C ABI).
 

@@ -374,6 +374,28 @@ const char *fi_batch_variant_name(int32_t variant);
 fi_status fi_batch_set_variant(fi_batch *b, int32_t variant);
 fi_status fi_batch_autotune(fi_batch *b, int32_t iters, int32_t *best, double *ms);
 
+/* ---- batched 3D immersed-boundary iterations ------------------------------------
+ * Several 3D immersed-boundary models (one dtype, one device, reference-shaped path)
+ * advanced by shared launches: one iteration of every member is eight launches --
+ * the masked update_σ! over a work list that concatenates the members' blocks (each
+ * member's block list once its stored zeros hold), the stress boundary batches of
+ * all members per dimension, the masked update_V!, the velocity boundary batches --
+ * and pairs of iterations replay as one CUDA graph.  Each member's iteration is the
+ * one fi_model_advance runs for it, so its result is the same alone or in the batch;
+ * a member whose state changed runs its first two full iterations alone.  The models
+ * must outlive the batch; after fi_ib_batch_advance each member's stream is ordered
+ * after the shared launches.  No counterpart in the reference, which runs one model
+ * per driver loop (scripts_future_API/tm_stokes_chmy.jl:283-305). */
+typedef struct fi_ib_batch fi_ib_batch;
+fi_status fi_ib_batch_create(fi_model *const *models, int32_t count, fi_ib_batch **out);
+fi_status fi_ib_batch_destroy(fi_ib_batch *b);
+fi_status fi_ib_batch_add(fi_ib_batch *b, fi_model *m);
+fi_status fi_ib_batch_remove(fi_ib_batch *b, fi_model *m);
+int32_t fi_ib_batch_size(const fi_ib_batch *b);
+/* niter iterations of every member */
+fi_status fi_ib_batch_advance(fi_ib_batch *b, int32_t niter);
+fi_status fi_ib_batch_synchronize(fi_ib_batch *b);
+
 /* ---- subdomains: halo layers of a domain split into slabs ---------------------
  * Replaces the halo exchange of the reference's distributed architecture
  * (Chmy.Distributed exchange_halo! of V and η_next after update_V!,
