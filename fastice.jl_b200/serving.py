@@ -10,9 +10,11 @@ served alone or in the mix:
 * 2D requests join one :class:`BatchedStokes2D`; each loop turn runs one
   check-to-check round (ncheck iterations, device-side check, retirement and
   work-list compaction) of every 2D member still iterating;
-* 3D requests each keep their own model and CUDA stream; each loop turn queues
-  ncheck iterations on every 3D stream before the 2D round runs, so their sweeps
-  overlap the batch's, then takes each 3D model's residual check.
+* 3D requests (immersed-boundary models) join one :class:`BatchedIB3D`; each loop
+  turn queues ncheck iterations of all of them as shared launches (eight per
+  iteration whatever their number, replayed as CUDA graphs) on the batch's stream
+  before the 2D round runs, so the 3D and 2D sweeps overlap, then takes each 3D
+  model's residual check.
 
 Admission is first come, first served: the head of the queue is admitted once its
 estimated device footprint fits the budget beside the requests in flight;
@@ -29,7 +31,7 @@ from typing import Callable, List, Optional
 
 import numpy as np
 
-from .models import BatchedStokes2D
+from .models import BatchedIB3D, BatchedStokes2D
 
 
 @dataclasses.dataclass
@@ -110,6 +112,7 @@ class SolveServer:
         active3d = {}
         used = 0
         batch: Optional[BatchedStokes2D] = None
+        batch3: Optional[BatchedIB3D] = None
         t0 = time.perf_counter()
         done: List[SolveRequest] = []
 
@@ -135,6 +138,10 @@ class SolveServer:
                         batch.add(m)
                     active2d[r.rid] = (r, m)
                 else:
+                    if batch3 is None:
+                        batch3 = BatchedIB3D([m])
+                    else:
+                        batch3.add(m)
                     active3d[r.rid] = (r, m)
             if queue and not active2d and not active3d and used + queue[0].bytes > self.budget:
                 raise RuntimeError(f"request {queue[0].rid} needs {queue[0].bytes} bytes, over the budget")
@@ -143,11 +150,12 @@ class SolveServer:
                     time.sleep(max(0.0, min(pending[0].arrival - now(), 0.01)))
                 continue
             self.turns += 1
-            # 3D: queue ncheck iterations on each model's stream (asynchronous)
-            for r, m in active3d.values():
-                k = min(self.ncheck, r.max_iter - r.iterations)
-                m.advance(k)
-                r.meta["_k"] = k
+            # 3D: ncheck iterations of every 3D request, shared launches on the batch's
+            # stream (asynchronous; each model's stream then waits for them)
+            if active3d:
+                batch3.advance(self.ncheck)
+                for r, m in active3d.values():
+                    r.meta["_k"] = self.ncheck
             # 2D: one check round of the batch (its own stream, overlapping the 3D sweeps)
             retired = []
             if active2d:
@@ -187,11 +195,15 @@ class SolveServer:
                 used -= r.bytes
                 if r.kind == "2d":
                     batch.remove(m)
+                else:
+                    batch3.remove(m)
                 r.meta["result"] = self._keep(m)
                 m.close()
                 done.append(r)
         if batch is not None:
             batch.close()
+        if batch3 is not None:
+            batch3.close()
         return done
 
     def _keep(self, m):
