@@ -428,7 +428,7 @@ def run_batched(args):
                  "error_vs_fp64_solve": errs,
                  "gpu_launches": "k sweeps + 4 bookkeeping kernels per check round, replayed as one graph; per outer "
                                  "step of the defect correction a few FP64 kernels per member"})
-    print(json.dumps(line))
+    return line
 
 
 def _serving_requests(fi, scale, duration, rate, seed=0):
@@ -489,7 +489,7 @@ def run_serving(args):
                       b["requests"], 0, 1e3 * b["makespan_s"] / max(1, b["requests"]), "f64", cfg)
     line.update({"batched": b, "sequential": out["sequential"],
                  "speedup_vs_sequential": b["solves_per_s"] / out["sequential"]["solves_per_s"]})
-    print(json.dumps(line))
+    return line
 
 
 def run_mixed(args):
@@ -561,7 +561,7 @@ def run_mixed(args):
     line.update({"plain_fp64": res["plain"], "mixed": res["mixed"], "max_rel_diff_V_vs_fp64": dv})
     if not both:
         line["invalid"] = "a solve stopped before reaching the tolerance; no speed-up is reported"
-    print(json.dumps(line))
+    return line
 
 
 def glacier_rheology(fi, kind):
@@ -652,7 +652,7 @@ def run_glacier(args):
                               "note": "achieved counts 36 passes over the whole box; dram_gbs is the measured "
                                       "traffic per iteration over its time"},
                  "per_dtype": res, "clocks": clocks})
-    print(json.dumps(line))
+    return line
 
 
 def run_heat(args):
@@ -708,7 +708,7 @@ def run_heat(args):
     line.update({"gpu_launches": args.steps, "clocks": ck,
                  "roofline": {"bound": "hbm", "achieved": teff, "peak": peak, "unit": "GB/s", "frac": teff / peak,
                               "peak_source": peak_kind, "algorithmic_bytes": a_eff}})
-    print(json.dumps(line))
+    return line
 
 
 def run_shapes(args):
@@ -756,6 +756,8 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--n", type=int, default=511)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the glacier sweep, the mixed-precision glacier "
+                                                            "solve and the heat sweep in the default line")
     ap.add_argument("--no-parity", action="store_true", help="skip the oracle comparison and manufactured-solution "
                                                             "errors (profiling runs)")
     ap.add_argument("--cpu-baseline-only", action="store_true", help=argparse.SUPPRESS)
@@ -792,8 +794,10 @@ def main():
         print(json.dumps({"iterations": its, "seconds": el, "threads": threads}))
         return
     if args.workload != "slab":
-        {"batched": run_batched, "serving": run_serving, "mixed": run_mixed,
-         "glacier": run_glacier, "heat": run_heat, "shapes": run_shapes}[args.workload](args)
+        line = {"batched": run_batched, "serving": run_serving, "mixed": run_mixed,
+                "glacier": run_glacier, "heat": run_heat, "shapes": run_shapes}[args.workload](args)
+        if line is not None:
+            print(json.dumps(line))
         return
     n = (args.n, args.n, args.n)
     ws, rank, local = dist_setup()
@@ -910,6 +914,20 @@ def main():
         mm = mms_errors(fi)
         line["mms_error"] = mm["mms3d_127"]["l2_rel_error"]
         line["mms"] = mm
+    if rank == 0 and ws == 1 and not args.no_extras:
+        # the other workloads, measured in the same run (one sub-object each)
+        import copy
+        extras = {}
+        ga = copy.copy(args)
+        ga.n, ga.steps, ga.warmup, ga.dtypes, ga.rheology = 383, 20, 3, "f64,f32", "linear"
+        extras["glacier_sweep"] = run_glacier(ga)
+        ma = copy.copy(args)
+        ma.n, ma.scenario, ma.rheology, ma.tol = 383, "glacier", "linear", 1e-8
+        extras["mixed_glacier"] = run_mixed(ma)
+        ha = copy.copy(args)
+        ha.n, ha.steps, ha.warmup, ha.dtypes = 511, 20, 3, "f64"
+        extras["heat"] = run_heat(ha)
+        line["other_workloads"] = extras
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         its, el, cores = cpu_baseline(n, seconds=12.0)
         line["cpu_baseline"] = {"value": A * 8 * its / el / 1e9, "unit": "GB/s", "cores": cores, "kind": "port",
