@@ -175,7 +175,9 @@ __global__ void __launch_bounds__(256) scatter_rows(const E *__restrict__ src, E
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     if (x >= nx) return;
     const long long z = blockIdx.y;
-    for (int y = 0; y < ny; y++) dst[x + pitch * (y + rows * z)] = src[x + (long long)nx * (y + (long long)ny * z)];
+    // rows split over grid.z: a 2D field (one plane) still spreads over many blocks
+    for (int y = blockIdx.z; y < ny; y += gridDim.z)
+        dst[x + pitch * (y + rows * z)] = src[x + (long long)nx * (y + (long long)ny * z)];
 }
 
 fi_status upload_interior(fi_model *m, int field, const void *host) {
@@ -199,7 +201,7 @@ fi_status upload_interior(fi_model *m, int field, const void *host) {
         FI_CHECK_CUDA(cudaMemcpyAsync(m->d_stage, src + plane * z0, plane * zc, cudaMemcpyHostToDevice, m->stream),
                       "set_field copy");
         char *d = dev + (long long)z0 * m->g.sxy * (long long)m->esz;
-        const dim3 grd((nx + 255) / 256, zc);
+        const dim3 grd((nx + 255) / 256, zc, std::max(1, std::min(ny, std::max(1, 4096 / zc))));
         if (m->esz == 8)
             scatter_rows<unsigned long long><<<grd, 256, 0, m->stream>>>(
                 (const unsigned long long *)m->d_stage, (unsigned long long *)d, nx, ny, m->g.pitch, m->g.rows);
