@@ -10,8 +10,8 @@ from .grids import Center, UniformGrid, Vertex, flip
 from .levelsets import compute_levelset_from_dem, omega_from_psi
 from .models import (Arch, BatchedIB3D, BatchedStokes2D, FieldRef, IsothermalFullStokesModel, IsothermalImmersedBoundaryFullStokesModel,
                      advance_iteration, compute_residuals, interior, pt_params, set_)
-from .physics import (ArrayField, BoundaryCondition, ConstantField, FunctionField, LinearViscousRheology, OneField,
-                      PBC, Periodic, PowerLawRheology, Relaxation, SBC, Slip, TBC, Traction, VBC, ValueField, Velocity,
+from .physics import (ArrayField, BoundaryCondition, ConstantField, FunctionField, Halo, HBC, LinearViscousRheology,
+                      OneField, PBC, Periodic, PowerLawRheology, Relaxation, SBC, Slip, TBC, Traction, VBC, ValueField, Velocity,
                       ViscoplasticRegularisation, ZeroField, glen_regularised)
 from . import scenarios  # noqa: E402  (seeded problem set-ups over the names above)
 from . import writers  # noqa: E402
@@ -22,7 +22,7 @@ from .writers import write_h5, write_xdmf  # noqa: E402
 __all__ = [
     "FastIceError", "BatchedIB3D", "BatchedStokes2D", "Center", "Vertex", "UniformGrid", "flip", "compute_levelset_from_dem", "omega_from_psi", "Arch",
     "FieldRef", "IsothermalFullStokesModel", "IsothermalImmersedBoundaryFullStokesModel", "advance_iteration",
-    "compute_residuals", "interior", "pt_params", "set_", "ArrayField", "BoundaryCondition", "ConstantField",
+    "compute_residuals", "interior", "pt_params", "set_", "ArrayField", "BoundaryCondition", "ConstantField", "Halo", "HBC",
     "FunctionField", "LinearViscousRheology", "OneField", "PBC", "Periodic", "PowerLawRheology", "Relaxation", "SBC",
     "Slip", "TBC", "Traction", "VBC", "ValueField", "Velocity", "ViscoplasticRegularisation", "ZeroField",
     "glen_regularised", "load_library", "scenarios", "writers", "write_h5", "write_xdmf", "heat", "HeatDiffusionModel",

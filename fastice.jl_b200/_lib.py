@@ -13,7 +13,7 @@ LIB_NAMES = {"fast": "libfastice_b200.so", "strict": "libfastice_b200_strict.so"
 
 FI_OK, FI_ERR_ARG, FI_ERR_OOM, FI_ERR_DIVERGED, FI_ERR_TIMEOUT, FI_ERR_CUDA, FI_ERR_UNSUPPORTED, FI_ERR_STATE = range(8)
 FI_F64, FI_F32 = 0, 1
-FI_BC_SLIP, FI_BC_TRACTION, FI_BC_VELOCITY, FI_BC_PERIODIC = 0, 1, 2, 3
+FI_BC_SLIP, FI_BC_TRACTION, FI_BC_VELOCITY, FI_BC_PERIODIC, FI_BC_HALO = 0, 1, 2, 3, 4
 FI_RHEO_LINEAR, FI_RHEO_POWER = 0, 1
 FI_RELAX_NONE, FI_RELAX_LIN, FI_RELAX_LOG, FI_RELAX_LOG10 = 0, 1, 2, 3
 FI_G_VALUE, FI_G_FIELD = 0, 1

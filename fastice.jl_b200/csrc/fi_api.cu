@@ -87,9 +87,13 @@ fi_status validate(const fi_model_desc *d) {
     for (int k = 0; k < gr.nd; k++) {
         bool p0 = d->bc[k][0].kind == FI_BC_PERIODIC, p1 = d->bc[k][1].kind == FI_BC_PERIODIC;
         if (p0 != p1) return set_error("a periodic dimension must be periodic on both sides"), FI_ERR_ARG;
-        for (int s = 0; s < 2; s++)
-            if (d->bc[k][s].kind < 0 || d->bc[k][s].kind > FI_BC_PERIODIC)
+        for (int s = 0; s < 2; s++) {
+            if (d->bc[k][s].kind < 0 || d->bc[k][s].kind > FI_BC_HALO)
                 return set_error("unknown boundary-condition kind"), FI_ERR_ARG;
+            if (d->bc[k][s].kind == FI_BC_HALO && (k > 1 || gr.nd != 3 || d->immersed))
+                return set_error("halo sides are supported along x or y of 3D FullStokes subdomains"),
+                       FI_ERR_UNSUPPORTED;
+        }
     }
     const fi_rheology &r = d->rheology;
     if (r.inner != FI_RHEO_LINEAR && r.inner != FI_RHEO_POWER) return set_error("unknown rheology"), FI_ERR_ARG;
@@ -230,6 +234,7 @@ BcBatch stress_batch(const fi_model *m, int d) {
     const int nd = m->d.grid.nd;
     for (int s = 0; s < 2; s++) {
         const fi_bc &bc = m->d.bc[d][s];
+        if (bc.kind == FI_BC_HALO) continue;  // the neighbour's values arrive by the halo exchange
         if (bc.kind == FI_BC_PERIODIC) {
             if (s == 1) continue;
             int fl3[] = {FI_FIELD_P, FI_FIELD_TXX, FI_FIELD_TYY, FI_FIELD_TZZ, FI_FIELD_TXY, FI_FIELD_TXZ, FI_FIELD_TYZ};
@@ -279,6 +284,7 @@ BcBatch velocity_batch(const fi_model *m, int d) {
     const int Vf[3] = {FI_FIELD_VX, FI_FIELD_VY, FI_FIELD_VZ};
     for (int s = 0; s < 2; s++) {
         const fi_bc &bc = m->d.bc[d][s];
+        if (bc.kind == FI_BC_HALO) continue;
         if (bc.kind == FI_BC_PERIODIC) {
             if (s == 1) continue;
             for (int q = 0; q < nd; q++) add_op(b, m->cur(Vf[q]), Vf[q], 0, BC_PERIODIC, 0);
@@ -300,6 +306,7 @@ BcBatch eta_batch(const fi_model *m, int d, int field) {
     b.dim = d;
     for (int s = 0; s < 2; s++) {
         const fi_bc &bc = m->d.bc[d][s];
+        if (bc.kind == FI_BC_HALO) continue;
         if (bc.kind == FI_BC_PERIODIC) {
             if (s == 0) add_op(b, m->cur(field), field, 0, BC_PERIODIC, 0);
         } else {
@@ -315,7 +322,7 @@ BcBatch residual_batch(const fi_model *m, int d) {
     const int Rf[3] = {FI_FIELD_RVX, FI_FIELD_RVY, FI_FIELD_RVZ};
     for (int s = 0; s < 2; s++) {
         int k = m->d.bc[d][s].kind;
-        if (k == FI_BC_TRACTION || k == FI_BC_PERIODIC) continue;
+        if (k == FI_BC_TRACTION || k == FI_BC_PERIODIC || k == FI_BC_HALO) continue;
         add_op(b, m->base[Rf[d]], Rf[d], s, BC_DIRICHLET, 0.0);
     }
     return b;
@@ -688,6 +695,12 @@ fi_status fi_model_create(const fi_model_desc *desc, fi_model **out) {
         return fail(FI_ERR_UNSUPPORTED);
     }
     m->path = (want == FI_PATH_REFERENCE || !fok) ? FI_PATH_REFERENCE : FI_PATH_FUSED;
+    for (int k = 0; k < gr.nd; k++)
+        for (int s2 = 0; s2 < 2; s2++)
+            if (desc->bc[k][s2].kind == FI_BC_HALO && m->path != FI_PATH_FUSED) {
+                set_error("a subdomain with halo sides runs the fused sweep (its ghost stresses follow the exchanged velocities)");
+                return fail(FI_ERR_UNSUPPORTED);
+            }
 
     const size_t bytes = m->elems * m->esz;
     for (int f = 0; f < FI_FIELD_COUNT; f++) {
@@ -868,8 +881,9 @@ fi_status fi_model_advance_begin(fi_model *m, int32_t dim) {
     if (!m || (dim != 0 && dim != 1)) return set_error("bad argument"), FI_ERR_ARG;
     if (fi_status js = join_overlap(m); js != FI_OK) return js;
     if (m->path != FI_PATH_FUSED) return set_error("an overlapped iteration needs the fused sweep"), FI_ERR_UNSUPPORTED;
-    if (dim >= m->d.grid.nd || m->d.bc[dim][0].kind != FI_BC_PERIODIC)
-        return set_error("the split dimension must be declared periodic on the subdomain model"), FI_ERR_STATE;
+    auto away = [](int k) { return k == FI_BC_PERIODIC || k == FI_BC_HALO; };
+    if (dim >= m->d.grid.nd || !(away(m->d.bc[dim][0].kind) || away(m->d.bc[dim][1].kind)))
+        return set_error("the split dimension needs a periodic or halo side on the subdomain model"), FI_ERR_STATE;
     FI_CHECK_CUDA(cudaSetDevice(m->d.device), "cudaSetDevice");
     if (!m->stream2) {
         FI_CHECK_CUDA(cudaStreamCreateWithFlags(&m->stream2, cudaStreamNonBlocking), "second stream");

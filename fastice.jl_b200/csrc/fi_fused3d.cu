@@ -163,7 +163,9 @@ struct Ctx {
     int i0, j0, kb, ke;
     int n0, n1, n2;
     long long sx, sxy;
-    bool perx, pery;
+    // the ghost layer on the low / high side of x / y comes from elsewhere: a periodic
+    // image, or a neighbouring subdomain's halo (FI_BC_PERIODIC / FI_BC_HALO)
+    bool hx0, hx1, hy0, hy1;
     bool bnd_x, bnd_y;  // column touches an x / y boundary (needs fix-ups or ghost writes)
     // Ring positions relative to the plane step sref: element offsets of the
     // planes around sref inside three- and four-slot rings, computed once per plane
@@ -283,9 +285,9 @@ __device__ __forceinline__ void sigma_point(const Ctx<T, TX, TY, TRIM> &c, const
     constexpr int BV = FBox<T, TX, TY, TRIM, M_VX>::bw;  // row pitch of the V and η boxes
     const T idx = q.inv_dx[0], idy = q.inv_dx[1], idz = q.inv_dx[2];
     const bool cz = s >= 1 && s <= c.n2, vz = s >= 1 && s <= c.n2 + 1;
-    const bool cx = XYI || (i >= 1 && i <= c.n0) || (c.perx && (i == 0 || i == c.n0 + 1));
+    const bool cx = XYI || (i >= 1 && i <= c.n0) || (c.hx0 && i == 0) || (c.hx1 && i == c.n0 + 1);
     const bool vx = XYI || (i >= 1 && i <= c.n0 + 1);
-    const bool cy = XYI || (j >= 1 && j <= c.n1) || (c.pery && (j == 0 || j == c.n1 + 1));
+    const bool cy = XYI || (j >= 1 && j <= c.n1) || (c.hy0 && j == 0) || (c.hy1 && j == c.n1 + 1);
     const bool vy = XYI || (j >= 1 && j <= c.n1 + 1);
     const int a = c.template ix<M_VX>(i, j);
     const T *vxs = c.slot(S_VX, R_VX, s), *vys = c.slot(S_VY, R_VY, s), *vzs = c.slot(S_VZ, R_VZ, s);
@@ -454,7 +456,7 @@ __device__ __forceinline__ void sigma_plane(const Ctx<T, TX, TY, TRIM> &c, const
     if (!late) return;
     constexpr int NREG = (TX + 2) * (TY + 2);
     if constexpr (!TRIM) {
-        if (c.bnd_x && !c.perx) {
+        if (c.bnd_x && !(c.hx0 && c.hx1)) {  // fix_x leaves periodic and halo sides alone
             for (int r = tid; r < NREG; r += Lay::NT) {
                 const int i = c.i0 - 1 + r % (TX + 2), j = c.j0 - 1 + r / (TX + 2);
                 fix_x<T, TX, TY, TRIM>(c, p, q, s, i, j, 0);
@@ -462,7 +464,7 @@ __device__ __forceinline__ void sigma_plane(const Ctx<T, TX, TY, TRIM> &c, const
             }
             __syncthreads();
         }
-        if (c.bnd_y && !c.pery) {
+        if (c.bnd_y && !(c.hy0 && c.hy1)) {
             for (int r = tid; r < NREG; r += Lay::NT) {
                 const int i = c.i0 - 1 + r % (TX + 2), j = c.j0 - 1 + r / (TX + 2);
                 fix_y<T, TX, TY, TRIM>(c, p, q, s, i, j, 0);
@@ -538,33 +540,35 @@ __device__ __forceinline__ Img<T> img_own(int q) {
     d.pos[2] = 0; d.ok[2] = false; d.dir[2] = false; d.c[2] = T(0);
     return d;
 }
-// Center-located value at index q (1..N) along a dim with BC kinds kl/kr.
-// comp >= 0: Velocity-BC ghosts of that velocity component; comp < 0: Neumann (η_next)
+// Center-located value at index q (1..N) along a dim with BC kinds kl/kr; lo / hi:
+// the low / high ghost comes from elsewhere (a periodic image of this model's own
+// value, which a subdomain's halo exchange replaces with its neighbour's).
+// neumann: copies (η_next); else Velocity-BC ghosts 2c - v of a velocity component
 template <typename T>
-__device__ __forceinline__ Img<T> img_center(int q, int N, bool periodic, int kl, int kr, T cl, T cr, bool neumann) {
+__device__ __forceinline__ Img<T> img_center(int q, int N, bool lo, bool hi, int kl, int kr, T cl, T cr, bool neumann) {
     Img<T> d = img_own<T>(q);
-    if (periodic) {
+    if (lo) {
         if (q == N) { d.pos[1] = 0; d.ok[1] = true; }
-        if (q == 1) { d.pos[2] = N + 1; d.ok[2] = true; }
-        return d;
-    }
-    if (neumann) {
+    } else if (neumann) {
         if (q == 1) { d.pos[1] = 0; d.ok[1] = true; }
+    } else if (q == 1 && kl == FI_BC_VELOCITY) {
+        d.pos[1] = 0; d.ok[1] = true; d.dir[1] = true; d.c[1] = cl;
+    }
+    if (hi) {
+        if (q == 1) { d.pos[2] = N + 1; d.ok[2] = true; }
+    } else if (neumann) {
         if (q == N) { d.pos[2] = N + 1; d.ok[2] = true; }
-    } else {
-        if (q == 1 && kl == FI_BC_VELOCITY) { d.pos[1] = 0; d.ok[1] = true; d.dir[1] = true; d.c[1] = cl; }
-        if (q == N && kr == FI_BC_VELOCITY) { d.pos[2] = N + 1; d.ok[2] = true; d.dir[2] = true; d.c[2] = cr; }
+    } else if (q == N && kr == FI_BC_VELOCITY) {
+        d.pos[2] = N + 1; d.ok[2] = true; d.dir[2] = true; d.c[2] = cr;
     }
     return d;
 }
 template <typename T>
-__device__ __forceinline__ Img<T> img_vertex(int q, int N, bool periodic) {
+__device__ __forceinline__ Img<T> img_vertex(int q, int N, bool lo, bool hi) {
     Img<T> d = img_own<T>(q);
-    if (periodic) {
-        if (q == N) { d.pos[1] = 0; d.ok[1] = true; }
-        if (q == 1) { d.pos[2] = N + 1; d.ok[2] = true; }
-        if (q == 2) { d.pos[2] = N + 2; d.ok[2] = true; }
-    }
+    if (lo && q == N) { d.pos[1] = 0; d.ok[1] = true; }
+    if (hi && q == 1) { d.pos[2] = N + 1; d.ok[2] = true; }
+    if (hi && q == 2) { d.pos[2] = N + 2; d.ok[2] = true; }
     return d;
 }
 
@@ -660,14 +664,14 @@ __device__ __forceinline__ void v_point(const Ctx<T, TX, TY, TRIM> &c, const KPa
     const int xl = p.bc_kind[0][0], xr = p.bc_kind[0][1], yl = p.bc_kind[1][0], yr = p.bc_kind[1][1];
     const int zl = p.bc_kind[2][0], zr = p.bc_kind[2][1];
     // ---- V.x at (V, C, C)
-    if (j <= n1 && t >= 1 && t <= n2 && !(c.perx && i == n0 + 1)) {
+    if (j <= n1 && t >= 1 && t <= n2 && !(c.hx1 && i == n0 + 1)) {
         T v;
-        if (!c.perx && i == 1 && node_fixed(xl)) v = q.bc_val[0][0][0];
-        else if (!c.perx && i == n0 + 1 && node_fixed(xr)) v = q.bc_val[0][1][0];
+        if (!c.hx0 && i == 1 && node_fixed(xl)) v = q.bc_val[0][0][0];
+        else if (!c.hx1 && i == n0 + 1 && node_fixed(xr)) v = q.bc_val[0][1][0];
         else v = vx_raw(c, p, q, in, t, i, j, I);
-        write_images(c, out.Vx, v, img_vertex<T>(i, n0, c.perx),
-                     img_center<T>(j, n1, c.pery, yl, yr, q.bc_val[1][0][0], q.bc_val[1][1][0], false),
-                     img_center<T>(t, n2, false, zl, zr, q.bc_val[2][0][0], q.bc_val[2][1][0], false));
+        write_images(c, out.Vx, v, img_vertex<T>(i, n0, c.hx0, c.hx1),
+                     img_center<T>(j, n1, c.hy0, c.hy1, yl, yr, q.bc_val[1][0][0], q.bc_val[1][1][0], false),
+                     img_center<T>(t, n2, false, false, zl, zr, q.bc_val[2][0][0], q.bc_val[2][1][0], false));
     }
     // A value on a fixed node of its own dim d is written there last by the
     // reference's dim-d node assignment, which spans the ghosts of the dims before
@@ -678,15 +682,15 @@ __device__ __forceinline__ void v_point(const Ctx<T, TX, TY, TRIM> &c, const KPa
         return d;
     };
     // ---- V.y at (C, V, C)
-    if (i <= n0 && t >= 1 && t <= n2 && !(c.pery && j == n1 + 1)) {
+    if (i <= n0 && t >= 1 && t <= n2 && !(c.hy1 && j == n1 + 1)) {
         T v;
-        const bool y_node = !c.pery && ((j == 1 && node_fixed(yl)) || (j == n1 + 1 && node_fixed(yr)));
-        if (!c.pery && j == 1 && node_fixed(yl)) v = q.bc_val[1][0][1];
-        else if (!c.pery && j == n1 + 1 && node_fixed(yr)) v = q.bc_val[1][1][1];
+        const bool y_node = (!c.hy0 && j == 1 && node_fixed(yl)) || (!c.hy1 && j == n1 + 1 && node_fixed(yr));
+        if (!c.hy0 && j == 1 && node_fixed(yl)) v = q.bc_val[1][0][1];
+        else if (!c.hy1 && j == n1 + 1 && node_fixed(yr)) v = q.bc_val[1][1][1];
         else v = vy_raw(c, p, q, in, t, i, j, I);
-        Img<T> ix = img_center<T>(i, n0, c.perx, xl, xr, q.bc_val[0][0][1], q.bc_val[0][1][1], false);
-        write_images(c, out.Vy, v, y_node ? as_copies(ix) : ix, img_vertex<T>(j, n1, c.pery),
-                     img_center<T>(t, n2, false, zl, zr, q.bc_val[2][0][1], q.bc_val[2][1][1], false));
+        Img<T> ix = img_center<T>(i, n0, c.hx0, c.hx1, xl, xr, q.bc_val[0][0][1], q.bc_val[0][1][1], false);
+        write_images(c, out.Vy, v, y_node ? as_copies(ix) : ix, img_vertex<T>(j, n1, c.hy0, c.hy1),
+                     img_center<T>(t, n2, false, false, zl, zr, q.bc_val[2][0][1], q.bc_val[2][1][1], false));
     }
     // ---- V.z at (C, C, V)
     if (i <= n0 && j <= n1 && t >= 1 && t <= n2 + 1) {
@@ -695,16 +699,16 @@ __device__ __forceinline__ void v_point(const Ctx<T, TX, TY, TRIM> &c, const KPa
         if (t == 1 && node_fixed(zl)) v = q.bc_val[2][0][2];
         else if (t == n2 + 1 && node_fixed(zr)) v = q.bc_val[2][1][2];
         else v = vz_raw(c, p, q, in, t, i, j, I);
-        Img<T> ix = img_center<T>(i, n0, c.perx, xl, xr, q.bc_val[0][0][2], q.bc_val[0][1][2], false);
-        Img<T> iy = img_center<T>(j, n1, c.pery, yl, yr, q.bc_val[1][0][2], q.bc_val[1][1][2], false);
+        Img<T> ix = img_center<T>(i, n0, c.hx0, c.hx1, xl, xr, q.bc_val[0][0][2], q.bc_val[0][1][2], false);
+        Img<T> iy = img_center<T>(j, n1, c.hy0, c.hy1, yl, yr, q.bc_val[1][0][2], q.bc_val[1][1][2], false);
         write_images(c, out.Vz, v, z_node ? as_copies(ix) : ix, z_node ? as_copies(iy) : iy, img_own<T>(t));
     }
     // ---- η_next at (C, C, C), Neumann / periodic ghosts
     if (!p.freeze_eta && i <= n0 && j <= n1 && t >= 1 && t <= n2) {
         T en = eta_raw(c, p, q, in, t, i, j, I);
-        write_images(c, out.eta_next, en, img_center<T>(i, n0, c.perx, xl, xr, T(0), T(0), true),
-                     img_center<T>(j, n1, c.pery, yl, yr, T(0), T(0), true),
-                     img_center<T>(t, n2, false, zl, zr, T(0), T(0), true));
+        write_images(c, out.eta_next, en, img_center<T>(i, n0, c.hx0, c.hx1, xl, xr, T(0), T(0), true),
+                     img_center<T>(j, n1, c.hy0, c.hy1, yl, yr, T(0), T(0), true),
+                     img_center<T>(t, n2, false, false, zl, zr, T(0), T(0), true));
     }
 }
 
@@ -790,8 +794,11 @@ __device__ __forceinline__ void init_ctx(Ctx<T, TX, TY, TRIM> &c, const Geom &g,
     c.ke = min(c.kb + zb, c.n2 + 2);
     c.sx = g.pitch;
     c.sxy = g.sxy;
-    c.perx = p.bc_kind[0][0] == FI_BC_PERIODIC;
-    c.pery = p.bc_kind[1][0] == FI_BC_PERIODIC;
+    auto away = [](int k) { return k == FI_BC_PERIODIC || k == FI_BC_HALO; };
+    c.hx0 = away(p.bc_kind[0][0]);
+    c.hx1 = away(p.bc_kind[0][1]);
+    c.hy0 = away(p.bc_kind[1][0]);
+    c.hy1 = away(p.bc_kind[1][1]);
     c.bnd_x = c.i0 == 1 || c.i0 + TX >= c.n0 + 1;
     c.bnd_y = c.j0 == 1 || c.j0 + TY >= c.n1 + 1;
 }

@@ -132,13 +132,17 @@ fi_status halo_move(fi_model *m, int d, int side, int what, void *buf, bool pack
     return FI_OK;
 }
 
-fi_status halo_check(const fi_model *m, int32_t dim, int32_t side, int32_t what) {
+// side_moves: the side itself must take part in the exchange (pack / unpack); the
+// byte count of a message only needs the dimension to be split (a periodic or halo side)
+fi_status halo_check(const fi_model *m, int32_t dim, int32_t side, int32_t what, bool side_moves = true) {
     if (!m) return set_error("null model"), FI_ERR_ARG;
     if (dim < 0 || dim > 1 || dim >= m->d.grid.nd) return set_error("halo dimension must be x (0) or y (1)"), FI_ERR_ARG;
     if (side != 0 && side != 1) return set_error("side must be 0 (low) or 1 (high)"), FI_ERR_ARG;
     if (what != FI_HALO_ITERATION && what != FI_HALO_STATE) return set_error("unknown halo content"), FI_ERR_ARG;
-    if (m->d.bc[dim][0].kind != FI_BC_PERIODIC)
-        return set_error("a split dimension must be declared periodic on the subdomain model"), FI_ERR_STATE;
+    auto away = [](int k) { return k == FI_BC_PERIODIC || k == FI_BC_HALO; };
+    if (side_moves ? !away(m->d.bc[dim][side].kind) : !(away(m->d.bc[dim][0].kind) || away(m->d.bc[dim][1].kind)))
+        return set_error("the side of a split dimension must be periodic or a halo side on the subdomain model"),
+               FI_ERR_STATE;
     if (m->ib) return set_error("halo exchange of the immersed-boundary model is not covered"), FI_ERR_UNSUPPORTED;
     // the reference-shaped path fills ghost stresses by the boundary copy after
     // update_σ!, so a split would need a second (stress) exchange inside the
@@ -157,7 +161,7 @@ using namespace fi;
 extern "C" {
 
 fi_status fi_model_halo_bytes(const fi_model *m, int32_t dim, int32_t side, int32_t what, size_t *bytes) {
-    fi_status st = halo_check(m, dim, side, what);
+    fi_status st = halo_check(m, dim, side, what, false);
     if (st != FI_OK) return st;
     if (!bytes) return set_error("null argument"), FI_ERR_ARG;
     int fl[16];

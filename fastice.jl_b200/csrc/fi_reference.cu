@@ -790,7 +790,7 @@ __global__ void __launch_bounds__(kNormThreads) residual_norms_kernel(Geom g, KP
     for (int d = 0; d < 3; d++)
         for (int s = 0; s < 2; s++) {
             int k = d < ND ? p.bc_kind[d][s] : FI_BC_TRACTION;
-            wall0[d][s] = !(k == FI_BC_TRACTION || k == FI_BC_PERIODIC);
+            wall0[d][s] = !(k == FI_BC_TRACTION || k == FI_BC_PERIODIC || k == FI_BC_HALO);
         }
     // grid-stride loop over the vertex range; the position (ii, jj, kk) steps by the
     // stride's own decomposition with carries instead of two 64-bit divisions per point

@@ -78,17 +78,23 @@ def measure_of(norms, measure: str = "abs_inf", nd: int = 3, rho_g_inf: float = 
 
 
 class TorchTransport:
-    """Ring point-to-point exchange over torch.distributed (NCCL or gloo)."""
+    """Point-to-point exchange over torch.distributed (NCCL or gloo) between the
+    slabs of a split dimension: a ring when the dimension is periodic, else a chain
+    (the first rank has no low neighbour, the last no high one)."""
 
-    def __init__(self, group=None):
+    def __init__(self, group=None, periodic: bool = True):
         import torch.distributed as dist
         self.dist = dist
         self.group = group
         self.rank = dist.get_rank(group)
         self.size = dist.get_world_size(group)
+        self.periodic = periodic
 
     def neighbours(self):
-        return (self.rank - 1) % self.size, (self.rank + 1) % self.size
+        """(low, high) neighbour ranks, None where a chain ends."""
+        if self.periodic:
+            return (self.rank - 1) % self.size, (self.rank + 1) % self.size
+        return (self.rank - 1 if self.rank > 0 else None, self.rank + 1 if self.rank < self.size - 1 else None)
 
     def _global(self, r):
         return r if self.group is None else self.dist.get_global_rank(self.group, r)
@@ -111,14 +117,21 @@ class TorchTransport:
 
     def exchange(self, send_low, send_high, recv_low, recv_high) -> None:
         """send_low -> low neighbour (its recv_high), send_high -> high neighbour
-        (its recv_low).  Waiting on the operations orders torch's current stream
-        after them (device tensors) or blocks until they completed (host tensors)."""
+        (its recv_low); the operations toward a missing neighbour (a chain's end) are
+        left out.  Waiting on the operations orders torch's current stream after them
+        (device tensors) or blocks until they completed (host tensors)."""
         d = self.dist
-        low, high = (self._global(r) for r in self.neighbours())
-        ops = [d.P2POp(d.isend, send_low, low, self.group, TAG_TO_LOW),
-               d.P2POp(d.irecv, recv_high, high, self.group, TAG_TO_LOW),
-               d.P2POp(d.isend, send_high, high, self.group, TAG_TO_HIGH),
-               d.P2POp(d.irecv, recv_low, low, self.group, TAG_TO_HIGH)]
+        low, high = self.neighbours()
+        ops = []
+        if low is not None:
+            ops.append(d.P2POp(d.isend, send_low, self._global(low), self.group, TAG_TO_LOW))
+        if high is not None:
+            ops.append(d.P2POp(d.irecv, recv_high, self._global(high), self.group, TAG_TO_LOW))
+            ops.append(d.P2POp(d.isend, send_high, self._global(high), self.group, TAG_TO_HIGH))
+        if low is not None:
+            ops.append(d.P2POp(d.irecv, recv_low, self._global(low), self.group, TAG_TO_HIGH))
+        if not ops:
+            return
         for req in d.batch_isend_irecv(ops):
             req.wait()
 
@@ -140,6 +153,9 @@ class Slab:
             import torch
             dev = torch.device("cuda", torch.cuda.current_device())
             alloc = (lambda nb: torch.empty(nb, dtype=torch.uint8, device=dev))
+        # the sides with a neighbour (both in a ring; a chain's ends have one)
+        low, high = transport.neighbours() if transport.size > 1 else (None, None)
+        self.sides = tuple(s for s, nb in ((0, low), (1, high)) if nb is not None)
         self.buf = {}
         for what in ("iteration", "state"):
             nb_low, nb_high = model.halo_bytes(self.dim, 0, what), model.halo_bytes(self.dim, 1, what)
@@ -153,12 +169,14 @@ class Slab:
 
     def _steps(self, what):
         b, m, d = self.buf[what], self.model, self.dim
-        m.halo_pack(d, 0, self._ptr(b["send_low"]), what)
-        m.halo_pack(d, 1, self._ptr(b["send_high"]), what)
+        for side, key in ((0, "send_low"), (1, "send_high")):
+            if side in self.sides:
+                m.halo_pack(d, side, self._ptr(b[key]), what)
         yield
         self.transport.exchange(b["send_low"], b["send_high"], b["recv_low"], b["recv_high"])
-        m.halo_unpack(d, 0, self._ptr(b["recv_low"]), what)
-        m.halo_unpack(d, 1, self._ptr(b["recv_high"]), what)
+        for side, key in ((0, "recv_low"), (1, "recv_high")):
+            if side in self.sides:
+                m.halo_unpack(d, side, self._ptr(b[key]), what)
 
     def exchange(self, what: str = "iteration") -> None:
         if self.transport.size == 1:
@@ -224,9 +242,10 @@ class Slab:
         return rep
 
 
-def advance_local(slabs, dim: int, niter: int, overlap: bool = False) -> None:
-    """``Slab.advance`` for a ring of slabs held by one process (one device): every
-    slab's iteration (in two halves with ``overlap``), then ``exchange_local``."""
+def advance_local(slabs, dim: int, niter: int, overlap: bool = False, periodic: bool = True) -> None:
+    """``Slab.advance`` for a ring (periodic) or chain of slabs held by one process
+    (one device): every slab's iteration (in two halves with ``overlap``), then
+    ``exchange_local``."""
     for _ in range(int(niter)):
         for m in slabs:
             if overlap:
@@ -236,32 +255,42 @@ def advance_local(slabs, dim: int, niter: int, overlap: bool = False) -> None:
         if overlap:
             for m in slabs:
                 m.advance_end()
-        exchange_local(slabs, dim)
+        exchange_local(slabs, dim, periodic=periodic)
 
 
-def exchange_local(slabs, dim: int, what: str = "iteration") -> None:
-    """The halo exchange of a ring of slabs held by one process (one device):
-    every slab packs its two messages, each is copied to the neighbour that
-    expects it, every slab unpacks.  The same messages and layers as a
-    multi-rank run over ``TorchTransport``."""
+def exchange_local(slabs, dim: int, what: str = "iteration", periodic: bool = True) -> None:
+    """The halo exchange of a ring (periodic) or chain of slabs held by one process
+    (one device): every slab packs its messages toward its neighbours, each is
+    copied to the neighbour that expects it, every slab unpacks.  The same messages
+    and layers as a multi-rank run over ``TorchTransport``."""
     import torch
     R = len(slabs)
     if R == 1:
         return
+
+    def has(r, side):
+        return periodic or (r > 0 if side == 0 else r < R - 1)
+
     bufs = []
-    for m in slabs:
+    for r, m in enumerate(slabs):
         lo = torch.empty(m.halo_bytes(dim, 0, what), dtype=torch.uint8, device="cuda")
         hi = torch.empty(m.halo_bytes(dim, 1, what), dtype=torch.uint8, device="cuda")
-        m.halo_pack(dim, 0, lo.data_ptr(), what)
-        m.halo_pack(dim, 1, hi.data_ptr(), what)
+        if has(r, 0):
+            m.halo_pack(dim, 0, lo.data_ptr(), what)
+        if has(r, 1):
+            m.halo_pack(dim, 1, hi.data_ptr(), what)
         m.synchronize()
         bufs.append((lo, hi))
     for r, m in enumerate(slabs):
-        from_low = bufs[(r - 1) % R][1].clone()   # the low neighbour's message toward its high side
-        from_high = bufs[(r + 1) % R][0].clone()  # the high neighbour's message toward its low side
         torch.cuda.synchronize()
-        m.halo_unpack(dim, 0, from_low.data_ptr(), what)
-        m.halo_unpack(dim, 1, from_high.data_ptr(), what)
+        if has(r, 0):
+            from_low = bufs[(r - 1) % R][1].clone()   # the low neighbour's message toward its high side
+            torch.cuda.synchronize()
+            m.halo_unpack(dim, 0, from_low.data_ptr(), what)
+        if has(r, 1):
+            from_high = bufs[(r + 1) % R][0].clone()  # the high neighbour's message toward its low side
+            torch.cuda.synchronize()
+            m.halo_unpack(dim, 1, from_high.data_ptr(), what)
         m.synchronize()
 
 
@@ -282,7 +311,7 @@ def halo_plan(nd: int, n, dim: int, side: int, what: str = "iteration", pack: bo
 
 
 def solve_local(slabs, dim: int, *, max_iter: int, ncheck: int, tol: float, measure: str = "abs_inf",
-                rho_g_inf: float = 1.0, length_z: float = 1.0, overlap: bool = False) -> dict:
+                rho_g_inf: float = 1.0, length_z: float = 1.0, overlap: bool = False, periodic: bool = True) -> dict:
     """``Slab.solve`` for a ring of slabs held by one process (one device): the same
     iterations, exchanges (``exchange_local``), norm reduction (``combine_norms``)
     and decision as a multi-rank run."""
@@ -290,7 +319,7 @@ def solve_local(slabs, dim: int, *, max_iter: int, ncheck: int, tol: float, meas
     it, rep = 0, {"converged": False, "diverged": False, "measure": float("nan"), "norms": None}
     while it < max_iter:
         k = min(ncheck, max_iter - it)
-        advance_local(slabs, dim, k, overlap=overlap)
+        advance_local(slabs, dim, k, overlap=overlap, periodic=periodic)
         it += k
         norms = combine_norms([m.residual_norms() for m in slabs])
         meas = measure_of(norms, measure, nd, rho_g_inf, length_z)

@@ -191,12 +191,19 @@ class Periodic:
     kind = L.FI_BC_PERIODIC
 
 
+class Halo:
+    """The side of a subdomain whose ghost layer comes from its neighbour (the
+    reference's distributed boundary, exchanged by Chmy.Distributed): x or y of a 3D
+    FullStokes subdomain; the other side of that dimension may be physical."""
+    kind = L.FI_BC_HALO
+
+
 class BoundaryCondition:
     """``BoundaryCondition{Kind}(components...)``; e.g. ``BoundaryCondition(Slip, 0.0, 0.0, 0.0)``."""
 
     def __init__(self, kind, *components: float):
-        if kind not in (Traction, Velocity, Slip, Periodic):
-            raise TypeError("kind must be Traction, Velocity, Slip or Periodic")
+        if kind not in (Traction, Velocity, Slip, Periodic, Halo):
+            raise TypeError("kind must be Traction, Velocity, Slip, Periodic or Halo")
         self.kind = kind
         self.components = tuple(float(c) for c in components)
 
@@ -218,3 +225,7 @@ def VBC(*c):
 
 def PBC():
     return BoundaryCondition(Periodic)
+
+
+def HBC():
+    return BoundaryCondition(Halo)

@@ -48,7 +48,10 @@ typedef enum { FI_F64 = 0, FI_F32 = 1 } fi_dtype;
 /* ---- boundary conditions: BoundaryCondition{Slip|Traction|Velocity}(components...)
  *      src/Models/FullStokes/Isothermal/boundary_conditions.jl:1-13.  PERIODIC is
  *      an extension (both sides of a dim must be PERIODIC). */
-typedef enum { FI_BC_SLIP = 0, FI_BC_TRACTION = 1, FI_BC_VELOCITY = 2, FI_BC_PERIODIC = 3 } fi_bc_kind;
+typedef enum { FI_BC_SLIP = 0, FI_BC_TRACTION = 1, FI_BC_VELOCITY = 2, FI_BC_PERIODIC = 3, FI_BC_HALO = 4 } fi_bc_kind;
+/* FI_BC_HALO: the side of a subdomain whose ghost layer comes from its neighbour
+ * (the reference's distributed boundary, exchanged by Chmy.Distributed); x or y only,
+ * fused sweep only; the other side of that dimension may be a physical boundary */
 
 typedef struct {
     int32_t kind;   /* fi_bc_kind */
@@ -400,13 +403,16 @@ fi_status fi_ib_batch_synchronize(fi_ib_batch *b);
  * Replaces the halo exchange of the reference's distributed architecture
  * (Chmy.Distributed exchange_halo! of V and η_next after update_V!,
  * src/Models/FullStokes/Isothermal/Isothermal.jl:103-104).  A slab is a model of
- * its own cells whose split dimension (x or y) is declared periodic; after each
- * PT iteration the caller moves the halo messages between neighbouring slabs (over
+ * its own cells whose split dimension (x or y) has a periodic pair of sides (a ring
+ * of slabs over a periodic domain) or a FI_BC_HALO side toward every neighbour (a
+ * chain of slabs: the outer sides keep their physical conditions); after each PT
+ * iteration the caller moves the halo messages between neighbouring slabs (over
  * NCCL, MPI or a device copy) and unpacks them, replacing the ghost images the
  * sweep wrote.  Messages are device buffers in the model's dtype.
  *   fi_model_halo_bytes(m, dim, side, what, &b): size of the message packed toward
  *       `side` (0 = low neighbour, 1 = high neighbour); the neighbour unpacks it
- *       from its opposite side
+ *       from its opposite side (any side of a split dimension: a chain's end slab
+ *       sizes the buffer it receives into from the side it sends toward)
  *   fi_model_halo_pack(m, dim, side, what, dst): fill that message (on the model's stream)
  *   fi_model_halo_unpack(m, dim, side, what, src): write the message received from
  *       the neighbour on `side` into the ghost layers (on the model's stream)

@@ -12,7 +12,7 @@ from conftest import load_fastice, load_oracle
 STATE_3D = ("P", "txx", "tyy", "tzz", "txy", "txz", "tyz", "Vx", "Vy", "Vz", "eta")
 STATE_2D = ("P", "txx", "tyy", "txy", "Vx", "Vy", "eta")
 
-KIND = {"slip": 0, "traction": 1, "velocity": 2, "periodic": 3}
+KIND = {"slip": 0, "traction": 1, "velocity": 2, "periodic": 3, "halo": 4}
 
 
 def make_bcs(fi, spec_bcs, nd):
@@ -24,6 +24,8 @@ def make_bcs(fi, spec_bcs, nd):
         for kind, comps in spec_bcs[d]:
             if kind == "periodic":
                 pair.append(fi.PBC())
+            elif kind == "halo":
+                pair.append(fi.HBC())
             else:
                 pair.append(ctor[kind](*comps))
         out[nm] = tuple(pair)

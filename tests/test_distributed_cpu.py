@@ -221,25 +221,31 @@ def test_combine_norms_slots():
 SHAPE_LOCAL = (6, 5, 4)
 
 
-def _field_global(name, dim, R, seed):
-    """Values of a periodic field: unique positions 1..N along dim (N = R * n),
-    every storage position (ghosts included) along the other dims."""
+def _field_global(name, dim, R, seed, extra=0):
+    """Values of a field along a split dimension: positions 1..N (N = R * n; one more
+    node for a vertex field of a bounded dimension, extra=1), every storage
+    position (ghosts included) along the other dims."""
     rng = np.random.default_rng(seed)
     nl = list(SHAPE_LOCAL)
     e = [x + 3 for x in nl]
-    e[dim] = nl[dim] * R
+    e[dim] = nl[dim] * R + extra
     return rng.standard_normal(tuple(reversed(e)))  # numpy order (z, y, x)
 
 
-def _local_index(r, n, N, i):
-    return (r * n + i - 1) % N  # position index (0-based) in the global periodic array
+def _local_index(r, n, N, i, periodic=True):
+    """Position index (0-based) in the global array of a slab's index i; None past a
+    bounded dimension's ends."""
+    q = r * n + i - 1
+    if periodic:
+        return q % N
+    return q if 0 <= q < N else None
 
 
 def _layer(a, dim, i):
     return a[:, :, i] if dim == 0 else a[:, i, :]
 
 
-def _plan_rank(rank, R, dim, what, port, out):
+def _plan_rank(rank, R, dim, what, port, out, periodic=True):
     import torch.distributed as dist
     fi = load_fastice()
     from fastice_b200 import distributed as D
@@ -252,13 +258,15 @@ def _plan_rank(rank, R, dim, what, port, out):
                  for pk in (True, False)}
         names = sorted({f for pl in plans.values() for f, _ in pl})
         local = {}
+        glob = {}
         for k, name in enumerate(names):
-            g = _field_global(name, dim, R, 100 + k)
             vert = fi._lib.FIELD_LOC[name][dim] == 1
+            extra = 1 if (vert and not periodic) else 0
+            g = glob[name] = _field_global(name, dim, R, 100 + k, extra)
             shape = list(reversed([x + 3 for x in SHAPE_LOCAL]))
             a = np.full(shape, np.nan)
             for i in range(1, n + (2 if vert else 1)):
-                _layer(a, dim, i)[...] = np.take(g, _local_index(rank, n, N, i), axis=2 - dim)
+                _layer(a, dim, i)[...] = np.take(g, _local_index(rank, n, N + extra, i, periodic), axis=2 - dim)
             local[name] = a
 
         class Host:
@@ -279,29 +287,38 @@ def _plan_rank(rank, R, dim, what, port, out):
                     L[...] = vals[q:q + L.size].reshape(L.shape)
                     q += L.size
 
-        slab = D.Slab(Host(), dim, D.TorchTransport(), alloc=lambda nb: torch.empty(nb, dtype=torch.uint8))
+        slab = D.Slab(Host(), dim, D.TorchTransport(periodic=periodic),
+                      alloc=lambda nb: torch.empty(nb, dtype=torch.uint8))
         slab.exchange(what)
         bad = []
         for k, name in enumerate(names):
-            g = _field_global(name, dim, R, 100 + k)
+            g = glob[name]
             vert = fi._lib.FIELD_LOC[name][dim] == 1
+            extra = 1 if (vert and not periodic) else 0
             for i in range(0, n + (3 if vert else 2)):
-                want = np.take(g, _local_index(rank, n, N, i), axis=2 - dim)
-                if not np.array_equal(_layer(local[name], dim, i), want):
+                q = _local_index(rank, n, N + extra, i, periodic)
+                got = _layer(local[name], dim, i)
+                if q is None:  # past a chain's end: no neighbour wrote it
+                    if not np.isnan(got).all():
+                        bad.append((name, i, "written"))
+                elif not np.array_equal(got, np.take(g, q, axis=2 - dim)):
                     bad.append((name, i))
         out.put((rank, bad, names))
     finally:
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("R,dim,what", [(2, 0, "iteration"), (3, 0, "state"), (3, 1, "iteration"), (2, 1, "state")])
-def test_gloo_ranks_fill_ghost_layers_by_the_library_plan(R, dim, what):
+@pytest.mark.parametrize("R,dim,what,periodic", [(2, 0, "iteration", True), (3, 0, "state", True),
+                                                 (3, 1, "iteration", True), (2, 1, "state", True),
+                                                 (3, 0, "iteration", False), (2, 1, "state", False)])
+def test_gloo_ranks_fill_ghost_layers_by_the_library_plan(R, dim, what, periodic):
     # every slab's ghost layers (and node n+1, which the high neighbour owns) must
-    # hold the periodic domain's values after one exchange by the library's plan
+    # hold the domain's values after one exchange by the library's plan: a ring over
+    # a periodic dimension, or a chain over a bounded one (whose outer ghosts stay)
     ctx = mp.get_context("spawn")
     out = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_plan_rank, args=(r, R, dim, what, port, out)) for r in range(R)]
+    procs = [ctx.Process(target=_plan_rank, args=(r, R, dim, what, port, out, periodic)) for r in range(R)]
     for p in procs:
         p.start()
     got = [out.get(timeout=120) for _ in range(R)]

@@ -83,6 +83,63 @@ def test_split_run_matches_undivided(dim, ranks, overlap):
     assert not bad, bad
 
 
+@pytest.mark.parametrize("dim,ranks,overlap", [(0, 2, False), (0, 3, True), (1, 3, False), (1, 2, True)])
+def test_chain_split_of_a_bounded_domain_matches_undivided(dim, ranks, overlap):
+    # a dimension with physical sides split into a chain of slabs: the outer sides keep
+    # their boundary conditions (non-zero wall velocities and tractions), the inner
+    # sides are halo sides whose ghosts come from the neighbours
+    fi = load_fastice()
+    from fastice_b200 import distributed as D
+    nl = [80, 16, 14] if dim == 0 else [24, 40, 14]
+    ng = list(nl)
+    ng[dim] *= ranks
+    ext = [1.0, 0.8, 0.3]
+    ext_l = list(ext)
+    ext_l[dim] /= ranks
+    lo_bc = ("velocity", (0.1, -0.05, 0.02))
+    hi_bc = ("traction", (0.05, 0.0, 0.0))
+    sides = [(PER, PER), (PER, PER), (SLIP, TRAC)]
+    sides[dim] = (lo_bc, hi_bc)
+    whole = _model(fi, tuple(ng), tuple(ext), tuple(sides), "fused")
+    sp = fi.pt_params(whole.grid)
+    HALO = ("halo", ())
+    slabs = []
+    for r in range(ranks):
+        sl = list(sides)
+        sl[dim] = (lo_bc if r == 0 else HALO, hi_bc if r == ranks - 1 else HALO)
+        slabs.append(_model(fi, tuple(nl), tuple(ext_l), tuple(sl), "fused", sp))
+    rng = np.random.default_rng(17 + dim + ranks)
+    for name in STATE:
+        shape = whole.field_shape(name)
+        vals = np.exp(0.3 * rng.standard_normal(shape)) if name == "eta" else 0.1 * rng.standard_normal(shape)
+        whole.set_field(name, vals)
+        loc = fi._lib.FIELD_LOC[name]
+        for r, s_ in enumerate(slabs):
+            s_.set_field(name, np.ascontiguousarray(D.slab_of(vals, dim, r, ranks, loc[dim] == 1)))
+        if name == "eta":
+            whole.set_field("eta_next", vals)
+            for r, s_ in enumerate(slabs):
+                s_.set_field("eta_next", np.ascontiguousarray(D.slab_of(vals, dim, r, ranks, False)))
+    whole.apply_bcs()
+    for s_ in slabs:
+        s_.apply_bcs()
+    D.exchange_local(slabs, dim, "state", periodic=False)
+    for _ in range(6):
+        whole.advance(1)
+        D.advance_local(slabs, dim, 1, overlap=overlap, periodic=False)
+    bad = []
+    for name in STATE:
+        g = whole.get_field(name)
+        loc = fi._lib.FIELD_LOC[name]
+        for r, s_ in enumerate(slabs):
+            a, b = s_.get_field(name), np.ascontiguousarray(D.slab_of(g, dim, r, ranks, loc[dim] == 1))
+            if not np.array_equal(_bits(a), _bits(b)):
+                bad.append((name, r, int(np.sum(a != b))))
+    for m in slabs + [whole]:
+        m.close()
+    assert not bad, bad
+
+
 def test_split_solve_matches_undivided_solve():
     # the driver loop over a split domain (ranks emulated on one device): the same
     # checks, the norms reduced over the slabs, the same decision -- the iteration
