@@ -48,7 +48,9 @@ struct fi_ib_batch {
     uint4 *d_items = nullptr;
     long long items_cap = 0;
     int nitems = 0;
-    BcMember *d_bc = nullptr;  // [6][count]: stress x, y, z, velocity x, y, z
+    // [9][count]: stress x, y, z; velocity x, y, z with the η roles of the table
+    // (epar 0), then with them swapped (epar 1: the η_next Neumann ops follow η_next)
+    BcMember *d_bc = nullptr;
     int bc_cap = 0;
     int max_a[3] = {0, 0, 0}, max_c[3] = {0, 0, 0};
     int epar = 0;  // iterations since the table was built, mod 2 (the members' η roles)
@@ -108,7 +110,7 @@ template <typename T>
 fi_status build_table(fi_ib_batch *b, const std::vector<fi_model *> &shared) {
     const int n = (int)shared.size();
     std::vector<IbMember<T>> mem(n);
-    std::vector<BcMember> bc((size_t)6 * n);
+    std::vector<BcMember> bc((size_t)9 * n);
     long long total = 0;
     std::vector<long long> off(n);
     for (int d = 0; d < 3; d++) b->max_a[d] = b->max_c[d] = 0;
@@ -133,12 +135,16 @@ fi_status build_table(fi_ib_batch *b, const std::vector<fi_model *> &shared) {
         b->table_list[q] = list;
         b->table_nblist[q] = m->n_blist;
         for (int d = 0; d < 3; d++) {
-            BcMember &s = bc[(size_t)d * n + q], &v = bc[(size_t)(3 + d) * n + q];
-            s.g = v.g = m->g;
+            BcMember &s = bc[(size_t)d * n + q], &v = bc[(size_t)(3 + d) * n + q], &w = bc[(size_t)(6 + d) * n + q];
+            s.g = v.g = w.g = m->g;
             s.b = model_stress_batch(m, d);
             v.b = model_velocity_batch(m, d);
             bc_set_serial(m->g, s.b);
             bc_set_serial(m->g, v.b);
+            // the same ops one iteration later, when η and η_next have traded buffers
+            w.b = v.b;
+            for (int o = 0; o < w.b.count; o++)
+                if (w.b.ops[o].f == u.f[0].eta_next) w.b.ops[o].f = (void *)u.f[1].eta_next;
             const int e1 = d == 0 ? 1 : 0, e2 = d == 2 ? 1 : 2;
             b->max_a[d] = std::max(b->max_a[d], m->g.n[e1] + 3);
             b->max_c[d] = std::max(b->max_c[d], m->g.n[e2] + 3);
@@ -152,12 +158,12 @@ fi_status build_table(fi_ib_batch *b, const std::vector<fi_model *> &shared) {
     FB_CHECK(regrow(&b->d_items, (size_t)total, &cap_i), "work items");
     b->items_cap = (long long)cap_i;
     size_t cap_b = (size_t)b->bc_cap;
-    FB_CHECK(regrow(&b->d_bc, (size_t)6 * n, &cap_b), "boundary table");
+    FB_CHECK(regrow(&b->d_bc, (size_t)9 * n, &cap_b), "boundary table");
     b->bc_cap = (int)cap_b;
     FB_CHECK(cudaMemcpyAsync(b->d_members, mem.data(), sizeof(IbMember<T>) * n, cudaMemcpyHostToDevice, b->stream),
              "batch table");
     // the boundary table is laid out [kind][member] with the member count as stride
-    FB_CHECK(cudaMemcpyAsync(b->d_bc, bc.data(), sizeof(BcMember) * 6 * n, cudaMemcpyHostToDevice, b->stream),
+    FB_CHECK(cudaMemcpyAsync(b->d_bc, bc.data(), sizeof(BcMember) * 9 * n, cudaMemcpyHostToDevice, b->stream),
              "boundary table");
     for (int q = 0; q < n; q++) {
         fi_model *m = shared[q];
@@ -182,7 +188,7 @@ cudaError_t enqueue_iteration(fi_ib_batch *b, int n, int epar) {
         e = launch_bc_batched<T>(b->d_bc + (size_t)d * n, n, b->max_a[d], b->max_c[d], b->stream);
     if (e == cudaSuccess) e = launch_ib_batched<T>(mem, b->d_items, b->nitems, epar, true, b->stream);
     for (int d = 0; d < 3 && e == cudaSuccess; d++)
-        e = launch_bc_batched<T>(b->d_bc + (size_t)(3 + d) * n, n, b->max_a[d], b->max_c[d], b->stream);
+        e = launch_bc_batched<T>(b->d_bc + (size_t)((epar ? 6 : 3) + d) * n, n, b->max_a[d], b->max_c[d], b->stream);
     return e;
 }
 
