@@ -520,6 +520,11 @@ def run_mixed(args):
             m.apply_bcs()
             grid = m.grid
             kw = dict(max_iter=1000 * n, ncheck=n, tol=tol, measure="rel_slab", rho_g_inf=1.0, length_z=0.6)
+        glen = args.scenario == "glacier" and args.rheology == "glen"
+        if glen:
+            # from rest only the continuation's first (linear) stage is stable
+            stages = scenarios.glacier_glen_stages(grid, tol=tol)
+            m.set_params(stages[0][0], stages[0][1])
         m.solve(mode=mode, **dict(kw, max_iter=2 * n, tol=1e-30))  # warm-up (shadow model, launch shapes)
         for f in fields:
             m.set_field(f, 0.0)
@@ -528,9 +533,8 @@ def run_mixed(args):
         m.apply_bcs()
         m.synchronize()
         t0 = time.perf_counter()
-        if args.scenario == "glacier" and args.rheology == "glen":
+        if glen:
             # Glen's law needs a continuation: linear, then the viscosity cap raised stage by stage
-            stages = scenarios.glacier_glen_stages(grid, tol=tol)
             r = m.solve_continuation(stages, mode=mode, **{k: v for k, v in kw.items() if k != "tol"})
         else:
             r = m.solve(mode=mode, **kw)

@@ -1212,6 +1212,42 @@ fi_status mixed_shadow(fi_model *m) {
     return FI_OK;
 }
 
+// The reference's driver loop: ncheck iterations, the residual norms, the
+// convergence test on the solve's measure; `it0` sweeps already spent (the
+// mixed solve's FP32 phase) count against max_iter.
+static fi_status solve_plain(fi_model *m, const fi_solve_opts *o, fi_solve_report *rep, int it0) {
+    auto t0 = std::chrono::steady_clock::now();
+    const bool trace = std::getenv("FI_SOLVE_TRACE") != nullptr;
+    int it = it0;
+    fi_status st = FI_OK;
+    double norms[FI_NORMS_LEN];
+    while (it < o->max_iter) {
+        int n = o->ncheck;
+        if (it + n > o->max_iter) n = o->max_iter - it;
+        st = fi_model_advance(m, n);
+        if (st != FI_OK) return st;
+        it += n;
+        st = fi_model_residual_norms(m, norms);
+        if (st != FI_OK) return st;
+        double meas = measure_of(m, o, norms);
+        if (trace) std::fprintf(stderr, "[fi solve] sweeps=%d measure=%.3e\n", it, meas);
+        rep->measure = meas;
+        std::memcpy(rep->norms, norms, sizeof(norms));
+        if (norms[11] != 0.0 || !std::isfinite(meas)) {
+            rep->iterations = it;
+            set_error("simulation failed: non-finite residual");
+            return FI_ERR_DIVERGED;
+        }
+        if (meas < o->tol) {
+            rep->converged = 1;
+            break;
+        }
+    }
+    rep->iterations = it;
+    rep->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return rep->converged ? FI_OK : FI_ERR_TIMEOUT;
+}
+
 static fi_status solve_mixed(fi_model *m, const fi_solve_opts *o, fi_solve_report *rep) {
     m->full_iters = 0;  // the solve writes the FP64 state outside its sweeps
     // the shadow, its volume fractions refreshed every solve (the caller may have
@@ -1234,10 +1270,14 @@ static fi_status solve_mixed(fi_model *m, const fi_solve_opts *o, fi_solve_repor
     // FP32 sweeps on the shadow, a check every ncheck, until (a) the FP64 tolerance
     // in the solve's measure (phase A only), (b) the four residual inf-norms drop to
     // target, (c) they reach the FP32 rounding floor (phase A only), (d) the best of
-    // them has not halved for `window` sweeps, or (e) max_sweeps
+    // them has not halved for `window` sweeps (phase A: not fallen by a fifth for
+    // twice that -- a stiff stage of a viscosity continuation converges slowly but
+    // steadily), or (e) max_sweeps
     auto stage = [&](bool phase_a, double target, int max_sweeps, const char *what) -> fi_status {
         double best = 1e300;
         int since = 0, done = 0;
+        const double gain = phase_a ? 0.8 : 0.5;
+        const int win = phase_a ? 2 * window : window;
         double nn[FI_NORMS_LEN];
         s->full_iters = 0;  // the shadow's state was set outside its sweeps
         while (done < max_sweeps && sweeps < o->max_iter) {
@@ -1264,10 +1304,10 @@ static fi_status solve_mixed(fi_model *m, const fi_solve_opts *o, fi_solve_repor
             // target or when it stalls (its own floor scales with the correction and
             // would stop it before it has reduced anything)
             if (phase_a && nn[0] <= fl_P && rv <= fl_V) break;
-            if (r < 0.5 * best) {
+            if (r < gain * best) {
                 best = r;
                 since = 0;
-            } else if ((since += k) >= window) {
+            } else if ((since += k) >= win) {
                 break;
             }
         }
@@ -1278,6 +1318,29 @@ static fi_status solve_mixed(fi_model *m, const fi_solve_opts *o, fi_solve_repor
     if ((st = mixed_phase_a_begin(m)) != FI_OK) return st;
     if ((st = stage(true, 0.0, o->max_iter, "fp32 phase")) != FI_OK) return st;
     if ((st = mixed_phase_a_end(m)) != FI_OK) return st;
+
+    // A power law makes η a function of the iterate: the correction below freezes η
+    // and an outer step refreshes it from τ (a Picard step), whose slope in log η is
+    // 1 - m for the local exponent m = 1 + (n-1)(1 - η/η_reg) where the strain rate
+    // is held -- -2 for n = 3, a divergent iteration (and damped to contract, it
+    // still needs an outer step per halving, measured far slower than PT).  The
+    // FP64 PT iteration, which updates η inside every sweep, finishes such a solve
+    // from the FP32 phase's state instead.
+    if (m->kp.rheo_inner == FI_RHEO_POWER && m->kp.rheo_n != 1) {
+        if (sweeps < o->max_iter) {
+            st = solve_plain(m, o, rep, sweeps);
+        } else {  // the FP32 phase used every sweep: report the FP64 iterate
+            if ((st = norms_t<double>(m, norms)) != FI_OK) return st;
+            rep->measure = measure_of(m, o, norms);
+            std::memcpy(rep->norms, norms, sizeof(norms));
+            rep->converged = rep->measure < o->tol;
+            rep->iterations = sweeps;
+            st = rep->converged ? FI_OK : FI_ERR_TIMEOUT;
+        }
+        rep->outer = 0;
+        rep->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        return st;
+    }
 
     // ---- phase B: FP64 defect correction with FP32 correction sweeps
     //
@@ -1343,36 +1406,7 @@ fi_status fi_model_solve(fi_model *m, const fi_solve_opts *o, fi_solve_report *r
     if (o->mode != FI_SOLVE_PLAIN && o->mode != FI_SOLVE_MIXED) return set_error("unknown solve mode"), FI_ERR_ARG;
     std::memset(rep, 0, sizeof(*rep));
     if (o->mode == FI_SOLVE_MIXED) return solve_mixed(m, o, rep);
-    auto t0 = std::chrono::steady_clock::now();
-    const bool trace = std::getenv("FI_SOLVE_TRACE") != nullptr;
-    int it = 0;
-    fi_status st = FI_OK;
-    double norms[FI_NORMS_LEN];
-    while (it < o->max_iter) {
-        int n = o->ncheck;
-        if (it + n > o->max_iter) n = o->max_iter - it;
-        st = fi_model_advance(m, n);
-        if (st != FI_OK) return st;
-        it += n;
-        st = fi_model_residual_norms(m, norms);
-        if (st != FI_OK) return st;
-        double meas = measure_of(m, o, norms);
-        if (trace) std::fprintf(stderr, "[fi solve] sweeps=%d measure=%.3e\n", it, meas);
-        rep->measure = meas;
-        std::memcpy(rep->norms, norms, sizeof(norms));
-        if (norms[11] != 0.0 || !std::isfinite(meas)) {
-            rep->iterations = it;
-            set_error("simulation failed: non-finite residual");
-            return FI_ERR_DIVERGED;
-        }
-        if (meas < o->tol) {
-            rep->converged = 1;
-            break;
-        }
-    }
-    rep->iterations = it;
-    rep->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    return rep->converged ? FI_OK : FI_ERR_TIMEOUT;
+    return solve_plain(m, o, rep, 0);
 }
 
 fi_status fi_model_volfrac_from_levelset(fi_model *m, int32_t group, const double *psi_host) {

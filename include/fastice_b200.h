@@ -210,7 +210,9 @@ typedef struct {
     int32_t measure;        /* fi_conv_measure */
     double rho_g_inf;       /* FI_CONV_REL_SLAB: ||ρg||∞ */
     double length_z;        /* FI_CONV_REL_SLAB: L_z */
-    int32_t mode;           /* fi_solve_mode: MIXED = FP32 sweeps in FP64 defect correction */
+    int32_t mode;           /* fi_solve_mode: MIXED = FP32 sweeps in FP64 defect correction;
+                               with a power-law rheology the FP32 phase is followed by FP64
+                               sweeps (the plain iteration) instead of frozen-η corrections */
     int32_t inner_iter;     /* MIXED: most FP32 sweeps per correction (0: 50 * ncheck) */
     double inner_reduction; /* MIXED: stop a correction once its residual dropped by this
                                factor (0: 1e-3) or stopped halving for 2(n+1) sweeps */
