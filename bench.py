@@ -508,7 +508,8 @@ def run_mixed(args):
         eta0 = 1.0
     if args.scenario == "glacier" and args.rheology == "glen":
         eta0 = 1.0  # the continuation starts from the linear problem
-        rdesc += "; solved by continuation: linear, then the cap 10, 100, 1000, 5000 (PT velocity step /4 from 1000)"
+        rdesc += ("; solved by continuation: linear, then the cap 10, 100, 1000, 5000 (PT velocity step factor 4.4 "
+                  "from 1000; a diverged stage is retried from its start with the factor doubled)")
     for mode in ("plain", "mixed"):
         if args.scenario == "mms":
             grid, m = scenarios.mms3d_model(n)
@@ -524,7 +525,7 @@ def run_mixed(args):
         if glen:
             # from rest only the continuation's first (linear) stage is stable
             stages = scenarios.glacier_glen_stages(grid, tol=tol)
-            m.set_params(stages[0][0], stages[0][1])
+            m.set_params(stages[0][0], stages[0][1](0))
         m.solve(mode=mode, **dict(kw, max_iter=2 * n, tol=1e-30))  # warm-up (shadow model, launch shapes)
         for f in fields:
             m.set_field(f, 0.0)
@@ -535,7 +536,7 @@ def run_mixed(args):
         t0 = time.perf_counter()
         if glen:
             # Glen's law needs a continuation: linear, then the viscosity cap raised stage by stage
-            r = m.solve_continuation(stages, mode=mode, **{k: v for k, v in kw.items() if k != "tol"})
+            r = m.solve_continuation(stages, retries=2, mode=mode, **{k: v for k, v in kw.items() if k != "tol"})
         else:
             r = m.solve(mode=mode, **kw)
         sec = time.perf_counter() - t0

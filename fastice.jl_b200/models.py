@@ -16,6 +16,7 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import time
 from types import SimpleNamespace
 from typing import Optional
 
@@ -250,21 +251,43 @@ class _StokesBase:
         L.check(self.lib, self.lib.fi_model_set_params(self._h, C.byref(rdesc), C.byref(dt)))
         self.rheology, self.solver_params = rheology, solver_params
 
-    def solve_continuation(self, stages, **solve_kw) -> dict:
+    def solve_continuation(self, stages, retries: int = 0, **solve_kw) -> dict:
         """A continuation driver: for each stage (rheology, solver_params, tol) set the
         parameters and solve to that stage's tolerance from the previous stage's state
-        (e.g. a viscosity cap raised stage by stage for Glen's law).  Returns the last
-        stage's report with the sweeps, outer steps and seconds of every stage summed."""
+        (e.g. a viscosity cap raised stage by stage for Glen's law).  A stage's
+        solver_params is a dict, or a function attempt -> dict: a stage whose solve
+        diverges (non-finite residual) is run again, up to ``retries`` times, from the
+        state it started from (kept on the host) with the parameters of the next
+        attempt.  Returns the last stage's report with the sweeps, outer steps and
+        seconds of every stage and attempt summed."""
+        from .writers import STATE_FIELDS_2D, STATE_FIELDS_3D
+        names = STATE_FIELDS_3D if self.grid.ndims == 3 else STATE_FIELDS_2D
         total = {"iterations": 0, "outer": 0, "seconds": 0.0, "stages": []}
         rep = None
         for rheology, solver_params, tol in stages:
-            self.set_params(rheology, solver_params)
-            rep = self.solve(tol=tol, **solve_kw)
+            saved = {f: self.get_field(f) for f in names} if retries > 0 else None
+            for attempt in range(retries + 1):
+                sp = solver_params(attempt) if callable(solver_params) else solver_params
+                self.set_params(rheology, sp)
+                t0 = time.perf_counter()
+                try:
+                    rep = self.solve(tol=tol, **solve_kw)
+                except L.FastIceError as e:
+                    if e.status != L.FI_ERR_DIVERGED or attempt == retries:
+                        raise
+                    total["seconds"] += time.perf_counter() - t0
+                    total["stages"].append({"tol": tol, "attempt": attempt, "diverged": True})
+                    for f in names:
+                        self.set_field(f, saved[f])
+                    self.copy_field("eta_next", "eta")
+                    self.apply_bcs()
+                    continue
+                break
             total["iterations"] += rep["iterations"]
             total["outer"] += rep["outer"]
             total["seconds"] += rep["seconds"]
-            total["stages"].append({"tol": tol, "iterations": rep["iterations"], "measure": rep["measure"],
-                                    "converged": rep["converged"]})
+            total["stages"].append({"tol": tol, "attempt": attempt, "iterations": rep["iterations"],
+                                    "measure": rep["measure"], "converged": rep["converged"]})
             if not rep["converged"]:
                 break
         out = dict(rep)

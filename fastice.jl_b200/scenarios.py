@@ -169,12 +169,17 @@ def glacier_glen_stages(grid, tol: float = 1e-8, stage_tol: float = 1e-6, n: int
     then the regularised power law with its viscosity cap raised 10 -> 100 -> 1000 ->
     ``cap`` (5000: the Glen viscosity at the strain rate 1e-6), each stage to
     ``stage_tol`` and the last to ``tol``; from the cap of 1000 on, the velocity PT
-    step is four times smaller (factor 4.4 instead of 1.1), without which those
-    stages diverge (measured at 127^3).  The reference's PT iteration started from
-    rest with the cap of 5000 diverges on this geometry."""
+    step factor is 4.4 instead of 1.1, without which those stages diverge (measured at
+    127^3).  The solver parameters are functions of the attempt: a retried stage
+    doubles the factor (at 383^3 the cap of 5000 diverges with 4.4 and converges with
+    8.8).  The reference's PT iteration started from rest with the cap of 5000
+    diverges on this geometry."""
     from .physics import PowerLawRheology, ViscoplasticRegularisation
     r, re = 0.9, 5 * math.pi
-    sp = lambda f: pt_params(grid, r=r, re_mech=re, vdtau_factor=f)
+
+    def sp(f):
+        return lambda attempt: pt_params(grid, r=r, re_mech=re, vdtau_factor=f * 2.0 ** attempt)
+
     caps = [c for c in (10.0, 100.0, 1000.0) if c < cap] + [cap]
     stages = [(LinearViscousRheology(1.0), sp(1.1), stage_tol)]
     for c in caps:
