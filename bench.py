@@ -746,6 +746,60 @@ def run_shapes(args):
                       "shapes": out}))
 
 
+def run_ibbatch(args):
+    """3D immersed-boundary glaciers of uneven sizes (seeded beds, n^3 with n drawn
+    uniformly from --sizes, 48 to 160 by default) advanced together by shared launches (BatchedIB3D:
+    eight launches per iteration of all members, iteration pairs replayed as a CUDA
+    graph) against the same models advanced one at a time (each model's own
+    graph-replayed iterations, synchronised before the next model).  One step = one
+    PT iteration of every member; value = member iterations per second of the
+    batch, wall time around the advance and a synchronize, after warm-up."""
+    fi = load_fastice()
+    from fastice_b200 import scenarios
+    dtype = args.dtypes.split(",")[0]
+    count = args.instances if args.instances != 256 else 12
+    rng = np.random.default_rng(7)
+    lo, hi = (int(v) for v in args.sizes.split(","))
+    sizes = [int(v) for v in rng.integers(lo, hi + 1, count)]
+    models = [scenarios.bed_model(q, n, dtype=dtype)[0] for q, n in enumerate(sizes)]
+    esz = 8 if dtype == "f64" else 4
+    teff_bytes = sum(36 * n ** 3 * esz for n in sizes)  # the reference's 36-pass convention, whole boxes
+    K, W = args.steps, max(args.warmup, 3)
+    res = {}
+    # one at a time (first, so that both arms start from the same state age)
+    for m in models:
+        m.advance(W)
+        m.synchronize()
+    t0 = time.perf_counter()
+    for m in models:
+        m.advance(K)
+        m.synchronize()
+    res["one_at_a_time_s"] = time.perf_counter() - t0
+    b = fi.BatchedIB3D(models)
+    b.advance(W)
+    b.synchronize()
+    t0 = time.perf_counter()
+    b.advance(K)
+    b.synchronize()
+    res["batched_s"] = time.perf_counter() - t0
+    b.close()
+    for m in models:
+        m.close()
+    v = count * K / res["batched_s"]
+    line = _base_line(f"batched 3D immersed-boundary iterations/s ({count} glaciers, {dtype.upper()})", v,
+                      "member iterations/s", K, W, 1e3 * res["batched_s"] / K, dtype,
+                      {"workload": f"{count} immersed-boundary glaciers (seeded 64-bump beds, seeds 0..{count - 1}) "
+                                   f"of n^3 cells, n = {sizes}, linear viscosity, advanced together by shared "
+                                   "launches; one step = one PT iteration of every member",
+                       "members": count, "sizes": sizes, "timing": "wall clock around advance + synchronize"})
+    line.update({"one_at_a_time": {"member_iterations_per_s": count * K / res["one_at_a_time_s"],
+                                   "seconds": res["one_at_a_time_s"]},
+                 "speedup_vs_one_at_a_time": res["one_at_a_time_s"] / res["batched_s"],
+                 "teff_gbs_36_pass": teff_bytes * K / res["batched_s"] / 1e9,
+                 "gpu_launches": f"{8 * K} (eight per iteration of all members; graph-replayed pairs)"})
+    return line
+
+
 def dist_setup():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -771,12 +825,15 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape (profiling runs)")
     ap.add_argument("--variant", type=int, default=None, help="fused launch shape index (implies --no-autotune)")
     ap.add_argument("--dtypes", default="f64,f32", help="precisions to time, FP64 first")
-    ap.add_argument("--workload", choices=("slab", "batched", "serving", "mixed", "glacier", "heat", "shapes"),
+    ap.add_argument("--workload", choices=("slab", "batched", "serving", "mixed", "glacier", "heat", "shapes", "ibbatch"),
                     default="slab",
-                    help="slab: the headline T_eff line; batched / serving / mixed / glacier: the batched 2D solves, "
-                         "the continuous-batching server, the mixed-precision solve and the immersed-boundary "
-                         "glacier sweep, one JSON line each")
-    ap.add_argument("--instances", type=int, default=256, help="batched: number of 2D instances")
+                    help="slab: the headline T_eff line; batched / serving / mixed / glacier / heat / shapes / "
+                         "ibbatch: the batched 2D solves, the continuous-batching server, the mixed-precision solve, "
+                         "the immersed-boundary glacier sweep, the heat sweep, the fused sweep's launch shapes and "
+                         "the shared launches of 3D glaciers, one JSON line each")
+    ap.add_argument("--instances", type=int, default=256,
+                    help="batched: number of 2D instances; ibbatch: number of glaciers (default 12)")
+    ap.add_argument("--sizes", default="48,160", help="ibbatch: smallest,largest cells per side of the glaciers")
     ap.add_argument("--tol", type=float, default=None, help="batched / serving / mixed: stop tolerance")
     ap.add_argument("--scale", type=float, default=0.25, help="serving: linear size scale of the request stream")
     ap.add_argument("--duration", type=float, default=2.0, help="serving: seconds of Poisson arrivals")
@@ -800,7 +857,8 @@ def main():
         return
     if args.workload != "slab":
         line = {"batched": run_batched, "serving": run_serving, "mixed": run_mixed,
-                "glacier": run_glacier, "heat": run_heat, "shapes": run_shapes}[args.workload](args)
+                "glacier": run_glacier, "heat": run_heat, "shapes": run_shapes,
+                "ibbatch": run_ibbatch}[args.workload](args)
         if line is not None:
             print(json.dumps(line))
         return
