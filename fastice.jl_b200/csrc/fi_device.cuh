@@ -168,7 +168,7 @@ __device__ __forceinline__ bool active_dev(const T *const a[8], const T *const b
 // seven predicates of null_spaces.jl:41-43 evaluated here
 template <typename T>
 __device__ __forceinline__ unsigned ib_flags_at(const Ptrs<T> &f, long long I, long long sx, long long sxy, T thr) {
-    if (f.ibf) return f.ibf[I];
+    if (f.ibf) return __ldg(f.ibf + I);  // read-only while the kernels run
     unsigned b = 0;
     if (active_dev(f.wna, f.wns, W_CCC, I, sx, sxy, thr)) b |= IBF_S_CCC;
     if (active_dev(f.wna, f.wns, W_VVC, I, sx, sxy, thr)) b |= IBF_S_VVC;

@@ -120,11 +120,11 @@ __device__ __forceinline__ void ib_sigma_body(const Geom &g, const KParams &p, c
 #pragma unroll
         for (int c = 0; c < C; c++) {
             const long long I = r.I + 32 * c;
-            T exx = (nx[I + 1] * Vx[I + 1] - nx[I] * Vx[I]) * idx;
-            T eyy = (ny[I + sx] * Vy[I + sx] - ny[I] * Vy[I]) * idy;
-            T ezz = (nz[I + sxy] * Vz[I + sxy] - nz[I] * Vz[I]) * idz;
+            T exx = (__ldg(nx + I + 1) * __ldg(Vx + I + 1) - __ldg(nx + I) * __ldg(Vx + I)) * idx;
+            T eyy = (__ldg(ny + I + sx) * __ldg(Vy + I + sx) - __ldg(ny + I) * __ldg(Vy + I)) * idy;
+            T ezz = (__ldg(nz + I + sxy) * __ldg(Vz + I + sxy) - __ldg(nz + I) * __ldg(Vz + I)) * idz;
             T divV = exx + eyy + ezz;
-            T etac = eta[I];
+            T etac = __ldg(eta + I);
             nP[c] = f.P[I] - (p.p_forcing ? divV + f.fP[I] : divV) * etac * T(p.dt_P);
             nxx[c] = f.txx[I] - (f.txx[I] - T(2.0) * etac * (exx - third(divV))) * T(p.dt_tau[0]);
             nyy[c] = f.tyy[I] - (f.tyy[I] - T(2.0) * etac * (eyy - third(divV))) * T(p.dt_tau[1]);
@@ -158,8 +158,8 @@ __device__ __forceinline__ void ib_sigma_body(const Geom &g, const KParams &p, c
 #pragma unroll
         for (int c = 0; c < C; c++) {
             const long long I = r.I + 32 * c;
-            T exy = T(0.5) * ((ny[I] * Vy[I] - ny[I - 1] * Vy[I - 1]) * idx + (nx[I] * Vx[I] - nx[I - sx] * Vx[I - sx]) * idy);
-            T e_xy = h(h(eta[I - 1 - sx] + eta[I - sx]) + h(eta[I - 1] + eta[I]));
+            T exy = T(0.5) * ((__ldg(ny + I) * __ldg(Vy + I) - __ldg(ny + I - 1) * __ldg(Vy + I - 1)) * idx + (__ldg(nx + I) * __ldg(Vx + I) - __ldg(nx + I - sx) * __ldg(Vx + I - sx)) * idy);
+            T e_xy = h(h(__ldg(eta + I - 1 - sx) + __ldg(eta + I - sx)) + h(__ldg(eta + I - 1) + __ldg(eta + I)));
             v[c] = f.txy[I] - (f.txy[I] - T(2.0) * e_xy * exy) * T(p.dt_tau[3]);
         }
 #pragma unroll
@@ -177,8 +177,8 @@ __device__ __forceinline__ void ib_sigma_body(const Geom &g, const KParams &p, c
 #pragma unroll
         for (int c = 0; c < C; c++) {
             const long long I = r.I + 32 * c;
-            T exz = T(0.5) * ((nz[I] * Vz[I] - nz[I - 1] * Vz[I - 1]) * idx + (nx[I] * Vx[I] - nx[I - sxy] * Vx[I - sxy]) * idz);
-            T e_xz = h(h(eta[I - 1 - sxy] + eta[I - sxy]) + h(eta[I - 1] + eta[I]));
+            T exz = T(0.5) * ((__ldg(nz + I) * __ldg(Vz + I) - __ldg(nz + I - 1) * __ldg(Vz + I - 1)) * idx + (__ldg(nx + I) * __ldg(Vx + I) - __ldg(nx + I - sxy) * __ldg(Vx + I - sxy)) * idz);
+            T e_xz = h(h(__ldg(eta + I - 1 - sxy) + __ldg(eta + I - sxy)) + h(__ldg(eta + I - 1) + __ldg(eta + I)));
             v[c] = f.txz[I] - (f.txz[I] - T(2.0) * e_xz * exz) * T(p.dt_tau[4]);
         }
 #pragma unroll
@@ -196,8 +196,8 @@ __device__ __forceinline__ void ib_sigma_body(const Geom &g, const KParams &p, c
 #pragma unroll
         for (int c = 0; c < C; c++) {
             const long long I = r.I + 32 * c;
-            T eyz = T(0.5) * ((nz[I] * Vz[I] - nz[I - sx] * Vz[I - sx]) * idy + (ny[I] * Vy[I] - ny[I - sxy] * Vy[I - sxy]) * idz);
-            T e_yz = h(h(eta[I - sx - sxy] + eta[I - sxy]) + h(eta[I - sx] + eta[I]));
+            T eyz = T(0.5) * ((__ldg(nz + I) * __ldg(Vz + I) - __ldg(nz + I - sx) * __ldg(Vz + I - sx)) * idy + (__ldg(ny + I) * __ldg(Vy + I) - __ldg(ny + I - sxy) * __ldg(Vy + I - sxy)) * idz);
+            T e_yz = h(h(__ldg(eta + I - sx - sxy) + __ldg(eta + I - sxy)) + h(__ldg(eta + I - sx) + __ldg(eta + I)));
             v[c] = f.tyz[I] - (f.tyz[I] - T(2.0) * e_yz * eyz) * T(p.dt_tau[5]);
         }
 #pragma unroll
@@ -241,13 +241,13 @@ __device__ __forceinline__ void ib_V_body(const Geom &g, const KParams &p, const
         for (int c = 0; c < C; c++) {
             const long long I = r.I + 32 * c;
             const T gx = gravity_dev(p, f.gx, 0, I);
-            T ex = h(eta[I - 1] + eta[I]);
-            v[c] = f.Vx[I] + div_fast(div_fast(-(wc[I] * P[I] - wc[I - 1] * P[I - 1]) * idx +
-                                                   (wc[I] * txx[I] - wc[I - 1] * txx[I - 1]) * idx +
-                                                   (wvvc[I + sx] * txy[I + sx] - wvvc[I] * txy[I]) * idy +
-                                                   (wvcv[I + sxy] * txz[I + sxy] - wvcv[I] * txz[I]) * idz - gx,
+            T ex = h(__ldg(eta + I - 1) + __ldg(eta + I));
+            v[c] = f.Vx[I] + div_fast(div_fast(-(__ldg(wc + I) * __ldg(P + I) - __ldg(wc + I - 1) * __ldg(P + I - 1)) * idx +
+                                                   (__ldg(wc + I) * __ldg(txx + I) - __ldg(wc + I - 1) * __ldg(txx + I - 1)) * idx +
+                                                   (__ldg(wvvc + I + sx) * __ldg(txy + I + sx) - __ldg(wvvc + I) * __ldg(txy + I)) * idy +
+                                                   (__ldg(wvcv + I + sxy) * __ldg(txz + I + sxy) - __ldg(wvcv + I) * __ldg(txz + I)) * idz - gx,
                                                ex),
-                                      f.wns[W_VCC][I]) *
+                                      __ldg(f.wns[W_VCC] + I)) *
                                  T(p.dt_V[0]);
         }
 #pragma unroll
@@ -266,13 +266,13 @@ __device__ __forceinline__ void ib_V_body(const Geom &g, const KParams &p, const
         for (int c = 0; c < C; c++) {
             const long long I = r.I + 32 * c;
             const T gy = gravity_dev(p, f.gy, 1, I);
-            T ey = h(eta[I - sx] + eta[I]);
-            v[c] = f.Vy[I] + div_fast(div_fast(-(wc[I] * P[I] - wc[I - sx] * P[I - sx]) * idy +
-                                                   (wc[I] * tyy[I] - wc[I - sx] * tyy[I - sx]) * idy +
-                                                   (wvvc[I + 1] * txy[I + 1] - wvvc[I] * txy[I]) * idx +
-                                                   (wcvv[I + sxy] * tyz[I + sxy] - wcvv[I] * tyz[I]) * idz - gy,
+            T ey = h(__ldg(eta + I - sx) + __ldg(eta + I));
+            v[c] = f.Vy[I] + div_fast(div_fast(-(__ldg(wc + I) * __ldg(P + I) - __ldg(wc + I - sx) * __ldg(P + I - sx)) * idy +
+                                                   (__ldg(wc + I) * __ldg(tyy + I) - __ldg(wc + I - sx) * __ldg(tyy + I - sx)) * idy +
+                                                   (__ldg(wvvc + I + 1) * __ldg(txy + I + 1) - __ldg(wvvc + I) * __ldg(txy + I)) * idx +
+                                                   (__ldg(wcvv + I + sxy) * __ldg(tyz + I + sxy) - __ldg(wcvv + I) * __ldg(tyz + I)) * idz - gy,
                                                ey),
-                                      f.wns[W_CVC][I]) *
+                                      __ldg(f.wns[W_CVC] + I)) *
                                  T(p.dt_V[1]);
         }
 #pragma unroll
@@ -291,13 +291,13 @@ __device__ __forceinline__ void ib_V_body(const Geom &g, const KParams &p, const
         for (int c = 0; c < C; c++) {
             const long long I = r.I + 32 * c;
             const T gz = gravity_dev(p, f.gz, 2, I);
-            T ez = h(eta[I - sxy] + eta[I]);
-            v[c] = f.Vz[I] + div_fast(div_fast(-(wc[I] * P[I] - wc[I - sxy] * P[I - sxy]) * idz +
-                                                   (wc[I] * tzz[I] - wc[I - sxy] * tzz[I - sxy]) * idz +
-                                                   (wvcv[I + 1] * txz[I + 1] - wvcv[I] * txz[I]) * idx +
-                                                   (wcvv[I + sx] * tyz[I + sx] - wcvv[I] * tyz[I]) * idy - gz,
+            T ez = h(__ldg(eta + I - sxy) + __ldg(eta + I));
+            v[c] = f.Vz[I] + div_fast(div_fast(-(__ldg(wc + I) * __ldg(P + I) - __ldg(wc + I - sxy) * __ldg(P + I - sxy)) * idz +
+                                                   (__ldg(wc + I) * __ldg(tzz + I) - __ldg(wc + I - sxy) * __ldg(tzz + I - sxy)) * idz +
+                                                   (__ldg(wvcv + I + 1) * __ldg(txz + I + 1) - __ldg(wvcv + I) * __ldg(txz + I)) * idx +
+                                                   (__ldg(wcvv + I + sx) * __ldg(tyz + I + sx) - __ldg(wcvv + I) * __ldg(tyz + I)) * idy - gz,
                                                ez),
-                                      f.wns[W_CCV][I]) *
+                                      __ldg(f.wns[W_CCV] + I)) *
                                  T(p.dt_V[2]);
         }
 #pragma unroll
@@ -322,11 +322,11 @@ __device__ __forceinline__ void ib_V_body(const Geom &g, const KParams &p, const
 #pragma unroll
     for (int c = 0; c < C; c++) {
         const long long I = r.I + 32 * c;
-        T lxy = h(h(txy[I] + txy[I + 1]) + h(txy[I + sx] + txy[I + sx + 1]));
-        T lxz = h(h(txz[I] + txz[I + 1]) + h(txz[I + sxy] + txz[I + sxy + 1]));
-        T lyz = h(h(tyz[I] + tyz[I + sx]) + h(tyz[I + sxy] + tyz[I + sxy + sx]));
-        T s2 = T(0.5) * (txx[I] * txx[I] + tyy[I] * tyy[I] + tzz[I] * tzz[I]) + lxy * lxy + lxz * lxz + lyz * lyz;
-        en[c] = ok[c] ? rheology_s2(p, T(p.rheo_A), T(p.rheo_inv_eta_reg), f.eta_lin, f.A, eta[I], I, s2) : T(0);
+        T lxy = h(h(__ldg(txy + I) + __ldg(txy + I + 1)) + h(__ldg(txy + I + sx) + __ldg(txy + I + sx + 1)));
+        T lxz = h(h(__ldg(txz + I) + __ldg(txz + I + 1)) + h(__ldg(txz + I + sxy) + __ldg(txz + I + sxy + 1)));
+        T lyz = h(h(__ldg(tyz + I) + __ldg(tyz + I + sx)) + h(__ldg(tyz + I + sxy) + __ldg(tyz + I + sxy + sx)));
+        T s2 = T(0.5) * (__ldg(txx + I) * __ldg(txx + I) + __ldg(tyy + I) * __ldg(tyy + I) + __ldg(tzz + I) * __ldg(tzz + I)) + lxy * lxy + lxz * lxz + lyz * lyz;
+        en[c] = ok[c] ? rheology_s2(p, T(p.rheo_A), T(p.rheo_inv_eta_reg), f.eta_lin, f.A, __ldg(eta + I), I, s2) : T(0);
     }
 #pragma unroll
     for (int c = 0; c < C; c++)
