@@ -368,8 +368,8 @@ fi_status fi_batch_measure(fi_batch *b, double *out);
  * relative measure inner_tol (0: 1e-3), added to the FP64 state.  A member stops
  * when its FP64 measure drops below tol (CONVERGED), after three outer steps that
  * did not halve it (STALLED) or after max_iter FP32 sweeps (MAXITER); items get
- * the FP32 sweeps, the status and the last FP64 measure.  The north-star
- * precision pattern applied to the batch; no counterpart in the reference. */
+ * the FP32 sweeps, the status and the last FP64 measure.  The mixed-precision
+ * solve applied to the batch; no counterpart in the reference. */
 fi_status fi_batch_solve_mixed(fi_batch *b, const fi_batch_opts *opts, double inner_tol, fi_batch_item *items,
                                double *seconds);
 /* tile shapes of the batched sweep; autotune times each for `iters` iterations on
