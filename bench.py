@@ -466,7 +466,7 @@ def run_serving(args):
     from fastice_b200 import serving
     rate, budget = 50.0, 150 << 30
     out = {}
-    for mode, kw in (("batched", {}), ("sequential", {"max_active": 1})):
+    for mode, kw in (("batched", {"share3d": args.shared3d}), ("sequential", {"max_active": 1})):
         srv = serving.SolveServer(budget_bytes=budget, ncheck=200, window=100000, realtime=False, **kw)
         t0 = time.perf_counter()
         done = srv.run(_serving_requests(fi, args.scale, args.duration, rate))
@@ -482,6 +482,7 @@ def run_serving(args):
                        f"(128-1024 cells per side x {args.scale}), 30% 3D immersed-boundary glaciers over a seeded "
                        f"64-bump bed (64-255 cells per side x {args.scale}); FP64; stop at 1e-6",
            "budget_bytes": budget, "ncheck": 200,
+           "3d_requests": "shared launches (BatchedIB3D)" if args.shared3d else "each on its own stream",
            "scaled": "the full stream (60 s, unscaled sizes) needs about an hour of GPU time per arm at the "
                      "reference PT scheme's iteration counts"}
     b = out["batched"]
@@ -837,6 +838,8 @@ def main():
     ap.add_argument("--tol", type=float, default=None, help="batched / serving / mixed: stop tolerance")
     ap.add_argument("--scale", type=float, default=0.25, help="serving: linear size scale of the request stream")
     ap.add_argument("--duration", type=float, default=2.0, help="serving: seconds of Poisson arrivals")
+    ap.add_argument("--shared3d", action="store_true",
+                    help="serving: 3D requests advance by shared launches instead of each on its own stream")
     ap.add_argument("--rounds", type=int, default=0, help="batched: stop after this many check rounds (profiling)")
     ap.add_argument("--storage", choices=("f32", "f64"), default="f32",
                     help="batched: FP32 sweeps in an FP64 defect correction (f32) or plain FP64 sweeps")

@@ -439,9 +439,10 @@ class IsothermalImmersedBoundaryFullStokesModel(_StokesBase):
 
 class BatchedIB3D:
     """Several 3D immersed-boundary models advanced by shared launches
-    (fi_ib_batch_* in the C ABI): one iteration of every member is eight launches
-    whatever their number, and pairs of iterations replay as a CUDA graph.  Each
-    member's iteration is the one ``advance`` runs for it alone."""
+    (fi_ib_batch_* in the C ABI): one iteration of every small member is eight
+    launches whatever their number, and pairs of iterations replay as a CUDA graph;
+    a member whose launch spans more than 2048 blocks advances on its own stream.
+    Each member's iteration is the one ``advance`` runs for it alone."""
 
     def __init__(self, models=()):
         models = list(models)

@@ -387,7 +387,9 @@ fi_status fi_batch_autotune(fi_batch *b, int32_t iters, int32_t *best, double *m
  * all members per dimension, the masked update_V!, the velocity boundary batches --
  * and pairs of iterations replay as one CUDA graph.  Each member's iteration is the
  * one fi_model_advance runs for it, so its result is the same alone or in the batch;
- * a member whose state changed runs its first two full iterations alone.  The models
+ * a member whose state changed runs its first two full iterations alone, and a member
+ * whose launch already spans more than 2048 blocks (about two waves) always advances
+ * alone on its own stream, overlapping the others.  The models
  * must outlive the batch; after fi_ib_batch_advance each member's stream is ordered
  * after the shared launches.  No counterpart in the reference, which runs one model
  * per driver loop (scripts_future_API/tm_stokes_chmy.jl:283-305). */

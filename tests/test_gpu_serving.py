@@ -36,9 +36,10 @@ def _serve(fi, **kw):
     return {r.rid: r for r in done}, srv
 
 
-def test_results_alone_and_in_the_mix_agree():
+@pytest.mark.parametrize("share3d", [False, True], ids=["3d-streams", "3d-shared"])
+def test_results_alone_and_in_the_mix_agree(share3d):
     fi = load_fastice()
-    mix, srv = _serve(fi, budget_bytes=8 << 30, realtime=True)
+    mix, srv = _serve(fi, budget_bytes=8 << 30, realtime=True, share3d=share3d)
     alone, _ = _serve(fi, budget_bytes=8 << 30, realtime=False, max_active=1)
     assert set(mix) == set(alone) == set(range(len(STREAM)))
     for rid in mix:
