@@ -319,6 +319,10 @@ fi_status fi_ib_batch_remove(fi_ib_batch *b, fi_model *m) {
     FB_CHECK(cudaSetDevice(b->device), "cudaSetDevice");
     FB_CHECK(cudaStreamSynchronize(b->stream), "batch sync");
     b->models.erase(it);
+    // the table names members by address: a model created later at the same address
+    // must not find the old entry current
+    b->table_models.clear();
+    drop_graphs(b);
     return FI_OK;
 }
 
