@@ -19,6 +19,10 @@
 // A member whose state was written from outside since its last two full iterations
 // (fi_model_set_field, ω_from_ψ!, a new member) runs those iterations alone first,
 // exactly as fi_model_advance does, and joins the shared launches from the next call.
+// A member whose own launch spans more than kShareBlocks blocks, or the only member
+// left to share, advances by fi_model_advance on its own stream.  The shared launches
+// wait for the members' streams by events; the members' streams wait for them by the
+// `done` event.
 #include <algorithm>
 #include <cstring>
 #include <vector>
