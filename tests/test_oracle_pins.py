@@ -223,6 +223,47 @@ def test_oracle_immersed_boundary_with_full_fractions_is_the_plain_model(fi, orc
         assert np.array_equal(a.view(np.uint64), b.view(np.uint64)), name
 
 
+# ---- rheologies at a known stress invariant (src/Physics.jl:7-53) ----------------------------
+@pytest.mark.parametrize("case", ["linear", "power", "power_capped", "relax_lin", "relax_log", "relax_log10"])
+def test_oracle_rheology_at_a_known_stress(fi, orc, case):
+    # a uniform τxx = a with every other field zero on a periodic box: one iteration
+    # relaxes it to a(1 - Δτ.τxx) (update_σ!, kernels_3d.jl:3-25), leaves V at rest,
+    # and sets η_next = rheology(τII) with τII = |a (1 - Δτ.τxx)| / √2 at every cell
+    # (update_V!, kernels_3d.jl:27-40); the swap makes it η.  Expected values from
+    # Physics.jl's formulas: linear η, 0.5 / (A τII^(n-1)), the cap 1 / (1/η + 1/η_reg),
+    # the relaxation η_old (1-r) + target r in linear, log or log10 scale.
+    n, ext, org = (6, 5, 4), (1.0, 0.8, 0.6), (0.0, 0.0, 0.0)
+    dt = fi.pt_params(fi.UniformGrid(origin=org, extent=ext, dims=n))["Δτ"]
+    taus = ("xx", "yy", "zz", "xy", "xz", "yz")
+    per = (orc.BC_PERIODIC, (0, 0, 0))
+    A, nexp, eta_reg, rate, eta0, a = 2.0, 3, 50.0, 0.3, 7.0, 0.8
+    kw = {"linear": dict(rheo_inner=orc.RHEO_LINEAR, rheo_eta_val=3.5),
+          "power": dict(rheo_inner=orc.RHEO_POWER, rheo_A=A, rheo_n=nexp),
+          "power_capped": dict(rheo_inner=orc.RHEO_POWER, rheo_A=A, rheo_n=nexp, rheo_has_reg=1,
+                               rheo_inv_eta_reg=1.0 / eta_reg)}
+    for scale, code in (("lin", orc.RELAX_LIN), ("log", orc.RELAX_LOG), ("log10", orc.RELAX_LOG10)):
+        kw["relax_" + scale] = dict(rheo_inner=orc.RHEO_POWER, rheo_A=A, rheo_n=nexp, rheo_relax=code, rheo_rate=rate)
+    spec = orc.Spec(nd=3, n=n, extent=ext, origin=org, bcs=((per, per), (per, per), (per, per)), dt_P=dt["Pr"],
+                    dt_tau=tuple(dt["τ"][k] for k in taus), dt_V=tuple(dt["V"][k] for k in "xyz"),
+                    g_val=(0.0, 0.0, 0.0), **kw[case])
+    m = orc.OracleStokes(spec)
+    m.set_interior("txx", np.full(m.interior("txx").shape, a))
+    m.a["eta"][:] = eta0
+    m.a["eta_next"][:] = eta0
+    m.apply_initial_bcs()
+    m.advance(1)
+    tII = abs(a * (1.0 - dt["τ"]["xx"])) / math.sqrt(2.0)
+    power = 0.5 / (A * tII ** (nexp - 1))
+    expected = {"linear": 3.5, "power": power, "power_capped": 1.0 / (1.0 / power + 1.0 / eta_reg),
+                "relax_lin": eta0 * (1 - rate) + power * rate,
+                "relax_log": math.exp(math.log(eta0) * (1 - rate) + math.log(power) * rate),
+                "relax_log10": 10.0 ** (math.log10(eta0) * (1 - rate) + math.log10(power) * rate)}[case]
+    eta = m.interior("eta")
+    np.testing.assert_allclose(eta, expected, rtol=1e-13, atol=0)
+    for f in ("Vx", "Vy", "Vz", "P"):
+        assert np.max(np.abs(m.interior(f))) == 0.0, f
+
+
 # ---- cut-cell volumes (volume_fractions.jl) -------------------------------------------------
 def test_vol_box_full_and_empty(orc):
     d = (0.3, 0.2, 0.5)
