@@ -264,6 +264,35 @@ def test_oracle_rheology_at_a_known_stress(fi, orc, case):
         assert np.max(np.abs(m.interior(f))) == 0.0, f
 
 
+# ---- simple shear: the staggered shear strain rate and its stress (kernels_3d.jl:3-25) ---------
+def test_oracle_simple_shear_stress(fi, orc):
+    # Vx = γ z between a bottom at rest and a top moving at γ L (Velocity conditions
+    # continue the line into the ghosts), η uniform: ε̇xz = ½(∂z Vx + ∂x Vz) = γ/2 at
+    # every interior (V, C, V) point and ∇·V = 0, so one iteration from rest sets
+    # τxz = Δτ.τxz · 2η · γ/2 and leaves P and the other stresses at zero.
+    n, ext, org = (6, 5, 8), (1.0, 0.8, 0.6), (0.0, 0.0, 0.0)
+    dt = fi.pt_params(fi.UniformGrid(origin=org, extent=ext, dims=n))["Δτ"]
+    taus = ("xx", "yy", "zz", "xy", "xz", "yz")
+    per = (orc.BC_PERIODIC, (0, 0, 0))
+    gamma, eta0, L = 0.4, 2.5, ext[2]
+    bcs = ((per, per), (per, per), ((orc.BC_VELOCITY, (0.0, 0.0, 0.0)), (orc.BC_VELOCITY, (gamma * L, 0.0, 0.0))))
+    spec = orc.Spec(nd=3, n=n, extent=ext, origin=org, bcs=bcs, dt_P=dt["Pr"], dt_tau=tuple(dt["τ"][k] for k in taus),
+                    dt_V=tuple(dt["V"][k] for k in "xyz"), g_val=(0.0, 0.0, 0.0), rheo_eta_val=eta0)
+    m = orc.OracleStokes(spec)
+    dz = L / n[2]
+    zc = org[2] + (np.arange(n[2]) + 0.5) * dz
+    vx = m.interior("Vx")
+    m.set_interior("Vx", np.broadcast_to((gamma * zc)[:, None, None], vx.shape).copy())
+    m.a["eta"][:] = eta0
+    m.a["eta_next"][:] = eta0
+    m.apply_initial_bcs()
+    m.advance(1)
+    txz = m.interior("txz")  # (z vertices 1..n+1, y centres, x vertices 1..n+1)
+    np.testing.assert_allclose(txz[1:-1], dt["τ"]["xz"] * 2.0 * eta0 * 0.5 * gamma, rtol=1e-13, atol=0)
+    for f in ("P", "txx", "tyy", "tzz", "txy", "tyz"):
+        assert np.max(np.abs(m.interior(f))) <= 1e-15, f
+
+
 # ---- cut-cell volumes (volume_fractions.jl) -------------------------------------------------
 def test_vol_box_full_and_empty(orc):
     d = (0.3, 0.2, 0.5)
