@@ -333,11 +333,10 @@ __device__ __forceinline__ void ib_V_body(const Geom &g, const KParams &p, const
         if (ok[c]) f.eta_next[r.I + 32 * c] = en[c];
 }
 
-// resident blocks per SM asked of the compiler: 5 (46 registers) for one point per
-// thread (6 at 40 registers measured 2 % slower at 383^3 in FP64), 4 (64) for two
-// (5 at 48 registers with spills measured 2 % slower in FP32)
+// resident blocks per SM asked of the compiler: 6 (40 registers) for one point per
+// thread, 4 (64) for two (5 at 48 registers with spills measured 2 % slower in FP32)
 template <typename T, int C>
-__global__ void __launch_bounds__(256, C == 1 ? 5 : 4) ib_V_kernel(Geom g, KParams p, Ptrs<T> f, BlockList bl) {
+__global__ void __launch_bounds__(256, C == 1 ? 6 : 4) ib_V_kernel(Geom g, KParams p, Ptrs<T> f, BlockList bl) {
     ib_V_body<T, C>(g, p, f, ib_row(g, bl, C));
 }
 
