@@ -3,12 +3,14 @@
 The reference's distributed architecture (Chmy.Distributed with a Cartesian
 topology; src/Models/FullStokes/Isothermal/Isothermal.jl:101-107) splits the
 grid into per-rank subdomains and exchanges the halos of V and η_next after
-update_V!.  Here a domain that is periodic along x (or y) is split into R slabs
-along that dimension, one model per rank, each declared periodic along the split
-dimension; after every iteration each slab sends its boundary layers to its two
-neighbours (a ring) and unpacks what it receives into its ghost layers
-(fi_model_halo_*).  The sweep recomputes the ghost stresses from the exchanged
-velocities, so the split run reproduces the undivided domain exactly.
+update_V!.  Here a domain is split into R slabs along x (or y), one model per
+rank.  Along a periodic dimension the slabs form a ring and each is declared
+periodic along it; along a bounded one they form a chain: the sides between
+ranks are FI_BC_HALO (the neighbour's values arrive by the exchange) and the two
+outer sides keep the domain's own conditions.  After every iteration each slab
+sends its boundary layers to its neighbours and unpacks what it receives into its
+ghost layers (fi_model_halo_*).  The sweep recomputes the ghost stresses from the
+exchanged velocities, so the split run reproduces the undivided domain exactly.
 
 Transport: ``TorchTransport`` moves the messages with torch.distributed
 point-to-point operations (NCCL between GPUs, gloo on CPU), grouped in one
