@@ -964,7 +964,13 @@ def main():
                         "frac": (A * 4 / (res["f32"]["ms_per_step"] / 1e3) / 1e9) / peak}
     if not args.no_e2e and prim == "f64":
         v64 = res["f64"]["tuned"]["variant"] if res["f64"]["tuned"] else None
+        if pg:
+            pg.barrier()
         dt, h2d, d2h, _ = e2e_run(fi, n, "f64", local, args.steps, torch, variant=v64)
+        if pg:  # every rank's replica, timed as the slowest one
+            t = torch.tensor([dt], dtype=torch.float64, device="cuda")
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            dt = float(t.item())
         line["e2e"] = {"value": ws * A * 8 * args.steps / dt / 1e9, "unit": "GB/s",
                        "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                        "includes": "pinned host->device upload of the state, K iterations through the C ABI, "
