@@ -661,6 +661,84 @@ def run_glacier(args):
     return line
 
 
+def run_split(args):
+    """The per-GPU cost of a domain split on the slab workload at n^3 (one rank's
+    slab of a weak-scaling run), measured on one GPU for a split along x and along y:
+    K iterations timed with CUDA events on the model's stream (a) plain, (b) each
+    followed by the halo exchange of V and η (pack toward both neighbours, the
+    messages moved by a device copy, unpack), (c) the same with the overlapped
+    iteration (the split-face tiles first, the others on the model's second stream
+    while the halo moves).  The slab's own periodic images are its neighbours here
+    (a one-rank ring), so every kernel of a multi-rank iteration runs; the transfer
+    between GPUs is the only part replaced, by a copy in HBM, and its NVLink time is
+    estimated from the message size at the measured 770 GB/s per direction.
+    value = the x split with the plain exchange (the default of a split run; x is
+    the fastest dimension, so its layers are the strided ones)."""
+    import torch
+    fi = load_fastice()
+    n = (args.n,) * 3
+    A = a_eff_elements(n)
+    m = make_model(fi, n, "f64", 0)
+    stream = torch.cuda.ExternalStream(m.stream_ptr)
+
+    def timed(step, K):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        m.synchronize()
+        e0.record(stream)
+        for _ in range(K):
+            step()
+        m.synchronize()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / K
+
+    K = args.steps
+    W = max(args.warmup, 3)
+    plain = lambda: m.advance(1)
+    for _ in range(W):
+        plain()
+    ms_plain = timed(plain, K)
+    per_dim = {}
+    for dim, name in ((0, "x"), (1, "y")):
+        nb = [m.halo_bytes(dim, side, "iteration") for side in (0, 1)]
+        send = [torch.empty(b, dtype=torch.uint8, device="cuda") for b in nb]
+        recv = [torch.empty(b, dtype=torch.uint8, device="cuda") for b in nb[::-1]]
+
+        def exchange():
+            for side in (0, 1):
+                m.halo_pack(dim, side, send[side].data_ptr(), "iteration")
+            with torch.cuda.stream(stream):
+                recv[1].copy_(send[0])  # toward low, received on the high side
+                recv[0].copy_(send[1])
+            m.halo_unpack(dim, 1, recv[1].data_ptr(), "iteration")
+            m.halo_unpack(dim, 0, recv[0].data_ptr(), "iteration")
+
+        res = {}
+        for case, step in (("exchange", lambda: (m.advance(1), exchange())),
+                           ("overlapped", lambda: (m.advance_begin(dim), m.advance_end(), exchange()))):
+            for _ in range(W):
+                step()
+            res[case] = timed(step, K)
+        per_dim[name] = {"ms_with_exchange": res["exchange"], "ms_overlapped": res["overlapped"],
+                         "teff_gbs_overlapped": A * 8 / (res["overlapped"] / 1e3) / 1e9,
+                         "message_bytes_per_side": nb, "nvlink_ms_at_770_gbs": sum(nb) / 770e9 * 1e3}
+        del send, recv
+    norms = m.residual_norms()
+    m.close()
+    line = _base_line("split slab: ms per iteration with the halo exchange (one rank's share, 1 GPU)",
+                      per_dim["x"]["ms_with_exchange"], "ms", K, W, per_dim["x"]["ms_with_exchange"], "f64",
+                      {"workload": f"3D tilted ice slab {n[0]}^3 (one rank's slab), split along x (and along y), halo "
+                                   "of V and eta exchanged after every iteration with its two neighbours (here its own "
+                                   "periodic images; the transfer by a device copy)", "grid": list(n)},
+                      hib=False)
+    line.update({"ms_plain": ms_plain, "teff_gbs_plain": A * 8 / (ms_plain / 1e3) / 1e9, "split": per_dim,
+                 "finite": bool(norms[11] == 0.0),
+                 "gpu_launches": 5 * K,
+                 "gpu_launches_per_iteration": "plain: 1 sweep; exchange: + 2 packs and 2 unpacks (the 2 copies are "
+                                               "torch's); overlapped: the sweep in two launches"})
+    return line
+
+
 def run_heat(args):
     """Heat diffusion (src/Models/Diffusion/Heat/ restated): the implicit step of the
     driver scripts_future_API/heat_wip.jl (Value sides south/north, Flux 0 elsewhere,
@@ -826,7 +904,8 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape (profiling runs)")
     ap.add_argument("--variant", type=int, default=None, help="fused launch shape index (implies --no-autotune)")
     ap.add_argument("--dtypes", default="f64,f32", help="precisions to time, FP64 first")
-    ap.add_argument("--workload", choices=("slab", "batched", "serving", "mixed", "glacier", "heat", "shapes", "ibbatch"),
+    ap.add_argument("--workload", choices=("slab", "batched", "serving", "mixed", "glacier", "heat", "shapes", "ibbatch",
+                                           "split"),
                     default="slab",
                     help="slab: the headline T_eff line; batched / serving / mixed / glacier / heat / shapes / "
                          "ibbatch: the batched 2D solves, the continuous-batching server, the mixed-precision solve, "
@@ -861,7 +940,7 @@ def main():
     if args.workload != "slab":
         line = {"batched": run_batched, "serving": run_serving, "mixed": run_mixed,
                 "glacier": run_glacier, "heat": run_heat, "shapes": run_shapes,
-                "ibbatch": run_ibbatch}[args.workload](args)
+                "ibbatch": run_ibbatch, "split": run_split}[args.workload](args)
         if line is not None:
             print(json.dumps(line))
         return

@@ -96,19 +96,32 @@ long long layer_elems(const fi_model *m, int d) {
     return d == 0 ? e1 * e2 : e0 * e2;
 }
 
+// the layers of one message: field base and index along d, in message order
+// (at most 11 fields, three of them with two layers)
+constexpr int kMaxLayers = 16;
+struct LayerSet {
+    void *field[kMaxLayers];
+    int at[kMaxLayers];
+};
+
 template <typename T>
-__global__ void layer_copy_kernel(T *field, T *buf, int d, int at, long long pitch, long long rows, int e_other0,
-                                  long long planes, bool pack) {
-    // the layer at index `at` of dimension d; (a, k) run over the other two dims
+__global__ void layers_copy_kernel(LayerSet ls, T *buf, int d, long long pitch, long long rows, int e_other0,
+                                   long long planes, bool pack) {
+    // layer blockIdx.y of the message: its index ls.at along dimension d; (a, k) run
+    // over the other two dims, and the layer's slice of the buffer follows the earlier ones
     const long long total = (long long)e_other0 * planes;
+    T *field = (T *)ls.field[blockIdx.y];
+    const long long at = ls.at[blockIdx.y];
+    T *b = buf + total * blockIdx.y;
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
         const long long a = t % e_other0, k = t / e_other0;
-        const long long I = d == 0 ? (long long)at + pitch * (a + rows * k) : a + pitch * ((long long)at + rows * k);
-        if (pack) buf[t] = field[I];
-        else field[I] = buf[t];
+        const long long I = d == 0 ? at + pitch * (a + rows * k) : a + pitch * (at + rows * k);
+        if (pack) b[t] = field[I];
+        else field[I] = b[t];
     }
 }
 
+// one launch per message: every layer of every field of it
 template <typename T>
 fi_status halo_move(fi_model *m, int d, int side, int what, void *buf, bool pack) {
     int fl[16];
@@ -116,19 +129,21 @@ fi_status halo_move(fi_model *m, int d, int side, int what, void *buf, bool pack
     const long long le = layer_elems(m, d);
     const int e_other0 = d == 0 ? m->d.grid.n[1] + 3 : m->d.grid.n[0] + 3;
     const long long planes = m->d.grid.nd == 3 ? m->d.grid.n[2] + 3 : 1;
-    T *b = (T *)buf;
+    LayerSet ls{};
+    int nl_total = 0;
     for (int q = 0; q < nf; q++) {
         int idx[2];
         const int nl = layers(m, fl[q], d, side, pack, idx);
-        T *f = (T *)m->cur(fl[q]);
         for (int l = 0; l < nl; l++) {
-            const int blocks = (int)std::min<long long>((le + 255) / 256, 4096);
-            layer_copy_kernel<T><<<blocks, 256, 0, m->stream>>>(f, b, d, idx[l], m->g.pitch, m->g.rows, e_other0,
-                                                                planes, pack);
-            FI_CHECK_CUDA(cudaGetLastError(), pack ? "halo pack" : "halo unpack");
-            b += le;
+            if (nl_total == kMaxLayers) return set_error("halo message with too many layers"), FI_ERR_UNSUPPORTED;
+            ls.field[nl_total] = m->cur(fl[q]);
+            ls.at[nl_total++] = idx[l];
         }
     }
+    const int blocks = (int)std::min<long long>((le + 255) / 256, 4096);
+    layers_copy_kernel<T><<<dim3(blocks, nl_total), 256, 0, m->stream>>>(ls, (T *)buf, d, m->g.pitch, m->g.rows,
+                                                                        e_other0, planes, pack);
+    FI_CHECK_CUDA(cudaGetLastError(), pack ? "halo pack" : "halo unpack");
     return FI_OK;
 }
 
