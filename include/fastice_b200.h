@@ -423,7 +423,10 @@ fi_status fi_ib_batch_synchronize(fi_ib_batch *b);
  * what: FI_HALO_ITERATION (V, η: after every iteration) or FI_HALO_STATE (P, τ, V,
  * η: once, after the initial state is set).  Slabs run the fused sweep (it recomputes
  * the ghost stresses from the exchanged velocities); reference-shaped and
- * immersed-boundary models are rejected with FI_ERR_UNSUPPORTED. */
+ * immersed-boundary models are rejected with FI_ERR_UNSUPPORTED.  Each pack or
+ * unpack is one launch.  Where either dimension may be split, y is the cheaper one:
+ * its layers are whole rows, while x layers take one value per row (at 511^3 FP64
+ * about 44 against 156 us of pack and unpack per iteration). */
 typedef enum { FI_HALO_ITERATION = 0, FI_HALO_STATE = 1 } fi_halo_what;
 fi_status fi_model_halo_bytes(const fi_model *m, int32_t dim, int32_t side, int32_t what, size_t *bytes);
 fi_status fi_model_halo_pack(fi_model *m, int32_t dim, int32_t side, int32_t what, void *dst_dev);
