@@ -217,6 +217,26 @@ def test_combine_norms_slots():
         assert c[q] == pytest.approx(np.hypot(a[q], b[q]))
 
 
+def test_halo_messages_fit_one_pack_launch():
+    """Every message's layers go to one pack or unpack launch whose layer table holds
+    16 entries: the longest plan (3D state, split along x or y) has 14 layers, and a
+    message's byte count is its layers times one storage plane."""
+    load_fastice()
+    from fastice_b200 import distributed as D
+    n = (7, 6, 5)
+    longest = 0
+    for nd in (2, 3):
+        for dim in (0, 1):
+            for side in (0, 1):
+                for what in ("iteration", "state"):
+                    for pack in (True, False):
+                        plan = D.halo_plan(nd, n[:nd], dim, side, what, pack)
+                        longest = max(longest, len(plan))
+                        assert len(plan) <= 16
+                        assert all(name in ("Vx", "Vy", "Vz", "eta") for name, _ in plan) or what == "state"
+    assert longest == 14
+
+
 # ---- the library's own halo layer plan (fi_halo_plan) over gloo ranks
 SHAPE_LOCAL = (6, 5, 4)
 
