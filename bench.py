@@ -908,9 +908,10 @@ def main():
                                            "split"),
                     default="slab",
                     help="slab: the headline T_eff line; batched / serving / mixed / glacier / heat / shapes / "
-                         "ibbatch: the batched 2D solves, the continuous-batching server, the mixed-precision solve, "
-                         "the immersed-boundary glacier sweep, the heat sweep, the fused sweep's launch shapes and "
-                         "the shared launches of 3D glaciers, one JSON line each")
+                         "ibbatch / split: the batched 2D solves, the continuous-batching server, the mixed-precision "
+                         "solve, the immersed-boundary glacier sweep, the heat sweep, the fused sweep's launch "
+                         "shapes, the shared launches of 3D glaciers and one rank's share of a split slab (halo "
+                         "exchange along x and y), one JSON line each")
     ap.add_argument("--instances", type=int, default=256,
                     help="batched: number of 2D instances; ibbatch: number of glaciers (default 12)")
     ap.add_argument("--sizes", default="48,160", help="ibbatch: smallest,largest cells per side of the glaciers")
